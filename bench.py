@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the TBLIS-compatible contraction hot path on B200.
+
+Headline workload (one "step" = one contraction through tblis_tensor_mult):
+the ladder term C[abij] = A[abef] * B[efij] with o=48, v=160 (m=25600,
+n=2304, k=25600; 3.02 TFLOP), FP64 inputs uniform(-1,1) * 2^k with k a
+uniform integer in [-20, 20] per element, computed by the fastest method
+whose normwise relative error against the FP64 path is at most 1e-12.
+
+Prints one JSON line (rank 0). Extra keys: the plain FP64 (DMMA) rate on the
+same workload, the ring contraction and the transpose bandwidth case, the
+roofline of the dominant kernel, the CPU baseline (the TBLIS reference built
+from its own sources, timed on a bounded slice on this host) and the
+end-to-end rate through the C ABI with pinned host buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+O, V = 48, 160
+FLOPS_LADDER = 2.0 * V * V * V * V * O * O
+WORKLOAD = "ladder C[abij]=A[abef]*B[efij] o=48 v=160 fp64 exponent spread 2^[-20,20]"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------------------
+# CPU reference leg (oracle/_ref: the TBLIS reference compiled from its own sources)
+# ---------------------------------------------------------------------------------------
+
+def cpu_reference_sample(threads=None, reps=2):
+    """Times the reference's tblis_tensor_mult on a bounded slice of the ladder
+    workload: a restricted to the first 16 of 160 (m = 2560 of 25600 rows),
+    i.e. 1/10 of the contraction, same exponent-spread inputs. Returns
+    (GFLOP/s, cores, sample text)."""
+    import numpy as np
+    import oracle
+    if not oracle.have_ref():
+        return None
+    cores = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    asub = 16
+
+    def spread(shape):
+        x = np.asfortranarray(rng.uniform(-1, 1, shape))
+        x *= np.ldexp(1.0, rng.integers(-20, 21, shape, dtype=np.int32))
+        return x
+    A = spread((asub, V, V, V))
+    B = spread((V, V, O, O))
+    C = np.asfortranarray(np.zeros((asub, V, O, O)))
+    flops = 2.0 * asub * V ** 3 * O * O
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        oracle.ref_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij", threads=cores)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return flops / best / 1e9, cores, ("ladder slice a<16 of 160 (m=2560 of 25600, %.0f GFLOP), best of %d, "
+                                       "tblis_tensor_mult of the reference built from its own sources, %d threads"
+                                       % (flops / 1e9, reps, cores))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources at build time)"}))
+        return
+    cores = os.cpu_count() or 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_sample(cores, reps=1)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 3))):
+        v, _, sample = cpu_reference_sample(cores, reps=1)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.median(vals)
+    print(json.dumps({
+        "impl": "reference", "metric": "contraction GFLOP/s at <=1e-12 normwise rel err",
+        "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": len(vals), "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / len(vals), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_index):
+        self.proc = None
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ids = [x.strip() for x in vis.split(",")] if vis else []
+        self.gpu = ids[local_index] if local_index < len(ids) else str(local_index)
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def spread_tensor(torch, shape, seed, dev):
+    """uniform(-1,1) * 2^k, k uniform integer in [-20, 20], column-major in
+    label order, generated in chunks on the device."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    rev = list(reversed(shape))
+    t = torch.empty(rev, dtype=torch.float64, device=dev)
+    flat = t.view(-1)
+    chunk = 1 << 26
+    for s in range(0, flat.numel(), chunk):
+        e = min(flat.numel(), s + chunk)
+        u = torch.empty(e - s, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        k = torch.randint(-20, 21, (e - s,), device=dev, generator=g, dtype=torch.int32)
+        flat[s:e] = torch.ldexp(u, k)
+    return t.permute(*reversed(range(len(shape))))
+
+
+def time_steps(torch, fn, steps, stream):
+    """Times `steps` calls of fn with CUDA events on `stream`; per-step event
+    pairs give the kernel duration of the (single-launch) step."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(steps):
+        starts[i].record(stream)
+        fn()
+        ends[i].record(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    return e0.elapsed_time(e1), per
+
+
+def measure_fp64_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 (best of 5): the FP64 tensor-core denominator."""
+    n = 8192
+    a = torch.rand((n, n), dtype=torch.float64, device=dev)
+    b = torch.rand((n, n), dtype=torch.float64, device=dev)
+    c = torch.empty((n, n), dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = None
+    for _ in range(5):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b, out=c)
+        e.record()
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e)
+        best = t if best is None else min(best, t)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import tblis_b200 as tb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    stream = torch.cuda.current_stream()
+    tb.set_stream(stream.cuda_stream)
+
+    # --- headline workload: ladder with exponent spread --------------------------------
+    A = spread_tensor(torch, [V, V, V, V], 1001 + rank, dev)
+    B = spread_tensor(torch, [V, V, O, O], 1002 + rank, dev)
+    C = torch.zeros((O, O, V, V), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
+
+    # method selection: Ozaki INT8 when it is built and meets 1e-12 on this input,
+    # else the plain FP64 DMMA path (its error is the FP64 rounding itself)
+    method, method_name, err = 1, "fp64_dmma", 0.0
+    Cref = torch.zeros_like(C)
+    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cref, "abij", method=1)
+    try:
+        rep = tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=2, tolerance=1e-12)
+        torch.cuda.synchronize()
+        err = (torch.linalg.vector_norm(C - Cref) / torch.linalg.vector_norm(Cref)).item()
+        if err <= 1e-12:
+            method, method_name = 2, "ozaki_int8_%d_slices" % rep["slices"]
+    except tb.TblisError:
+        pass
+    del Cref
+    torch.cuda.empty_cache()
+
+    def step():
+        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
+
+    def step_fp64():
+        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=1)
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    k0 = tb.kernel_count()
+    total_ms, per = time_steps(torch, step, args.steps, stream)
+    launches = tb.kernel_count() - k0
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = t.item()
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * FLOPS_LADDER * args.steps / (total_ms * 1e-3) / 1e9
+
+    result = {
+        "metric": "contraction GFLOP/s at <=1e-12 normwise rel err",
+        "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "method": method_name, "m": V * V, "n": O * O, "k": V * V,
+                   "normwise_rel_err_vs_fp64": err, "l2": "inputs larger than L2 (A is 5.24 GB)",
+                   "parallelism": "replicas x%d (one contraction per GPU)" % world},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+
+    if rank == 0:
+        peaks = load_peaks()
+        extra = {}
+        # plain FP64 rate on the same workload and the roofline of its kernel
+        fp64_peak = measure_fp64_peak(torch, dev)
+        for _ in range(2):
+            step_fp64()
+        fp_ms, fp_per = time_steps(torch, step_fp64, max(3, args.steps // 2), stream)
+        fp_kernel_ms = statistics.mean(fp_per)
+        fp64_gflops = FLOPS_LADDER / (fp_kernel_ms * 1e-3) / 1e9
+        extra["fp64_dmma_gflops"] = fp64_gflops
+        extra["speedup_vs_fp64_path"] = value / world / fp64_gflops
+        kernel_ms = statistics.mean(per)
+        if method == 1:
+            achieved = FLOPS_LADDER / (kernel_ms * 1e-3) / 1e12
+            result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                                  "frac": achieved / fp64_peak, "traffic": None,
+                                  "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor cores)",
+                                  "kernel": "gemm_f64_kernel"}
+        else:
+            achieved = FLOPS_LADDER / (kernel_ms * 1e-3) / 1e12
+            result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                                  "frac": achieved / fp64_peak, "traffic": None, "kernel": "ozaki"}
+        del A, B, C
+        torch.cuda.empty_cache()
+
+        if not args.no_extra:
+            extra.update(extra_workloads(torch, tb, dev, stream, peaks))
+
+        # end-to-end through the C ABI with pinned host buffers (copies inside the timed region)
+        result["e2e"] = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)))
+
+        if world == 1 and not args.no_cpu:
+            cb = cpu_reference_sample()
+            if cb:
+                v, cores, sample = cb
+                result["cpu_baseline"] = {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "reference",
+                                          "sample": sample}
+        result["extra"] = extra
+        print(json.dumps(result))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e_ladder(torch, tb, method, steps):
+    A = spread_tensor(torch, [V, V, V, V], 1001, torch.device("cuda")).cpu().pin_memory()
+    B = spread_tensor(torch, [V, V, O, O], 1002, torch.device("cuda")).cpu().pin_memory()
+    C = torch.zeros((O, O, V, V), dtype=torch.float64).pin_memory().permute(3, 2, 1, 0)
+    h2d = (A.numel() + B.numel()) * 8
+    d2h = C.numel() * 8
+    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": FLOPS_LADDER / dt / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
+            "note": "host pinned buffers through tblis_tensor_mult; H2D of A,B and D2H of C inside each call"}
+
+
+def extra_workloads(torch, tb, dev, stream, peaks):
+    out = {}
+    # ring: C[aibj] += A[aeim]*B[mbej], o=64, v=256 (8.8 TFLOP), FP64 DMMA
+    o, v = 64, 256
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+
+    def cm(shape):
+        return torch.empty(list(reversed(shape)), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g) \
+            .permute(*reversed(range(len(shape))))
+    A = cm([v, v, o, o])
+    B = cm([o, v, v, o])
+    C = cm([v, o, v, o])
+    fl = 2.0 * v ** 3 * o ** 3
+
+    def ring():
+        tb.mult_ex(1.0, A, "aeim", B, "mbej", 1.0, C, "aibj", method=1)
+    ring()
+    ms, per = time_steps(torch, ring, 2, stream)
+    out["ring_fp64_gflops"] = fl / (statistics.mean(per) * 1e-3) / 1e9
+    del A, B
+    # transpose D[ijab] = C[abij] at the same size (bytes = read + write)
+    Cs = cm([v, v, o, o])
+    D = torch.zeros((v, v, o, o), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
+
+    def tr():
+        tb.add(1.0, Cs, "abij", 0.0, D, "ijab")
+    for _ in range(3):
+        tr()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    pers = []
+    for _ in range(5):
+        flush.fill_(1)
+        _, p = time_steps(torch, tr, 1, stream)
+        pers.append(p[0])
+    gbs = 2 * Cs.numel() * 8 / (statistics.median(pers) * 1e-3) / 1e9
+    out["transpose_gbs"] = gbs
+    if peaks.get("hbm_gbs"):
+        out["transpose_frac_of_measured_hbm"] = gbs / peaks["hbm_gbs"]
+    del C, Cs, D, flush
+    torch.cuda.empty_cache()
+    return out
+
+
+if __name__ == "__main__":
+    main()

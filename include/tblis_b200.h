@@ -1,0 +1,230 @@
+/*
+ * tblis_b200.h -- public C ABI of the B200 (sm_100a) TBLIS drop-in.
+ *
+ * The first part re-declares TBLIS's own C ABI with byte-identical types, so
+ * a program built against TBLIS's headers (src/tblis.h) links against
+ * libtblis_b200.so instead of libtblis.so unchanged. Each declaration cites
+ * the reference interface it replaces (paths relative to the TBLIS tree).
+ *
+ * Data residency: tensor data may live in device memory (cudaMalloc'd or
+ * managed; the call is stream-ordered on the library stream and returns
+ * without waiting, except dot/reduce which return a host scalar and so
+ * synchronise) or in host memory (the call stages the touched extent to the
+ * device and back and returns when the result is in host memory). No call
+ * computes on the CPU.
+ *
+ * Errors: the TBLIS entry points return void like the reference. A failure
+ * (unsupported type, malformed labels, CUDA error, no device) records a
+ * thread-local error readable with tblis_b200_last_error(); with the
+ * environment variable TBLIS_B200_ABORT_ON_ERROR=1 it aborts, like the
+ * reference's TBLIS_ASSERT in debug builds (src/util/basic_types.h:612-621).
+ */
+#ifndef TBLIS_B200_H
+#define TBLIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- types (src/util/basic_types.h) ------------------------------------ */
+
+typedef ptrdiff_t len_type;     /* configure.ac:91-101 default */
+typedef ptrdiff_t stride_type;  /* configure.ac:103-113 default */
+typedef char label_type;        /* configure.ac:115-123 default */
+
+/* src/util/basic_types.h:53-64 */
+typedef enum
+{
+    REDUCE_SUM      = 0,
+    REDUCE_SUM_ABS  = 1,
+    REDUCE_MAX      = 2,
+    REDUCE_MAX_ABS  = 3,
+    REDUCE_MIN      = 4,
+    REDUCE_MIN_ABS  = 5,
+    REDUCE_NORM_1   = REDUCE_SUM_ABS,
+    REDUCE_NORM_2   = 6,
+    REDUCE_NORM_INF = REDUCE_MAX_ABS
+} reduce_t;
+
+/* src/util/basic_types.h:66-73 */
+typedef enum
+{
+    TYPE_SINGLE   = 0,
+    TYPE_FLOAT    = TYPE_SINGLE,
+    TYPE_DOUBLE   = 1,
+    TYPE_SCOMPLEX = 2,
+    TYPE_DCOMPLEX = 3
+} type_t;
+
+/* src/util/basic_types.h:154-175: 16-byte value union + type tag (24 bytes) */
+typedef struct tblis_scalar
+{
+    union
+    {
+        float s;
+        double d;
+        float c[2];
+        double z[2];
+    } data;
+    type_t type;
+} tblis_scalar;
+
+/* src/util/basic_types.h:471-479 (64 bytes) */
+typedef struct tblis_tensor
+{
+    type_t type;
+    int conj;
+    tblis_scalar scalar;
+    void* data;
+    unsigned ndim;
+    len_type* len;
+    stride_type* stride;
+} tblis_tensor;
+
+/* src/util/thread.h:13 (tci_comm) and src/util/basic_types.h:51: opaque here.
+ * A non-null comm means the caller is inside a TCI parallel region; only its
+ * master thread may call this library (the GPU is driven by one host thread). */
+typedef struct tci_comm tblis_comm;
+typedef struct tblis_config_s tblis_config;
+
+/* ---- reference C ABI ---------------------------------------------------- */
+
+/* src/iface/3t/mult.h:17-20, src/iface/3t/mult.cxx:24-165 */
+void tblis_tensor_mult(const tblis_comm* comm, const tblis_config* cfg,
+                       const tblis_tensor* A, const label_type* idx_A,
+                       const tblis_tensor* B, const label_type* idx_B,
+                             tblis_tensor* C, const label_type* idx_C);
+
+/* src/iface/1t/add.h:17-19, src/iface/1t/add.cxx:24-110 */
+void tblis_tensor_add(const tblis_comm* comm, const tblis_config* cfg,
+                      const tblis_tensor* A, const label_type* idx_A,
+                            tblis_tensor* B, const label_type* idx_B);
+
+/* src/iface/1t/dot.h:17-20, src/iface/1t/dot.cxx:16-74 */
+void tblis_tensor_dot(const tblis_comm* comm, const tblis_config* cfg,
+                      const tblis_tensor* A, const label_type* idx_A,
+                      const tblis_tensor* B, const label_type* idx_B,
+                      tblis_scalar* result);
+
+/* src/iface/1t/reduce.h:17-19, src/iface/1t/reduce.cxx:16-68 */
+void tblis_tensor_reduce(const tblis_comm* comm, const tblis_config* cfg, reduce_t op,
+                         const tblis_tensor* A, const label_type* idx_A,
+                         tblis_scalar* result, len_type* idx);
+
+/* src/iface/1t/scale.h:17-18, src/iface/1t/scale.cxx:20-60 */
+void tblis_tensor_scale(const tblis_comm* comm, const tblis_config* cfg,
+                        tblis_tensor* A, const label_type* idx_A);
+
+/* src/iface/1t/set.h:17-18, src/iface/1t/set.cxx:16-50 */
+void tblis_tensor_set(const tblis_comm* comm, const tblis_config* cfg,
+                      const tblis_scalar* alpha, tblis_tensor* A, const label_type* idx_A);
+
+/* src/iface/1t/shift.h:17-18, src/iface/1t/shift.cxx:14-75 */
+void tblis_tensor_shift(const tblis_comm* comm, const tblis_config* cfg,
+                        const tblis_scalar* alpha, tblis_tensor* A, const label_type* idx_A);
+
+/* src/util/basic_types.h:549-579, defs src/util/basic_types.cxx:197-247 */
+void tblis_init_scalar_s(tblis_scalar* s, float value);
+void tblis_init_scalar_d(tblis_scalar* s, double value);
+void tblis_init_tensor_scaled_s(tblis_tensor* t, float scalar, unsigned ndim,
+                                len_type* len, float* data, stride_type* stride);
+void tblis_init_tensor_scaled_d(tblis_tensor* t, double scalar, unsigned ndim,
+                                len_type* len, double* data, stride_type* stride);
+void tblis_init_tensor_s(tblis_tensor* t, unsigned ndim, len_type* len, float* data,
+                         stride_type* stride);
+void tblis_init_tensor_d(tblis_tensor* t, unsigned ndim, len_type* len, double* data,
+                         stride_type* stride);
+
+/* src/util/thread.h:21-23, src/util/thread.cxx:108-118: kept for source
+ * compatibility; the value is recorded and returned but the GPU path does not
+ * use CPU threads. */
+unsigned tblis_get_num_threads(void);
+void tblis_set_num_threads(unsigned num_threads);
+
+/* src/util/configs.h:11: returns a GPU configuration by name, or NULL.
+ * Names: "b200_fp64" (default; FP64 DMMA), "b200_ozaki_i8" (INT8 Ozaki
+ * slices on tcgen05, slice count chosen from the tolerance). */
+const tblis_config* tblis_get_config(const char* name);
+
+/* ---- extensions (no counterpart in the reference) ------------------------ */
+
+/* Last error of the calling thread: 0 = none. The message is kept until the
+ * next failing call; tblis_b200_clear_error() resets it. */
+int tblis_b200_last_error(void);
+const char* tblis_b200_last_error_string(void);
+void tblis_b200_clear_error(void);
+
+/* Stream (a cudaStream_t) that subsequent calls of this host thread enqueue
+ * on; NULL = the legacy default stream. */
+void tblis_b200_set_stream(void* stream);
+void* tblis_b200_get_stream(void);
+/* Waits for all work this library enqueued on the current stream. */
+void tblis_b200_synchronize(void);
+
+/* Normwise relative tolerance carried by a configuration (used by the Ozaki
+ * configurations to pick the slice count; 0 restores the default 1e-12). */
+void tblis_b200_config_set_tolerance(tblis_config* cfg, double tol);
+double tblis_b200_config_get_tolerance(const tblis_config* cfg);
+
+/* Per-call options and report of the extended contraction entry point. */
+typedef struct tblis_b200_opts
+{
+    int method;          /* 0 = from cfg, 1 = FP64 DMMA, 2 = Ozaki INT8 */
+    int slices;          /* Ozaki slice count; 0 = choose from tolerance */
+    double tolerance;    /* normwise relative target; 0 = from cfg */
+} tblis_b200_opts;
+
+typedef struct tblis_b200_report
+{
+    int method;          /* method that ran */
+    int slices;          /* slice count used (0 for FP64) */
+    double est_error;    /* a-priori normwise error estimate */
+    double flops;        /* algorithmic FLOPs, 2*m*n*k*l */
+    int64_t m, n, k, l;  /* GEMM view of the contraction */
+    int kernels;         /* kernels launched by this call */
+} tblis_b200_report;
+
+/* tblis_tensor_mult with explicit method/tolerance and a report; returns 0
+ * on success, else an error code (also recorded as the last error). */
+int tblis_b200_tensor_mult_ex(const tblis_config* cfg,
+                              const tblis_tensor* A, const label_type* idx_A,
+                              const tblis_tensor* B, const label_type* idx_B,
+                                    tblis_tensor* C, const label_type* idx_C,
+                              const tblis_b200_opts* opts, tblis_b200_report* report);
+
+/* The product's block-scatter vector builder (restating
+ * src/matrix/block_scatter_matrix.hpp:249-258 for double), exported so the
+ * tests can compare it bit for bit with the reference. */
+void tblis_b200_fill_block_scatter(unsigned ndim, const len_type* len,
+                                   const stride_type* stride, len_type BS,
+                                   stride_type off, stride_type size,
+                                   stride_type* scat, stride_type* bs, int pack_3d);
+
+/* The product's index-group split of a contraction (src/iface/3t/mult.cxx:30-116
+ * and src/internal/3t/dense/mult.cxx:214-263), as label strings per group in
+ * their GEMM order and m/n/k/l. Returns 0 or an error code. */
+int tblis_b200_mult_groups(const tblis_tensor* A, const label_type* idx_A,
+                           const tblis_tensor* B, const label_type* idx_B,
+                           const tblis_tensor* C, const label_type* idx_C,
+                           char* idx_AB, char* idx_AC, char* idx_BC, char* idx_ABC,
+                           int64_t* mnkl);
+
+/* Number of kernels this library launched since the process started. */
+int64_t tblis_b200_kernel_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif

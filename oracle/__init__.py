@@ -1,0 +1,279 @@
+"""oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes access to (1) the C restatement of the TBLIS reference algorithms
+(oracle/tblis_oracle.c, built to oracle/_build/libtblis_oracle.so) and (2) the
+reference library itself, compiled from its own sources by oracle/Makefile into
+oracle/_ref/ (libtblis_ref.so plus librefshim.so, a shim exposing the block
+scatter builder, the DPD layout and the C++ DPD entry point).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this package, and only as the checker or the timed CPU
+baseline. The product (tblis_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(_HERE, "_build", "libtblis_oracle.so")
+REF_SO = os.path.join(_HERE, "_ref", "libtblis_ref.so")
+SHIM_SO = os.path.join(_HERE, "_ref", "librefshim.so")
+
+_P = ctypes.POINTER
+_sz = ctypes.c_ssize_t
+
+_orc = None
+_ref = None
+_shim = None
+
+
+class Scalar(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_double * 2), ("type", ctypes.c_int)]
+
+
+class Tensor(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("conj", ctypes.c_int), ("scalar", Scalar),
+                ("data", ctypes.c_void_p), ("ndim", ctypes.c_uint),
+                ("len", _P(_sz)), ("stride", _P(_sz))]
+
+
+def orc():
+    """The C restatement (always available once built)."""
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle not built: make -C oracle oracle")
+        _orc = ctypes.CDLL(ORACLE_SO)
+        _orc.orc_tensor_reduce_d.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_uint, _P(_sz), _P(_sz),
+                                             ctypes.c_void_p, ctypes.c_char_p, _P(ctypes.c_double), _P(_sz)]
+        for f in ("orc_tensor_mult_d", "orc_tensor_add_d", "orc_tensor_dot_d", "orc_tensor_mult_sample_d",
+                  "orc_mult_groups_build", "orc_tensor_scale_d", "orc_tensor_set_d", "orc_tensor_shift_d"):
+            getattr(_orc, f).restype = ctypes.c_int
+    return _orc
+
+
+def have_ref():
+    return os.path.exists(REF_SO) and os.path.exists(SHIM_SO)
+
+
+def ref():
+    """The reference TBLIS library built from its own sources."""
+    global _ref, _shim
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)   # local: its static libstdc++ must not interpose
+        _shim = ctypes.CDLL(SHIM_SO)
+        _shim.refshim_dpd_layout.restype = ctypes.c_long
+    return _ref
+
+
+def shim():
+    ref()
+    return _shim
+
+
+# ---- array helpers ------------------------------------------------------------------
+
+def _lens_strides(a):
+    n = a.ndim
+    L = (_sz * max(n, 1))(*a.shape)
+    S = (_sz * max(n, 1))(*[s // a.itemsize for s in a.strides])
+    return L, S
+
+
+def _lab(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+def _tensor(a, alpha=1.0, keep=None):
+    L, S = _lens_strides(a)
+    t = Tensor()
+    t.type = 1
+    t.conj = 0
+    t.scalar.data[0] = alpha
+    t.scalar.type = 1
+    t.data = a.ctypes.data
+    t.ndim = a.ndim
+    t.len = ctypes.cast(L, _P(_sz))
+    t.stride = ctypes.cast(S, _P(_sz))
+    if keep is not None:
+        keep.extend([L, S])
+    return t
+
+
+# ---- the C restatement ----------------------------------------------------------------
+
+def orc_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
+    """C = alpha*A*B + beta*C in place (numpy float64 arrays, any strides)."""
+    lA, sA = _lens_strides(A)
+    lB, sB = _lens_strides(B)
+    lC, sC = _lens_strides(C)
+    rc = orc().orc_tensor_mult_d(ctypes.c_double(alpha), A.ndim, lA, sA, ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+                                 B.ndim, lB, sB, ctypes.c_void_p(B.ctypes.data), _lab(idx_B),
+                                 ctypes.c_double(beta), C.ndim, lC, sC, ctypes.c_void_p(C.ctypes.data), _lab(idx_C))
+    if rc:
+        raise ValueError("oracle mult failed: %d" % rc)
+
+
+def orc_mult_sample(alpha, A, idx_A, B, idx_B, beta, C, idx_C, sample_idx):
+    """alpha*sum A*B + beta*C at the given multi-indices of C (rows of sample_idx)."""
+    sample_idx = np.ascontiguousarray(sample_idx, dtype=np.int64)
+    out = np.empty(sample_idx.shape[0], dtype=np.float64)
+    lA, sA = _lens_strides(A)
+    lB, sB = _lens_strides(B)
+    lC, sC = _lens_strides(C)
+    rc = orc().orc_tensor_mult_sample_d(
+        ctypes.c_double(alpha), A.ndim, lA, sA, ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+        B.ndim, lB, sB, ctypes.c_void_p(B.ctypes.data), _lab(idx_B),
+        ctypes.c_double(beta), C.ndim, lC, sC, ctypes.c_void_p(C.ctypes.data), _lab(idx_C),
+        _sz(sample_idx.shape[0]), ctypes.c_void_p(sample_idx.ctypes.data), ctypes.c_void_p(out.ctypes.data))
+    if rc:
+        raise ValueError("oracle sample failed: %d" % rc)
+    return out
+
+
+def orc_add(alpha, A, idx_A, beta, B, idx_B):
+    lA, sA = _lens_strides(A)
+    lB, sB = _lens_strides(B)
+    rc = orc().orc_tensor_add_d(ctypes.c_double(alpha), A.ndim, lA, sA, ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+                                ctypes.c_double(beta), B.ndim, lB, sB, ctypes.c_void_p(B.ctypes.data), _lab(idx_B))
+    if rc:
+        raise ValueError("oracle add failed: %d" % rc)
+
+
+def orc_dot(A, idx_A, B, idx_B, alpha_A=1.0, alpha_B=1.0):
+    lA, sA = _lens_strides(A)
+    lB, sB = _lens_strides(B)
+    r = ctypes.c_double()
+    rc = orc().orc_tensor_dot_d(ctypes.c_double(alpha_A), A.ndim, lA, sA, ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+                                ctypes.c_double(alpha_B), B.ndim, lB, sB, ctypes.c_void_p(B.ctypes.data), _lab(idx_B),
+                                ctypes.byref(r))
+    if rc:
+        raise ValueError("oracle dot failed: %d" % rc)
+    return r.value
+
+
+def orc_reduce(op, A, idx_A, alpha=1.0):
+    lA, sA = _lens_strides(A)
+    r = ctypes.c_double()
+    i = _sz()
+    rc = orc().orc_tensor_reduce_d(op, alpha, A.ndim, lA, sA, ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+                                   ctypes.byref(r), ctypes.byref(i))
+    if rc:
+        raise ValueError("oracle reduce failed: %d" % rc)
+    return r.value, i.value
+
+
+def orc_unary(kind, A, alpha=1.0, shift=0.0):
+    """kind: 'set' (A = alpha), 'scale' (A *= alpha), 'shift' (A = shift + alpha*A)."""
+    lA, sA = _lens_strides(A)
+    p = ctypes.c_void_p(A.ctypes.data)
+    if kind == "set":
+        return orc().orc_tensor_set_d(ctypes.c_double(alpha), A.ndim, lA, sA, p)
+    if kind == "scale":
+        return orc().orc_tensor_scale_d(ctypes.c_double(alpha), A.ndim, lA, sA, p)
+    return orc().orc_tensor_shift_d(ctypes.c_double(shift), ctypes.c_double(alpha), A.ndim, lA, sA, p)
+
+
+def orc_fill_block_scatter(lens, strides, BS, off, size, pack_3d):
+    n = len(lens)
+    L = (_sz * max(n, 1))(*lens)
+    S = (_sz * max(n, 1))(*strides)
+    scat = np.zeros(max(size, 1), dtype=np.int64)
+    bs = np.zeros(max(size, 1), dtype=np.int64)
+    orc().orc_fill_block_scatter(n, L, S, _sz(BS), _sz(off), _sz(size), ctypes.c_void_p(scat.ctypes.data),
+                                 ctypes.c_void_p(bs.ctypes.data), int(pack_3d))
+    return scat[:size], bs[:size]
+
+
+def orc_mult_groups(A, idx_A, B, idx_B, C, idx_C):
+    """Group split of the restatement: dict of label strings after fold."""
+    class G(ctypes.Structure):
+        M = 16
+        _fields_ = ([("n_AB", ctypes.c_uint), ("n_AC", ctypes.c_uint), ("n_BC", ctypes.c_uint), ("n_ABC", ctypes.c_uint)]
+                    + [(n, ctypes.c_char * 16) for n in ("idx_AB", "idx_AC", "idx_BC", "idx_ABC")]
+                    + [(n, _sz * 16) for n in ("len_AB", "len_AC", "len_BC", "len_ABC", "sA_AB", "sB_AB",
+                                               "sA_AC", "sC_AC", "sB_BC", "sC_BC", "sA_ABC", "sB_ABC", "sC_ABC")])
+    lA, sA = _lens_strides(A)
+    lB, sB = _lens_strides(B)
+    lC, sC = _lens_strides(C)
+    g = G()
+    rc = orc().orc_mult_groups_build(A.ndim, lA, sA, _lab(idx_A), B.ndim, lB, sB, _lab(idx_B),
+                                     C.ndim, lC, sC, _lab(idx_C), ctypes.byref(g))
+    if rc:
+        raise ValueError("oracle groups failed: %d" % rc)
+    out = {}
+    for grp in ("AB", "AC", "BC", "ABC"):
+        n = getattr(g, "n_" + grp)
+        out[grp] = bytes(getattr(g, "idx_" + grp)[:n]).decode("latin1")
+        out["len_" + grp] = list(getattr(g, "len_" + grp)[:n])
+    return out
+
+
+# ---- the reference itself -----------------------------------------------------------------
+
+def ref_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, threads=None):
+    keep = []
+    r = ref()
+    if threads:
+        r.tblis_set_num_threads(int(threads))
+    tA = _tensor(A, alpha, keep)
+    tB = _tensor(B, 1.0, keep)
+    tC = _tensor(C, beta, keep)
+    r.tblis_tensor_mult(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B),
+                        ctypes.byref(tC), _lab(idx_C))
+
+
+def ref_add(alpha, A, idx_A, beta, B, idx_B, threads=None):
+    keep = []
+    r = ref()
+    if threads:
+        r.tblis_set_num_threads(int(threads))
+    tA = _tensor(A, alpha, keep)
+    tB = _tensor(B, beta, keep)
+    r.tblis_tensor_add(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B))
+
+
+def ref_dot(A, idx_A, B, idx_B):
+    keep = []
+    tA = _tensor(A, 1.0, keep)
+    tB = _tensor(B, 1.0, keep)
+    s = Scalar()
+    s.type = 1
+    ref().tblis_tensor_dot(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B), ctypes.byref(s))
+    return s.data[0]
+
+
+def ref_reduce(op, A, idx_A, alpha=1.0):
+    keep = []
+    tA = _tensor(A, alpha, keep)
+    s = Scalar()
+    s.type = 1
+    i = _sz(-1)
+    ref().tblis_tensor_reduce(None, None, op, ctypes.byref(tA), _lab(idx_A), ctypes.byref(s), ctypes.byref(i))
+    return s.data[0], i.value
+
+
+def ref_fill_block_scatter(lens, strides, BS, off, size, pack_3d):
+    n = len(lens)
+    L = (_sz * max(n, 1))(*lens)
+    S = (_sz * max(n, 1))(*strides)
+    scat = np.zeros(max(size, 1), dtype=np.int64)
+    bs = np.zeros(max(size, 1), dtype=np.int64)
+    shim().refshim_fill_block_scatter(n, L, S, _sz(BS), _sz(off), _sz(size), ctypes.c_void_p(scat.ctypes.data),
+                                      ctypes.c_void_p(bs.ctypes.data), int(pack_3d))
+    return scat[:size], bs[:size]
+
+
+def ref_dpd_layout(irrep, nirrep, lens, layout=5):
+    """(total_size, block_offsets[nblock], block_strides[nblock][ndim]) from MArray."""
+    ndim = len(lens)
+    flat = (_sz * (ndim * nirrep))(*[x for row in lens for x in row])
+    nb = nirrep ** (ndim - 1)
+    offs = np.zeros(nb, dtype=np.int64)
+    strides = np.zeros(nb * ndim, dtype=np.int64)
+    total = shim().refshim_dpd_layout(irrep, nirrep, ndim, flat, layout, ctypes.c_void_p(offs.ctypes.data),
+                                      ctypes.c_void_p(strides.ctypes.data), ctypes.c_long(nb))
+    return total, offs, strides.reshape(nb, ndim)

@@ -1,0 +1,114 @@
+/*
+ * refshim.cxx -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A thin C-linkage shim over the TBLIS reference headers, compiled by
+ * oracle/Makefile into oracle/_ref/librefshim.so next to the reference
+ * library. It exposes internals that the reference's C ABI does not: the
+ * block-scatter vector builder (src/matrix/block_scatter_matrix.hpp:249-258),
+ * the MArray DPD block layout (src/external/marray/include/dpd_marray_base.hpp)
+ * and the C++ DPD contraction entry point (src/iface/3t/mult.cxx:170-298), so
+ * that the tests can pin the oracle restatement and the product's planner
+ * against the reference bit for bit.
+ */
+#include "util/basic_types.h"
+#include "util/tensor.hpp"
+#include "matrix/block_scatter_matrix.hpp"
+#include "iface/3t/mult.h"
+#include "iface/1t/add.h"
+
+using namespace tblis;
+
+namespace
+{
+struct bsm_access : block_scatter_matrix<double>
+{
+    using block_scatter_matrix<double>::fill_block_scatter;
+};
+}
+
+extern "C"
+{
+
+int refshim_version() { return 1; }
+
+void refshim_fill_block_scatter(unsigned ndim, const len_type* len, const stride_type* stride,
+                                len_type BS, stride_type off, stride_type size,
+                                stride_type* scat, stride_type* bs, int pack_3d)
+{
+    len_vector l(len, len+ndim);
+    stride_vector s(stride, stride+ndim);
+    bsm_access::fill_block_scatter(l, s, BS, off, size, scat, bs, pack_3d != 0);
+}
+
+/*
+ * DPD layout of a dense-stored DPD tensor: for every block (irreps tuple with
+ * XOR equal to `irrep`, enumerated with the first dimension's irrep fastest),
+ * writes the block's data offset from the tensor base and its strides.
+ * lens is [ndim][nirrep]. layout: MArray dpd_layout enum value.
+ * Returns the total number of elements, or -1.
+ */
+long refshim_dpd_layout(unsigned irrep, unsigned nirrep, unsigned ndim, const len_type* lens,
+                        int layout, long* block_offsets, long* block_strides, long max_blocks)
+{
+    std::vector<std::vector<len_type>> len(ndim, std::vector<len_type>(nirrep));
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++)
+            len[i][j] = lens[i*nirrep+j];
+
+    MArray::dpd_varray<double> A(irrep, nirrep, len, 0.0, (MArray::dpd_layout)layout);
+
+    long nblock = 0;
+    MArray::irrep_vector irreps(ndim);
+    long total = 1;
+    for (unsigned i = 0; i+1 < ndim; i++) total *= nirrep;
+    for (long b = 0; b < total && nblock < max_blocks; b++)
+    {
+        long t = b;
+        unsigned x = irrep;
+        for (unsigned i = 1; i < ndim; i++)
+        {
+            irreps[i] = t % nirrep;
+            t /= nirrep;
+            x ^= irreps[i];
+        }
+        irreps[0] = x;
+        auto v = A(irreps);
+        block_offsets[nblock] = v.data() - A.data();
+        for (unsigned i = 0; i < ndim; i++) block_strides[nblock*ndim+i] = v.stride(i);
+        nblock++;
+    }
+    return (long)A.size();
+}
+
+/*
+ * C = alpha*A*B + beta*C through the reference's own C++ DPD entry point
+ * (tblis::mult over dpd_varray_view, src/iface/3t/mult.cxx:170-298). The three
+ * tensors are given by their lens ([ndim][nirrep]), irrep and dense storage
+ * (default MArray layout). Returns 0 on success.
+ */
+int refshim_dpd_mult(unsigned nirrep,
+                     double alpha, unsigned irrep_A, unsigned ndim_A, const len_type* lens_A,
+                     const double* data_A, const char* idx_A,
+                     unsigned irrep_B, unsigned ndim_B, const len_type* lens_B,
+                     const double* data_B, const char* idx_B,
+                     double beta, unsigned irrep_C, unsigned ndim_C, const len_type* lens_C,
+                     double* data_C, const char* idx_C)
+{
+    auto mk = [&](unsigned ndim, const len_type* lens)
+    {
+        std::vector<std::vector<len_type>> len(ndim, std::vector<len_type>(nirrep));
+        for (unsigned i = 0; i < ndim; i++)
+            for (unsigned j = 0; j < nirrep; j++)
+                len[i][j] = lens[i*nirrep+j];
+        return len;
+    };
+
+    MArray::dpd_varray_view<const double> A(irrep_A, nirrep, mk(ndim_A, lens_A), data_A);
+    MArray::dpd_varray_view<const double> B(irrep_B, nirrep, mk(ndim_B, lens_B), data_B);
+    MArray::dpd_varray_view<double> C(irrep_C, nirrep, mk(ndim_C, lens_C), data_C);
+
+    tblis::mult<double>(alpha, A, idx_A, B, idx_B, beta, C, idx_C);
+    return 0;
+}
+
+}

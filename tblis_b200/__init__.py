@@ -1,0 +1,262 @@
+"""tblis_b200 -- Python mirror of TBLIS's tensor interface over the B200 C ABI.
+
+The functions mirror the reference's C++ wrappers (src/iface/3t/mult.h:28-38,
+src/iface/1t/add.h:27-35, src/iface/1t/dot.h, src/iface/1t/reduce.h:28-60,
+src/iface/1t/scale.h, set.h, shift.h): same names, same argument order and
+meaning (alpha/beta carried as tensor scalars, index strings as labels), and
+every call goes through ``libtblis_b200.so``'s C ABI (``tblis_tensor_*``), which
+runs hand-written sm_100a kernels. There is no CPU fallback: importing fails if
+the shared library is missing, and calls fail if no CUDA device is visible.
+
+Tensors may be torch tensors (device or host) or numpy arrays (host); host
+data is staged to the GPU by the library around the call.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libtblis_b200.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        "tblis_b200: %s is not built (run `make -C tblis_b200` or __graft_entry__.build())"
+        % _LIB_PATH)
+
+lib = ctypes.CDLL(_LIB_PATH)
+
+TYPE_FLOAT, TYPE_DOUBLE, TYPE_SCOMPLEX, TYPE_DCOMPLEX = 0, 1, 2, 3
+REDUCE_SUM, REDUCE_SUM_ABS, REDUCE_MAX, REDUCE_MAX_ABS = 0, 1, 2, 3
+REDUCE_MIN, REDUCE_MIN_ABS, REDUCE_NORM_2 = 4, 5, 6
+REDUCE_NORM_1, REDUCE_NORM_INF = REDUCE_SUM_ABS, REDUCE_MAX_ABS
+
+
+class tblis_scalar(ctypes.Structure):
+    """src/util/basic_types.h:154-175 (16-byte value union + type tag)."""
+    _fields_ = [("data", ctypes.c_double * 2), ("type", ctypes.c_int)]
+
+
+class tblis_tensor(ctypes.Structure):
+    """src/util/basic_types.h:471-479."""
+    _fields_ = [("type", ctypes.c_int), ("conj", ctypes.c_int), ("scalar", tblis_scalar),
+                ("data", ctypes.c_void_p), ("ndim", ctypes.c_uint),
+                ("len", ctypes.POINTER(ctypes.c_ssize_t)),
+                ("stride", ctypes.POINTER(ctypes.c_ssize_t))]
+
+
+class tblis_b200_opts(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("slices", ctypes.c_int), ("tolerance", ctypes.c_double)]
+
+
+class tblis_b200_report(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("slices", ctypes.c_int), ("est_error", ctypes.c_double),
+                ("flops", ctypes.c_double), ("m", ctypes.c_int64), ("n", ctypes.c_int64),
+                ("k", ctypes.c_int64), ("l", ctypes.c_int64), ("kernels", ctypes.c_int)]
+
+
+assert ctypes.sizeof(tblis_scalar) == 24 and ctypes.sizeof(tblis_tensor) == 64
+
+_P = ctypes.POINTER
+lib.tblis_tensor_mult.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p,
+                                  _P(tblis_tensor), ctypes.c_char_p, _P(tblis_tensor), ctypes.c_char_p]
+lib.tblis_tensor_add.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p,
+                                 _P(tblis_tensor), ctypes.c_char_p]
+lib.tblis_tensor_dot.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p,
+                                 _P(tblis_tensor), ctypes.c_char_p, _P(tblis_scalar)]
+lib.tblis_tensor_reduce.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(tblis_tensor),
+                                    ctypes.c_char_p, _P(tblis_scalar), _P(ctypes.c_ssize_t)]
+lib.tblis_tensor_scale.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p]
+lib.tblis_tensor_set.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _P(tblis_scalar), _P(tblis_tensor),
+                                 ctypes.c_char_p]
+lib.tblis_tensor_shift.argtypes = lib.tblis_tensor_set.argtypes
+lib.tblis_get_config.argtypes = [ctypes.c_char_p]
+lib.tblis_get_config.restype = ctypes.c_void_p
+lib.tblis_b200_last_error.restype = ctypes.c_int
+lib.tblis_b200_last_error_string.restype = ctypes.c_char_p
+lib.tblis_b200_tensor_mult_ex.argtypes = [ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p,
+                                          _P(tblis_tensor), ctypes.c_char_p, _P(tblis_tensor),
+                                          ctypes.c_char_p, _P(tblis_b200_opts), _P(tblis_b200_report)]
+lib.tblis_b200_tensor_mult_ex.restype = ctypes.c_int
+lib.tblis_b200_fill_block_scatter.argtypes = [ctypes.c_uint, _P(ctypes.c_ssize_t), _P(ctypes.c_ssize_t),
+                                              ctypes.c_ssize_t, ctypes.c_ssize_t, ctypes.c_ssize_t,
+                                              _P(ctypes.c_ssize_t), _P(ctypes.c_ssize_t), ctypes.c_int]
+lib.tblis_b200_mult_groups.argtypes = [_P(tblis_tensor), ctypes.c_char_p, _P(tblis_tensor),
+                                       ctypes.c_char_p, _P(tblis_tensor), ctypes.c_char_p,
+                                       ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                       ctypes.c_char_p, _P(ctypes.c_int64)]
+lib.tblis_b200_mult_groups.restype = ctypes.c_int
+lib.tblis_b200_kernel_count.restype = ctypes.c_int64
+lib.tblis_b200_set_stream.argtypes = [ctypes.c_void_p]
+lib.tblis_b200_get_stream.restype = ctypes.c_void_p
+lib.tblis_b200_config_set_tolerance.argtypes = [ctypes.c_void_p, ctypes.c_double]
+
+
+class TblisError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("tblis_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check():
+    code = lib.tblis_b200_last_error()
+    if code:
+        msg = lib.tblis_b200_last_error_string().decode()
+        lib.tblis_b200_clear_error()
+        raise TblisError(code, msg)
+
+
+def _labels(idx):
+    if isinstance(idx, bytes):
+        return idx
+    return idx.encode()
+
+
+def _dtype_code(x):
+    name = str(getattr(x, "dtype", ""))
+    if name.endswith("float64"):
+        return TYPE_DOUBLE, 8
+    if name.endswith("float32"):
+        return TYPE_FLOAT, 4
+    raise TypeError("tblis_b200: unsupported dtype %s" % name)
+
+
+class _View:
+    """A tblis_tensor describing a torch tensor or numpy array (no copy)."""
+
+    def __init__(self, x, scalar=1.0):
+        self.obj = x
+        code, esize = _dtype_code(x)
+        if hasattr(x, "data_ptr"):          # torch
+            shape = tuple(x.shape)
+            strides = tuple(x.stride())
+            ptr = x.data_ptr()
+        else:                                # numpy
+            shape = tuple(x.shape)
+            strides = tuple(s // esize for s in x.strides)
+            ptr = x.ctypes.data
+        n = len(shape)
+        self.len = (ctypes.c_ssize_t * max(n, 1))(*shape)
+        self.stride = (ctypes.c_ssize_t * max(n, 1))(*strides)
+        t = tblis_tensor()
+        t.type = code
+        t.conj = 0
+        t.scalar.type = code
+        if code == TYPE_DOUBLE:
+            t.scalar.data[0] = float(scalar)
+        else:
+            ctypes.cast(ctypes.byref(t.scalar), _P(ctypes.c_float))[0] = float(scalar)
+        t.data = ptr
+        t.ndim = n
+        t.len = ctypes.cast(self.len, _P(ctypes.c_ssize_t))
+        t.stride = ctypes.cast(self.stride, _P(ctypes.c_ssize_t))
+        self.t = t
+
+    @property
+    def ref(self):
+        return ctypes.byref(self.t)
+
+
+def get_config(name):
+    """src/util/configs.h:11 -- a configuration handle by name (or None)."""
+    p = lib.tblis_get_config(name.encode())
+    return p
+
+
+def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, cfg=None):
+    """C[idx_C] = alpha*A[idx_A]*B[idx_B] + beta*C[idx_C] (src/iface/3t/mult.h:28-38)."""
+    a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+    lib.tblis_tensor_mult(None, cfg, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref, _labels(idx_C))
+    _check()
+
+
+def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, tolerance=0.0, cfg=None):
+    """mult with an explicit method (1 = FP64 DMMA, 2 = Ozaki INT8) and a report dict."""
+    a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+    o = tblis_b200_opts(method, slices, tolerance)
+    r = tblis_b200_report()
+    lib.tblis_b200_tensor_mult_ex(cfg, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref,
+                                  _labels(idx_C), ctypes.byref(o), ctypes.byref(r))
+    _check()
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
+def add(alpha, A, idx_A, beta, B, idx_B):
+    """B[idx_B] = alpha*A[idx_A] + beta*B[idx_B] (src/iface/1t/add.h:27-35)."""
+    a, b = _View(A, alpha), _View(B, beta)
+    lib.tblis_tensor_add(None, None, a.ref, _labels(idx_A), b.ref, _labels(idx_B))
+    _check()
+
+
+def dot(A, idx_A, B, idx_B):
+    """sum over all labels of A*B (src/iface/1t/dot.h)."""
+    a, b = _View(A), _View(B)
+    r = tblis_scalar()
+    lib.tblis_tensor_dot(None, None, a.ref, _labels(idx_A), b.ref, _labels(idx_B), ctypes.byref(r))
+    _check()
+    return _scalar_value(r, a.t.type)
+
+
+def reduce(op, A, idx_A):
+    """(value, offset) of a reduction (src/iface/1t/reduce.h:47-53)."""
+    a = _View(A)
+    r = tblis_scalar()
+    r.type = a.t.type
+    idx = ctypes.c_ssize_t(-1)
+    lib.tblis_tensor_reduce(None, None, int(op), a.ref, _labels(idx_A), ctypes.byref(r), ctypes.byref(idx))
+    _check()
+    return _scalar_value(r, a.t.type), idx.value
+
+
+def scale(alpha, A, idx_A):
+    """A = alpha*A (src/iface/1t/scale.h)."""
+    a = _View(A, alpha)
+    lib.tblis_tensor_scale(None, None, a.ref, _labels(idx_A))
+    _check()
+
+
+def set(alpha, A, idx_A):  # noqa: A001 -- mirrors tblis::set
+    """A = alpha (src/iface/1t/set.h)."""
+    a = _View(A)
+    s = _make_scalar(alpha, a.t.type)
+    lib.tblis_tensor_set(None, None, ctypes.byref(s), a.ref, _labels(idx_A))
+    _check()
+
+
+def shift(alpha, beta, A, idx_A):
+    """A = alpha + beta*A (src/iface/1t/shift.h)."""
+    a = _View(A, beta)
+    s = _make_scalar(alpha, a.t.type)
+    lib.tblis_tensor_shift(None, None, ctypes.byref(s), a.ref, _labels(idx_A))
+    _check()
+
+
+def _make_scalar(v, code):
+    s = tblis_scalar()
+    s.type = code
+    if code == TYPE_DOUBLE:
+        s.data[0] = float(v)
+    else:
+        ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))[0] = float(v)
+    return s
+
+
+def _scalar_value(s, code):
+    if code == TYPE_DOUBLE:
+        return s.data[0]
+    return ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))[0]
+
+
+def kernel_count():
+    """Kernels this library launched in this process."""
+    return lib.tblis_b200_kernel_count()
+
+
+def set_stream(stream_handle):
+    """Make the library enqueue on a cudaStream_t (int handle); 0 = default stream."""
+    lib.tblis_b200_set_stream(ctypes.c_void_p(stream_handle))
+
+
+def synchronize():
+    lib.tblis_b200_synchronize()
+    _check()

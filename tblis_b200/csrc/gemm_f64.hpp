@@ -1,0 +1,33 @@
+// gemm_f64.hpp -- FP64 DMMA block-scatter contraction kernel (see gemm_f64.cu)
+#pragma once
+
+#include "common.hpp"
+
+namespace tb
+{
+
+struct GemmF64Args
+{
+    const double* A;
+    const double* B;
+    double* C;
+    // scatter vectors (device): element offsets per GEMM index
+    const i64 *a_m, *a_k, *b_k, *b_n, *c_m, *c_n, *a_l, *b_l, *c_l;
+    // per-BK-block common k strides of A and B (0 = irregular block)
+    const i64 *a_kbs, *b_kbs;
+    i64 M, N, K, L;
+    double alpha, beta;
+    int amode, bmode;        // gather directions (see GemmView)
+    int splits;              // split-K factor
+    i64 k_per_split;         // set by the launcher
+    double* partial;         // split-K workspace (splits*L*M*N doubles)
+};
+
+i64 gemm_f64_tile_m();
+i64 gemm_f64_tile_n();
+i64 gemm_f64_tile_k();
+int gemm_f64_choose_splits(i64 M, i64 N, i64 K, i64 L, int num_sms);
+size_t gemm_f64_workspace_bytes(i64 M, i64 N, i64 L, int splits);
+void gemm_f64_launch(GemmF64Args a, cudaStream_t stream);
+
+} // namespace tb

@@ -1,0 +1,532 @@
+// level1.cu -- strided level-1 tensor kernels.
+//
+// GPU counterparts of TBLIS's level-1 tensor operations
+// (src/internal/1t/dense/{add,dot,reduce,scale,set,shift}.cxx and their
+// microkernels src/kernels/1v/*.hpp, src/kernels/1m/trans.hpp). The host folds
+// each operand's dims first (the reference's fold), so most tensors arrive as
+// one or two long dims; the kernels then walk "segments" (a run of the inner
+// dimension of one outer row) with a warp per segment, 128-bit vector
+// accesses where the inner dim is unit-stride and 16-byte aligned, and
+// shared-memory tiles for transposes (the inner dims of A and B differ).
+// Reductions are two-pass and deterministic (fixed grid, fixed combine
+// order, no atomics).
+#include "level1.hpp"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+namespace tb
+{
+
+namespace
+{
+
+constexpr int SEG = 1024;          // inner elements per segment
+constexpr int L1_THREADS = 256;
+constexpr int RED_BLOCKS = 148*4;  // fixed grid of the reductions
+
+int l1_grid(i64 work_items, int per_block)
+{
+    i64 b = (work_items + per_block - 1)/per_block;
+    return (int)std::max<i64>(1, std::min<i64>(b, 148*32));
+}
+
+__device__ __forceinline__ i64 row_offset(const i64* len, const i64* stride, int ndim, i64 r)
+{
+    i64 off = 0;
+    for (int d = 1; d < ndim; d++)
+    {
+        i64 q = r / len[d];
+        off += (r - q*len[d])*stride[d];
+        r = q;
+    }
+    return off;
+}
+
+__device__ __forceinline__ void row_offset2(const Strided2& s, i64 r, i64& oa, i64& ob)
+{
+    oa = 0; ob = 0;
+    for (int d = 1; d < s.ndim; d++)
+    {
+        i64 q = r / s.len[d];
+        i64 i = r - q*s.len[d];
+        oa += i*s.sa[d];
+        ob += i*s.sb[d];
+        r = q;
+    }
+}
+
+// ---- set / scale / shift ------------------------------------------------------
+
+// op: 0 = set(value), 1 = scale(alpha), 2 = shift: shift + alpha*A
+template <typename T, int OP>
+__global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v0, T v1)
+{
+    const i64 n0 = s.ndim ? s.len[0] : 1;
+    const i64 st0 = s.ndim ? s.stride[0] : 0;
+    i64 rows = 1;
+    for (int d = 1; d < s.ndim; d++) rows *= s.len[d];
+    const i64 nchunk = (n0 + SEG - 1)/SEG;
+    const i64 nseg = rows*nchunk;
+    const int lane = threadIdx.x & 31;
+    const i64 warp0 = (blockIdx.x*(i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
+    for (i64 sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        T* base = A + row_offset(s.len, s.stride, s.ndim, r);
+        const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        for (i64 i = i0 + lane; i < i1; i += 32)
+        {
+            T* p = base + i*st0;
+            if (OP == 0) *p = v0;
+            else if (OP == 1) *p = v0*(*p);
+            else *p = v0 + v1*(*p);
+        }
+    }
+}
+
+// ---- add: permute / trace / replicate ------------------------------------------
+
+template <typename T, bool BETA0>
+__global__ void __launch_bounds__(L1_THREADS)
+k_add_general(const T* __restrict__ A, T* __restrict__ B, const Strided2 ab, const Strided ao,
+              const Strided bo, T alpha, T beta)
+{
+    const i64 n0 = ab.len[0];
+    i64 rows = 1;
+    for (int d = 1; d < ab.ndim; d++) rows *= ab.len[d];
+    i64 nao = 1, nbo = 1;
+    for (int d = 0; d < ao.ndim; d++) nao *= ao.len[d];
+    for (int d = 0; d < bo.ndim; d++) nbo *= bo.len[d];
+    const i64 total = rows*n0;
+    for (i64 e = blockIdx.x*(i64)blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x*blockDim.x)
+    {
+        const i64 r = e / n0, i = e - r*n0;
+        i64 oa, ob;
+        row_offset2(ab, r, oa, ob);
+        oa += i*ab.sa[0];
+        ob += i*ab.sb[0];
+        T sum = T(0);
+        for (i64 t = 0; t < nao; t++)
+        {
+            i64 x = t, o = 0;
+            for (int d = 0; d < ao.ndim; d++) { i64 q = x/ao.len[d]; o += (x - q*ao.len[d])*ao.stride[d]; x = q; }
+            sum += A[oa + o];
+        }
+        const T v = alpha*sum;
+        for (i64 t = 0; t < nbo; t++)
+        {
+            i64 x = t, o = 0;
+            for (int d = 0; d < bo.ndim; d++) { i64 q = x/bo.len[d]; o += (x - q*bo.len[d])*bo.stride[d]; x = q; }
+            T* p = B + ob + o;
+            *p = BETA0 ? v : v + beta*(*p);
+        }
+    }
+}
+
+// same unit-stride dimension in A and B: warp per segment of the inner dim,
+// 16-byte vectors when both inner strides are 1 and the rows are aligned
+template <typename T, bool BETA0>
+__global__ void __launch_bounds__(L1_THREADS)
+k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha, T beta)
+{
+    const i64 n0 = s.len[0];
+    i64 rows = 1;
+    for (int d = 1; d < s.ndim; d++) rows *= s.len[d];
+    const i64 nchunk = (n0 + SEG - 1)/SEG;
+    const i64 nseg = rows*nchunk;
+    const int lane = threadIdx.x & 31;
+    const i64 warp0 = (blockIdx.x*(i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
+    const bool unit = s.sa[0] == 1 && s.sb[0] == 1;
+    constexpr int VW = 16/sizeof(T);
+    for (i64 sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        i64 oa, ob;
+        row_offset2(s, r, oa, ob);
+        const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        const T* a = A + oa;
+        T* b = B + ob;
+        const bool vec = unit && ((((uintptr_t)(a + i0)) | ((uintptr_t)(b + i0))) & 15) == 0;
+        if (vec)
+        {
+            const i64 nv = (i1 - i0)/VW;
+            typedef typename std::conditional<sizeof(T) == 8, double2, float4>::type V;
+            const V* av = reinterpret_cast<const V*>(a + i0);
+            V* bv = reinterpret_cast<V*>(b + i0);
+            for (i64 v = lane; v < nv; v += 32)
+            {
+                V x = av[v];
+                T* xs = reinterpret_cast<T*>(&x);
+                V y;
+                T* ys = reinterpret_cast<T*>(&y);
+                if (!BETA0) y = bv[v];
+                #pragma unroll
+                for (int q = 0; q < VW; q++) ys[q] = BETA0 ? alpha*xs[q] : alpha*xs[q] + beta*ys[q];
+                bv[v] = y;
+            }
+            for (i64 i = i0 + nv*VW + lane; i < i1; i += 32)
+                b[i] = BETA0 ? alpha*a[i] : alpha*a[i] + beta*b[i];
+        }
+        else
+        {
+            for (i64 i = i0 + lane; i < i1; i += 32)
+            {
+                const T x = a[i*s.sa[0]];
+                T* p = b + i*s.sb[0];
+                *p = BETA0 ? alpha*x : alpha*x + beta*(*p);
+            }
+        }
+    }
+}
+
+// transpose: dim p is A's unit dim, dim q is B's unit dim, the rest are outer.
+// 64x64 tile through shared memory; reads coalesced along p, writes along q.
+constexpr int TT = 64;
+
+template <typename T, bool BETA0>
+__global__ void __launch_bounds__(L1_THREADS)
+k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p, int q,
+            i64 tiles_p, i64 tiles_q, i64 outer, T alpha, T beta)
+{
+    __shared__ T tile[TT][TT + 1];
+    const i64 np = s.len[p], nq = s.len[q];
+    const i64 ntiles = tiles_p*tiles_q*outer;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x)
+    {
+        i64 o = t / (tiles_p*tiles_q);
+        i64 pq = t - o*tiles_p*tiles_q;
+        i64 tq = pq / tiles_p, tp = pq - tq*tiles_p;
+        // outer offsets: decompose o over dims other than p and q
+        i64 oa = 0, ob = 0;
+        for (int d = 0; d < s.ndim; d++)
+        {
+            if (d == p || d == q) continue;
+            i64 qq = o / s.len[d];
+            i64 i = o - qq*s.len[d];
+            oa += i*s.sa[d]; ob += i*s.sb[d];
+            o = qq;
+        }
+        const i64 p0 = tp*TT, q0 = tq*TT;
+        // load: lanes along p (A contiguous)
+        #pragma unroll
+        for (int j = 0; j < TT/8; j++)
+        {
+            const int ql = ty + 8*j;
+            #pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const int pl = tx + 32*h;
+                const i64 pi = p0 + pl, qi = q0 + ql;
+                if (pi < np && qi < nq) tile[ql][pl] = A[oa + pi*s.sa[p] + qi*s.sa[q]];
+            }
+        }
+        __syncthreads();
+        // store: lanes along q (B contiguous)
+        #pragma unroll
+        for (int j = 0; j < TT/8; j++)
+        {
+            const int pl = ty + 8*j;
+            #pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const int ql = tx + 32*h;
+                const i64 pi = p0 + pl, qi = q0 + ql;
+                if (pi < np && qi < nq)
+                {
+                    T* dst = B + ob + pi*s.sb[p] + qi*s.sb[q];
+                    const T v = alpha*tile[ql][pl];
+                    *dst = BETA0 ? v : v + beta*(*dst);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- dot / reduce -----------------------------------------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(L1_THREADS)
+k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s, T* partial)
+{
+    const i64 n0 = s.ndim ? s.len[0] : 1;
+    i64 rows = 1;
+    for (int d = 1; d < s.ndim; d++) rows *= s.len[d];
+    const i64 nchunk = (n0 + SEG - 1)/SEG;
+    const i64 nseg = rows*nchunk;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const i64 warp0 = (blockIdx.x*(i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
+    const i64 sa0 = s.ndim ? s.sa[0] : 0, sb0 = s.ndim ? s.sb[0] : 0;
+    T acc = T(0);
+    for (i64 sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        i64 oa, ob;
+        row_offset2(s, r, oa, ob);
+        const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        for (i64 i = i0 + lane; i < i1; i += 32) acc += A[oa + i*sa0]*B[ob + i*sb0];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ T ws[L1_THREADS/32];
+    if (lane == 0) ws[wib] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        T t = T(0);
+        for (int w = 0; w < L1_THREADS/32; w++) t += ws[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+template <typename T>
+__global__ void k_sum_partials(const T* partial, int n, T* out)
+{
+    // one warp, fixed order
+    const int lane = threadIdx.x;
+    T acc = T(0);
+    for (int i = lane; i < n; i += 32) acc += partial[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) *out = acc;
+}
+
+// candidate of a MAX/MIN-type reduction: value, linear position, offset
+template <typename T>
+struct Cand { T v; i64 lin; i64 off; };
+
+template <typename T>
+__device__ __forceinline__ bool better(int op, const Cand<T>& a, const Cand<T>& b)
+{
+    // is a preferred over b? strict comparison; ties go to the earlier
+    // position in iteration order (the reference's sequential result)
+    if (a.lin < 0) return false;
+    if (b.lin < 0) return true;
+    bool gt = a.v > b.v, lt = a.v < b.v;
+    bool maxop = op == REDUCE_MAX || op == REDUCE_MAX_ABS;
+    if (maxop ? gt : lt) return true;
+    if (a.v == b.v) return a.lin < b.lin;
+    return false;
+}
+
+template <typename T>
+__device__ __forceinline__ T red_val(int op, T x)
+{
+    switch (op)
+    {
+        case REDUCE_SUM_ABS: case REDUCE_MAX_ABS: case REDUCE_MIN_ABS: return x < T(0) ? -x : x;
+        case REDUCE_NORM_2: return x*x;
+        default: return x;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(L1_THREADS)
+k_reduce_partial(int op, const T* __restrict__ A, const Strided s, T* pv, i64* plin, i64* poff)
+{
+    const i64 n0 = s.ndim ? s.len[0] : 1;
+    i64 rows = 1;
+    for (int d = 1; d < s.ndim; d++) rows *= s.len[d];
+    const i64 nchunk = (n0 + SEG - 1)/SEG;
+    const i64 nseg = rows*nchunk;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const i64 warp0 = (blockIdx.x*(i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
+    const i64 st0 = s.ndim ? s.stride[0] : 0;
+    const bool is_sum = op == REDUCE_SUM || op == REDUCE_SUM_ABS || op == REDUCE_NORM_2;
+    T acc = T(0);
+    Cand<T> best = {T(0), -1, -1};
+    for (i64 sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 ro = row_offset(s.len, s.stride, s.ndim, r);
+        const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        for (i64 i = i0 + lane; i < i1; i += 32)
+        {
+            const i64 off = ro + i*st0;
+            const T x = red_val(op, A[off]);
+            if (is_sum) acc += x;
+            else
+            {
+                Cand<T> cnd = {x, r*n0 + i, off};
+                if (better(op, cnd, best)) best = cnd;
+            }
+        }
+    }
+    __shared__ T sv[L1_THREADS];
+    __shared__ i64 sl[L1_THREADS], so[L1_THREADS];
+    if (is_sum)
+    {
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) sv[wib] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            T t = T(0);
+            for (int w = 0; w < L1_THREADS/32; w++) t += sv[w];
+            pv[blockIdx.x] = t; plin[blockIdx.x] = -1; poff[blockIdx.x] = -1;
+        }
+    }
+    else
+    {
+        sv[threadIdx.x] = best.v; sl[threadIdx.x] = best.lin; so[threadIdx.x] = best.off;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            Cand<T> b = {sv[0], sl[0], so[0]};
+            for (int t = 1; t < L1_THREADS; t++)
+            {
+                Cand<T> c = {sv[t], sl[t], so[t]};
+                if (better(op, c, b)) b = c;
+            }
+            pv[blockIdx.x] = b.v; plin[blockIdx.x] = b.lin; poff[blockIdx.x] = b.off;
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_reduce_final(int op, const T* pv, const i64* plin, const i64* poff, int n,
+                               T* out_v, i64* out_idx)
+{
+    if (threadIdx.x != 0) return;
+    const bool is_sum = op == REDUCE_SUM || op == REDUCE_SUM_ABS || op == REDUCE_NORM_2;
+    if (is_sum)
+    {
+        T t = T(0);
+        for (int i = 0; i < n; i++) t += pv[i];
+        if (op == REDUCE_NORM_2) t = sqrt(t);
+        *out_v = t; *out_idx = -1;
+        return;
+    }
+    Cand<T> b = {pv[0], plin[0], poff[0]};
+    for (int i = 1; i < n; i++)
+    {
+        Cand<T> c = {pv[i], plin[i], poff[i]};
+        if (better(op, c, b)) b = c;
+    }
+    if (b.lin < 0)
+    {
+        // empty tensor: the reference's initial values
+        switch (op)
+        {
+            case REDUCE_MAX: b.v = sizeof(T) == 8 ? (T)-DBL_MAX : (T)-FLT_MAX; break;
+            case REDUCE_MIN: case REDUCE_MIN_ABS: b.v = sizeof(T) == 8 ? (T)DBL_MAX : (T)FLT_MAX; break;
+            default: b.v = T(0);
+        }
+    }
+    *out_v = b.v; *out_idx = b.off;
+}
+
+} // namespace
+
+// ---- host launchers -------------------------------------------------------------------
+
+static i64 total_of(const Strided& s) { i64 t = 1; for (int d = 0; d < s.ndim; d++) t *= s.len[d]; return t; }
+static i64 total_of(const Strided2& s) { i64 t = 1; for (int d = 0; d < s.ndim; d++) t *= s.len[d]; return t; }
+
+template <typename T>
+static void unary_launch(int op, T* A, const Strided& s, T v0, T v1, cudaStream_t st)
+{
+    i64 total = total_of(s);
+    if (total == 0) return;
+    i64 n0 = s.ndim ? s.len[0] : 1;
+    i64 segs = (total/n0)*((n0 + SEG - 1)/SEG);
+    int grid = l1_grid(segs, L1_THREADS/32);
+    if (op == 0) k_unary<T, 0><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
+    else if (op == 1) k_unary<T, 1><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
+    else k_unary<T, 2><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
+    check_launch("k_unary");
+}
+
+template <typename T> void l1_set(T* A, const Strided& s, T value, cudaStream_t st) { unary_launch<T>(0, A, s, value, T(0), st); }
+template <typename T> void l1_scale(T* A, const Strided& s, T alpha, cudaStream_t st) { unary_launch<T>(1, A, s, alpha, T(0), st); }
+template <typename T> void l1_shift(T* A, const Strided& s, T shift, T alpha, cudaStream_t st) { unary_launch<T>(2, A, s, shift, alpha, st); }
+
+template <typename T>
+void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strided& bo,
+            T alpha, T beta, cudaStream_t st)
+{
+    i64 nab = total_of(ab);
+    if (nab == 0 || total_of(bo) == 0) return;
+    const bool b0 = beta == T(0);
+
+    if (ao.ndim == 0 && bo.ndim == 0 && ab.ndim > 0)
+    {
+        // find the unit-stride dims of A and B (smallest |stride| otherwise)
+        int pa = 0, pb = 0;
+        for (int d = 1; d < ab.ndim; d++)
+        {
+            if (std::llabs(ab.sa[d]) < std::llabs(ab.sa[pa])) pa = d;
+            if (std::llabs(ab.sb[d]) < std::llabs(ab.sb[pb])) pb = d;
+        }
+        if (pa == pb || ab.len[pa] == 1 || ab.len[pb] == 1)
+        {
+            // rows along the common fastest dim
+            Strided2 s = ab;
+            std::swap(s.len[0], s.len[pa]); std::swap(s.sa[0], s.sa[pa]); std::swap(s.sb[0], s.sb[pa]);
+            i64 n0 = s.len[0];
+            i64 segs = (nab/n0)*((n0 + SEG - 1)/SEG);
+            int grid = l1_grid(segs, L1_THREADS/32);
+            if (b0) k_add_rows<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
+            else k_add_rows<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
+            check_launch("k_add_rows");
+            return;
+        }
+        i64 tp = (ab.len[pa] + TT - 1)/TT, tq = (ab.len[pb] + TT - 1)/TT;
+        i64 outer = nab/(ab.len[pa]*ab.len[pb]);
+        i64 ntiles = tp*tq*outer;
+        int grid = (int)std::min<i64>(ntiles, 148*16);
+        if (b0) k_transpose<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
+        else k_transpose<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
+        check_launch("k_transpose");
+        return;
+    }
+
+    Strided2 s = ab;
+    if (s.ndim == 0) { s.ndim = 1; s.len[0] = 1; s.sa[0] = 0; s.sb[0] = 0; }
+    int grid = l1_grid(nab, L1_THREADS);
+    if (b0) k_add_general<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta);
+    else k_add_general<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta);
+    check_launch("k_add_general");
+}
+
+template <typename T>
+void l1_dot(const T* A, const T* B, const Strided2& ab, T* d_result, cudaStream_t st)
+{
+    dbuf part(RED_BLOCKS*sizeof(T), st);
+    k_dot_partial<T><<<RED_BLOCKS, L1_THREADS, 0, st>>>(A, B, ab, part.as<T>());
+    check_launch("k_dot_partial");
+    k_sum_partials<T><<<1, 32, 0, st>>>(part.as<T>(), RED_BLOCKS, d_result);
+    check_launch("k_sum_partials");
+}
+
+template <typename T>
+void l1_reduce(int op, const T* A, const Strided& s, T* d_value, i64* d_idx, cudaStream_t st)
+{
+    TB_CHECK(op >= 0 && op <= 6, TB_ERR_ARG, "unknown reduce op");
+    dbuf part(RED_BLOCKS*(sizeof(T) + 2*sizeof(i64)), st);
+    T* pv = part.as<T>();
+    i64* pl = reinterpret_cast<i64*>(part.as<char>() + RED_BLOCKS*sizeof(T));
+    i64* po = pl + RED_BLOCKS;
+    k_reduce_partial<T><<<RED_BLOCKS, L1_THREADS, 0, st>>>(op, A, s, pv, pl, po);
+    check_launch("k_reduce_partial");
+    k_reduce_final<T><<<1, 32, 0, st>>>(op, pv, pl, po, RED_BLOCKS, d_value, d_idx);
+    check_launch("k_reduce_final");
+}
+
+#define TB_L1_INST(T) \
+    template void l1_set<T>(T*, const Strided&, T, cudaStream_t); \
+    template void l1_scale<T>(T*, const Strided&, T, cudaStream_t); \
+    template void l1_shift<T>(T*, const Strided&, T, T, cudaStream_t); \
+    template void l1_add<T>(const T*, T*, const Strided2&, const Strided&, const Strided&, T, T, cudaStream_t); \
+    template void l1_dot<T>(const T*, const T*, const Strided2&, T*, cudaStream_t); \
+    template void l1_reduce<T>(int, const T*, const Strided&, T*, i64*, cudaStream_t);
+
+TB_L1_INST(float)
+TB_L1_INST(double)
+
+} // namespace tb
