@@ -40,7 +40,16 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    return p.parse_args()
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
+    p.add_argument("--o", type=int, default=48, help="occupied extent (profiling runs use a smaller case)")
+    p.add_argument("--v", type=int, default=160, help="virtual extent")
+    a = p.parse_args()
+    global O, V, FLOPS_LADDER, WORKLOAD
+    if (a.o, a.v) != (O, V):
+        O, V = a.o, a.v
+        FLOPS_LADDER = 2.0 * V * V * V * V * O * O
+        WORKLOAD = "ladder C[abij]=A[abef]*B[efij] o=%d v=%d fp64 exponent spread 2^[-20,20]" % (O, V)
+    return a
 
 
 def load_peaks():
@@ -304,7 +313,8 @@ def main():
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "method": method_name, "m": V * V, "n": O * O, "k": V * V,
-                   "normwise_rel_err_vs_fp64": err, "l2": "inputs larger than L2 (A is 5.24 GB)",
+                   "normwise_rel_err_vs_fp64": err,
+                   "l2": "inputs larger than L2 (A is %.2f GB)" % (V ** 4 * 8 / 1e9),
                    "parallelism": "replicas x%d (one contraction per GPU)" % world},
         "gpu_launches": int(launches),
         "clocks": clocks,
@@ -340,7 +350,8 @@ def main():
             extra.update(extra_workloads(torch, tb, dev, stream, peaks))
 
         # end-to-end through the C ABI with pinned host buffers (copies inside the timed region)
-        result["e2e"] = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)))
+        if not args.no_e2e:
+            result["e2e"] = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)))
 
         if world == 1 and not args.no_cpu:
             cb = cpu_reference_sample()
