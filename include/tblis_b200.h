@@ -219,6 +219,24 @@ int tblis_b200_mult_groups(const tblis_tensor* A, const label_type* idx_A,
 /* Number of kernels this library launched since the process started. */
 int64_t tblis_b200_kernel_count(void);
 
+/* No counterpart in the reference. tblis_tensor_mult for callers that cannot
+ * let a library allocate device memory (their device memory is owned by
+ * another allocator, or they must avoid cudaMalloc/cudaFree because those can
+ * synchronise the device): the same FP64 DMMA kernel, with its scatter vectors
+ * and split-K partial tiles in one fixed file-scope device array of
+ * TBLIS_B200_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit. Tensors must be in device memory; a contraction whose scatter
+ * vectors exceed the array is rejected (TB_ERR_SIZE = 5), and split-K is
+ * reduced until its partials fit. Calls share the array: calls that overlap on
+ * the GPU race and must be serialised. The first call on a device looks up the
+ * array's address; make it before any stream capture. Returns 0 or an error
+ * code (also recorded as the last error). */
+#define TBLIS_B200_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int tblis_b200_tensor_mult_noalloc(const tblis_tensor* A, const label_type* idx_A,
+                                   const tblis_tensor* B, const label_type* idx_B,
+                                         tblis_tensor* C, const label_type* idx_C);
+size_t tblis_b200_noalloc_scratch_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif
