@@ -10,6 +10,7 @@
 #include "gemm_f64.hpp"
 #include "level1.hpp"
 #include "mult.hpp"
+#include "ozaki.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -517,7 +518,14 @@ void tblis_b200_clear_error(void) { t_err_code = 0; t_err_msg.clear(); }
 
 void tblis_b200_set_stream(void* stream) { t_stream = static_cast<cudaStream_t>(stream); }
 void* tblis_b200_get_stream(void) { return t_stream; }
-void tblis_b200_synchronize(void) { guarded([&] { TB_CUDA(cudaStreamSynchronize(t_stream)); }); }
+void tblis_b200_synchronize(void)
+{
+    guarded([&]
+    {
+        TB_CUDA(cudaStreamSynchronize(t_stream));
+        TB_CHECK(ozaki_error_flag() == 0, TB_ERR_TIMEOUT, "an Ozaki kernel gave up a bounded wait");
+    });
+}
 
 void tblis_b200_fill_block_scatter(unsigned ndim, const len_type* len, const stride_type* stride,
                                    len_type BS, stride_type off, stride_type size,

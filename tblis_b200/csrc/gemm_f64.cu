@@ -1,4 +1,4 @@
-// gemm_f64.cu -- FP64 tensor-core (DMMA) contraction kernel with
+// gemm_f64.cu -- FP64 tensor-core (DMMA) contraction kernels with
 // block-scatter gathers.
 //
 // Replaces TBLIS's pack + microkernel + scatter-accumulate chain
@@ -6,19 +6,26 @@
 // src/nodes/gemm_ukr.hpp:16-126 and :193-364): every operand tile is gathered
 // straight from the strided tensor into shared memory with cp.async, driven by
 // the scatter vectors of the GEMM view (element offset of each row / column /
-// k index, with per-BK-block common strides that turn the k gather into
+// k index, with per-16-block common strides that turn the k gather into
 // strided arithmetic whenever the block is regular). No packed copy of A or B
 // is written to HBM. The alpha/beta update of C is scattered back through C's
 // scatter vectors in the epilogue; beta == 0 never reads C.
 //
-// Tile: 128x128x16 per CTA, 8 warps as 2 (m) x 4 (n), each warp 64x32 built
-// from mma.sync.m8n8k4 f64 (sm_100a has no tcgen05 FP64 kind; DMMA is the
-// FP64 tensor-core path). 4-stage cp.async pipeline. Split-K partial tiles go
-// to a workspace and are summed in a fixed order by gemm_f64_reduce (no
-// atomics: results do not depend on scheduling).
+// A family of tile shapes shares one kernel template: CTA tile BM x BN x 16,
+// warps of WM x WN built from mma.sync.m8n8k4 f64 (sm_100a has no tcgen05
+// FP64 kind; DMMA is the FP64 tensor-core path), a STAGES-deep cp.async
+// pipeline. Each operand is gathered along the GEMM dimension with its
+// smallest stride (m or k for A, n or k for B) and laid out in shared memory
+// so that both the cp.async writes and the fragment reads are free of bank
+// conflicts. The first k entry and block stride of the next tile are fetched
+// one iteration ahead so the gather addresses never wait on L2.
+//
+// Split-K partial tiles go to a workspace and are summed in a fixed order by
+// gemm_f64_reduce (no atomics: results do not depend on scheduling).
 #include "gemm_f64.hpp"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace tb
 {
@@ -26,15 +33,8 @@ namespace tb
 namespace
 {
 
-constexpr int BM = 128, BN = 128, BK = 16;
-constexpr int WM = 64, WN = 32;
-constexpr int MS = WM/8, NS = WN/8;
-constexpr int NTHREADS = 256;
-constexpr int STAGES = 4;
-constexpr int PADA = 4, PADB = 4;              // bank-conflict-free fragment loads
-constexpr int LDA = BM + PADA, LDB = BN + PADB;
-constexpr int STAGE_DOUBLES = BK*LDA + BK*LDB;
-constexpr size_t SMEM_BYTES = (size_t)STAGES*STAGE_DOUBLES*sizeof(double) + (BM + BN)*sizeof(i64)*2;
+constexpr int BK = 16;
+constexpr int PAD = 4;                         // doubles of padding per smem row
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid)
 {
@@ -55,20 +55,54 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
 }
 
-// offset of k index k within operand X: regular BK-blocks use strided
-// arithmetic from the block's first entry, irregular ones read the vector
-__device__ __forceinline__ i64 k_offset(const i64* __restrict__ scat, i64 k0, i64 bstride, int kl)
+// shared-memory geometry of one operand tile (ROWS = BM or BN)
+template <int ROWS, int MODE>
+struct Tile
 {
-    return bstride != 0 ? __ldg(scat + k0) + (i64)kl*bstride : __ldg(scat + k0 + kl);
+    // MODE 0: [BK][ROWS+PAD] (rows contiguous); MODE 1: [ROWS][BK+PAD] (k contiguous)
+    static constexpr int SIZE = MODE == 0 ? BK*(ROWS + PAD) : ROWS*(BK + PAD);
+    __device__ static __forceinline__ int idx(int r, int k)
+    {
+        return MODE == 0 ? k*(ROWS + PAD) + r : r*(BK + PAD) + k;
+    }
+};
+
+// k-offset information of one BK block of one operand
+struct KInfo
+{
+    i64 first;     // offset of the block's first k
+    i64 stride;    // common stride inside the block, 0 if irregular
+};
+
+__device__ __forceinline__ KInfo fetch_kinfo(const i64* __restrict__ scat, const i64* __restrict__ bstr,
+                                             i64 k0, bool valid)
+{
+    KInfo r = {0, 1};
+    if (valid)
+    {
+        r.first = __ldg(scat + k0);
+        r.stride = __ldg(bstr + k0/BK);
+    }
+    return r;
 }
 
-template <int AMODE, int BMODE>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__device__ __forceinline__ i64 koff(const i64* __restrict__ scat, const KInfo& ki, i64 k0, int kl)
+{
+    return ki.stride != 0 ? ki.first + (i64)kl*ki.stride : __ldg(scat + k0 + kl);
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, int MINB>
+__global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
 gemm_f64_kernel(const GemmF64Args p)
 {
+    constexpr int NT = (BM/WM)*(BN/WN)*32;
+    constexpr int MS = WM/8, NS = WN/8;
+    using TA = Tile<BM, AMODE>;
+    using TB = Tile<BN, BMODE>;
+    constexpr int STAGE = TA::SIZE + TB::SIZE;
+
     extern __shared__ __align__(16) double smem[];
-    double* sbase = smem;
-    i64* sAm = reinterpret_cast<i64*>(smem + STAGES*STAGE_DOUBLES);
+    i64* sAm = reinterpret_cast<i64*>(smem + STAGES*STAGE);
     i64* sBn = sAm + BM;
     i64* sCm = sBn + BN;
     i64* sCn = sCm + BM;
@@ -76,16 +110,16 @@ gemm_f64_kernel(const GemmF64Args p)
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
 
-    // tile rasterisation: groups of 8 m-tiles sweep the n-tiles together so
+    // rasterisation: groups of 8 m-tiles sweep the n-tiles together so
     // concurrently running CTAs share A and B panels in L2
     const i64 tiles_m = (p.M + BM - 1)/BM, tiles_n = (p.N + BN - 1)/BN;
-    i64 tile = blockIdx.x;
+    const i64 tile = blockIdx.x;
     const i64 group = 8;
-    i64 gid = tile/(group*tiles_n);
-    i64 first_m = gid*group;
-    i64 gsize = min(group, tiles_m - first_m);
-    i64 tm = first_m + (tile % (group*tiles_n)) % gsize;
-    i64 tn = (tile % (group*tiles_n)) / gsize;
+    const i64 gid = tile/(group*tiles_n);
+    const i64 first_m = gid*group;
+    const i64 gsize = min(group, tiles_m - first_m);
+    const i64 tm = first_m + (tile % (group*tiles_n)) % gsize;
+    const i64 tn = (tile % (group*tiles_n)) / gsize;
     const i64 m0 = tm*BM, n0 = tn*BN;
 
     const i64 l = blockIdx.y;
@@ -96,15 +130,15 @@ gemm_f64_kernel(const GemmF64Args p)
     const double* __restrict__ A = p.A + p.a_l[l];
     const double* __restrict__ B = p.B + p.b_l[l];
 
-    for (int i = tid; i < BM; i += NTHREADS)
+    for (int i = tid; i < BM; i += NT)
     {
-        i64 m = m0 + i;
+        const i64 m = m0 + i;
         sAm[i] = m < p.M ? p.a_m[m] : -1;
         sCm[i] = m < p.M ? p.c_m[m] : -1;
     }
-    for (int i = tid; i < BN; i += NTHREADS)
+    for (int i = tid; i < BN; i += NT)
     {
-        i64 n = n0 + i;
+        const i64 n = n0 + i;
         sBn[i] = n < p.N ? p.b_n[n] : -1;
         sCn[i] = n < p.N ? p.c_n[n] : -1;
     }
@@ -112,70 +146,31 @@ gemm_f64_kernel(const GemmF64Args p)
 
     const i64 kt_count = (k_end - k_begin + BK - 1)/BK;
 
-    auto load_tile = [&](int stage, i64 kt)
+    auto load_tile = [&](int stage, i64 kt, const KInfo& ka, const KInfo& kb)
     {
-        double* As = sbase + stage*STAGE_DOUBLES;
-        double* Bs = As + BK*LDA;
+        double* As = smem + stage*STAGE;
+        double* Bs = As + TA::SIZE;
         const i64 k0 = k_begin + kt*BK;
-        const i64 kblk = k0/BK;
-        const i64 abs_ = __ldg(p.a_kbs + kblk);
-        const i64 bbs_ = __ldg(p.b_kbs + kblk);
         const int kvalid = (int)min((i64)BK, k_end - k0);
-
-        if (AMODE == 0)
+        #pragma unroll
+        for (int e = tid; e < BK*BM; e += NT)
         {
-            const int ml = tid % BM;
+            const int ml = AMODE == 0 ? e % BM : e / BK;
+            const int kl = AMODE == 0 ? e / BM : e % BK;
             const i64 ro = sAm[ml];
-            #pragma unroll
-            for (int j = 0; j < BK*BM/NTHREADS; j++)
-            {
-                const int kl = tid/BM + j*(NTHREADS/BM);
-                const bool ok = ro >= 0 && kl < kvalid;
-                const i64 ko = ok ? k_offset(p.a_k, k0, abs_, kl) : 0;
-                cp_async8(As + kl*LDA + ml, ok ? A + ro + ko : p.A, ok);
-            }
+            const bool ok = ro >= 0 && kl < kvalid;
+            const i64 ko = ok ? koff(p.a_k, ka, k0, kl) : 0;
+            cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
         }
-        else
+        #pragma unroll
+        for (int e = tid; e < BK*BN; e += NT)
         {
-            const int kl = tid % BK;
-            const bool kok = kl < kvalid;
-            const i64 ko = kok ? k_offset(p.a_k, k0, abs_, kl) : 0;
-            #pragma unroll
-            for (int j = 0; j < BK*BM/NTHREADS; j++)
-            {
-                const int ml = tid/BK + j*(NTHREADS/BK);
-                const i64 ro = sAm[ml];
-                const bool ok = kok && ro >= 0;
-                cp_async8(As + kl*LDA + ml, ok ? A + ro + ko : p.A, ok);
-            }
-        }
-
-        if (BMODE == 0)
-        {
-            const int nl = tid % BN;
+            const int nl = BMODE == 0 ? e % BN : e / BK;
+            const int kl = BMODE == 0 ? e / BN : e % BK;
             const i64 co = sBn[nl];
-            #pragma unroll
-            for (int j = 0; j < BK*BN/NTHREADS; j++)
-            {
-                const int kl = tid/BN + j*(NTHREADS/BN);
-                const bool ok = co >= 0 && kl < kvalid;
-                const i64 ko = ok ? k_offset(p.b_k, k0, bbs_, kl) : 0;
-                cp_async8(Bs + kl*LDB + nl, ok ? B + co + ko : p.B, ok);
-            }
-        }
-        else
-        {
-            const int kl = tid % BK;
-            const bool kok = kl < kvalid;
-            const i64 ko = kok ? k_offset(p.b_k, k0, bbs_, kl) : 0;
-            #pragma unroll
-            for (int j = 0; j < BK*BN/NTHREADS; j++)
-            {
-                const int nl = tid/BK + j*(NTHREADS/BK);
-                const i64 co = sBn[nl];
-                const bool ok = kok && co >= 0;
-                cp_async8(Bs + kl*LDB + nl, ok ? B + co + ko : p.B, ok);
-            }
+            const bool ok = co >= 0 && kl < kvalid;
+            const i64 ko = ok ? koff(p.b_k, kb, k0, kl) : 0;
+            cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
         }
     };
 
@@ -188,12 +183,20 @@ gemm_f64_kernel(const GemmF64Args p)
     #pragma unroll
     for (int s = 0; s < STAGES-1; s++)
     {
-        if (s < kt_count) load_tile(s, s);
+        if (s < kt_count)
+        {
+            const i64 k0 = k_begin + s*BK;
+            load_tile(s, s, fetch_kinfo(p.a_k, p.a_kbs, k0, true), fetch_kinfo(p.b_k, p.b_kbs, k0, true));
+        }
         cp_async_commit();
     }
+    // k information of the next tile to load, one iteration ahead
+    i64 nk = STAGES - 1;
+    KInfo ka = fetch_kinfo(p.a_k, p.a_kbs, k_begin + nk*BK, nk < kt_count);
+    KInfo kb = fetch_kinfo(p.b_k, p.b_kbs, k_begin + nk*BK, nk < kt_count);
 
-    const int wm0 = (warp / (BN/WN))*WM;   // 2 warps along m
-    const int wn0 = (warp % (BN/WN))*WN;   // 4 warps along n
+    const int wm0 = (warp / (BN/WN))*WM;
+    const int wn0 = (warp % (BN/WN))*WN;
     const int fr = lane >> 2, fc = lane & 3;
 
     for (i64 kt = 0; kt < kt_count; kt++)
@@ -201,20 +204,22 @@ gemm_f64_kernel(const GemmF64Args p)
         cp_async_wait<STAGES-2>();
         __syncthreads();
 
-        const i64 nk = kt + STAGES - 1;
-        if (nk < kt_count) load_tile((int)(nk % STAGES), nk);
+        if (nk < kt_count) load_tile((int)(nk % STAGES), nk, ka, kb);
         cp_async_commit();
+        nk++;
+        ka = fetch_kinfo(p.a_k, p.a_kbs, k_begin + nk*BK, nk < kt_count);
+        kb = fetch_kinfo(p.b_k, p.b_kbs, k_begin + nk*BK, nk < kt_count);
 
-        const double* As = sbase + (kt % STAGES)*STAGE_DOUBLES;
-        const double* Bs = As + BK*LDA;
+        const double* As = smem + (kt % STAGES)*STAGE;
+        const double* Bs = As + TA::SIZE;
         #pragma unroll
         for (int kk = 0; kk < BK; kk += 4)
         {
             double af[MS], bf[NS];
             #pragma unroll
-            for (int i = 0; i < MS; i++) af[i] = As[(kk + fc)*LDA + wm0 + i*8 + fr];
+            for (int i = 0; i < MS; i++) af[i] = As[TA::idx(wm0 + i*8 + fr, kk + fc)];
             #pragma unroll
-            for (int j = 0; j < NS; j++) bf[j] = Bs[(kk + fc)*LDB + wn0 + j*8 + fr];
+            for (int j = 0; j < NS; j++) bf[j] = Bs[TB::idx(wn0 + j*8 + fr, kk + fc)];
             #pragma unroll
             for (int i = 0; i < MS; i++)
                 #pragma unroll
@@ -224,7 +229,6 @@ gemm_f64_kernel(const GemmF64Args p)
     }
     cp_async_wait<0>();
 
-    // epilogue
     if (p.splits > 1)
     {
         // raw partial sums into the workspace, [split][l][m][n] dense
@@ -236,14 +240,12 @@ gemm_f64_kernel(const GemmF64Args p)
             if (m >= p.M) continue;
             #pragma unroll
             for (int j = 0; j < NS; j++)
-            {
                 #pragma unroll
                 for (int h = 0; h < 2; h++)
                 {
                     const i64 n = n0 + wn0 + j*8 + fc*2 + h;
                     if (n < p.N) W[m*p.N + n] = acc[i][j][h];
                 }
-            }
         }
         return;
     }
@@ -253,12 +255,10 @@ gemm_f64_kernel(const GemmF64Args p)
     #pragma unroll
     for (int i = 0; i < MS; i++)
     {
-        const int ml = wm0 + i*8 + fr;
-        const i64 rc = sCm[ml];
+        const i64 rc = sCm[wm0 + i*8 + fr];
         if (rc < 0) continue;
         #pragma unroll
         for (int j = 0; j < NS; j++)
-        {
             #pragma unroll
             for (int h = 0; h < 2; h++)
             {
@@ -268,7 +268,6 @@ gemm_f64_kernel(const GemmF64Args p)
                 const double v = alpha*acc[i][j][h];
                 *dst = beta == 0.0 ? v : v + beta*(*dst);
             }
-        }
     }
 }
 
@@ -290,32 +289,88 @@ __global__ void gemm_f64_reduce(const GemmF64Args p)
     }
 }
 
-template <int AM, int BMd>
-void launch_one(const GemmF64Args& a, dim3 grid, cudaStream_t s)
+// one tile configuration
+struct Variant
 {
-    auto kern = gemm_f64_kernel<AM, BMd>;
-    static bool attr_set = false;
-    if (!attr_set)
+    int bm, bn;
+    void (*launch)(const GemmF64Args&, dim3, cudaStream_t, int amode, int bmode);
+};
+
+template <int BM_, int BN_, int WM, int WN, int STAGES, int MINB>
+struct Config
+{
+    static constexpr int NT = (BM_/WM)*(BN_/WN)*32;
+    static size_t smem_bytes(int am, int bmd)
     {
-        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-        attr_set = true;
+        size_t a = am == 0 ? BK*(BM_ + PAD) : BM_*(BK + PAD);
+        size_t b = bmd == 0 ? BK*(BN_ + PAD) : BN_*(BK + PAD);
+        return (size_t)STAGES*(a + b)*sizeof(double) + (2*BM_ + 2*BN_)*sizeof(i64);
     }
-    kern<<<grid, NTHREADS, SMEM_BYTES, s>>>(a);
-    check_launch("gemm_f64_kernel");
+    template <int AM, int BMd>
+    static void go(const GemmF64Args& a, dim3 grid, cudaStream_t s)
+    {
+        auto kern = gemm_f64_kernel<BM_, BN_, WM, WN, STAGES, AM, BMd, MINB>;
+        const size_t bytes = smem_bytes(AM, BMd);
+        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        kern<<<grid, NT, bytes, s>>>(a);
+        check_launch("gemm_f64_kernel");
+    }
+    static void launch(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
+    {
+        switch (am*2 + bmd)
+        {
+            case 0: go<0,0>(a, grid, s); break;
+            case 1: go<0,1>(a, grid, s); break;
+            case 2: go<1,0>(a, grid, s); break;
+            default: go<1,1>(a, grid, s); break;
+        }
+    }
+};
+
+// the tile family (index = variant id - 1)
+const Variant kVariants[] = {
+    {128, 128, Config<128, 128, 64, 32, 4, 1>::launch},   // 1: 8 warps, 1 CTA/SM
+    {64, 128, Config<64, 128, 32, 64, 3, 2>::launch},     // 2: 4 warps, 2 CTAs/SM
+    {128, 64, Config<128, 64, 64, 32, 3, 2>::launch},     // 3: 4 warps, 2 CTAs/SM
+    {64, 64, Config<64, 64, 32, 32, 3, 3>::launch},       // 4: 4 warps, 3 CTAs/SM
+};
+constexpr int kNumVariants = sizeof(kVariants)/sizeof(kVariants[0]);
+
+int env_variant()
+{
+    static int v = -1;
+    if (v < 0)
+    {
+        const char* s = getenv("TBLIS_B200_GEMM_VARIANT");
+        v = s ? atoi(s) : 0;
+        if (v < 0 || v > kNumVariants) v = 0;
+    }
+    return v;
+}
+
+int pick_variant(const GemmF64Args& a)
+{
+    if (a.variant > 0 && a.variant <= kNumVariants) return a.variant;
+    if (env_variant()) return env_variant();
+    // 64 x 64 tiles, three CTAs per SM: fastest of the family on B200 for
+    // both the large (ladder, ring, 8192^3) and the small (24^4) workloads
+    return 4;
 }
 
 } // namespace
 
-i64 gemm_f64_tile_m() { return BM; }
-i64 gemm_f64_tile_n() { return BN; }
+i64 gemm_f64_tile_m() { return 128; }
+i64 gemm_f64_tile_n() { return 128; }
 i64 gemm_f64_tile_k() { return BK; }
 
 int gemm_f64_choose_splits(i64 M, i64 N, i64 K, i64 L, int num_sms)
 {
-    const i64 tiles = ((M + BM - 1)/BM)*((N + BN - 1)/BN)*L;
+    // tiles of the default variant (64 x 64), three resident per SM
+    const i64 tiles = ((M + 63)/64)*((N + 63)/64)*L;
     const i64 kt = (K + BK - 1)/BK;
-    if (tiles >= num_sms || kt < 8) return 1;
-    i64 s = (2*num_sms + tiles - 1)/tiles;
+    const i64 slots = 3*(i64)num_sms;
+    if (tiles >= slots || kt < 8) return 1;
+    i64 s = (slots + tiles - 1)/tiles;
     s = std::min<i64>(s, kt/4);
     s = std::min<i64>(s, 32);
     return (int)std::max<i64>(1, s);
@@ -329,8 +384,10 @@ size_t gemm_f64_workspace_bytes(i64 M, i64 N, i64 L, int splits)
 void gemm_f64_launch(GemmF64Args a, cudaStream_t stream)
 {
     if (a.M == 0 || a.N == 0 || a.L == 0) return;
-    const i64 tiles_m = (a.M + BM - 1)/BM, tiles_n = (a.N + BN - 1)/BN;
+    const Variant& v = kVariants[pick_variant(a) - 1];
+    const i64 tiles_m = (a.M + v.bm - 1)/v.bm, tiles_n = (a.N + v.bn - 1)/v.bn;
     TB_CHECK(a.L <= 65535 && a.splits <= 65535, TB_ERR_SIZE, "batch extent too large");
+    TB_CHECK(tiles_m*tiles_n < (1ll << 31), TB_ERR_SIZE, "tile grid too large");
     if (a.splits < 1) a.splits = 1;
     // split boundaries on BK multiples
     const i64 kt = (a.K + BK - 1)/BK;
@@ -338,16 +395,9 @@ void gemm_f64_launch(GemmF64Args a, cudaStream_t stream)
     a.k_per_split = std::max<i64>(1, kt_per)*BK;
     a.splits = (int)std::max<i64>(1, (a.K + a.k_per_split - 1)/a.k_per_split);
     TB_CHECK(a.splits == 1 || a.partial, TB_ERR_ARG, "split-K needs a workspace");
-    dim3 grid((unsigned)(tiles_m*tiles_n), (unsigned)a.L, (unsigned)a.splits);
     if (a.K == 0) return;
-
-    switch (a.amode*2 + a.bmode)
-    {
-        case 0: launch_one<0,0>(a, grid, stream); break;
-        case 1: launch_one<0,1>(a, grid, stream); break;
-        case 2: launch_one<1,0>(a, grid, stream); break;
-        default: launch_one<1,1>(a, grid, stream); break;
-    }
+    dim3 grid((unsigned)(tiles_m*tiles_n), (unsigned)a.L, (unsigned)a.splits);
+    v.launch(a, grid, stream, a.amode, a.bmode);
 
     if (a.splits > 1)
     {

@@ -21,6 +21,7 @@ struct GemmF64Args
     int splits;              // split-K factor
     i64 k_per_split;         // set by the launcher
     double* partial;         // split-K workspace (splits*L*M*N doubles)
+    int variant;             // tile configuration, 0 = automatic
 };
 
 i64 gemm_f64_tile_m();

@@ -1,13 +1,726 @@
-// ozaki.cu -- Ozaki split-precision contraction.
+// ozaki.cu -- Ozaki split-precision contraction on the INT8 tensor cores.
+//
+// C = alpha*A*B + beta*C in FP64 accuracy from INT8 products (Ozaki scheme I
+// with per-row / per-column power-of-two scaling):
+//
+//  1. row statistics: e_r = max exponent of row r of A (of column n of B) so
+//     that |x| < 2^e_r, plus the row's sum of squares for the error estimate;
+//  2. slicing: x' = x*2^-e_r in (-1,1) is split into S signed digits
+//     d_p in [-64, 64] by round-to-nearest, x' = sum_p d_p*2^(1-7p) + r_S,
+//     |r_S| <= 2^-7S, every step exact in FP64. Digits are written as INT8
+//     planes [l][p][row][k] (k contiguous, 16-byte row pitch) straight from
+//     the strided tensor through the GEMM view's scatter vectors;
+//  3. one fused tcgen05 kernel per 128x64 output tile: for every k block,
+//     TMA brings the S planes of A and B into shared memory and one thread
+//     issues tcgen05.mma.kind::i8 for every slice pair (p, q) with
+//     p + q <= S + 1, accumulating pairs of equal p + q ("diagonal" d) in
+//     their own INT32 accumulator in tensor memory (exact: |sum| <=
+//     (d-1)*K*64^2 < 2^31 for the K of one launch); the epilogue sums the
+//     diagonals in FP64 with weights 2^(2-7d), applies 2^(e_m + f_n),
+//     alpha and beta, and scatters into C through C's scatter vectors.
+//
+// FP64 arithmetic is used only for the exponent extraction and scaling, the
+// digit extraction, the cross-diagonal summation and the alpha/beta update.
+// The slice count S is chosen per call from an a-priori estimate of the
+// normwise error (row maxima and norms of A and B) to meet the tolerance.
 #include "ozaki.hpp"
+#include "mult.hpp"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
 
 namespace tb
 {
 
-OzakiResult ozaki_mult(const GemmView&, const double*, const double*, double*,
-                       double, double, double, int, cudaStream_t)
+namespace
 {
-    throw error(TB_ERR_ARG, "Ozaki method not built yet");
+
+constexpr int OZ_BM = 128;           // tile rows (TMEM lanes)
+constexpr int OZ_BN = 64;            // tile columns per diagonal accumulator
+constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step)
+constexpr int OZ_SMAX = 8;           // 8 diagonals x 64 columns = all 512 TMEM columns
+constexpr int OZ_THREADS = 192;      // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int A_TILE = OZ_BM*OZ_BK;  // bytes of one A slice tile
+constexpr int B_TILE = OZ_BN*OZ_BK;  // bytes of one B slice tile
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded waits: 2 s
+
+__device__ int g_oz_error = 0;       // set by a kernel whose bounded wait gave up
+
+// ---------------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// waits for the phase with the given parity to complete, at most WAIT_NS;
+// returns false (and records the error) when the wait gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (unsigned it = 0;; it++)
+    {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255) == 0)
+        {
+            if (*abort_flag) return false;
+            if (globaltimer() - t0 > WAIT_NS)
+            {
+                *abort_flag = 1;
+                atomicExch(&g_oz_error, 1);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4, %5}], [%2];"
+                 :: "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(slot)), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                 :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// shared-memory matrix descriptor: K-major tile of 32-byte rows with the
+// 32-byte swizzle TMA writes (8-row atoms of 256 bytes, SBO = 256 B)
+__device__ __forceinline__ uint64_t sdesc_sw32(const void* p)
+{
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull)          // start address
+         | (1ull << 16)                        // leading byte offset (unused when swizzled)
+         | ((uint64_t)(256 >> 4) << 32)        // stride byte offset: 8 rows x 32 B
+         | (1ull << 46)                        // descriptor version (sm100)
+         | (6ull << 61);                       // SWIZZLE_32B
+}
+
+// instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = 64
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
+                              ((uint32_t)(OZ_BM >> 4) << 24);
+
+struct OzGemmArgs
+{
+    double* C;
+    const i64 *c_m, *c_n, *c_l;
+    const int *eA, *eB;          // [l][m], [l][n] exponents
+    i64 M, N, K, L;
+    int k_begin, k_count;        // k range of this launch (multiples of OZ_BK except the tail)
+    double alpha, beta;
+};
+
+// TMEM columns for S diagonal accumulators of OZ_BN columns (a power of two >= 32)
+template <int S>
+struct TmemCols
+{
+    static constexpr uint32_t need = (uint32_t)(S*OZ_BN);
+    static constexpr uint32_t value = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
+};
+
+template <int S, int STAGES>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                  const OzGemmArgs p)
+{
+    constexpr int STAGE_BYTES = S*(A_TILE + B_TILE);
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned base for the swizzled tiles
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES*STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accum = empty + STAGES;
+    uint64_t* done = accum + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    i64* sCm = reinterpret_cast<i64*>(tmem_slot + 4);
+    i64* sCn = sCm + OZ_BM;
+    double* sScaleN = reinterpret_cast<double*>(sCn + OZ_BN);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const i64 tiles_n = (p.N + OZ_BN - 1)/OZ_BN;
+    const i64 tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
+    const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*OZ_BN);
+    const int l = blockIdx.y;
+    const int kt_count = (p.k_count + OZ_BK - 1)/OZ_BK;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(accum, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, TmemCols<S>::value);
+    for (int i = threadIdx.x; i < OZ_BM; i += OZ_THREADS)
+    {
+        const i64 m = m0 + i;
+        sCm[i] = m < p.M ? p.c_m[m] : -1;
+    }
+    for (int i = threadIdx.x; i < OZ_BN; i += OZ_THREADS)
+    {
+        const i64 n = n0 + i;
+        sCn[i] = n < p.N ? p.c_n[n] : -1;
+        sScaleN[i] = n < p.N ? ldexp(1.0, p.eB[(i64)l*p.N + n]) : 0.0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0)
+    {
+        // ---- TMA producer -------------------------------------------------------
+        if (lane == 0)
+        {
+            for (int kt = 0; kt < kt_count && !*abort_flag; kt++)
+            {
+                const int s = kt % STAGES;
+                if (kt >= STAGES && !mbar_wait(&empty[s], ((kt/STAGES) & 1) ^ 1, abort_flag)) break;
+                unsigned char* st = smem + s*STAGE_BYTES;
+                mbar_expect_tx(&full[s], STAGE_BYTES);
+                const int kx = p.k_begin + kt*OZ_BK;
+                #pragma unroll
+                for (int q = 0; q < S; q++)
+                    tma_load_3d(st + q*A_TILE, &tmA, &full[s], kx, m0, l*S + q);
+                #pragma unroll
+                for (int q = 0; q < S; q++)
+                    tma_load_3d(st + S*A_TILE + q*B_TILE, &tmB, &full[s], kx, n0, l*S + q);
+            }
+            // drain: the copies of the last stages must have landed before exit
+            const int last = min(kt_count, STAGES);
+            for (int i = 0; i < last; i++)
+            {
+                const int kt = kt_count - 1 - i;
+                mbar_wait(&full[kt % STAGES], (kt/STAGES) & 1, abort_flag);
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        // ---- MMA issuer ----------------------------------------------------------
+        if (lane == 0)
+        {
+            for (int kt = 0; kt < kt_count; kt++)
+            {
+                const int s = kt % STAGES;
+                if (!mbar_wait(&full[s], (kt/STAGES) & 1, abort_flag)) break;
+                tc_fence_after();
+                const unsigned char* st = smem + s*STAGE_BYTES;
+                #pragma unroll
+                for (int d = 2; d <= S + 1; d++)
+                {
+                    const uint32_t acc_addr = tmem_base + (uint32_t)((d - 2)*OZ_BN);
+                    #pragma unroll
+                    for (int pa = 1; pa <= S; pa++)
+                    {
+                        const int qb = d - pa;
+                        if (qb < 1 || qb > S) continue;
+                        const uint64_t ad = sdesc_sw32(st + (pa - 1)*A_TILE);
+                        const uint64_t bd = sdesc_sw32(st + S*A_TILE + (qb - 1)*B_TILE);
+                        const bool first = kt == 0 && pa == max(1, d - S);
+                        mma_i8(acc_addr, ad, bd, IDESC_I8, first ? 0u : 1u);
+                    }
+                }
+                mma_commit(&empty[s]);
+            }
+            mma_commit(accum);
+            mma_commit(done);
+            mbar_wait(done, 0, abort_flag);
+        }
+    }
+    else
+    {
+        // ---- epilogue: warps 2..5, one TMEM lane quarter each --------------------
+        const int quarter = warp & 3;
+        const int row = quarter*32 + lane;
+        const bool ok = mbar_wait(accum, 0, abort_flag);
+        tc_fence_after();
+        const i64 rc = sCm[row];
+        const i64 m = (i64)m0 + row;
+        const double rscale = (rc >= 0 && ok) ? p.alpha*ldexp(1.0, p.eA[(i64)l*p.M + m]) : 0.0;
+        double* C = p.C + p.c_l[l];
+        #pragma unroll 1
+        for (int c = 0; c < OZ_BN/16; c++)
+        {
+            double v[16];
+            #pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = 0.0;
+            // smallest weights first
+            #pragma unroll
+            for (int d = S + 1; d >= 2; d--)
+            {
+                int r[16];
+                tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*OZ_BN + c*16), r);
+                const double w = ldexp(1.0, 2 - 7*d);
+                #pragma unroll
+                for (int j = 0; j < 16; j++) v[j] += (double)r[j]*w;
+            }
+            if (rc >= 0 && ok)
+            {
+                #pragma unroll
+                for (int j = 0; j < 16; j++)
+                {
+                    const i64 cc = sCn[c*16 + j];
+                    if (cc < 0) continue;
+                    double* dst = C + rc + cc;
+                    const double val = rscale*sScaleN[c*16 + j]*v[j];
+                    *dst = p.beta == 0.0 ? val : val + p.beta*(*dst);
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1)
+    {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, TmemCols<S>::value);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// statistics and slicing
+// ---------------------------------------------------------------------------------
+
+// view of one operand as rows x k (rows = m for A, n for B)
+struct OzOperand
+{
+    const double* X;
+    const i64 *r_off, *k_off, *l_off;
+    i64 R, K, L;
+    int rmode;                     // 0: gather along rows (rows contiguous), 1: along k
+};
+
+constexpr int ST_THREADS = 256;
+
+__device__ __forceinline__ int exp_of(double x)
+{
+    int e = 0;
+    if (x != 0.0) frexp(x, &e);
+    return x != 0.0 ? e : -100000;
+}
+
+// rows contiguous: a thread per row, k split over blockIdx.y; partial
+// (max exponent, sum of squares) per split
+__global__ void __launch_bounds__(ST_THREADS)
+oz_stats_rows(const OzOperand o, int ksplit, int* pexp, double* pss)
+{
+    const i64 r = blockIdx.x*(i64)ST_THREADS + threadIdx.x;
+    const int sp = blockIdx.y;
+    const int l = blockIdx.z;
+    if (r >= o.R) return;
+    const i64 kchunk = (o.K + ksplit - 1)/ksplit;
+    const i64 k0 = sp*kchunk, k1 = min(o.K, k0 + kchunk);
+    const double* X = o.X + o.l_off[l] + o.r_off[r];
+    int e = -100000;
+    double ss = 0.0;
+    for (i64 k = k0; k < k1; k++)
+    {
+        const double x = X[o.k_off[k]];
+        e = max(e, exp_of(x));
+        ss += x*x;
+    }
+    const i64 idx = ((i64)l*ksplit + sp)*o.R + r;
+    pexp[idx] = e;
+    pss[idx] = ss;
+}
+
+// k contiguous: a warp per row, lanes along k
+__global__ void __launch_bounds__(ST_THREADS)
+oz_stats_k(const OzOperand o, int* pexp, double* pss)
+{
+    const i64 r = (blockIdx.x*(i64)ST_THREADS + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int l = blockIdx.z;
+    if (r >= o.R) return;
+    const double* X = o.X + o.l_off[l] + o.r_off[r];
+    int e = -100000;
+    double ss = 0.0;
+    for (i64 k = lane; k < o.K; k += 32)
+    {
+        const double x = X[o.k_off[k]];
+        e = max(e, exp_of(x));
+        ss += x*x;
+    }
+    for (int s = 16; s > 0; s >>= 1)
+    {
+        e = max(e, __shfl_xor_sync(0xffffffffu, e, s));
+        ss += __shfl_xor_sync(0xffffffffu, ss, s);
+    }
+    if (lane == 0) { pexp[(i64)l*o.R + r] = e; pss[(i64)l*o.R + r] = ss; }
+}
+
+// combines the per-split partials in split order
+__global__ void oz_stats_final(i64 R, i64 L, int ksplit, const int* pexp, const double* pss, int* e_out,
+                               double* ss_out)
+{
+    const i64 i = blockIdx.x*(i64)blockDim.x + threadIdx.x;
+    if (i >= R*L) return;
+    const i64 l = i / R, r = i - l*R;
+    int e = -100000;
+    double ss = 0.0;
+    for (int sp = 0; sp < ksplit; sp++)
+    {
+        const i64 idx = (l*ksplit + sp)*R + r;
+        e = max(e, pexp[idx]);
+        ss += pss[idx];
+    }
+    e_out[i] = e == -100000 ? 0 : e;
+    ss_out[i] = ss;
+}
+
+// digits of one value: x' = x*2^-e, d_1 = rint(64 x'), then 7 bits per digit
+template <int S>
+__device__ __forceinline__ void digits(double xs, signed char (&d)[S])
+{
+    double y = xs*64.0;
+    #pragma unroll
+    for (int p = 0; p < S; p++)
+    {
+        const double t = rint(y);
+        d[p] = (signed char)(int)t;
+        y = (y - t)*128.0;
+    }
+}
+
+constexpr int SL_T = 64;     // 64 rows x 64 k per block
+
+// writes the S digit planes of a 64x64 tile, out[(l*S + p)][r][k], pitch kp
+template <int S>
+__global__ void __launch_bounds__(256)
+oz_slice(const OzOperand o, const int* e_rows, signed char* out, i64 kp)
+{
+    __shared__ double tile[SL_T][SL_T + 1];
+    const i64 r0 = blockIdx.x*(i64)SL_T, k0 = blockIdx.y*(i64)SL_T;
+    const int l = blockIdx.z;
+    const double* X = o.X + o.l_off[l];
+    const int t = threadIdx.x;
+    #pragma unroll
+    for (int j = 0; j < SL_T*SL_T/256; j++)
+    {
+        const int e = t + j*256;
+        const int rl = o.rmode == 0 ? e % SL_T : e / SL_T;
+        const int kl = o.rmode == 0 ? e / SL_T : e % SL_T;
+        const i64 r = r0 + rl, k = k0 + kl;
+        tile[rl][kl] = (r < o.R && k < o.K) ? X[o.r_off[r] + o.k_off[k]] : 0.0;
+    }
+    __syncthreads();
+    // 4 threads per row, 16 consecutive k each
+    const int rl = t >> 2, seg = (t & 3)*16;
+    const i64 r = r0 + rl;
+    if (r >= o.R) return;
+    const double sc = ldexp(1.0, -e_rows[(i64)l*o.R + r]);
+    signed char dg[16][S];
+    #pragma unroll
+    for (int j = 0; j < 16; j++)
+    {
+        signed char d[S];
+        digits<S>(tile[rl][seg + j]*sc, d);
+        #pragma unroll
+        for (int q = 0; q < S; q++) dg[j][q] = d[q];
+    }
+    const i64 kk = k0 + seg;
+    if (kk >= kp) return;
+    #pragma unroll
+    for (int q = 0; q < S; q++)
+    {
+        uint4 v;
+        unsigned char* b = reinterpret_cast<unsigned char*>(&v);
+        #pragma unroll
+        for (int j = 0; j < 16; j++) b[j] = (unsigned char)dg[j][q];
+        *reinterpret_cast<uint4*>(out + (((i64)l*S + q)*o.R + r)*kp + kk) = v;
+    }
+}
+
+template <int S>
+void launch_slice(const OzOperand& o, const int* e, signed char* out, i64 kp, cudaStream_t st)
+{
+    dim3 grid((unsigned)((o.R + SL_T - 1)/SL_T), (unsigned)((o.K + SL_T - 1)/SL_T), (unsigned)o.L);
+    oz_slice<S><<<grid, 256, 0, st>>>(o, e, out, kp);
+    check_launch("oz_slice");
+}
+
+void slice_dispatch(int S, const OzOperand& o, const int* e, signed char* out, i64 kp, cudaStream_t st)
+{
+    switch (S)
+    {
+        case 1: launch_slice<1>(o, e, out, kp, st); break;
+        case 2: launch_slice<2>(o, e, out, kp, st); break;
+        case 3: launch_slice<3>(o, e, out, kp, st); break;
+        case 4: launch_slice<4>(o, e, out, kp, st); break;
+        case 5: launch_slice<5>(o, e, out, kp, st); break;
+        case 6: launch_slice<6>(o, e, out, kp, st); break;
+        case 7: launch_slice<7>(o, e, out, kp, st); break;
+        default: launch_slice<8>(o, e, out, kp, st); break;
+    }
+}
+
+void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
+{
+    if (o.rmode == 0)
+    {
+        const int ksplit = (int)std::min<i64>(32, std::max<i64>(1, o.K/256));
+        dbuf pe((size_t)o.L*ksplit*o.R*sizeof(int), st), ps((size_t)o.L*ksplit*o.R*sizeof(double), st);
+        dim3 grid((unsigned)((o.R + ST_THREADS - 1)/ST_THREADS), (unsigned)ksplit, (unsigned)o.L);
+        oz_stats_rows<<<grid, ST_THREADS, 0, st>>>(o, ksplit, pe.as<int>(), ps.as<double>());
+        check_launch("oz_stats_rows");
+        oz_stats_final<<<(unsigned)((o.R*o.L + 255)/256), 256, 0, st>>>(o.R, o.L, ksplit, pe.as<int>(),
+                                                                        ps.as<double>(), e_out, ss_out);
+        check_launch("oz_stats_final");
+    }
+    else
+    {
+        dbuf pe((size_t)o.L*o.R*sizeof(int), st), ps((size_t)o.L*o.R*sizeof(double), st);
+        dim3 grid((unsigned)((o.R*32 + ST_THREADS - 1)/ST_THREADS), 1, (unsigned)o.L);
+        oz_stats_k<<<grid, ST_THREADS, 0, st>>>(o, pe.as<int>(), ps.as<double>());
+        check_launch("oz_stats_k");
+        oz_stats_final<<<(unsigned)((o.R*o.L + 255)/256), 256, 0, st>>>(o.R, o.L, 1, pe.as<int>(),
+                                                                        ps.as<double>(), e_out, ss_out);
+        check_launch("oz_stats_final");
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static std::mutex mtx;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::lock_guard<std::mutex> lk(mtx);
+    if (!fn)
+    {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        TB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        TB_CHECK(q == cudaDriverEntryPointSuccess && p, TB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map over the digit planes [L*S][R][kp] (bytes), box 32 x rows x 1
+CUtensorMap make_map(const signed char* base, i64 K, i64 R, i64 planes, i64 kp, int box_rows)
+{
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)R, (cuuint64_t)planes};
+    cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)(kp*R)};
+    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char*>(base), dims, strides,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TB_CHECK(r == CUDA_SUCCESS, TB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+template <int S>
+constexpr int stages_for()
+{
+    return std::min(6, (200*1024)/(S*(A_TILE + B_TILE)));
+}
+
+template <int S>
+size_t gemm_smem_bytes()
+{
+    return (size_t)stages_for<S>()*S*(A_TILE + B_TILE) + 1024 /* alignment */ +
+           (2*stages_for<S>() + 2)*8 + 16 + (OZ_BM + OZ_BN)*8 + OZ_BN*8;
+}
+
+template <int S>
+void launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb_, const OzGemmArgs& a, cudaStream_t st)
+{
+    constexpr int STG = stages_for<S>();
+    auto kern = ozaki_gemm_kernel<S, STG>;
+    const size_t bytes = gemm_smem_bytes<S>();
+    TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    const i64 tiles = ((a.M + OZ_BM - 1)/OZ_BM)*((a.N + OZ_BN - 1)/OZ_BN);
+    dim3 grid((unsigned)tiles, (unsigned)a.L, 1);
+    kern<<<grid, OZ_THREADS, bytes, st>>>(ta, tb_, a);
+    check_launch("ozaki_gemm_kernel");
+}
+
+void gemm_dispatch(int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a, cudaStream_t st)
+{
+    switch (S)
+    {
+        case 1: launch_gemm<1>(ta, tbm, a, st); break;
+        case 2: launch_gemm<2>(ta, tbm, a, st); break;
+        case 3: launch_gemm<3>(ta, tbm, a, st); break;
+        case 4: launch_gemm<4>(ta, tbm, a, st); break;
+        case 5: launch_gemm<5>(ta, tbm, a, st); break;
+        case 6: launch_gemm<6>(ta, tbm, a, st); break;
+        case 7: launch_gemm<7>(ta, tbm, a, st); break;
+        default: launch_gemm<8>(ta, tbm, a, st); break;
+    }
+}
+
+// a-priori normwise error estimate for S slices (rounding of both operands
+// to S digits plus the dropped cross terms), from per-row maxima and norms
+double estimate_error(int S, const std::vector<int>& eA, const std::vector<double>& ssA, i64 KA,
+                      const std::vector<int>& eB, const std::vector<double>& ssB, i64 KB)
+{
+    auto rel = [&](const std::vector<int>& e, const std::vector<double>& ss, i64 K)
+    {
+        double num = 0.0, den = 0.0;
+        for (size_t i = 0; i < e.size(); i++)
+        {
+            num += (double)K*std::ldexp(1.0, 2*(e[i] - 7*S))/3.0;
+            den += ss[i];
+        }
+        return den > 0 ? std::sqrt(num/den) : 0.0;
+    };
+    const double ra = rel(eA, ssA, KA), rb = rel(eB, ssB, KB);
+    // dropped pairs p + q > S + 1 are below the rounding terms by ~2^-7
+    return (ra + rb)*(1.0 + 2.0*S*std::ldexp(1.0, -7));
+}
+
+} // namespace
+
+int ozaki_error_flag()
+{
+    int v = 0;
+    cudaMemcpyFromSymbol(&v, g_oz_error, sizeof(int));
+    return v;
+}
+
+OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
+                       double alpha, double beta, double tol, int slices, cudaStream_t st)
+{
+    OzakiResult res;
+    const i64 BMt = 128, BNt = 128, BKt = 16;
+    auto tab = gemm_tables(v, BMt, BNt, BKt, st);
+    TB_CHECK(v.m < (1ll << 31) && v.n < (1ll << 31) && v.k < (1ll << 31), TB_ERR_SIZE,
+             "Ozaki path: extents beyond 2^31");
+    TB_CHECK(v.l*OZ_SMAX < (1ll << 31), TB_ERR_SIZE, "Ozaki path: batch too large");
+
+    OzOperand oa = {A, tab->a_m, tab->a_k, tab->a_l, v.m, v.k, v.l, v.amode};
+    OzOperand ob = {B, tab->b_n, tab->b_k, tab->b_l, v.n, v.k, v.l, v.bmode};
+
+    dbuf eA((size_t)v.l*v.m*sizeof(int), st), eB((size_t)v.l*v.n*sizeof(int), st);
+    dbuf sA((size_t)v.l*v.m*sizeof(double), st), sB((size_t)v.l*v.n*sizeof(double), st);
+    stats(oa, eA.as<int>(), sA.as<double>(), st);
+    stats(ob, eB.as<int>(), sB.as<double>(), st);
+
+    int S = slices;
+    if (S <= 0)
+    {
+        std::vector<int> heA(v.l*v.m), heB(v.l*v.n);
+        std::vector<double> hsA(v.l*v.m), hsB(v.l*v.n);
+        TB_CUDA(cudaMemcpyAsync(heA.data(), eA.ptr, heA.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
+        TB_CUDA(cudaMemcpyAsync(heB.data(), eB.ptr, heB.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
+        TB_CUDA(cudaMemcpyAsync(hsA.data(), sA.ptr, hsA.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
+        TB_CUDA(cudaMemcpyAsync(hsB.data(), sB.ptr, hsB.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
+        TB_CUDA(cudaStreamSynchronize(st));
+        S = OZ_SMAX;
+        for (int s = 1; s <= OZ_SMAX; s++)
+        {
+            // safety factor 4 between the estimate and the target
+            if (estimate_error(s, heA, hsA, v.k, heB, hsB, v.k)*4.0 <= tol) { S = s; break; }
+        }
+        res.est_error = estimate_error(S, heA, hsA, v.k, heB, hsB, v.k);
+    }
+    TB_CHECK(S >= 1 && S <= OZ_SMAX, TB_ERR_ARG, "Ozaki slice count must be 1..8");
+    res.slices = S;
+
+    const i64 kp = (v.k + 63)/64*64;       // row pitch: TMA strides and 16-byte digit stores
+    dbuf pa((size_t)v.l*S*v.m*kp, st), pb((size_t)v.l*S*v.n*kp, st);
+    slice_dispatch(S, oa, eA.as<int>(), pa.as<signed char>(), kp, st);
+    slice_dispatch(S, ob, eB.as<int>(), pb.as<signed char>(), kp, st);
+
+    const CUtensorMap ta = make_map(pa.as<signed char>(), v.k, v.m, v.l*S, kp, OZ_BM);
+    const CUtensorMap tbm = make_map(pb.as<signed char>(), v.k, v.n, v.l*S, kp, OZ_BN);
+
+    // INT32 exactness: (#pairs on a diagonal) * K_launch * 64^2 < 2^31
+    const i64 klimit = ((i64)0x7fffffff/((i64)S*64*64))/OZ_BK*OZ_BK;
+    for (i64 k0 = 0; k0 < v.k; k0 += klimit)
+    {
+        OzGemmArgs g;
+        g.C = C;
+        g.c_m = tab->c_m; g.c_n = tab->c_n; g.c_l = tab->c_l;
+        g.eA = eA.as<int>(); g.eB = eB.as<int>();
+        g.M = v.m; g.N = v.n; g.K = v.k; g.L = v.l;
+        g.k_begin = (int)k0;
+        g.k_count = (int)std::min(klimit, v.k - k0);
+        g.alpha = alpha;
+        g.beta = k0 == 0 ? beta : 1.0;
+        gemm_dispatch(S, ta, tbm, g, st);
+    }
+    return res;
 }
 
 } // namespace tb

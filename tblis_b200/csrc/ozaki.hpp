@@ -16,3 +16,9 @@ OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, doub
                        double alpha, double beta, double tol, int slices, cudaStream_t st);
 
 } // namespace tb
+
+namespace tb
+{
+// nonzero when an Ozaki kernel gave up a bounded wait (reads a device flag)
+int ozaki_error_flag();
+}
