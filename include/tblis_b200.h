@@ -219,6 +219,61 @@ int tblis_b200_mult_groups(const tblis_tensor* A, const label_type* idx_A,
 /* Number of kernels this library launched since the process started. */
 int64_t tblis_b200_kernel_count(void);
 
+/* ---- DPD (irrep block-sparse) tensors ------------------------------------ */
+
+/* A dense-stored DPD tensor as MArray's dpd_varray lays it out
+ * (src/external/marray/include/dpd_varray_base.hpp:10-128,
+ * dpd_marray_base.hpp:34-228): the symmetry-allowed blocks of irrep `irrep`
+ * (XOR of the block's irreps) stored back to back in one buffer of
+ * tblis_b200_dpd_size() elements. len is [ndim][nirrep] row-major; layout is
+ * MArray's dpd_layout type (0 BALANCED_COLUMN_MAJOR, 1 BALANCED_ROW_MAJOR,
+ * 2 BLOCKED_COLUMN_MAJOR, 3 BLOCKED_ROW_MAJOR, 4 PREFIX_COLUMN_MAJOR,
+ * 5 PREFIX_ROW_MAJOR; -1 = MArray's default, PREFIX_ROW_MAJOR). */
+typedef struct tblis_b200_dpd_tensor
+{
+    type_t type;
+    int conj;
+    tblis_scalar scalar;
+    void* data;
+    unsigned ndim;
+    unsigned nirrep;
+    unsigned irrep;
+    const len_type* len;
+    int layout;
+} tblis_b200_dpd_tensor;
+
+/* C = alpha*A*B + beta*C over DPD tensors (alpha = A.scalar*B.scalar, beta =
+ * C.scalar), the C entry of tblis::mult over dpd_varray_view
+ * (src/iface/3t/mult.cxx:170-289, src/internal/3t/dpd/mult.cxx:223-356): one
+ * GEMM per irrep of the contracted labels, all in one grouped launch. Labels
+ * must be unique per tensor; labels shared by all three tensors are not
+ * supported. Returns 0 or an error code. report->m = irrep GEMMs launched,
+ * report->n = tile configuration picked by the autotuner. */
+int tblis_b200_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                        const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                              tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                        tblis_b200_report* report);
+
+/* Offset (from data), lengths and strides of one block (one irrep per
+ * dimension), as dpd_varray_view::operator()(irreps) gives them
+ * (dpd_marray_base.hpp:171-228). Returns 0 or an error code. */
+int tblis_b200_dpd_block(const tblis_b200_dpd_tensor* A, const unsigned* irreps, len_type* len,
+                         stride_type* stride, stride_type* offset);
+
+/* Number of stored elements (all allowed blocks), or -1 on error. */
+len_type tblis_b200_dpd_size(const tblis_b200_dpd_tensor* A);
+
+/* ---- batches -------------------------------------------------------------- */
+
+/* count independent contractions C[i] = alpha_i*A[i]*B[i] + beta_i*C[i] (each
+ * as tblis_tensor_mult) in one grouped launch of the FP64 kernel; device data
+ * only. The grouped plan (scatter vectors, tuned tile shape, CUDA graph) is
+ * cached per set of shapes. Returns 0 or an error code. */
+int tblis_b200_tensor_mult_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
+                                 const tblis_tensor* B, const label_type* const* idx_B,
+                                       tblis_tensor* C, const label_type* const* idx_C,
+                                 tblis_b200_report* report);
+
 /* No counterpart in the reference. tblis_tensor_mult for callers that cannot
  * let a library allocate device memory (their device memory is owned by
  * another allocator, or they must avoid cudaMalloc/cudaFree because those can

@@ -277,3 +277,41 @@ def ref_dpd_layout(irrep, nirrep, lens, layout=5):
     total = shim().refshim_dpd_layout(irrep, nirrep, ndim, flat, layout, ctypes.c_void_p(offs.ctypes.data),
                                       ctypes.c_void_p(strides.ctypes.data), ctypes.c_long(nb))
     return total, offs, strides.reshape(nb, ndim)
+
+
+# ---- DPD ----------------------------------------------------------------------------------
+
+def orc_dpd_block(irrep, nirrep, lens, layout, irreps):
+    """(offset, lengths, strides) of one block from the C restatement."""
+    ndim = len(lens)
+    flat = (_sz * (ndim * nirrep))(*[x for row in lens for x in row])
+    irr = (ctypes.c_uint * ndim)(*irreps)
+    bl = (_sz * ndim)()
+    bs = (_sz * ndim)()
+    off = _sz()
+    rc = orc().orc_dpd_block(irrep, nirrep, ndim, flat, layout, irr, bl, bs, ctypes.byref(off))
+    if rc:
+        raise ValueError("oracle dpd_block failed: %d" % rc)
+    return off.value, list(bl), list(bs)
+
+
+def orc_dpd_size(irrep, nirrep, lens, layout):
+    ndim = len(lens)
+    flat = (_sz * (ndim * nirrep))(*[x for row in lens for x in row])
+    f = orc().orc_dpd_size
+    f.restype = _sz
+    return f(irrep, nirrep, ndim, flat, layout)
+
+
+def ref_dpd_mult(nirrep, alpha, irrep_A, lens_A, A, idx_A, irrep_B, lens_B, B, idx_B,
+                 beta, irrep_C, lens_C, C, idx_C):
+    """The reference's own C++ DPD contraction (tblis::mult over
+    dpd_varray_view, default layout) on flat numpy storage; C updated in place."""
+    def flat(lens):
+        return (_sz * (len(lens) * nirrep))(*[x for row in lens for x in row])
+    rc = shim().refshim_dpd_mult(
+        nirrep, ctypes.c_double(alpha), irrep_A, len(lens_A), flat(lens_A), ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+        irrep_B, len(lens_B), flat(lens_B), ctypes.c_void_p(B.ctypes.data), _lab(idx_B),
+        ctypes.c_double(beta), irrep_C, len(lens_C), flat(lens_C), ctypes.c_void_p(C.ctypes.data), _lab(idx_C))
+    if rc:
+        raise ValueError("reference dpd mult failed")

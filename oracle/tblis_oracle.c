@@ -713,3 +713,139 @@ int orc_tensor_shift_d(double shift, double alpha, unsigned ndim, const orc_len*
     while (it3_next(&it)) A[it.off[0]] = shift + alpha*A[it.off[0]];
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* DPD layout (src/external/marray/include/dpd_marray_base.hpp:34-228)       */
+/* ------------------------------------------------------------------------- */
+
+#define ORC_DPD_MAXN (2*ORC_MAX_DIM)
+
+typedef struct orc_dpd
+{
+    unsigned ndim, nirrep, irrep;
+    orc_len len[ORC_MAX_DIM][8];
+    orc_len size[ORC_DPD_MAXN][8];
+    unsigned leaf[ORC_MAX_DIM], parent[ORC_DPD_MAXN], perm[ORC_MAX_DIM];
+} orc_dpd;
+
+/* default_depth, :34-67 */
+static void dpd_depth(int layout, unsigned ndim, unsigned* depth)
+{
+    if (layout == 0 || layout == 1)
+    {
+        unsigned dl = 31 - __builtin_clz(ndim);
+        unsigned du = dl + ((ndim & (ndim - 1)) ? 1 : 0);
+        unsigned o = ndim - (1u << dl), k = 2*((o + 1)/2), l = 2*(o/2), h = (ndim + 1)/2;
+        for (unsigned i = 0; i < ndim; i++)
+            depth[i] = i < k ? du : i < h ? dl : i < h + l ? du : dl;
+    }
+    else if (layout == 4 || layout == 5)
+    {
+        depth[0] = ndim - 1;
+        for (unsigned i = 1; i < ndim; i++) depth[i] = ndim - i;
+    }
+    else
+    {
+        for (unsigned i = 0; i + 1 < ndim; i++) depth[i] = i + 1;
+        depth[ndim - 1] = ndim - 1;
+    }
+}
+
+/* set_tree :69-119 and set_size :121-169 */
+static int dpd_init(orc_dpd* t, unsigned irrep, unsigned nirrep, unsigned ndim, const orc_len* lens, int layout)
+{
+    if (ndim == 0 || ndim > ORC_MAX_DIM || nirrep > 8) return -1;
+    memset(t, 0, sizeof(*t));
+    t->ndim = ndim; t->nirrep = nirrep; t->irrep = irrep;
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++) t->len[i][j] = lens[i*nirrep + j];
+
+    unsigned depth[ORC_MAX_DIM], node[ORC_MAX_DIM];
+    long leaf_idx[ORC_MAX_DIM];
+    unsigned n = ndim;
+    dpd_depth(layout, ndim, depth);
+    for (unsigned i = 0; i < ndim; i++) leaf_idx[i] = i;
+    unsigned pos = 0;
+    for (unsigned d = ndim; d-- > 0;)
+    {
+        for (unsigned i = 0; i < n; i++)
+        {
+            if (depth[i] == d + 1)
+            {
+                if (i + 1 >= n || depth[i + 1] != d + 1) return -2;
+                t->parent[node[i]] = t->parent[node[i + 1]] = pos;
+                for (unsigned j = i + 1; j + 1 < n; j++)
+                {
+                    depth[j] = depth[j + 1]; node[j] = node[j + 1]; leaf_idx[j] = leaf_idx[j + 1];
+                }
+                n--;
+                depth[i]--;
+                node[i] = pos++;
+                leaf_idx[i] = -1;
+            }
+            else if (depth[i] == d)
+            {
+                node[i] = pos++;
+                if (leaf_idx[i] != -1) t->leaf[leaf_idx[i]] = node[i];
+            }
+        }
+    }
+    if (pos != 2*ndim - 1) return -3;
+
+    int colmajor = layout == 0 || layout == 2 || layout == 4;
+    for (unsigned i = 0; i < ndim; i++)
+    {
+        unsigned target = colmajor ? t->leaf[i] : t->leaf[ndim - 1 - i];
+        for (unsigned j = 0; j < nirrep; j++) t->size[target][j] = t->len[i][j];
+        t->perm[i] = colmajor ? i : ndim - 1 - i;
+    }
+    for (unsigned i = 0; i + 1 < ndim; i++)
+    {
+        unsigned next = t->parent[2*i];
+        for (unsigned a = 0; a < nirrep; a++)
+        {
+            orc_len s = 0;
+            for (unsigned b = 0; b < nirrep; b++) s += t->size[2*i][a ^ b]*t->size[2*i + 1][b];
+            t->size[next][a] = s;
+        }
+    }
+    return 0;
+}
+
+/* get_block :171-228 (unsliced tensor: off = 0, leap = 1) */
+int orc_dpd_block(unsigned irrep, unsigned nirrep, unsigned ndim, const orc_len* lens, int layout,
+                  const unsigned* irreps, orc_len* blen, orc_stride* bstride, orc_stride* offset)
+{
+    orc_dpd t;
+    int rc = dpd_init(&t, irrep, nirrep, ndim, lens, layout);
+    if (rc) return rc;
+    unsigned dirrep[ORC_DPD_MAXN] = {0};
+    orc_stride dstride[ORC_DPD_MAXN] = {0};
+    dstride[2*ndim - 2] = 1;
+    for (unsigned i = 0; i < ndim; i++) dirrep[t.leaf[t.perm[i]]] = irreps[i];
+    for (unsigned i = 0; i + 1 < ndim; i++) dirrep[t.parent[2*i]] = dirrep[2*i] ^ dirrep[2*i + 1];
+    orc_stride off = 0;
+    for (unsigned i = ndim - 1; i-- > 0;)
+    {
+        unsigned irr = dirrep[t.parent[2*i]];
+        dstride[2*i] = dstride[t.parent[2*i]];
+        dstride[2*i + 1] = dstride[2*i]*t.size[2*i][dirrep[2*i]];
+        orc_stride o = 0;
+        for (unsigned a = 0; a < dirrep[2*i + 1]; a++) o += t.size[2*i][a ^ irr]*t.size[2*i + 1][a];
+        off += o*dstride[2*i];
+    }
+    for (unsigned i = 0; i < ndim; i++)
+    {
+        bstride[i] = dstride[t.leaf[t.perm[i]]];
+        blen[i] = t.len[i][irreps[i]];
+    }
+    *offset = off;
+    return 0;
+}
+
+orc_len orc_dpd_size(unsigned irrep, unsigned nirrep, unsigned ndim, const orc_len* lens, int layout)
+{
+    orc_dpd t;
+    if (dpd_init(&t, irrep, nirrep, ndim, lens, layout)) return -1;
+    return t.size[2*ndim - 2][irrep];
+}

@@ -116,6 +116,13 @@ int orc_tensor_set_d(double alpha, unsigned ndim, const orc_len* len, const orc_
 int orc_tensor_shift_d(double shift, double alpha, unsigned ndim, const orc_len* len,
                        const orc_stride* stride, double* A);
 
+/* src/external/marray/include/dpd_marray_base.hpp:34-228: offset, lengths
+ * and strides of one block of a dense-stored DPD tensor (layout: MArray
+ * dpd_layout type 0..5), and the total number of stored elements. */
+int orc_dpd_block(unsigned irrep, unsigned nirrep, unsigned ndim, const orc_len* lens, int layout,
+                  const unsigned* irreps, orc_len* blen, orc_stride* bstride, orc_stride* offset);
+orc_len orc_dpd_size(unsigned irrep, unsigned nirrep, unsigned ndim, const orc_len* lens, int layout);
+
 #ifdef __cplusplus
 }
 #endif

@@ -260,3 +260,105 @@ def set_stream(stream_handle):
 def synchronize():
     lib.tblis_b200_synchronize()
     _check()
+
+
+# ---- DPD tensors and batches ---------------------------------------------------------------
+
+class tblis_b200_dpd_tensor(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("conj", ctypes.c_int), ("scalar", tblis_scalar),
+                ("data", ctypes.c_void_p), ("ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint),
+                ("irrep", ctypes.c_uint), ("len", ctypes.POINTER(ctypes.c_ssize_t)), ("layout", ctypes.c_int)]
+
+
+lib.tblis_b200_dpd_mult.argtypes = [_P(tblis_b200_dpd_tensor), ctypes.c_char_p, _P(tblis_b200_dpd_tensor),
+                                    ctypes.c_char_p, _P(tblis_b200_dpd_tensor), ctypes.c_char_p,
+                                    _P(tblis_b200_report)]
+lib.tblis_b200_dpd_mult.restype = ctypes.c_int
+lib.tblis_b200_dpd_block.argtypes = [_P(tblis_b200_dpd_tensor), _P(ctypes.c_uint), _P(ctypes.c_ssize_t),
+                                     _P(ctypes.c_ssize_t), _P(ctypes.c_ssize_t)]
+lib.tblis_b200_dpd_block.restype = ctypes.c_int
+lib.tblis_b200_dpd_size.argtypes = [_P(tblis_b200_dpd_tensor)]
+lib.tblis_b200_dpd_size.restype = ctypes.c_ssize_t
+lib.tblis_b200_tensor_mult_batch.restype = ctypes.c_int
+
+
+class DpdTensor:
+    """A DPD tensor (MArray dpd_varray layout) over a flat torch/numpy buffer.
+
+    lens: [ndim][nirrep] lengths per irrep; irrep: the tensor's irrep;
+    layout: MArray dpd_layout type (default 5 = PREFIX_ROW_MAJOR)."""
+
+    def __init__(self, irrep, nirrep, lens, data=None, layout=5):
+        self.irrep, self.nirrep, self.layout = int(irrep), int(nirrep), int(layout)
+        self.lens = [list(map(int, r)) for r in lens]
+        self.data = data
+        self._len = (ctypes.c_ssize_t * (len(self.lens) * self.nirrep))(*[x for r in self.lens for x in r])
+
+    def struct(self, scalar=1.0):
+        t = tblis_b200_dpd_tensor()
+        t.type = TYPE_DOUBLE
+        t.conj = 0
+        t.scalar.type = TYPE_DOUBLE
+        t.scalar.data[0] = float(scalar)
+        if self.data is None:
+            t.data = None
+        elif hasattr(self.data, "data_ptr"):
+            t.data = self.data.data_ptr()
+        else:
+            t.data = self.data.ctypes.data
+        t.ndim = len(self.lens)
+        t.nirrep = self.nirrep
+        t.irrep = self.irrep
+        t.len = ctypes.cast(self._len, _P(ctypes.c_ssize_t))
+        t.layout = self.layout
+        return t
+
+    def size(self):
+        t = self.struct()
+        n = lib.tblis_b200_dpd_size(ctypes.byref(t))
+        _check()
+        return n
+
+    def block(self, irreps):
+        """(offset, lengths, strides) of one block, as dpd_varray_view(irreps)."""
+        t = self.struct()
+        n = len(self.lens)
+        irr = (ctypes.c_uint * n)(*irreps)
+        L = (ctypes.c_ssize_t * n)()
+        S = (ctypes.c_ssize_t * n)()
+        off = ctypes.c_ssize_t()
+        lib.tblis_b200_dpd_block(ctypes.byref(t), irr, L, S, ctypes.byref(off))
+        _check()
+        return off.value, list(L), list(S)
+
+
+def dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
+    """C = alpha*A*B + beta*C over DPD tensors (src/iface/3t/mult.h:59-72)."""
+    a, b, c = A.struct(alpha), B.struct(), C.struct(beta)
+    r = tblis_b200_report()
+    lib.tblis_b200_dpd_mult(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B), ctypes.byref(c),
+                            _labels(idx_C), ctypes.byref(r))
+    _check()
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
+def mult_batch(items):
+    """items: list of (alpha, A, idx_A, B, idx_B, beta, C, idx_C) with device
+    tensors; all run in one grouped launch."""
+    n = len(items)
+    views = []
+    TA = (tblis_tensor * n)()
+    TB = (tblis_tensor * n)()
+    TC = (tblis_tensor * n)()
+    IA = (ctypes.c_char_p * n)()
+    IB = (ctypes.c_char_p * n)()
+    IC = (ctypes.c_char_p * n)()
+    for i, (alpha, A, ia, B, ib, beta, C, ic) in enumerate(items):
+        va, vb, vc = _View(A, alpha), _View(B), _View(C, beta)
+        views.append((va, vb, vc))
+        TA[i], TB[i], TC[i] = va.t, vb.t, vc.t
+        IA[i], IB[i], IC[i] = _labels(ia), _labels(ib), _labels(ic)
+    r = tblis_b200_report()
+    lib.tblis_b200_tensor_mult_batch(n, TA, IA, TB, IB, TC, IC, ctypes.byref(r))
+    _check()
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}

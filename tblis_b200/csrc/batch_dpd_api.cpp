@@ -1,0 +1,260 @@
+// batch_dpd_api.cpp -- C ABI of the DPD contraction, the DPD block layout
+// query and batched dense contractions (one grouped launch for many small
+// contractions of mixed shapes).
+#include "common.hpp"
+#include "dpd.hpp"
+#include "grouped.hpp"
+#include "level1.hpp"
+#include "mult.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace tb
+{
+
+namespace
+{
+
+void to_layout(const tblis_b200_dpd_tensor* t, DpdLayout& lay)
+{
+    TB_CHECK(t, TB_ERR_ARG, "null DPD tensor");
+    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "DPD: only double is supported");
+    TB_CHECK(t->len, TB_ERR_ARG, "DPD: null lengths");
+    std::vector<i64> lens(t->len, t->len + (size_t)t->ndim*t->nirrep);
+    lay.init(t->irrep, t->nirrep, t->ndim, lens.data(), t->layout < 0 ? 5 : t->layout);
+}
+
+// device view of a DPD tensor's storage (staged when it lives on the host)
+struct DpdStage
+{
+    dbuf buf;
+    double* host = nullptr;
+    double* dev = nullptr;
+    i64 n = 0;
+    void init(void* data, i64 total, bool copy_in, cudaStream_t st)
+    {
+        n = total;
+        if (!data || total == 0) { dev = static_cast<double*>(data); return; }
+        if (pointer_kind(data) == MEM_DEVICE) { dev = static_cast<double*>(data); return; }
+        host = static_cast<double*>(data);
+        buf = dbuf((size_t)total*sizeof(double), st);
+        dev = buf.as<double>();
+        if (copy_in) TB_CUDA(cudaMemcpyAsync(dev, host, (size_t)total*sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    void out(cudaStream_t st)
+    {
+        if (host) TB_CUDA(cudaMemcpyAsync(host, dev, (size_t)n*sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+};
+
+void run_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                  const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                  tblis_b200_dpd_tensor* C, const label_type* idx_C, tblis_b200_report* report)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    const int k0 = (int)g_kernel_count.load();
+    DpdTensor a, b, c;
+    to_layout(A, a.lay);
+    to_layout(B, b.lay);
+    to_layout(C, c.lay);
+    const double alpha = A->scalar.data.d*B->scalar.data.d, beta = C->scalar.data.d;
+    DpdStage sa, sb, sc;
+    sa.init(A->data, a.lay.total(), true, st);
+    sb.init(B->data, b.lay.total(), true, st);
+    sc.init(C->data, c.lay.total(), beta != 0.0, st);
+    a.data = sa.dev; b.data = sb.dev; c.data = sc.dev;
+    DpdMultReport r;
+    dpd_mult(a, idx_A, b, idx_B, c, idx_C, alpha, beta, st, &r);
+    sc.out(st);
+    if (sa.host || sb.host || sc.host) TB_CUDA(cudaStreamSynchronize(st));
+    C->scalar.data.d = 1.0;
+    C->scalar.type = TYPE_DOUBLE;
+    C->conj = 0;
+    if (report)
+    {
+        memset(report, 0, sizeof(*report));
+        report->method = 1;
+        report->flops = r.flops;
+        report->m = r.groups;            // number of irrep GEMMs in the grouped launch
+        report->n = r.variant;           // tile configuration the autotuner picked
+        report->kernels = (int)(g_kernel_count.load() - k0);
+    }
+}
+
+void run_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
+               const tblis_tensor* B, const label_type* const* idx_B,
+               tblis_tensor* C, const label_type* const* idx_C, tblis_b200_report* report)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    const int k0 = (int)g_kernel_count.load();
+    TB_CHECK(count >= 0, TB_ERR_ARG, "batch: negative count");
+    std::vector<const double*> ptrs(3*(size_t)count);
+    std::vector<double> alphas(count), betas(count);
+    std::string key;
+    std::vector<GemmView> views(count);
+    std::vector<char> trivial(count, 0);
+    for (int i = 0; i < count; i++)
+    {
+        TB_CHECK(A[i].type == TYPE_DOUBLE && B[i].type == TYPE_DOUBLE && C[i].type == TYPE_DOUBLE, TB_ERR_TYPE,
+                 "batch: only double tensors");
+        for (const tblis_tensor* t : {&A[i], &B[i], (const tblis_tensor*)&C[i]})
+        {
+            i64 lo, hi;
+            tensor_extent(t->ndim, t->len, t->stride, lo, hi);
+            TB_CHECK(hi < lo || !t->data || pointer_kind(t->data) == MEM_DEVICE, TB_ERR_ARG,
+                     "batch: tensors must be in device memory");
+        }
+        views[i] = gemm_view(mult_groups(&A[i], idx_A[i], &B[i], idx_B[i], &C[i], idx_C[i]));
+        ptrs[3*i] = static_cast<const double*>(A[i].data);
+        ptrs[3*i + 1] = static_cast<const double*>(B[i].data);
+        ptrs[3*i + 2] = static_cast<const double*>(C[i].data);
+        alphas[i] = A[i].scalar.data.d*B[i].scalar.data.d;
+        betas[i] = C[i].scalar.data.d;
+        const GemmView& v = views[i];
+        trivial[i] = alphas[i] == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
+        // the plan depends on shapes and strides only
+        for (const ivec* p : {&v.lenM, &v.lenN, &v.lenK, &v.lenL, &v.aM, &v.cM, &v.aK, &v.bK, &v.bN, &v.cN,
+                              &v.aL, &v.bL, &v.cL})
+        {
+            key.append(reinterpret_cast<const char*>(p->data()), p->size()*sizeof(i64));
+            key.push_back('|');
+        }
+        key.push_back(trivial[i] ? 't' : 'n');
+        key.push_back(v.pack_m_3d ? '1' : '0');
+        key.push_back(v.pack_n_3d ? '1' : '0');
+        key.push_back(v.pack_k_3d ? '1' : '0');
+        key.push_back(';');
+    }
+
+    // trivial members: alpha == 0 or empty contracted extent -> set/scale C
+    for (int i = 0; i < count; i++)
+    {
+        const GemmView& v = views[i];
+        if (!trivial[i] || v.m*v.n*v.l == 0 || betas[i] == 1.0) continue;
+        Strided s;
+        ivec len, str;
+        for (size_t j = 0; j < v.lenM.size(); j++) { len.push_back(v.lenM[j]); str.push_back(v.cM[j]); }
+        for (size_t j = 0; j < v.lenN.size(); j++) { len.push_back(v.lenN[j]); str.push_back(v.cN[j]); }
+        for (size_t j = 0; j < v.lenL.size(); j++) { len.push_back(v.lenL[j]); str.push_back(v.cL[j]); }
+        TB_CHECK(len.size() <= (size_t)L1_MAX_DIM, TB_ERR_SIZE, "too many dimensions");
+        s.ndim = (int)len.size();
+        for (size_t j = 0; j < len.size(); j++) { s.len[j] = len[j]; s.stride[j] = str[j]; }
+        if (betas[i] == 0.0) l1_set<double>(static_cast<double*>(C[i].data), s, 0.0, st);
+        else l1_scale<double>(static_cast<double*>(C[i].data), s, betas[i], st);
+    }
+
+    auto plan = grouped_plan_cache().find(key);
+    if (!plan)
+    {
+        auto p = std::make_shared<GroupedPlan>();
+        double flops = 0;
+        for (int i = 0; i < count; i++)
+        {
+            if (trivial[i]) continue;
+            const GemmView& v = views[i];
+            GroupTables base;
+            base.M = v.m; base.N = v.n; base.K = v.k;
+            base.a_m.resize(v.m); base.c_m.resize(v.m); base.a_k.resize(v.k); base.b_k.resize(v.k);
+            base.b_n.resize(v.n); base.c_n.resize(v.n);
+            std::vector<i64> bs(std::max({v.m, v.n, v.k, v.l}));
+            fill_block_scatter(v.lenM, v.aM, 1, 0, v.m, base.a_m.data(), bs.data(), v.pack_m_3d);
+            fill_block_scatter(v.lenM, v.cM, 1, 0, v.m, base.c_m.data(), bs.data(), v.pack_m_3d);
+            fill_block_scatter(v.lenN, v.bN, 1, 0, v.n, base.b_n.data(), bs.data(), v.pack_n_3d);
+            fill_block_scatter(v.lenN, v.cN, 1, 0, v.n, base.c_n.data(), bs.data(), v.pack_n_3d);
+            fill_block_scatter(v.lenK, v.aK, 1, 0, v.k, base.a_k.data(), bs.data(), v.pack_k_3d);
+            fill_block_scatter(v.lenK, v.bK, 1, 0, v.k, base.b_k.data(), bs.data(), v.pack_k_3d);
+            base.amode = v.amode; base.bmode = v.bmode;
+            base.a_slot = 3*i; base.b_slot = 3*i + 1; base.c_slot = 3*i + 2;
+            base.sidx = i;
+            std::vector<i64> al(v.l), bl(v.l), cl(v.l);
+            fill_block_scatter(v.lenL, v.aL, 1, 0, v.l, al.data(), bs.data(), false);
+            fill_block_scatter(v.lenL, v.bL, 1, 0, v.l, bl.data(), bs.data(), false);
+            fill_block_scatter(v.lenL, v.cL, 1, 0, v.l, cl.data(), bs.data(), false);
+            for (i64 l = 0; l < v.l; l++)
+            {
+                GroupTables g = base;
+                g.a_off = al[l]; g.b_off = bl[l]; g.c_off = cl[l];
+                p->groups.push_back(std::move(g));
+            }
+            flops += 2.0*v.m*v.n*v.k*v.l;
+        }
+        p->flops = flops;
+        p->nslots = 3*count;
+        p->finalize(st);
+        plan = grouped_plan_cache().insert(key, p);
+    }
+    grouped_run(*plan, ptrs.data(), alphas.data(), betas.data(), st);
+    for (int i = 0; i < count; i++)
+    {
+        C[i].scalar.data.d = 1.0;
+        C[i].scalar.type = TYPE_DOUBLE;
+        C[i].conj = 0;
+    }
+    if (report)
+    {
+        memset(report, 0, sizeof(*report));
+        report->method = 1;
+        report->flops = plan->flops;
+        report->m = (int64_t)plan->groups.size();
+        report->n = plan->variant;
+        report->kernels = (int)(g_kernel_count.load() - k0);
+    }
+}
+
+} // namespace
+
+} // namespace tb
+
+using namespace tb;
+
+extern "C" {
+
+int tblis_b200_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                        const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                              tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                        tblis_b200_report* report)
+{
+    return guarded([&] { run_dpd_mult(A, idx_A, B, idx_B, C, idx_C, report); });
+}
+
+int tblis_b200_dpd_block(const tblis_b200_dpd_tensor* A, const unsigned* irreps, len_type* len,
+                         stride_type* stride, stride_type* offset)
+{
+    return guarded([&]
+    {
+        DpdLayout lay;
+        to_layout(A, lay);
+        std::vector<i64> l(lay.ndim), s(lay.ndim);
+        i64 off;
+        unsigned x = 0;
+        for (unsigned i = 0; i < lay.ndim; i++)
+        {
+            TB_CHECK(irreps[i] < lay.nirrep, TB_ERR_ARG, "DPD: irrep out of range");
+            x ^= irreps[i];
+        }
+        TB_CHECK(x == lay.irrep, TB_ERR_ARG, "DPD: block not allowed by symmetry");
+        lay.block(irreps, l.data(), s.data(), off);
+        for (unsigned i = 0; i < lay.ndim; i++) { len[i] = l[i]; stride[i] = s[i]; }
+        *offset = off;
+    });
+}
+
+len_type tblis_b200_dpd_size(const tblis_b200_dpd_tensor* A)
+{
+    len_type n = -1;
+    guarded([&] { DpdLayout lay; to_layout(A, lay); n = lay.total(); });
+    return n;
+}
+
+int tblis_b200_tensor_mult_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
+                                 const tblis_tensor* B, const label_type* const* idx_B,
+                                       tblis_tensor* C, const label_type* const* idx_C,
+                                 tblis_b200_report* report)
+{
+    return guarded([&] { run_batch(count, A, idx_A, B, idx_B, C, idx_C, report); });
+}
+
+} // extern "C"

@@ -1,0 +1,440 @@
+// dpd.cpp -- DPD tensors: MArray's block layout and the block-sparse
+// contraction on the GPU.
+//
+// Layout: restates the binary layout tree of MArray's dpd_varray
+// (src/external/marray/include/dpd_marray_base.hpp:34-228: default_depth,
+// set_tree, set_size, get_block) so block offsets and strides are bit-exact.
+//
+// Contraction: as in src/internal/3t/dpd/mult.cxx:223-356, one GEMM per irrep
+// h of the contracted index group: rows are all AC irrep combinations with
+// XOR = irrep(A)^h, columns all BC combinations with XOR = irrep(B)^h, k all
+// AB combinations with XOR = h, each combination contributing its dense block
+// extent. For the layout trees MArray builds, the offset of element (row, k) of
+// such a "patch matrix" is row_part + k_part (checked for every block pair);
+// the patches then become ordinary GEMM views with scatter vectors, and all of
+// them run in ONE persistent grouped launch of the FP64 DMMA kernel. The tile
+// shape of that launch is chosen by a small autotuner keyed on the histogram of
+// group sizes, and the launch (descriptor upload + kernel) is captured once in
+// a CUDA graph and replayed.
+#include "dpd.hpp"
+#include "gemm_f64.hpp"
+#include "level1.hpp"
+#include "grouped.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+namespace tb
+{
+
+std::vector<unsigned> dpd_default_depth(int layout, unsigned ndim)
+{
+    std::vector<unsigned> depth(ndim);
+    if (layout == 0 || layout == 1)            // BALANCED_{COLUMN,ROW}_MAJOR
+    {
+        unsigned dl = sizeof(unsigned)*8 - __builtin_clz(ndim) - 1;
+        unsigned du = dl + ((ndim & (ndim - 1)) ? 1 : 0);
+        unsigned o = ndim - (1u << dl);
+        unsigned k = 2*((o + 1)/2);
+        unsigned l = 2*(o/2);
+        unsigned h = (ndim + 1)/2;
+        for (unsigned i = 0; i < k; i++) depth[i] = du;
+        for (unsigned i = k; i < h; i++) depth[i] = dl;
+        for (unsigned i = h; i < h + l; i++) depth[i] = du;
+        for (unsigned i = h + l; i < ndim; i++) depth[i] = dl;
+    }
+    else if (layout == 4 || layout == 5)       // PREFIX_{COLUMN,ROW}_MAJOR
+    {
+        depth[0] = ndim - 1;
+        for (unsigned i = 1; i < ndim; i++) depth[i] = ndim - i;
+    }
+    else                                       // BLOCKED_{COLUMN,ROW}_MAJOR
+    {
+        for (unsigned i = 0; i + 1 < ndim; i++) depth[i] = i + 1;
+        depth[ndim - 1] = ndim - 1;
+    }
+    return depth;
+}
+
+void DpdLayout::init(unsigned irrep_, unsigned nirrep_, unsigned ndim_, const i64* lens, int layout_)
+{
+    TB_CHECK(nirrep_ == 1 || nirrep_ == 2 || nirrep_ == 4 || nirrep_ == 8, TB_ERR_ARG,
+             "DPD: nirrep must be 1, 2, 4 or 8");
+    TB_CHECK(ndim_ > 0 && ndim_ <= 16, TB_ERR_ARG, "DPD: 1..16 dimensions");
+    TB_CHECK(layout_ >= 0 && layout_ <= 5, TB_ERR_ARG, "DPD: unknown layout");
+    TB_CHECK(irrep_ < nirrep_, TB_ERR_ARG, "DPD: irrep out of range");
+    ndim = ndim_; nirrep = nirrep_; irrep = irrep_; layout = layout_;
+    len.assign(ndim, std::vector<i64>(nirrep));
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++)
+        {
+            len[i][j] = lens[i*nirrep + j];
+            TB_CHECK(len[i][j] >= 0, TB_ERR_ARG, "DPD: negative length");
+        }
+
+    // set_tree (dpd_marray_base.hpp:69-119)
+    leaf.assign(ndim, 0);
+    parent.assign(2*ndim - 1, 0);
+    std::vector<unsigned> depth = dpd_default_depth(layout, ndim);
+    std::vector<unsigned> node(ndim);
+    std::vector<long> leaf_idx(ndim);
+    for (unsigned i = 0; i < ndim; i++) leaf_idx[i] = i;
+    unsigned pos = 0;
+    for (unsigned d = ndim; d-- > 0;)
+    {
+        for (unsigned i = 0; i < depth.size(); i++)
+        {
+            if (depth[i] == d + 1)
+            {
+                TB_CHECK(i + 1 < depth.size() && depth[i + 1] == d + 1, TB_ERR_ARG, "DPD: bad layout tree");
+                parent[node[i]] = parent[node[i + 1]] = pos;
+                depth.erase(depth.begin() + i + 1);
+                depth[i]--;
+                node.erase(node.begin() + i + 1);
+                node[i] = pos++;
+                leaf_idx.erase(leaf_idx.begin() + i + 1);
+                leaf_idx[i] = -1;
+            }
+            else if (depth[i] == d)
+            {
+                node[i] = pos++;
+                if (leaf_idx[i] != -1) leaf[leaf_idx[i]] = node[i];
+            }
+        }
+    }
+    TB_CHECK(pos == 2*ndim - 1, TB_ERR_ARG, "DPD: bad layout tree");
+
+    // set_size (dpd_marray_base.hpp:121-169)
+    size.assign(2*ndim - 1, std::vector<i64>(nirrep, 0));
+    perm.assign(ndim, 0);
+    const bool column_major = layout == 0 || layout == 2 || layout == 4;
+    for (unsigned i = 0; i < ndim; i++)
+    {
+        if (column_major)
+        {
+            size[leaf[i]] = len[i];
+            perm[i] = i;
+        }
+        else
+        {
+            size[leaf[ndim - 1 - i]] = len[i];
+            perm[i] = ndim - 1 - i;
+        }
+    }
+    for (unsigned i = 0; i + 1 < ndim; i++)
+    {
+        unsigned next = parent[2*i];
+        for (unsigned irr1 = 0; irr1 < nirrep; irr1++)
+        {
+            size[next][irr1] = 0;
+            for (unsigned irr2 = 0; irr2 < nirrep; irr2++)
+                size[next][irr1] += size[2*i][irr1 ^ irr2]*size[2*i + 1][irr2];
+        }
+    }
+}
+
+// get_block (dpd_marray_base.hpp:171-228) for a full (unsliced) tensor
+void DpdLayout::block(const unsigned* irreps, i64* blen, i64* bstride, i64& offset) const
+{
+    std::vector<unsigned> dirrep(2*ndim - 1, 0);
+    std::vector<i64> dstride(2*ndim - 1, 0);
+    dstride[2*ndim - 2] = 1;
+    // stored lengths are reversed for row-major layouts; perm maps them back
+    for (unsigned i = 0; i < ndim; i++) dirrep[leaf[perm[i]]] = irreps[i];
+    for (unsigned i = 0; i + 1 < ndim; i++) dirrep[parent[2*i]] = dirrep[2*i] ^ dirrep[2*i + 1];
+    offset = 0;
+    for (unsigned i = ndim - 1; i-- > 0;)
+    {
+        const unsigned irr = dirrep[parent[2*i]];
+        dstride[2*i] = dstride[parent[2*i]];
+        dstride[2*i + 1] = dstride[2*i]*size[2*i][dirrep[2*i]];
+        i64 off = 0;
+        for (unsigned irr1 = 0; irr1 < dirrep[2*i + 1]; irr1++)
+            off += size[2*i][irr1 ^ irr]*size[2*i + 1][irr1];
+        offset += off*dstride[2*i];
+    }
+    for (unsigned i = 0; i < ndim; i++)
+    {
+        bstride[i] = dstride[leaf[perm[i]]];
+        blen[i] = len[i][irreps[i]];
+    }
+}
+
+namespace
+{
+
+// irrep combinations of n labels with XOR == target, in the order of
+// src/internal/1t/dpd/util.hpp:14-68 (irrep_iterator: the last n-1 labels run
+// as an odometer with the second label fastest, the first label closes the XOR)
+std::vector<std::vector<unsigned>> combos(unsigned n, unsigned target, unsigned nirrep)
+{
+    std::vector<std::vector<unsigned>> out;
+    if (n == 0)
+    {
+        if (target == 0) out.push_back({});
+        return out;
+    }
+    std::vector<unsigned> pos(n - 1, 0);
+    while (true)
+    {
+        std::vector<unsigned> c(n);
+        unsigned x = target;
+        for (unsigned i = 1; i < n; i++) { c[i] = pos[i - 1]; x ^= pos[i - 1]; }
+        c[0] = x;
+        out.push_back(c);
+        unsigned d = 0;
+        while (d < n - 1 && ++pos[d] == nirrep) { pos[d] = 0; d++; }
+        if (d == n - 1) break;
+    }
+    return out;
+}
+
+// One operand's patch matrix for a (row group, column group) pair: offset of
+// element (r, c) = row[r] + col[c]. Returns false when the layout does not
+// split that way (checked on every block pair).
+bool patch_view(const DpdLayout& X, const std::vector<unsigned>& rdims,
+                const std::vector<std::vector<unsigned>>& rcombos,
+                const std::vector<unsigned>& cdims, const std::vector<std::vector<unsigned>>& ccombos,
+                ivec& row, ivec& col)
+{
+    row.clear(); col.clear();
+    const unsigned nd = X.ndim;
+    std::vector<unsigned> irr(nd);
+    std::vector<i64> bl(nd), bs(nd);
+    auto blk = [&](const std::vector<unsigned>& rc, const std::vector<unsigned>& cc, i64& off)
+    {
+        for (size_t i = 0; i < rdims.size(); i++) irr[rdims[i]] = rc[i];
+        for (size_t i = 0; i < cdims.size(); i++) irr[cdims[i]] = cc[i];
+        X.block(irr.data(), bl.data(), bs.data(), off);
+    };
+    auto extent = [&](const std::vector<unsigned>& dims, const std::vector<unsigned>& c)
+    {
+        i64 e = 1;
+        for (size_t i = 0; i < dims.size(); i++) e *= X.len[dims[i]][c[i]];
+        return e;
+    };
+    // reference combinations: the first non-empty ones
+    size_t r0 = rcombos.size(), c0 = ccombos.size();
+    for (size_t i = 0; i < rcombos.size(); i++) if (extent(rdims, rcombos[i]) > 0) { r0 = i; break; }
+    for (size_t i = 0; i < ccombos.size(); i++) if (extent(cdims, ccombos[i]) > 0) { c0 = i; break; }
+    if (r0 == rcombos.size() || c0 == ccombos.size()) return true;   // empty patch
+
+    i64 base00;
+    blk(rcombos[r0], ccombos[c0], base00);
+    std::vector<i64> rstr0, cstr0;
+    // rows
+    for (size_t ri = 0; ri < rcombos.size(); ri++)
+    {
+        const i64 ext = extent(rdims, rcombos[ri]);
+        if (ext == 0) continue;
+        i64 baseR;
+        blk(rcombos[ri], ccombos[c0], baseR);
+        ivec lens, strs;
+        for (unsigned d : rdims) { lens.push_back(bl[d]); strs.push_back(bs[d]); }
+        const i64 shift = baseR - base00;
+        std::vector<i64> sc(ext), tmp(ext);
+        fill_block_scatter(lens, strs, 1, 0, ext, sc.data(), tmp.data(), false);
+        for (i64 v : sc) row.push_back(v + shift);
+        // every column combination must see the same row strides
+        for (size_t ci = 0; ci < ccombos.size(); ci++)
+        {
+            if (extent(cdims, ccombos[ci]) == 0) continue;
+            i64 b;
+            blk(rcombos[ri], ccombos[ci], b);
+            for (size_t i = 0; i < rdims.size(); i++) if (bs[rdims[i]] != strs[i]) return false;
+            i64 b0c, bR0;
+            blk(rcombos[r0], ccombos[ci], b0c);
+            blk(rcombos[ri], ccombos[c0], bR0);
+            if (b - bR0 - b0c + base00 != 0) return false;
+        }
+    }
+    // columns
+    for (size_t ci = 0; ci < ccombos.size(); ci++)
+    {
+        const i64 ext = extent(cdims, ccombos[ci]);
+        if (ext == 0) continue;
+        i64 baseC;
+        blk(rcombos[r0], ccombos[ci], baseC);
+        ivec lens, strs;
+        for (unsigned d : cdims) { lens.push_back(bl[d]); strs.push_back(bs[d]); }
+        for (size_t ri = 0; ri < rcombos.size(); ri++)
+        {
+            if (extent(rdims, rcombos[ri]) == 0) continue;
+            i64 b;
+            blk(rcombos[ri], ccombos[ci], b);
+            for (size_t i = 0; i < cdims.size(); i++) if (bs[cdims[i]] != strs[i]) return false;
+        }
+        std::vector<i64> sc(ext), tmp(ext);
+        fill_block_scatter(lens, strs, 1, 0, ext, sc.data(), tmp.data(), false);
+        for (i64 v : sc) col.push_back(v + baseC);
+    }
+    return true;
+}
+
+int gather_mode(const ivec& mvec, const ivec& kvec)
+{
+    auto lead = [](const ivec& v) { return v.size() > 1 ? std::llabs(v[1] - v[0]) : (i64)1 << 60; };
+    return lead(mvec) < lead(kvec) ? 0 : 1;
+}
+
+} // namespace
+
+// key of everything a DPD plan depends on except the data pointers
+static std::string dpd_key(const DpdTensor& A, const char* ia, const DpdTensor& B, const char* ib,
+                           const DpdTensor& C, const char* ic)
+{
+    std::string k;
+    for (const DpdTensor* t : {&A, &B, &C})
+    {
+        const DpdLayout& l = t->lay;
+        k += std::to_string(l.ndim) + "," + std::to_string(l.nirrep) + "," + std::to_string(l.irrep) + "," +
+             std::to_string(l.layout) + ":";
+        for (auto& r : l.len) for (i64 x : r) k += std::to_string(x) + ",";
+        k += "|";
+    }
+    k += std::string(ia) + "|" + ib + "|" + ic;
+    return k;
+}
+
+void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+              DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
+              DpdMultReport* rep)
+{
+    const unsigned nirrep = A.lay.nirrep;
+    TB_CHECK(B.lay.nirrep == nirrep && C.lay.nirrep == nirrep, TB_ERR_ARG, "DPD: nirrep differs");
+    const std::string iA(idx_A, A.lay.ndim), iB(idx_B, B.lay.ndim), iC(idx_C, C.lay.ndim);
+    for (const std::string* s : {&iA, &iB, &iC})
+        for (size_t i = 0; i < s->size(); i++)
+            for (size_t j = 0; j < i; j++)
+                TB_CHECK((*s)[i] != (*s)[j], TB_ERR_ARG, "DPD: repeated label in one tensor");
+
+    std::string ABC, AB, AC, BC;
+    for (char c : iA)
+    {
+        bool b = iB.find(c) != std::string::npos, cc = iC.find(c) != std::string::npos;
+        if (b && cc) ABC.push_back(c);
+        else if (b) AB.push_back(c);
+        else if (cc) AC.push_back(c);
+        else throw error(TB_ERR_ARG, "DPD: label appears only in A");
+    }
+    for (char c : iB)
+        if (iA.find(c) == std::string::npos)
+        {
+            if (iC.find(c) != std::string::npos) BC.push_back(c);
+            else throw error(TB_ERR_ARG, "DPD: label appears only in B");
+        }
+    for (char c : iC)
+        TB_CHECK(iA.find(c) != std::string::npos || iB.find(c) != std::string::npos, TB_ERR_ARG,
+                 "DPD: label appears only in C");
+    auto pos = [](const std::string& s, char c) { return (unsigned)s.find(c); };
+    auto same_len = [&](const DpdTensor& X, const std::string& ix, const DpdTensor& Y, const std::string& iy,
+                        const std::string& labs)
+    {
+        for (char c : labs)
+            TB_CHECK(X.lay.len[pos(ix, c)] == Y.lay.len[pos(iy, c)], TB_ERR_ARG, "DPD: per-irrep lengths differ");
+    };
+    same_len(A, iA, B, iB, AB); same_len(A, iA, C, iC, AC); same_len(B, iB, C, iC, BC);
+    same_len(A, iA, B, iB, ABC); same_len(A, iA, C, iC, ABC);
+
+    // src/iface/3t/mult.cxx:270: "A.irrep()^B.irrep() != C.irrep()" parses as
+    // A.irrep() ^ (B.irrep() != C.irrep()); kept as is
+    const unsigned irrA = A.lay.irrep, irrB = B.lay.irrep, irrC = C.lay.irrep;
+    const bool mismatch = (irrA ^ (unsigned)(irrB != irrC)) != 0;
+    const i64 ctotal = C.lay.total();
+    if (alpha == 0.0 || (ABC.empty() && mismatch))
+    {
+        Strided s; s.ndim = 1; s.len[0] = ctotal; s.stride[0] = 1;
+        if (ctotal > 0)
+        {
+            if (beta == 0.0) l1_set<double>(C.data, s, 0.0, st);
+            else if (beta != 1.0) l1_scale<double>(C.data, s, beta, st);
+        }
+        return;
+    }
+    TB_CHECK(ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
+
+    // label order inside each group: stride order of the dense-equivalent
+    // layout (src/internal/3t/dpd/mult.cxx:256-270), C then A (AC), C then B
+    // (BC), A then B (AB)
+    auto dense_stride = [](const DpdTensor& X, unsigned d)
+    {
+        // row-major layouts: last dimension fastest
+        const bool cm = X.lay.layout == 0 || X.lay.layout == 2 || X.lay.layout == 4;
+        i64 s = 1;
+        if (cm) { for (unsigned j = 0; j < d; j++) { i64 t = 0; for (i64 x : X.lay.len[j]) t += x; s *= t; } }
+        else { for (unsigned j = X.lay.ndim - 1; j > d; j--) { i64 t = 0; for (i64 x : X.lay.len[j]) t += x; s *= t; } }
+        return s;
+    };
+    auto order = [&](std::string labs, const DpdTensor& X, const std::string& ix, const DpdTensor& Y,
+                     const std::string& iy)
+    {
+        ivec sx, sy;
+        for (char c : labs) { sx.push_back(dense_stride(X, pos(ix, c))); sy.push_back(dense_stride(Y, pos(iy, c))); }
+        auto p = sort_by_stride({&sx, &sy});
+        std::string r;
+        for (unsigned i : p) r.push_back(labs[i]);
+        return r;
+    };
+    AC = order(AC, C, iC, A, iA);
+    BC = order(BC, C, iC, B, iB);
+    AB = order(AB, A, iA, B, iB);
+    auto dims = [&](const std::string& labs, const std::string& ix)
+    {
+        std::vector<unsigned> d;
+        for (char c : labs) d.push_back(pos(ix, c));
+        return d;
+    };
+
+    const std::string key = dpd_key(A, idx_A, B, idx_B, C, idx_C);
+    auto plan = grouped_plan_cache().find(key);
+    if (!plan)
+    {
+        auto p = std::make_shared<GroupedPlan>();
+        double flops = 0;
+        for (unsigned h = 0; h < nirrep; h++)
+        {
+            const unsigned irr_AC = irrA ^ h, irr_BC = irrB ^ h;
+            auto rc = combos((unsigned)AC.size(), irr_AC, nirrep);
+            auto cc = combos((unsigned)BC.size(), irr_BC, nirrep);
+            auto kc = combos((unsigned)AB.size(), h, nirrep);
+            GroupTables g;
+            bool ok = patch_view(A.lay, dims(AC, iA), rc, dims(AB, iA), kc, g.a_m, g.a_k) &&
+                      patch_view(B.lay, dims(AB, iB), kc, dims(BC, iB), cc, g.b_k, g.b_n) &&
+                      patch_view(C.lay, dims(AC, iC), rc, dims(BC, iC), cc, g.c_m, g.c_n);
+            TB_CHECK(ok, TB_ERR_ARG, "DPD: layout does not split into row and column parts");
+            const i64 M = (i64)g.c_m.size(), N = (i64)g.c_n.size(), K = (i64)g.a_k.size();
+            if (M == 0 || N == 0) continue;
+            if (K == 0)
+            {
+                // no contracted blocks for this irrep: C patch = beta*C patch
+                p->empty_patches.push_back({g.c_m, g.c_n});
+                continue;
+            }
+            g.M = M; g.N = N; g.K = K;
+            g.amode = gather_mode(g.a_m, g.a_k);
+            g.bmode = gather_mode(g.b_n, g.b_k);
+            g.a_slot = 0; g.b_slot = 1; g.c_slot = 2;
+            flops += 2.0*M*N*K;
+            p->groups.push_back(std::move(g));
+        }
+        p->flops = flops;
+        p->finalize(st);
+        plan = grouped_plan_cache().insert(key, p);
+    }
+
+    const double* ptrs[3] = {A.data, B.data, C.data};
+    // C patches without contracted blocks: beta scaling (rare; irreps with K_h == 0)
+    for (auto& ep : plan->empty_patches)
+        scale_patch(C.data, ep.first, ep.second, beta, st);
+    grouped_run(*plan, ptrs, &alpha, &beta, st);
+    if (rep)
+    {
+        rep->groups = (int)plan->groups.size();
+        rep->flops = plan->flops;
+        rep->variant = plan->variant;
+    }
+}
+
+} // namespace tb

@@ -91,9 +91,31 @@ __device__ __forceinline__ i64 koff(const i64* __restrict__ scat, const KInfo& k
     return ki.stride != 0 ? ki.first + (i64)kl*ki.stride : __ldg(scat + k0 + kl);
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, int MINB>
-__global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
-gemm_f64_kernel(const GemmF64Args p)
+// arguments of one output tile
+struct TileArgs
+{
+    const double* A;          // already offset to the batch entry
+    const double* B;
+    double* C;
+    const i64 *a_m, *a_k, *b_k, *b_n, *c_m, *c_n, *a_kbs, *b_kbs;
+    i64 M, N;
+    i64 m0, n0;
+    i64 k_begin, k_end;
+    double alpha, beta;
+    double* W;                // split-K partial tile output (dense, ld = N), or null
+};
+
+template <int BM, int BN>
+__host__ __device__ constexpr int tile_smem_doubles(int STAGES)
+{
+    // the larger of the two gather layouts, so runtime-mode kernels fit both
+    return STAGES*((BK*(BM + PAD) > BM*(BK + PAD) ? BK*(BM + PAD) : BM*(BK + PAD)) +
+                   (BK*(BN + PAD) > BN*(BK + PAD) ? BK*(BN + PAD) : BN*(BK + PAD)));
+}
+
+// one BM x BN output tile: gathered cp.async mainloop + DMMA + scatter epilogue
+template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE>
+__device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* sAm, i64* sBn, i64* sCm, i64* sCn)
 {
     constexpr int NT = (BM/WM)*(BN/WN)*32;
     constexpr int MS = WM/8, NS = WN/8;
@@ -101,34 +123,12 @@ gemm_f64_kernel(const GemmF64Args p)
     using TB = Tile<BN, BMODE>;
     constexpr int STAGE = TA::SIZE + TB::SIZE;
 
-    extern __shared__ __align__(16) double smem[];
-    i64* sAm = reinterpret_cast<i64*>(smem + STAGES*STAGE);
-    i64* sBn = sAm + BM;
-    i64* sCm = sBn + BN;
-    i64* sCn = sCm + BM;
-
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-
-    // rasterisation: groups of 8 m-tiles sweep the n-tiles together so
-    // concurrently running CTAs share A and B panels in L2
-    const i64 tiles_m = (p.M + BM - 1)/BM, tiles_n = (p.N + BN - 1)/BN;
-    const i64 tile = blockIdx.x;
-    const i64 group = 8;
-    const i64 gid = tile/(group*tiles_n);
-    const i64 first_m = gid*group;
-    const i64 gsize = min(group, tiles_m - first_m);
-    const i64 tm = first_m + (tile % (group*tiles_n)) % gsize;
-    const i64 tn = (tile % (group*tiles_n)) / gsize;
-    const i64 m0 = tm*BM, n0 = tn*BN;
-
-    const i64 l = blockIdx.y;
-    const int split = blockIdx.z;
-    const i64 k_begin = (i64)split*p.k_per_split;
-    const i64 k_end = min(p.K, k_begin + p.k_per_split);
-
-    const double* __restrict__ A = p.A + p.a_l[l];
-    const double* __restrict__ B = p.B + p.b_l[l];
+    const i64 m0 = p.m0, n0 = p.n0;
+    const i64 k_begin = p.k_begin, k_end = p.k_end;
+    const double* __restrict__ A = p.A;
+    const double* __restrict__ B = p.B;
 
     for (int i = tid; i < BM; i += NT)
     {
@@ -229,10 +229,9 @@ gemm_f64_kernel(const GemmF64Args p)
     }
     cp_async_wait<0>();
 
-    if (p.splits > 1)
+    if (p.W)
     {
-        // raw partial sums into the workspace, [split][l][m][n] dense
-        double* W = p.partial + ((i64)split*p.L + l)*p.M*p.N;
+        // raw partial sums, dense [m][n]
         #pragma unroll
         for (int i = 0; i < MS; i++)
         {
@@ -244,30 +243,121 @@ gemm_f64_kernel(const GemmF64Args p)
                 for (int h = 0; h < 2; h++)
                 {
                     const i64 n = n0 + wn0 + j*8 + fc*2 + h;
-                    if (n < p.N) W[m*p.N + n] = acc[i][j][h];
+                    if (n < p.N) p.W[m*p.N + n] = acc[i][j][h];
                 }
         }
-        return;
     }
-
-    double* C = p.C + p.c_l[l];
-    const double alpha = p.alpha, beta = p.beta;
-    #pragma unroll
-    for (int i = 0; i < MS; i++)
+    else
     {
-        const i64 rc = sCm[wm0 + i*8 + fr];
-        if (rc < 0) continue;
+        double* C = p.C;
+        const double alpha = p.alpha, beta = p.beta;
         #pragma unroll
-        for (int j = 0; j < NS; j++)
+        for (int i = 0; i < MS; i++)
+        {
+            const i64 rc = sCm[wm0 + i*8 + fr];
+            if (rc < 0) continue;
             #pragma unroll
-            for (int h = 0; h < 2; h++)
-            {
-                const i64 cc = sCn[wn0 + j*8 + fc*2 + h];
-                if (cc < 0) continue;
-                double* dst = C + rc + cc;
-                const double v = alpha*acc[i][j][h];
-                *dst = beta == 0.0 ? v : v + beta*(*dst);
-            }
+            for (int j = 0; j < NS; j++)
+                #pragma unroll
+                for (int h = 0; h < 2; h++)
+                {
+                    const i64 cc = sCn[wn0 + j*8 + fc*2 + h];
+                    if (cc < 0) continue;
+                    double* dst = C + rc + cc;
+                    const double v = alpha*acc[i][j][h];
+                    *dst = beta == 0.0 ? v : v + beta*(*dst);
+                }
+        }
+    }
+    // shared memory is reused by the next tile of a persistent CTA
+    __syncthreads();
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, int MINB>
+__global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
+gemm_f64_kernel(const GemmF64Args p)
+{
+    extern __shared__ __align__(16) double smem[];
+    constexpr int SD = Tile<BM, AMODE>::SIZE + Tile<BN, BMODE>::SIZE;
+    i64* sAm = reinterpret_cast<i64*>(smem + STAGES*SD);
+    i64* sBn = sAm + BM;
+    i64* sCm = sBn + BN;
+    i64* sCn = sCm + BM;
+
+    // rasterisation: groups of 8 m-tiles sweep the n-tiles together so
+    // concurrently running CTAs share A and B panels in L2
+    const i64 tiles_m = (p.M + BM - 1)/BM, tiles_n = (p.N + BN - 1)/BN;
+    const i64 tile = blockIdx.x;
+    const i64 group = 8;
+    const i64 gid = tile/(group*tiles_n);
+    const i64 first_m = gid*group;
+    const i64 gsize = min(group, tiles_m - first_m);
+    const i64 tm = first_m + (tile % (group*tiles_n)) % gsize;
+    const i64 tn = (tile % (group*tiles_n)) / gsize;
+
+    const i64 l = blockIdx.y;
+    const int split = blockIdx.z;
+    TileArgs t;
+    t.A = p.A + p.a_l[l];
+    t.B = p.B + p.b_l[l];
+    t.C = p.C + p.c_l[l];
+    t.a_m = p.a_m; t.a_k = p.a_k; t.b_k = p.b_k; t.b_n = p.b_n; t.c_m = p.c_m; t.c_n = p.c_n;
+    t.a_kbs = p.a_kbs; t.b_kbs = p.b_kbs;
+    t.M = p.M; t.N = p.N;
+    t.m0 = tm*BM; t.n0 = tn*BN;
+    t.k_begin = (i64)split*p.k_per_split;
+    t.k_end = min(p.K, t.k_begin + p.k_per_split);
+    t.alpha = p.alpha; t.beta = p.beta;
+    t.W = p.splits > 1 ? p.partial + ((i64)split*p.L + l)*p.M*p.N : nullptr;
+    tile_body<BM, BN, WM, WN, STAGES, AMODE, BMODE>(t, smem, sAm, sBn, sCm, sCn);
+}
+
+// Persistent grouped kernel: every CTA walks the global tile list (all
+// groups' tiles, in group order) with a stride of the grid size; the group of
+// a tile is found by binary search in the tile prefix table. Gather modes are
+// per group (runtime), so the shared-memory stage is sized for either layout.
+template <int BM, int BN, int WM, int WN, int STAGES, int MINB>
+__global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
+gemm_f64_grouped_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__ tile_begin,
+                        int ngroups, i64 total_tiles)
+{
+    extern __shared__ __align__(16) double smem[];
+    i64* sAm = reinterpret_cast<i64*>(smem + tile_smem_doubles<BM, BN>(STAGES));
+    i64* sBn = sAm + BM;
+    i64* sCm = sBn + BN;
+    i64* sCn = sCm + BM;
+    for (i64 tile = blockIdx.x; tile < total_tiles; tile += gridDim.x)
+    {
+        int lo = 0, hi = ngroups - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(tile_begin + mid) <= tile) lo = mid; else hi = mid - 1;
+        }
+        const GroupDesc& g = groups[lo];
+        const i64 local = tile - tile_begin[lo];
+        const i64 tiles_n = (g.N + BN - 1)/BN;
+        TileArgs t;
+        t.A = g.A; t.B = g.B; t.C = g.C;
+        t.a_m = g.a_m; t.a_k = g.a_k; t.b_k = g.b_k; t.b_n = g.b_n; t.c_m = g.c_m; t.c_n = g.c_n;
+        t.a_kbs = g.a_kbs; t.b_kbs = g.b_kbs;
+        t.M = g.M; t.N = g.N;
+        t.m0 = (local / tiles_n)*BM; t.n0 = (local % tiles_n)*BN;
+        t.k_begin = 0; t.k_end = g.K;
+        t.alpha = g.alpha; t.beta = g.beta;
+        t.W = nullptr;
+        if (g.K == 0)
+        {
+            // empty contraction for this group: C = beta*C (beta == 0: set)
+            continue;
+        }
+        switch (g.amode*2 + g.bmode)
+        {
+            case 0: tile_body<BM, BN, WM, WN, STAGES, 0, 0>(t, smem, sAm, sBn, sCm, sCn); break;
+            case 1: tile_body<BM, BN, WM, WN, STAGES, 0, 1>(t, smem, sAm, sBn, sCm, sCn); break;
+            case 2: tile_body<BM, BN, WM, WN, STAGES, 1, 0>(t, smem, sAm, sBn, sCm, sCn); break;
+            default: tile_body<BM, BN, WM, WN, STAGES, 1, 1>(t, smem, sAm, sBn, sCm, sCn); break;
+        }
     }
 }
 
@@ -294,6 +384,7 @@ struct Variant
 {
     int bm, bn;
     void (*launch)(const GemmF64Args&, dim3, cudaStream_t, int amode, int bmode);
+    void (*grouped)(const GroupDesc*, const i64*, int, i64, cudaStream_t);
 };
 
 template <int BM_, int BN_, int WM, int WN, int STAGES, int MINB>
@@ -315,6 +406,20 @@ struct Config
         kern<<<grid, NT, bytes, s>>>(a);
         check_launch("gemm_f64_kernel");
     }
+    static void grouped(const GroupDesc* g, const i64* tb, int ngroups, i64 total, cudaStream_t s)
+    {
+        auto kern = gemm_f64_grouped_kernel<BM_, BN_, WM, WN, STAGES, MINB>;
+        const size_t bytes = (size_t)tile_smem_doubles<BM_, BN_>(STAGES)*sizeof(double) +
+                             (2*BM_ + 2*BN_)*sizeof(i64);
+        TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        int dev = 0, sms = 148;
+        TB_CUDA(cudaGetDevice(&dev));
+        TB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const i64 grid = std::min<i64>(total, (i64)sms*MINB);
+        if (grid <= 0) return;
+        kern<<<(unsigned)grid, NT, bytes, s>>>(g, tb, ngroups, total);
+        check_launch("gemm_f64_grouped_kernel");
+    }
     static void launch(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
     {
         switch (am*2 + bmd)
@@ -329,10 +434,10 @@ struct Config
 
 // the tile family (index = variant id - 1)
 const Variant kVariants[] = {
-    {128, 128, Config<128, 128, 64, 32, 4, 1>::launch},   // 1: 8 warps, 1 CTA/SM
-    {64, 128, Config<64, 128, 32, 64, 3, 2>::launch},     // 2: 4 warps, 2 CTAs/SM
-    {128, 64, Config<128, 64, 64, 32, 3, 2>::launch},     // 3: 4 warps, 2 CTAs/SM
-    {64, 64, Config<64, 64, 32, 32, 3, 3>::launch},       // 4: 4 warps, 3 CTAs/SM
+    {128, 128, Config<128, 128, 64, 32, 4, 1>::launch, Config<128, 128, 64, 32, 4, 1>::grouped},  // 1
+    {64, 128, Config<64, 128, 32, 64, 3, 2>::launch, Config<64, 128, 32, 64, 3, 2>::grouped},     // 2
+    {128, 64, Config<128, 64, 64, 32, 3, 2>::launch, Config<128, 64, 64, 32, 3, 2>::grouped},     // 3
+    {64, 64, Config<64, 64, 32, 32, 3, 3>::launch, Config<64, 64, 32, 32, 3, 3>::grouped},        // 4
 };
 constexpr int kNumVariants = sizeof(kVariants)/sizeof(kVariants[0]);
 
@@ -358,6 +463,21 @@ int pick_variant(const GemmF64Args& a)
 }
 
 } // namespace
+
+int gemm_f64_num_variants() { return kNumVariants; }
+void gemm_f64_variant_tile(int variant, int& bm, int& bn)
+{
+    const Variant& v = kVariants[std::max(1, std::min(variant, kNumVariants)) - 1];
+    bm = v.bm; bn = v.bn;
+}
+
+void gemm_f64_grouped_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups,
+                             i64 total_tiles, int variant, cudaStream_t stream)
+{
+    if (ngroups <= 0 || total_tiles <= 0) return;
+    const Variant& v = kVariants[std::max(1, std::min(variant, kNumVariants)) - 1];
+    v.grouped(d_groups, d_tile_begin, ngroups, total_tiles, stream);
+}
 
 i64 gemm_f64_tile_m() { return 128; }
 i64 gemm_f64_tile_n() { return 128; }

@@ -24,6 +24,24 @@ struct GemmF64Args
     int variant;             // tile configuration, 0 = automatic
 };
 
+// one GEMM of a grouped launch (no batch dimension: one entry per batch index)
+struct GroupDesc
+{
+    const double* A;
+    const double* B;
+    double* C;
+    const i64 *a_m, *a_k, *b_k, *b_n, *c_m, *c_n, *a_kbs, *b_kbs;
+    i64 M, N, K;
+    double alpha, beta;
+    int amode, bmode;
+};
+
+int gemm_f64_num_variants();
+void gemm_f64_variant_tile(int variant, int& bm, int& bn);
+// tile_begin[g] = first global tile of group g (tiles of BM x BN of the variant)
+void gemm_f64_grouped_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups,
+                             i64 total_tiles, int variant, cudaStream_t stream);
+
 i64 gemm_f64_tile_m();
 i64 gemm_f64_tile_n();
 i64 gemm_f64_tile_k();

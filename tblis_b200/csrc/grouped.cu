@@ -1,0 +1,325 @@
+// grouped.cu -- grouped GEMM plans: device tables, tile-shape autotuner and
+// CUDA-graph replay of the single persistent launch.
+//
+// Autotuner: the first time a plan with a new group-size histogram (count of
+// groups per (log2 M, log2 N, log2 K) bucket) runs, every tile configuration
+// of the FP64 DMMA family is timed once on the plan with C redirected to a
+// scratch buffer; the fastest is cached under the histogram and reused by
+// every plan with the same histogram.
+#include "grouped.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <list>
+
+namespace tb
+{
+
+namespace
+{
+
+std::mutex g_tune_mtx;
+std::map<std::string, int> g_tuned;         // histogram -> variant
+
+std::string histogram_key(const std::vector<GroupTables>& gs)
+{
+    std::map<std::string, int> h;
+    auto b = [](i64 x) { return x <= 1 ? 0 : (int)std::ceil(std::log2((double)x)); };
+    for (auto& g : gs) h[std::to_string(b(g.M)) + "," + std::to_string(b(g.N)) + "," + std::to_string(b(g.K))]++;
+    std::string k;
+    for (auto& kv : h) k += kv.first + ":" + std::to_string(kv.second) + ";";
+    return k;
+}
+
+__global__ void k_scale_patch(double* C, const i64* cm, const i64* cn, i64 M, i64 N, double beta)
+{
+    for (i64 e = blockIdx.x*(i64)blockDim.x + threadIdx.x; e < M*N; e += (i64)gridDim.x*blockDim.x)
+    {
+        const i64 i = e / N, j = e - i*N;
+        double* p = C + cm[i] + cn[j];
+        *p = beta == 0.0 ? 0.0 : beta*(*p);
+    }
+}
+
+void block_strides(const ivec& v, ivec& bs, i64 BK)
+{
+    const i64 n = (i64)v.size();
+    const i64 nb = (n + BK - 1)/BK;
+    bs.assign(nb, 0);
+    for (i64 b = 0; b < nb; b++)
+    {
+        const i64 i = b*BK;
+        const i64 bl = std::min(n - i, BK);
+        i64 s = bl > 1 ? v[i + 1] - v[i] : 1;
+        for (i64 j = i + 1; j + 1 < i + bl; j++)
+            if (v[j + 1] - v[j] != s) s = 0;
+        bs[b] = s;
+    }
+}
+
+} // namespace
+
+bool grouped_use_graphs()
+{
+    static int v = -1;
+    if (v < 0)
+    {
+        const char* s = getenv("TBLIS_B200_NO_GRAPHS");
+        v = (s && s[0] == '1') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+void GroupedPlan::finalize(cudaStream_t st)
+{
+    const i64 BK = gemm_f64_tile_k();
+    // device tables: for each group a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs
+    std::vector<i64> host;
+    std::vector<size_t> offs;
+    for (auto& g : groups)
+    {
+        ivec akbs, bkbs;
+        block_strides(g.a_k, akbs, BK);
+        block_strides(g.b_k, bkbs, BK);
+        const ivec* vecs[8] = {&g.a_m, &g.a_k, &g.b_k, &g.b_n, &g.c_m, &g.c_n, &akbs, &bkbs};
+        for (const ivec* v : vecs)
+        {
+            offs.push_back(host.size());
+            host.insert(host.end(), v->begin(), v->end());
+            if (v->empty()) host.push_back(0);
+        }
+    }
+    // the C extent is the sum of the extreme row and column offsets
+    {
+        i64 lo = 0, hi = 0;
+        for (auto& g : groups)
+        {
+            i64 mlo = 0, mhi = 0, nlo = 0, nhi = 0;
+            if (!g.c_m.empty()) { mlo = *std::min_element(g.c_m.begin(), g.c_m.end()); mhi = *std::max_element(g.c_m.begin(), g.c_m.end()); }
+            if (!g.c_n.empty()) { nlo = *std::min_element(g.c_n.begin(), g.c_n.end()); nhi = *std::max_element(g.c_n.begin(), g.c_n.end()); }
+            lo = std::min(lo, g.c_off + mlo + nlo);
+            hi = std::max(hi, g.c_off + mhi + nhi);
+        }
+        c_lo = lo; c_hi = hi;
+    }
+    if (!host.empty())
+    {
+        TB_CUDA(cudaMalloc(&d_tables, host.size()*sizeof(i64)));
+        TB_CUDA(cudaMemcpy(d_tables, host.data(), host.size()*sizeof(i64), cudaMemcpyHostToDevice));
+    }
+    d_ptr.resize(offs.size());
+    for (size_t i = 0; i < offs.size(); i++) d_ptr[i] = d_tables + offs[i];
+
+    const int nv = gemm_f64_num_variants();
+    tile_begin.assign(nv, {});
+    total_tiles.assign(nv, 0);
+    std::vector<i64> all;
+    for (int v = 1; v <= nv; v++)
+    {
+        int bm, bn;
+        gemm_f64_variant_tile(v, bm, bn);
+        i64 t = 0;
+        for (auto& g : groups)
+        {
+            tile_begin[v - 1].push_back(t);
+            t += ((g.M + bm - 1)/bm)*((g.N + bn - 1)/bn);
+        }
+        total_tiles[v - 1] = t;
+        all.insert(all.end(), tile_begin[v - 1].begin(), tile_begin[v - 1].end());
+    }
+    if (!all.empty())
+    {
+        TB_CUDA(cudaMalloc(&d_tile_begin, all.size()*sizeof(i64)));
+        TB_CUDA(cudaMemcpy(d_tile_begin, all.data(), all.size()*sizeof(i64), cudaMemcpyHostToDevice));
+    }
+    if (!groups.empty())
+    {
+        TB_CUDA(cudaMalloc(&d_descs, groups.size()*sizeof(GroupDesc)));
+        TB_CUDA(cudaMallocHost(&h_descs, groups.size()*sizeof(GroupDesc)));
+    }
+    TB_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
+    histogram = histogram_key(groups);
+    (void)st;
+}
+
+GroupedPlan::~GroupedPlan()
+{
+    if (graph) cudaGraphExecDestroy(graph);
+    if (last_use) { cudaEventSynchronize(last_use); cudaEventDestroy(last_use); }
+    if (d_tables) cudaFree(d_tables);
+    if (d_tile_begin) cudaFree(d_tile_begin);
+    if (d_descs) cudaFree(d_descs);
+    if (h_descs) cudaFreeHost(h_descs);
+}
+
+GroupedPlanCache& grouped_plan_cache()
+{
+    static GroupedPlanCache* c = new GroupedPlanCache();
+    return *c;
+}
+
+std::shared_ptr<GroupedPlan> GroupedPlanCache::find(const std::string& key)
+{
+    std::lock_guard<std::mutex> lk(mtx);
+    auto it = map.find(key);
+    return it == map.end() ? nullptr : it->second;
+}
+
+std::shared_ptr<GroupedPlan> GroupedPlanCache::insert(const std::string& key, std::shared_ptr<GroupedPlan> p)
+{
+    std::lock_guard<std::mutex> lk(mtx);
+    if (map.size() >= 256)
+    {
+        cudaDeviceSynchronize();
+        map.clear();
+    }
+    map[key] = p;
+    return p;
+}
+
+static void fill_descs(GroupedPlan& plan, GroupDesc* out, const double* const* ptrs, const double* alphas,
+                       const double* betas, double* c_override)
+{
+    for (size_t i = 0; i < plan.groups.size(); i++)
+    {
+        const GroupTables& g = plan.groups[i];
+        GroupDesc& d = out[i];
+        d.A = ptrs[g.a_slot] + g.a_off;
+        d.B = ptrs[g.b_slot] + g.b_off;
+        d.C = c_override ? c_override : const_cast<double*>(ptrs[g.c_slot]) + g.c_off;
+        d.a_m = plan.d_ptr[8*i + 0]; d.a_k = plan.d_ptr[8*i + 1];
+        d.b_k = plan.d_ptr[8*i + 2]; d.b_n = plan.d_ptr[8*i + 3];
+        d.c_m = plan.d_ptr[8*i + 4]; d.c_n = plan.d_ptr[8*i + 5];
+        d.a_kbs = plan.d_ptr[8*i + 6]; d.b_kbs = plan.d_ptr[8*i + 7];
+        d.M = g.M; d.N = g.N; d.K = g.K;
+        d.alpha = alphas[g.sidx]; d.beta = betas[g.sidx];
+        d.amode = g.amode; d.bmode = g.bmode;
+    }
+}
+
+static const i64* variant_tile_begin(GroupedPlan& plan, int v)
+{
+    return plan.d_tile_begin + (size_t)(v - 1)*plan.groups.size();
+}
+
+static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* alphas, const double* betas,
+                    cudaStream_t st)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mtx);
+        auto it = g_tuned.find(plan.histogram);
+        if (it != g_tuned.end()) return it->second;
+    }
+    const char* env = getenv("TBLIS_B200_GEMM_VARIANT");
+    if (env && atoi(env) >= 1 && atoi(env) <= gemm_f64_num_variants()) return atoi(env);
+
+    // scratch C covering the offsets of every group: candidates write there
+    const i64 span = plan.c_hi - plan.c_lo + 1;
+    dbuf scratch((size_t)std::max<i64>(span, 1)*sizeof(double), st);
+    TB_CUDA(cudaMemsetAsync(scratch.ptr, 0, (size_t)std::max<i64>(span, 1)*sizeof(double), st));
+    std::vector<GroupDesc> hd(plan.groups.size());
+    fill_descs(plan, hd.data(), ptrs, alphas, betas, scratch.as<double>() - plan.c_lo);
+    for (size_t i = 0; i < hd.size(); i++) hd[i].C = scratch.as<double>() - plan.c_lo + plan.groups[i].c_off;
+    dbuf dd(hd.size()*sizeof(GroupDesc), st);
+    TB_CUDA(cudaMemcpyAsync(dd.ptr, hd.data(), hd.size()*sizeof(GroupDesc), cudaMemcpyHostToDevice, st));
+    cudaEvent_t e0, e1;
+    TB_CUDA(cudaEventCreate(&e0));
+    TB_CUDA(cudaEventCreate(&e1));
+    int best = 1;
+    float best_ms = 1e30f;
+    for (int v = 1; v <= gemm_f64_num_variants(); v++)
+    {
+        gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
+                                plan.total_tiles[v - 1], v, st);     // warm-up
+        TB_CUDA(cudaEventRecord(e0, st));
+        gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
+                                plan.total_tiles[v - 1], v, st);
+        TB_CUDA(cudaEventRecord(e1, st));
+        TB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        TB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_tune_mtx);
+    g_tuned[plan.histogram] = best;
+    return best;
+}
+
+void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alphas, const double* betas,
+                 cudaStream_t st)
+{
+    if (plan.groups.empty()) return;
+    if (plan.variant == 0) plan.variant = autotune(plan, ptrs, alphas, betas, st);
+    const int v = plan.variant;
+
+    // the pinned descriptor buffer is read by the previous launch: wait for it
+    TB_CUDA(cudaEventSynchronize(plan.last_use));
+    fill_descs(plan, plan.h_descs, ptrs, alphas, betas, nullptr);
+
+    if (grouped_use_graphs() && !plan.graph_failed)
+    {
+        if (!plan.graph)
+        {
+            cudaStream_t cs;
+            TB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            TB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e1 = cudaMemcpyAsync(plan.d_descs, plan.h_descs, plan.groups.size()*sizeof(GroupDesc),
+                                             cudaMemcpyHostToDevice, cs);
+            bool ok = e1 == cudaSuccess;
+            if (ok)
+            {
+                try
+                {
+                    gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
+                                            plan.total_tiles[v - 1], v, cs);
+                }
+                catch (const error&) { ok = false; }
+            }
+            cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+            cudaStreamDestroy(cs);
+            if (ok && e2 == cudaSuccess && cudaGraphInstantiate(&plan.graph, g, 0) == cudaSuccess)
+                cudaGraphDestroy(g);
+            else
+            {
+                // capture unavailable here: run the launch directly from now on
+                if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                cudaGetLastError();
+                plan.graph = nullptr;
+                plan.graph_failed = true;
+            }
+        }
+    }
+    if (plan.graph)
+    {
+        TB_CUDA(cudaGraphLaunch(plan.graph, st));
+        count_launch();
+    }
+    else
+    {
+        TB_CUDA(cudaMemcpyAsync(plan.d_descs, plan.h_descs, plan.groups.size()*sizeof(GroupDesc),
+                                cudaMemcpyHostToDevice, st));
+        gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
+                                plan.total_tiles[v - 1], v, st);
+    }
+    TB_CUDA(cudaEventRecord(plan.last_use, st));
+}
+
+void scale_patch(double* C, const ivec& c_m, const ivec& c_n, double beta, cudaStream_t st)
+{
+    if (beta == 1.0 || c_m.empty() || c_n.empty()) return;
+    dbuf d((c_m.size() + c_n.size())*sizeof(i64), st);
+    std::vector<i64> h(c_m.begin(), c_m.end());
+    h.insert(h.end(), c_n.begin(), c_n.end());
+    TB_CUDA(cudaMemcpyAsync(d.ptr, h.data(), h.size()*sizeof(i64), cudaMemcpyHostToDevice, st));
+    TB_CUDA(cudaStreamSynchronize(st));     // h dies at return
+    const i64 M = (i64)c_m.size(), N = (i64)c_n.size();
+    const int blocks = (int)std::min<i64>((M*N + 255)/256, 148*8);
+    k_scale_patch<<<blocks, 256, 0, st>>>(C, d.as<i64>(), d.as<i64>() + M, M, N, beta);
+    check_launch("k_scale_patch");
+}
+
+} // namespace tb

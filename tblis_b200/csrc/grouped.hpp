@@ -1,0 +1,73 @@
+// grouped.hpp -- many GEMM views in one persistent launch: plans, the
+// tile-shape autotuner and CUDA-graph replay.
+#pragma once
+
+#include "planner.hpp"
+#include "gemm_f64.hpp"
+
+#include <map>
+#include <memory>
+#include <mutex>
+
+namespace tb
+{
+
+// host scatter vectors of one group (one GEMM view, one batch index)
+struct GroupTables
+{
+    ivec a_m, a_k, b_k, b_n, c_m, c_n;
+    i64 M = 0, N = 0, K = 0;
+    int amode = 0, bmode = 0;
+    int a_slot = 0, b_slot = 1, c_slot = 2;   // indices into the run's pointer array
+    i64 a_off = 0, b_off = 0, c_off = 0;      // element offsets added to those pointers
+    int sidx = 0;                             // index into the run's alpha/beta arrays
+};
+
+struct GroupedPlan
+{
+    std::vector<GroupTables> groups;
+    std::vector<std::pair<ivec, ivec>> empty_patches;   // C patches scaled by beta only
+    double flops = 0;
+    int nslots = 3;
+
+    // device state (finalize)
+    i64* d_tables = nullptr;
+    std::vector<const i64*> d_ptr;            // per group: a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs
+    std::vector<std::vector<i64>> tile_begin; // per variant (index variant-1)
+    std::vector<i64> total_tiles;
+    i64* d_tile_begin = nullptr;              // all variants, concatenated
+    GroupDesc* d_descs = nullptr;
+    GroupDesc* h_descs = nullptr;             // pinned
+    int variant = 0;                          // tuned tile configuration
+    cudaGraphExec_t graph = nullptr;
+    bool graph_failed = false;
+    cudaEvent_t last_use = nullptr;
+    i64 c_lo = 0, c_hi = -1;                  // extent of C offsets (for the tuner's scratch)
+    std::string histogram;
+
+    void finalize(cudaStream_t st);
+    ~GroupedPlan();
+};
+
+// plan cache keyed by a shape string (LRU)
+struct GroupedPlanCache
+{
+    std::shared_ptr<GroupedPlan> find(const std::string& key);
+    std::shared_ptr<GroupedPlan> insert(const std::string& key, std::shared_ptr<GroupedPlan> p);
+    std::mutex mtx;
+    std::map<std::string, std::shared_ptr<GroupedPlan>> map;
+};
+GroupedPlanCache& grouped_plan_cache();
+
+// runs every group of the plan: C_g = alphas[sidx_g]*A_g*B_g + betas[sidx_g]*C_g,
+// with A_g = ptrs[a_slot] + a_off etc. One launch, graph-replayed.
+void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alphas, const double* betas,
+                 cudaStream_t st);
+
+// C[c_m[i] + c_n[j]] = beta*C[...] (beta == 0: set) for a patch without contracted blocks
+void scale_patch(double* C, const ivec& c_m, const ivec& c_n, double beta, cudaStream_t st);
+
+// disables graph capture (debug / environments without graph support)
+bool grouped_use_graphs();
+
+} // namespace tb
