@@ -273,6 +273,20 @@ bool patch_view(const DpdLayout& X, const std::vector<unsigned>& rdims,
     return true;
 }
 
+// offsets inside the block `irr` of X over the dims `dims` (first fastest),
+// plus the block's base offset
+ivec block_part(const DpdLayout& X, const std::vector<unsigned>& irr, const std::vector<unsigned>& dims, i64& base)
+{
+    std::vector<i64> bl(X.ndim), bs(X.ndim);
+    X.block(irr.data(), bl.data(), bs.data(), base);
+    ivec lens, strs;
+    i64 ext = 1;
+    for (unsigned d : dims) { lens.push_back(bl[d]); strs.push_back(bs[d]); ext *= bl[d]; }
+    ivec out(ext), tmp(std::max<i64>(ext, 1));
+    if (ext > 0) fill_block_scatter(lens, strs, 1, 0, ext, out.data(), tmp.data(), false);
+    return out;
+}
+
 int gather_mode(const ivec& mvec, const ivec& kvec)
 {
     auto lead = [](const ivec& v) { return v.size() > 1 ? std::llabs(v[1] - v[0]) : (i64)1 << 60; };
@@ -403,21 +417,72 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
             bool ok = patch_view(A.lay, dims(AC, iA), rc, dims(AB, iA), kc, g.a_m, g.a_k) &&
                       patch_view(B.lay, dims(AB, iB), kc, dims(BC, iB), cc, g.b_k, g.b_n) &&
                       patch_view(C.lay, dims(AC, iC), rc, dims(BC, iC), cc, g.c_m, g.c_n);
-            TB_CHECK(ok, TB_ERR_ARG, "DPD: layout does not split into row and column parts");
-            const i64 M = (i64)g.c_m.size(), N = (i64)g.c_n.size(), K = (i64)g.a_k.size();
-            if (M == 0 || N == 0) continue;
-            if (K == 0)
+            if (ok)
             {
-                // no contracted blocks for this irrep: C patch = beta*C patch
-                p->empty_patches.push_back({g.c_m, g.c_n});
+                const i64 M = (i64)g.c_m.size(), N = (i64)g.c_n.size(), K = (i64)g.a_k.size();
+                if (M == 0 || N == 0) continue;
+                if (K == 0)
+                {
+                    // no contracted blocks for this irrep: C patch = beta*C patch
+                    p->empty_patches.push_back({g.c_m, g.c_n});
+                    continue;
+                }
+                g.M = M; g.N = N; g.K = K;
+                g.amode = gather_mode(g.a_m, g.a_k);
+                g.bmode = gather_mode(g.b_n, g.b_k);
+                g.a_slot = 0; g.b_slot = 1; g.c_slot = 2;
+                flops += 2.0*M*N*K;
+                p->groups.push_back(std::move(g));
                 continue;
             }
-            g.M = M; g.N = N; g.K = K;
-            g.amode = gather_mode(g.a_m, g.a_k);
-            g.bmode = gather_mode(g.b_n, g.b_k);
-            g.a_slot = 0; g.b_slot = 1; g.c_slot = 2;
-            flops += 2.0*M*N*K;
-            p->groups.push_back(std::move(g));
+            // the labels of a group interleave in the layout tree: one group per
+            // C block, one K segment per contributing (A block, B block) pair
+            const auto dAC = dims(AC, iA), dAB = dims(AB, iA), dBAB = dims(AB, iB), dBBC = dims(BC, iB);
+            const auto dCAC = dims(AC, iC), dCBC = dims(BC, iC);
+            for (auto& r : rc)
+                for (auto& c : cc)
+                {
+                    std::vector<unsigned> irrC(C.lay.ndim);
+                    for (size_t i = 0; i < AC.size(); i++) irrC[dCAC[i]] = r[i];
+                    for (size_t i = 0; i < BC.size(); i++) irrC[dCBC[i]] = c[i];
+                    i64 baseC;
+                    GroupTables gb;
+                    ivec cm = block_part(C.lay, irrC, dCAC, baseC);
+                    i64 dummy;
+                    gb.c_n = block_part(C.lay, irrC, dCBC, dummy);
+                    if (cm.empty() || gb.c_n.empty()) continue;
+                    for (i64& x : cm) x += baseC;
+                    gb.c_m = std::move(cm);
+                    gb.M = (i64)gb.c_m.size(); gb.N = (i64)gb.c_n.size(); gb.K = 0;
+                    for (auto& k : kc)
+                    {
+                        std::vector<unsigned> irrA(A.lay.ndim), irrB(B.lay.ndim);
+                        for (size_t i = 0; i < AC.size(); i++) irrA[dAC[i]] = r[i];
+                        for (size_t i = 0; i < AB.size(); i++) { irrA[dAB[i]] = k[i]; irrB[dBAB[i]] = k[i]; }
+                        for (size_t i = 0; i < BC.size(); i++) irrB[dBBC[i]] = c[i];
+                        SegTables sg;
+                        i64 baseA, baseB, d2;
+                        sg.a_m = block_part(A.lay, irrA, dAC, baseA);
+                        sg.a_k = block_part(A.lay, irrA, dAB, d2);
+                        sg.b_k = block_part(B.lay, irrB, dBAB, baseB);
+                        sg.b_n = block_part(B.lay, irrB, dBBC, d2);
+                        if (sg.a_k.empty()) continue;
+                        for (i64& x : sg.a_m) x += baseA;
+                        for (i64& x : sg.b_k) x += baseB;
+                        gb.K += (i64)sg.a_k.size();
+                        gb.segs.push_back(std::move(sg));
+                    }
+                    if (gb.segs.empty())
+                    {
+                        p->empty_patches.push_back({gb.c_m, gb.c_n});
+                        continue;
+                    }
+                    gb.amode = gather_mode(gb.segs[0].a_m, gb.segs[0].a_k);
+                    gb.bmode = gather_mode(gb.segs[0].b_n, gb.segs[0].b_k);
+                    gb.a_slot = 0; gb.b_slot = 1; gb.c_slot = 2;
+                    flops += 2.0*gb.M*gb.N*gb.K;
+                    p->groups.push_back(std::move(gb));
+                }
         }
         p->flops = flops;
         p->finalize(st);

@@ -103,6 +103,8 @@ struct TileArgs
     i64 k_begin, k_end;
     double alpha, beta;
     double* W;                // split-K partial tile output (dense, ld = N), or null
+    int nseg;                 // 0: the single segment above; else segs[0..nseg)
+    const SegDesc* segs;
 };
 
 template <int BM, int BN>
@@ -126,53 +128,19 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const i64 m0 = p.m0, n0 = p.n0;
-    const i64 k_begin = p.k_begin, k_end = p.k_end;
     const double* __restrict__ A = p.A;
     const double* __restrict__ B = p.B;
 
     for (int i = tid; i < BM; i += NT)
     {
         const i64 m = m0 + i;
-        sAm[i] = m < p.M ? p.a_m[m] : -1;
         sCm[i] = m < p.M ? p.c_m[m] : -1;
     }
     for (int i = tid; i < BN; i += NT)
     {
         const i64 n = n0 + i;
-        sBn[i] = n < p.N ? p.b_n[n] : -1;
         sCn[i] = n < p.N ? p.c_n[n] : -1;
     }
-    __syncthreads();
-
-    const i64 kt_count = (k_end - k_begin + BK - 1)/BK;
-
-    auto load_tile = [&](int stage, i64 kt, const KInfo& ka, const KInfo& kb)
-    {
-        double* As = smem + stage*STAGE;
-        double* Bs = As + TA::SIZE;
-        const i64 k0 = k_begin + kt*BK;
-        const int kvalid = (int)min((i64)BK, k_end - k0);
-        #pragma unroll
-        for (int e = tid; e < BK*BM; e += NT)
-        {
-            const int ml = AMODE == 0 ? e % BM : e / BK;
-            const int kl = AMODE == 0 ? e / BM : e % BK;
-            const i64 ro = sAm[ml];
-            const bool ok = ro >= 0 && kl < kvalid;
-            const i64 ko = ok ? koff(p.a_k, ka, k0, kl) : 0;
-            cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
-        }
-        #pragma unroll
-        for (int e = tid; e < BK*BN; e += NT)
-        {
-            const int nl = BMODE == 0 ? e % BN : e / BK;
-            const int kl = BMODE == 0 ? e / BN : e % BK;
-            const i64 co = sBn[nl];
-            const bool ok = co >= 0 && kl < kvalid;
-            const i64 ko = ok ? koff(p.b_k, kb, k0, kl) : 0;
-            cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
-        }
-    };
 
     double acc[MS][NS][2];
     #pragma unroll
@@ -180,54 +148,110 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
         #pragma unroll
         for (int j = 0; j < NS; j++) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
-    #pragma unroll
-    for (int s = 0; s < STAGES-1; s++)
-    {
-        if (s < kt_count)
-        {
-            const i64 k0 = k_begin + s*BK;
-            load_tile(s, s, fetch_kinfo(p.a_k, p.a_kbs, k0, true), fetch_kinfo(p.b_k, p.b_kbs, k0, true));
-        }
-        cp_async_commit();
-    }
-    // k information of the next tile to load, one iteration ahead
-    i64 nk = STAGES - 1;
-    KInfo ka = fetch_kinfo(p.a_k, p.a_kbs, k_begin + nk*BK, nk < kt_count);
-    KInfo kb = fetch_kinfo(p.b_k, p.b_kbs, k_begin + nk*BK, nk < kt_count);
-
     const int wm0 = (warp / (BN/WN))*WM;
     const int wn0 = (warp % (BN/WN))*WN;
     const int fr = lane >> 2, fc = lane & 3;
 
-    for (i64 kt = 0; kt < kt_count; kt++)
+    const int nseg = p.nseg > 0 ? p.nseg : 1;
+    for (int sg = 0; sg < nseg; sg++)
     {
-        cp_async_wait<STAGES-2>();
+        const i64 *a_m = p.a_m, *a_k = p.a_k, *b_k = p.b_k, *b_n = p.b_n, *a_kbs = p.a_kbs, *b_kbs = p.b_kbs;
+        i64 k_begin = p.k_begin, k_end = p.k_end;
+        if (p.nseg > 0)
+        {
+            const SegDesc& sd = p.segs[sg];
+            a_m = sd.a_m; a_k = sd.a_k; b_k = sd.b_k; b_n = sd.b_n; a_kbs = sd.a_kbs; b_kbs = sd.b_kbs;
+            k_begin = 0; k_end = sd.K;
+        }
+        for (int i = tid; i < BM; i += NT)
+        {
+            const i64 m = m0 + i;
+            sAm[i] = m < p.M ? a_m[m] : -1;
+        }
+        for (int i = tid; i < BN; i += NT)
+        {
+            const i64 n = n0 + i;
+            sBn[i] = n < p.N ? b_n[n] : -1;
+        }
         __syncthreads();
 
-        if (nk < kt_count) load_tile((int)(nk % STAGES), nk, ka, kb);
-        cp_async_commit();
-        nk++;
-        ka = fetch_kinfo(p.a_k, p.a_kbs, k_begin + nk*BK, nk < kt_count);
-        kb = fetch_kinfo(p.b_k, p.b_kbs, k_begin + nk*BK, nk < kt_count);
+        const i64 kt_count = (k_end - k_begin + BK - 1)/BK;
 
-        const double* As = smem + (kt % STAGES)*STAGE;
-        const double* Bs = As + TA::SIZE;
-        #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4)
+        auto load_tile = [&](int stage, i64 kt, const KInfo& ka, const KInfo& kb)
         {
-            double af[MS], bf[NS];
+            double* As = smem + stage*STAGE;
+            double* Bs = As + TA::SIZE;
+            const i64 k0 = k_begin + kt*BK;
+            const int kvalid = (int)min((i64)BK, k_end - k0);
             #pragma unroll
-            for (int i = 0; i < MS; i++) af[i] = As[TA::idx(wm0 + i*8 + fr, kk + fc)];
+            for (int e = tid; e < BK*BM; e += NT)
+            {
+                const int ml = AMODE == 0 ? e % BM : e / BK;
+                const int kl = AMODE == 0 ? e / BM : e % BK;
+                const i64 ro = sAm[ml];
+                const bool ok = ro >= 0 && kl < kvalid;
+                const i64 ko = ok ? koff(a_k, ka, k0, kl) : 0;
+                cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
+            }
             #pragma unroll
-            for (int j = 0; j < NS; j++) bf[j] = Bs[TB::idx(wn0 + j*8 + fr, kk + fc)];
-            #pragma unroll
-            for (int i = 0; i < MS; i++)
-                #pragma unroll
-                for (int j = 0; j < NS; j++)
-                    dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+            for (int e = tid; e < BK*BN; e += NT)
+            {
+                const int nl = BMODE == 0 ? e % BN : e / BK;
+                const int kl = BMODE == 0 ? e / BN : e % BK;
+                const i64 co = sBn[nl];
+                const bool ok = co >= 0 && kl < kvalid;
+                const i64 ko = ok ? koff(b_k, kb, k0, kl) : 0;
+                cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
+            }
+        };
+
+        #pragma unroll
+        for (int s = 0; s < STAGES-1; s++)
+        {
+            if (s < kt_count)
+            {
+                const i64 k0 = k_begin + s*BK;
+                load_tile(s, s, fetch_kinfo(a_k, a_kbs, k0, true), fetch_kinfo(b_k, b_kbs, k0, true));
+            }
+            cp_async_commit();
         }
+        // k information of the next tile to load, one iteration ahead
+        i64 nk = STAGES - 1;
+        KInfo ka = fetch_kinfo(a_k, a_kbs, k_begin + nk*BK, nk < kt_count);
+        KInfo kb = fetch_kinfo(b_k, b_kbs, k_begin + nk*BK, nk < kt_count);
+
+        for (i64 kt = 0; kt < kt_count; kt++)
+        {
+            cp_async_wait<STAGES-2>();
+            __syncthreads();
+
+            if (nk < kt_count) load_tile((int)(nk % STAGES), nk, ka, kb);
+            cp_async_commit();
+            nk++;
+            ka = fetch_kinfo(a_k, a_kbs, k_begin + nk*BK, nk < kt_count);
+            kb = fetch_kinfo(b_k, b_kbs, k_begin + nk*BK, nk < kt_count);
+
+            const double* As = smem + (kt % STAGES)*STAGE;
+            const double* Bs = As + TA::SIZE;
+            #pragma unroll
+            for (int kk = 0; kk < BK; kk += 4)
+            {
+                double af[MS], bf[NS];
+                #pragma unroll
+                for (int i = 0; i < MS; i++) af[i] = As[TA::idx(wm0 + i*8 + fr, kk + fc)];
+                #pragma unroll
+                for (int j = 0; j < NS; j++) bf[j] = Bs[TB::idx(wn0 + j*8 + fr, kk + fc)];
+                #pragma unroll
+                for (int i = 0; i < MS; i++)
+                    #pragma unroll
+                    for (int j = 0; j < NS; j++)
+                        dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+            }
+        }
+        cp_async_wait<0>();
+        // the next segment reuses the stages and the offset arrays
+        __syncthreads();
     }
-    cp_async_wait<0>();
 
     if (p.W)
     {
@@ -309,6 +333,8 @@ gemm_f64_kernel(const GemmF64Args p)
     t.k_end = min(p.K, t.k_begin + p.k_per_split);
     t.alpha = p.alpha; t.beta = p.beta;
     t.W = p.splits > 1 ? p.partial + ((i64)split*p.L + l)*p.M*p.N : nullptr;
+    t.nseg = 0;
+    t.segs = nullptr;
     tile_body<BM, BN, WM, WN, STAGES, AMODE, BMODE>(t, smem, sAm, sBn, sCm, sCn);
 }
 
@@ -346,7 +372,9 @@ gemm_f64_grouped_kernel(const GroupDesc* __restrict__ groups, const i64* __restr
         t.k_begin = 0; t.k_end = g.K;
         t.alpha = g.alpha; t.beta = g.beta;
         t.W = nullptr;
-        if (g.K == 0)
+        t.nseg = g.nseg;
+        t.segs = g.segs;
+        if (g.K == 0 && g.nseg == 0)
         {
             // empty contraction for this group: C = beta*C (beta == 0: set)
             continue;

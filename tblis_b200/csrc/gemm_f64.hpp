@@ -24,7 +24,17 @@ struct GemmF64Args
     int variant;             // tile configuration, 0 = automatic
 };
 
-// one GEMM of a grouped launch (no batch dimension: one entry per batch index)
+// one K segment of a grouped GEMM: the rows of A / columns of B it reads
+// and its k range (all segments of a group accumulate into the same C tile)
+struct SegDesc
+{
+    const i64 *a_m, *a_k, *b_k, *b_n, *a_kbs, *b_kbs;
+    i64 K;
+};
+
+// one GEMM of a grouped launch (no batch dimension: one entry per batch index).
+// With nseg == 0 the group has a single segment given by the inline fields;
+// otherwise segs[0..nseg) replace them (A and B offsets per segment).
 struct GroupDesc
 {
     const double* A;
@@ -34,6 +44,8 @@ struct GroupDesc
     i64 M, N, K;
     double alpha, beta;
     int amode, bmode;
+    int nseg;
+    const SegDesc* segs;
 };
 
 int gemm_f64_num_variants();

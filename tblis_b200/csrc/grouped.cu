@@ -74,20 +74,30 @@ bool grouped_use_graphs()
 void GroupedPlan::finalize(cudaStream_t st)
 {
     const i64 BK = gemm_f64_tile_k();
-    // device tables: for each group a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs
+    // device tables: for each group a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs,
+    // then for each segment a_m, a_k, b_k, b_n, a_kbs, b_kbs
     std::vector<i64> host;
-    std::vector<size_t> offs;
+    std::vector<size_t> offs, seg_offs;
+    auto put = [&](const ivec& v, std::vector<size_t>& o)
+    {
+        o.push_back(host.size());
+        host.insert(host.end(), v.begin(), v.end());
+        if (v.empty()) host.push_back(0);
+    };
     for (auto& g : groups)
     {
         ivec akbs, bkbs;
         block_strides(g.a_k, akbs, BK);
         block_strides(g.b_k, bkbs, BK);
         const ivec* vecs[8] = {&g.a_m, &g.a_k, &g.b_k, &g.b_n, &g.c_m, &g.c_n, &akbs, &bkbs};
-        for (const ivec* v : vecs)
+        for (const ivec* v : vecs) put(*v, offs);
+        for (auto& sg : g.segs)
         {
-            offs.push_back(host.size());
-            host.insert(host.end(), v->begin(), v->end());
-            if (v->empty()) host.push_back(0);
+            ivec sa, sb;
+            block_strides(sg.a_k, sa, BK);
+            block_strides(sg.b_k, sb, BK);
+            const ivec* sv[6] = {&sg.a_m, &sg.a_k, &sg.b_k, &sg.b_n, &sa, &sb};
+            for (const ivec* v : sv) put(*v, seg_offs);
         }
     }
     // the C extent is the sum of the extreme row and column offsets
@@ -110,6 +120,28 @@ void GroupedPlan::finalize(cudaStream_t st)
     }
     d_ptr.resize(offs.size());
     for (size_t i = 0; i < offs.size(); i++) d_ptr[i] = d_tables + offs[i];
+    // segment descriptors
+    std::vector<SegDesc> hs;
+    size_t so = 0;
+    for (auto& g : groups)
+    {
+        seg_begin.push_back((i64)hs.size());
+        for (auto& sg : g.segs)
+        {
+            SegDesc d;
+            d.a_m = d_tables + seg_offs[so + 0]; d.a_k = d_tables + seg_offs[so + 1];
+            d.b_k = d_tables + seg_offs[so + 2]; d.b_n = d_tables + seg_offs[so + 3];
+            d.a_kbs = d_tables + seg_offs[so + 4]; d.b_kbs = d_tables + seg_offs[so + 5];
+            d.K = (i64)sg.a_k.size();
+            so += 6;
+            hs.push_back(d);
+        }
+    }
+    if (!hs.empty())
+    {
+        TB_CUDA(cudaMalloc(&d_segs, hs.size()*sizeof(SegDesc)));
+        TB_CUDA(cudaMemcpy(d_segs, hs.data(), hs.size()*sizeof(SegDesc), cudaMemcpyHostToDevice));
+    }
 
     const int nv = gemm_f64_num_variants();
     tile_begin.assign(nv, {});
@@ -148,6 +180,7 @@ GroupedPlan::~GroupedPlan()
     if (graph) cudaGraphExecDestroy(graph);
     if (last_use) { cudaEventSynchronize(last_use); cudaEventDestroy(last_use); }
     if (d_tables) cudaFree(d_tables);
+    if (d_segs) cudaFree(d_segs);
     if (d_tile_begin) cudaFree(d_tile_begin);
     if (d_descs) cudaFree(d_descs);
     if (h_descs) cudaFreeHost(h_descs);
@@ -195,6 +228,8 @@ static void fill_descs(GroupedPlan& plan, GroupDesc* out, const double* const* p
         d.M = g.M; d.N = g.N; d.K = g.K;
         d.alpha = alphas[g.sidx]; d.beta = betas[g.sidx];
         d.amode = g.amode; d.bmode = g.bmode;
+        d.nseg = (int)g.segs.size();
+        d.segs = g.segs.empty() ? nullptr : plan.d_segs + plan.seg_begin[i];
     }
 }
 

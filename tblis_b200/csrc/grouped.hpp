@@ -12,9 +12,18 @@
 namespace tb
 {
 
-// host scatter vectors of one group (one GEMM view, one batch index)
+// host scatter vectors of one K segment of a segmented group
+struct SegTables
+{
+    ivec a_m, a_k, b_k, b_n;
+};
+
+// host scatter vectors of one group (one GEMM view, one batch index). A
+// segmented group (segs non-empty) takes A's rows, B's columns and the k range
+// from each segment in turn and ignores a_m, a_k, b_k, b_n, K.
 struct GroupTables
 {
+    std::vector<SegTables> segs;
     ivec a_m, a_k, b_k, b_n, c_m, c_n;
     i64 M = 0, N = 0, K = 0;
     int amode = 0, bmode = 0;
@@ -33,6 +42,8 @@ struct GroupedPlan
     // device state (finalize)
     i64* d_tables = nullptr;
     std::vector<const i64*> d_ptr;            // per group: a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs
+    SegDesc* d_segs = nullptr;                // all segments of all groups
+    std::vector<i64> seg_begin;               // per group: first entry in d_segs
     std::vector<std::vector<i64>> tile_begin; // per variant (index variant-1)
     std::vector<i64> total_tiles;
     i64* d_tile_begin = nullptr;              // all variants, concatenated
