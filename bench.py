@@ -419,8 +419,188 @@ def e2e_ladder(torch, tb, method, steps):
             "note": "host pinned buffers through tblis_tensor_mult; H2D of A,B and D2H of C inside each call"}
 
 
+OCC = [12, 4, 8, 6, 10, 3, 7, 5]
+VIR = [60, 22, 40, 30, 52, 14, 36, 26]
+
+
+def dpd_workload(torch, tb, dev, stream):
+    """DPD ladder C[abij] = A[abef]*B[efij] under D2h (8 irreps, XOR, total
+    irrep 0), occ [12,4,8,6,10,3,7,5], vir [60,22,40,30,52,14,36,26], default
+    MArray layout; one grouped launch per call (graph-replayed). Returns the
+    DPD rate and the dense-equivalent rate: dense FP64 GEMMs of the same
+    per-irrep M x N x K on the same kernel."""
+    out = {}
+    g = torch.Generator(device=dev)
+    g.manual_seed(41)
+    A = tb.DpdTensor(0, 8, [VIR, VIR, VIR, VIR])
+    B = tb.DpdTensor(0, 8, [VIR, VIR, OCC, OCC])
+    C = tb.DpdTensor(0, 8, [VIR, VIR, OCC, OCC])
+    A.data = torch.empty(A.size(), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+    B.data = torch.empty(B.size(), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+    C.data = torch.zeros(C.size(), dtype=torch.float64, device=dev)
+    rep = tb.dpd_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij")      # plan, tuning, graph
+    flops = rep["flops"]
+    for _ in range(2):
+        tb.dpd_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij")
+    ms, per = time_steps(torch, lambda: tb.dpd_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij"), 5, stream)
+    dpd_ms = statistics.median(per)
+    out["dpd_gflop"] = flops / 1e9
+    out["dpd_gflops"] = flops / (dpd_ms * 1e-3) / 1e9
+    out["dpd_groups"] = rep["m"]
+    out["dpd_tile_variant"] = rep["n"]
+    # dense-equivalent: per irrep h, M_h = sum_g v_g v_{g^h}, N_h = sum_g o_g o_{g^h}, K_h = M_h
+    tot_f, tot_ms = 0.0, 0.0
+    for h in range(8):
+        M = sum(VIR[x] * VIR[x ^ h] for x in range(8))
+        N = sum(OCC[x] * OCC[x ^ h] for x in range(8))
+        a = torch.empty((M, M), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        b = torch.empty((M, N), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        c = torch.zeros((M, N), dtype=torch.float64, device=dev)
+        f = lambda: tb.mult(1.0, a, "ik", b, "kj", 0.0, c, "ij")
+        f()
+        _, p = time_steps(torch, f, 3, stream)
+        tot_f += 2.0 * M * N * M
+        tot_ms += statistics.median(p)
+        del a, b, c
+    out["dpd_dense_equiv_gflops"] = tot_f / (tot_ms * 1e-3) / 1e9
+    out["dpd_frac_of_dense_equiv"] = out["dpd_gflops"] / out["dpd_dense_equiv_gflops"]
+    del A, B, C
+    torch.cuda.empty_cache()
+    return out
+
+
+def batch_workload(torch, tb, dev, stream, count=10000, serial_sample=500):
+    """A batch of `count` independent 4-index contractions (2 labels per group,
+    extents uniform 4..32, random index order of every operand) in one grouped
+    launch, against the same contractions issued one call at a time (timed on
+    the first `serial_sample` and scaled)."""
+    import random
+    rnd = random.Random(0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(43)
+    items, flops = [], 0.0
+    for _ in range(count):
+        l = {c: rnd.randint(4, 32) for c in "abefij"}
+        ia = "".join(rnd.sample("abef", 4))
+        ib = "".join(rnd.sample("efij", 4))
+        ic = "".join(rnd.sample("abij", 4))
+        mk = lambda ix: torch.empty([l[c] for c in ix], dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        items.append((1.0, mk(ia), ia, mk(ib), ib, 0.0, mk(ic), ic))
+        flops += 2.0 * l["a"] * l["b"] * l["e"] * l["f"] * l["i"] * l["j"]
+    tb.mult_batch(items)                   # plan + tuning + graph
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        tb.mult_batch(items)
+    torch.cuda.synchronize()
+    batch_s = (time.perf_counter() - t0) / reps
+    sample = items[:serial_sample]
+    for it in sample[:20]:
+        tb.mult(*it)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in sample:
+        tb.mult(*it)
+    torch.cuda.synchronize()
+    serial_s = (time.perf_counter() - t0) * count / len(sample)
+    return {"batch_count": count, "batch_gflop": flops / 1e9, "batch_gflops": flops / batch_s / 1e9,
+            "batch_ms": batch_s * 1e3, "serial_gflops_est": flops / serial_s / 1e9,
+            "batch_speedup_vs_serial": serial_s / batch_s}
+
+
+def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
+    """Stream of pairwise 4-index contraction requests: 6 labels split 2/2/2
+    into contracted, A-only and B-only groups at random, every operand's index
+    order permuted, extents log-uniform in 8..128, each operand at most 256 MB
+    (resampled otherwise), FP64, requested tolerance 1e-10 or 1e-13 (50/50),
+    Poisson arrivals at `rate` per second. Operands are device-resident: the
+    requests draw from a pool of `pool_size` resident problems (a solver's
+    amplitudes), each with two output buffers used alternately. Returns the
+    server's p50/p99 latency and throughput, and the throughput of the same
+    requests issued as serial plain calls."""
+    import math
+    import random
+    rnd = random.Random(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 1)
+    cap = (256 << 20) // 8
+    pool = []
+    while len(pool) < pool_size:
+        labs = list("abcdef")
+        rnd.shuffle(labs)
+        AB, AC, BC = labs[0:2], labs[2:4], labs[4:6]
+        l = {c: int(round(math.exp(rnd.uniform(math.log(8), math.log(128))))) for c in labs}
+        ia, ib, ic = AB + AC, AB + BC, AC + BC
+        sizes = [math.prod(l[c] for c in x) for x in (ia, ib, ic)]
+        if max(sizes) > cap:
+            continue
+        rnd.shuffle(ia); rnd.shuffle(ib); rnd.shuffle(ic)
+        ia, ib, ic = "".join(ia), "".join(ib), "".join(ic)
+        mk = lambda ix: torch.empty([l[c] for c in ix], dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        fl = 2.0 * math.prod(l.values())
+        pool.append(dict(A=mk(ia), B=mk(ib), C=[mk(ic), mk(ic)], ia=ia, ib=ib, ic=ic, flops=fl))
+    picks = [rnd.randrange(pool_size) for _ in range(nreq)]
+    tols = [1e-10 if rnd.random() < 0.5 else 1e-13 for _ in range(nreq)]
+    gaps = [rnd.expovariate(rate) for _ in range(nreq)]
+    total_flops = sum(pool[i]["flops"] for i in picks)
+
+    # serial plain calls, back to back
+    for i in picks[:10]:
+        p = pool[i]
+        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][0], p["ic"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j, i in enumerate(picks):
+        p = pool[i]
+        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"])
+    torch.cuda.synchronize()
+    serial_s = time.perf_counter() - t0
+
+    srv = tb.Server(hbm_budget_bytes=150 << 30, slots=4)
+    ids = []
+    t0 = time.perf_counter()
+    due = t0
+    for j, i in enumerate(picks):
+        due += gaps[j]
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        p = pool[i]
+        ids.append(srv.submit(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"], tols[j]))
+    for rid in ids:
+        srv.wait(rid)
+    served_s = time.perf_counter() - t0
+    arrivals_s = due - t0
+    st = srv.stats()
+    srv.close()
+    del pool
+    torch.cuda.empty_cache()
+    return {"rate_req_s": rate, "requests": nreq, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "max_ms": st["max_ms"], "batches": st["batches"], "mean_batch": st["mean_batch"],
+            "max_concurrent_batches": st["max_concurrent_batches"],
+            "served_req_s": nreq / served_s, "served_gflops": total_flops / served_s / 1e9,
+            "arrival_window_s": arrivals_s,
+            "serial_req_s": nreq / serial_s, "serial_gflops": total_flops / serial_s / 1e9,
+            "throughput_vs_serial": serial_s / served_s}
+
+
 def extra_workloads(torch, tb, dev, stream, peaks):
     out = {}
+    for rate, n in ((2000, 2000), (50, 150), (1e9, 2000)):
+        try:
+            out["serve_%s" % ("burst" if rate > 1e6 else int(rate))] = serve_workload(torch, tb, dev, rate, n)
+        except Exception as e:
+            out["serve_%d_error" % rate] = str(e)[:200]
+    try:
+        out.update(dpd_workload(torch, tb, dev, stream))
+    except Exception as e:     # keep the headline line even if a secondary workload fails
+        out["dpd_error"] = str(e)[:200]
+    try:
+        out.update(batch_workload(torch, tb, dev, stream))
+    except Exception as e:
+        out["batch_error"] = str(e)[:200]
+    torch.cuda.empty_cache()
     # ring: C[aibj] += A[aeim]*B[mbej], o=64, v=256 (8.8 TFLOP), FP64 DMMA
     o, v = 64, 256
     g = torch.Generator(device=dev)

@@ -274,6 +274,45 @@ int tblis_b200_tensor_mult_batch(int count, const tblis_tensor* A, const label_t
                                        tblis_tensor* C, const label_type* const* idx_C,
                                  tblis_b200_report* report);
 
+/* ---- serving ---------------------------------------------------------------- */
+
+/* A continuous-batching contraction server (no counterpart in the reference;
+ * it serves the calls of src/iface/3t/mult.cxx:24-165 issued by a solver whose
+ * operands stay device-resident). Requests queue in arrival order; a scheduler
+ * thread admits them while their operand footprint (A, B and C extents) fits
+ * the HBM budget, folds every admitted request into one grouped launch and
+ * keeps up to `slots` launches in flight on separate streams, so requests that
+ * arrive while others run start as soon as a slot and budget free up. A
+ * request's result is the same alone and in any mix (every output tile is
+ * computed by one CTA with a fixed k order). Tensors must be in device memory
+ * and stay valid until the request completes; the tensor descriptors are
+ * copied at submit. */
+typedef struct tblis_b200_server tblis_b200_server;
+
+typedef struct tblis_b200_server_stats
+{
+    int64_t completed;
+    int64_t failed;
+    int64_t batches;                 /* grouped launches */
+    int64_t queued;                  /* waiting for admission */
+    double mean_batch;               /* requests per launch */
+    int max_concurrent_batches;      /* most launches seen in flight at once */
+    double p50_ms, p99_ms, max_ms;   /* submit-to-completion latency */
+} tblis_b200_server_stats;
+
+tblis_b200_server* tblis_b200_server_create(size_t hbm_budget_bytes, int slots);
+/* waits for every queued and running request, then frees the server */
+void tblis_b200_server_destroy(tblis_b200_server* srv);
+/* returns the request id (> 0), or -1 (last error: 7 = larger than the budget) */
+int64_t tblis_b200_server_submit(tblis_b200_server* srv,
+                                 const tblis_tensor* A, const label_type* idx_A,
+                                 const tblis_tensor* B, const label_type* idx_B,
+                                 const tblis_tensor* C, const label_type* idx_C, double tolerance);
+/* 0 = done (the id is released), 1 = pending, else the request's error code */
+int tblis_b200_server_poll(tblis_b200_server* srv, int64_t id, double* latency_ms);
+int tblis_b200_server_wait(tblis_b200_server* srv, int64_t id, double* latency_ms);
+int tblis_b200_server_get_stats(tblis_b200_server* srv, tblis_b200_server_stats* out);
+
 /* No counterpart in the reference. tblis_tensor_mult for callers that cannot
  * let a library allocate device memory (their device memory is owned by
  * another allocator, or they must avoid cudaMalloc/cudaFree because those can

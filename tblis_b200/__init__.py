@@ -362,3 +362,82 @@ def mult_batch(items):
     lib.tblis_b200_tensor_mult_batch(n, TA, IA, TB, IB, TC, IC, ctypes.byref(r))
     _check()
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
+# ---- serving -----------------------------------------------------------------------------------
+
+class tblis_b200_server_stats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("mean_batch", ctypes.c_double),
+                ("max_concurrent_batches", ctypes.c_int), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double)]
+
+
+lib.tblis_b200_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int]
+lib.tblis_b200_server_create.restype = ctypes.c_void_p
+lib.tblis_b200_server_destroy.argtypes = [ctypes.c_void_p]
+lib.tblis_b200_server_submit.argtypes = [ctypes.c_void_p, _P(tblis_tensor), ctypes.c_char_p, _P(tblis_tensor),
+                                         ctypes.c_char_p, _P(tblis_tensor), ctypes.c_char_p, ctypes.c_double]
+lib.tblis_b200_server_submit.restype = ctypes.c_int64
+lib.tblis_b200_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_int64, _P(ctypes.c_double)]
+lib.tblis_b200_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_int64, _P(ctypes.c_double)]
+lib.tblis_b200_server_get_stats.argtypes = [ctypes.c_void_p, _P(tblis_b200_server_stats)]
+
+
+class Server:
+    """Continuous-batching contraction server over device-resident operands
+    (see tblis_b200_server_* in include/tblis_b200.h)."""
+
+    def __init__(self, hbm_budget_bytes=150 << 30, slots=4):
+        self.h = lib.tblis_b200_server_create(int(hbm_budget_bytes), int(slots))
+        _check()
+        if not self.h:
+            raise TblisError(3, "server creation failed")
+        self._live = {}
+
+    def submit(self, alpha, A, idx_A, B, idx_B, beta, C, idx_C, tolerance=1e-13):
+        a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+        rid = lib.tblis_b200_server_submit(self.h, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref,
+                                           _labels(idx_C), float(tolerance))
+        if rid < 0:
+            _check()
+            raise TblisError(1, "submit failed")
+        self._live[rid] = (a, b, c)
+        return rid
+
+    def wait(self, rid):
+        lat = ctypes.c_double(0)
+        rc = lib.tblis_b200_server_wait(self.h, rid, ctypes.byref(lat))
+        self._live.pop(rid, None)
+        if rc:
+            _check()
+            raise TblisError(rc, "request failed")
+        return lat.value
+
+    def poll(self, rid):
+        lat = ctypes.c_double(0)
+        rc = lib.tblis_b200_server_poll(self.h, rid, ctypes.byref(lat))
+        if rc == 1:
+            return False, None
+        self._live.pop(rid, None)
+        if rc:
+            _check()
+            raise TblisError(rc, "request failed")
+        return True, lat.value
+
+    def stats(self):
+        s = tblis_b200_server_stats()
+        lib.tblis_b200_server_get_stats(self.h, ctypes.byref(s))
+        _check()
+        return {f: getattr(s, f) for f, _ in tblis_b200_server_stats._fields_}
+
+    def close(self):
+        if self.h:
+            lib.tblis_b200_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,495 @@
+// serve.cpp -- a continuous-batching contraction server.
+//
+// Requests (tblis_tensor_mult calls on device-resident operands) are queued
+// by tblis_b200_server_submit from any host thread. One scheduler thread
+// admits queued requests in arrival order while their operand footprint fits
+// the HBM budget, folds every admitted request into one grouped launch of the
+// FP64 DMMA kernel (scatter vectors, descriptors and tile prefix table packed
+// into one pinned buffer and copied with a single transfer), and launches it
+// on the next free slot -- each slot owns a stream, so up to `slots` batches
+// run on the GPU at once and requests that arrive while others run are
+// admitted as soon as a slot and budget free up. Completion is detected with
+// events; each request records its latency (submit to completion).
+//
+// Each request's result does not depend on the batch it lands in: every
+// output tile is computed by one CTA with a fixed k order and a fixed tile
+// shape, whatever else runs.
+#include "common.hpp"
+#include "planner.hpp"
+#include "gemm_f64.hpp"
+#include "level1.hpp"
+#include "mult.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+
+namespace tb
+{
+
+namespace
+{
+
+using clk = std::chrono::steady_clock;
+
+struct Request
+{
+    int64_t id;
+    tblis_tensor A, B, C;
+    std::vector<len_type> len[3];
+    std::vector<stride_type> stride[3];
+    std::string idx[3];
+    double tol;
+    i64 footprint;                   // bytes of A, B and C counted against the budget
+    clk::time_point t_submit, t_done;
+    int state = 0;                   // 0 queued, 1 running, 2 done, 3 failed
+    int err = 0;
+    std::string msg;
+};
+
+struct Slot
+{
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    char* hbuf = nullptr;            // pinned staging
+    size_t hcap = 0;
+    char* dbuf_ = nullptr;           // device copy
+    size_t dcap = 0;
+    std::vector<int64_t> reqs;
+    bool busy = false;
+    i64 footprint = 0;
+};
+
+constexpr int kVariant = 4;          // 64 x 64 tiles: every batch uses the same tile shape
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+} // namespace
+
+struct Server
+{
+    std::mutex mtx;
+    std::condition_variable cv, done_cv;
+    std::deque<int64_t> queue;
+    std::map<int64_t, std::unique_ptr<Request>> reqs;
+    std::vector<Slot> slots;
+    std::thread worker;
+    bool stop = false;
+    int64_t next_id = 1;
+    i64 budget = 0, in_use = 0;
+    int device = 0;
+    int max_batch = 256;
+    // statistics
+    int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_requests = 0;
+    int max_running = 0;
+    std::vector<double> latencies;
+    std::string fatal;
+
+    Server(size_t budget_bytes, int nslots)
+    {
+        budget = (i64)budget_bytes;
+        TB_CUDA(cudaGetDevice(&device));
+        slots.resize(std::max(1, nslots));
+        for (auto& s : slots)
+        {
+            TB_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+            TB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        }
+        worker = std::thread([this] { loop(); });
+    }
+
+    ~Server()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mtx);
+            stop = true;
+        }
+        cv.notify_all();
+        if (worker.joinable()) worker.join();
+        for (auto& s : slots)
+        {
+            if (s.stream) cudaStreamSynchronize(s.stream);
+            if (s.hbuf) cudaFreeHost(s.hbuf);
+            if (s.dbuf_) cudaFree(s.dbuf_);
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.stream) cudaStreamDestroy(s.stream);
+        }
+    }
+
+    int64_t submit(const tblis_tensor* A, const char* ia, const tblis_tensor* B, const char* ib,
+                   const tblis_tensor* C, const char* ic, double tol)
+    {
+        auto r = std::make_unique<Request>();
+        const tblis_tensor* in[3] = {A, B, C};
+        const char* ix[3] = {ia, ib, ic};
+        r->footprint = 0;
+        for (int t = 0; t < 3; t++)
+        {
+            TB_CHECK(in[t] && in[t]->type == TYPE_DOUBLE, TB_ERR_TYPE, "server: double tensors only");
+            const unsigned nd = in[t]->ndim;
+            r->len[t].assign(in[t]->len, in[t]->len + nd);
+            r->stride[t].assign(in[t]->stride, in[t]->stride + nd);
+            r->idx[t] = ix[t] ? std::string(ix[t], nd) : std::string();
+            i64 lo, hi;
+            tensor_extent(nd, in[t]->len, in[t]->stride, lo, hi);
+            if (hi >= lo)
+            {
+                TB_CHECK(pointer_kind(in[t]->data) == MEM_DEVICE, TB_ERR_ARG,
+                         "server: operands must be device-resident");
+                r->footprint += (hi - lo + 1)*(i64)sizeof(double);
+            }
+        }
+        TB_CHECK(r->footprint <= budget, TB_ERR_BUDGET, "server: request larger than the HBM budget");
+        r->A = *A; r->B = *B; r->C = *C;
+        r->A.len = r->len[0].data(); r->A.stride = r->stride[0].data();
+        r->B.len = r->len[1].data(); r->B.stride = r->stride[1].data();
+        r->C.len = r->len[2].data(); r->C.stride = r->stride[2].data();
+        r->tol = tol;
+        r->t_submit = clk::now();
+        std::lock_guard<std::mutex> lk(mtx);
+        TB_CHECK(fatal.empty(), TB_ERR_CUDA, "server stopped: " + fatal);
+        const int64_t id = next_id++;
+        r->id = id;
+        reqs[id] = std::move(r);
+        queue.push_back(id);
+        cv.notify_all();
+        return id;
+    }
+
+    // 0 done, 1 pending, else the request's error code
+    int status(int64_t id, double* latency_ms, bool wait)
+    {
+        std::unique_lock<std::mutex> lk(mtx);
+        auto it = reqs.find(id);
+        TB_CHECK(it != reqs.end(), TB_ERR_ARG, "server: unknown request id");
+        if (wait)
+            done_cv.wait(lk, [&] { return it->second->state >= 2 || !fatal.empty(); });
+        Request& r = *it->second;
+        if (r.state < 2)
+        {
+            TB_CHECK(fatal.empty(), TB_ERR_CUDA, "server stopped: " + fatal);
+            return 1;
+        }
+        if (latency_ms)
+            *latency_ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
+        const int e = r.state == 3 ? (r.err ? r.err : TB_ERR_ARG) : 0;
+        if (e) set_last_error(e, r.msg.c_str());
+        reqs.erase(it);
+        return e;
+    }
+
+    // builds one batch into a slot's staging buffer and launches it
+    void launch(Slot& s, std::vector<Request*>& batch)
+    {
+        cudaStream_t st = s.stream;
+        struct Prep
+        {
+            Request* r;
+            GemmView v;
+            bool trivial;
+            double alpha, beta;
+        };
+        std::vector<Prep> prep;
+        size_t table_elems = 0;
+        size_t ngroups = 0;
+        const i64 BK = gemm_f64_tile_k();
+        for (Request* r : batch)
+        {
+            try
+            {
+                GemmView v = gemm_view(mult_groups(&r->A, r->idx[0].c_str(), &r->B, r->idx[1].c_str(),
+                                                   &r->C, r->idx[2].c_str()));
+                const double alpha = r->A.scalar.data.d*r->B.scalar.data.d, beta = r->C.scalar.data.d;
+                const bool trivial = alpha == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
+                if (!trivial)
+                {
+                    table_elems += 2*v.m + 2*v.n + 2*v.k + 2*((v.k + BK - 1)/BK) + 8;
+                    ngroups += v.l;
+                }
+                prep.push_back({r, v, trivial, alpha, beta});
+            }
+            catch (const error& e)
+            {
+                r->state = 3; r->err = e.code; r->msg = e.what();
+            }
+        }
+        const size_t tab_bytes = align_up(table_elems*sizeof(i64));
+        const size_t desc_bytes = align_up(ngroups*sizeof(GroupDesc));
+        const size_t tb_bytes = align_up((ngroups + 1)*sizeof(i64));
+        const size_t need = tab_bytes + desc_bytes + tb_bytes;
+        if (need > s.hcap)
+        {
+            if (s.hbuf) cudaFreeHost(s.hbuf);
+            s.hcap = std::max(need, 2*s.hcap);
+            TB_CUDA(cudaMallocHost(&s.hbuf, s.hcap));
+        }
+        if (need > s.dcap)
+        {
+            if (s.dbuf_) cudaFree(s.dbuf_);
+            s.dcap = std::max(need, 2*s.dcap);
+            TB_CUDA(cudaMalloc(&s.dbuf_, s.dcap));
+        }
+        i64* htab = reinterpret_cast<i64*>(s.hbuf);
+        GroupDesc* hdesc = reinterpret_cast<GroupDesc*>(s.hbuf + tab_bytes);
+        i64* htb = reinterpret_cast<i64*>(s.hbuf + tab_bytes + desc_bytes);
+        const i64* dtab = reinterpret_cast<const i64*>(s.dbuf_);
+        GroupDesc* ddesc = reinterpret_cast<GroupDesc*>(s.dbuf_ + tab_bytes);
+        const i64* dtb = reinterpret_cast<const i64*>(s.dbuf_ + tab_bytes + desc_bytes);
+
+        size_t pos = 0, g = 0;
+        i64 tiles = 0;
+        int bm, bn;
+        gemm_f64_variant_tile(kVariant, bm, bn);
+        std::vector<i64> bs;
+        for (Prep& p : prep)
+        {
+            const GemmView& v = p.v;
+            if (p.trivial)
+            {
+                if (v.m*v.n*v.l == 0 || p.beta == 1.0) continue;
+                Strided sc;
+                ivec len, str;
+                for (size_t j = 0; j < v.lenM.size(); j++) { len.push_back(v.lenM[j]); str.push_back(v.cM[j]); }
+                for (size_t j = 0; j < v.lenN.size(); j++) { len.push_back(v.lenN[j]); str.push_back(v.cN[j]); }
+                for (size_t j = 0; j < v.lenL.size(); j++) { len.push_back(v.lenL[j]); str.push_back(v.cL[j]); }
+                sc.ndim = (int)len.size();
+                for (size_t j = 0; j < len.size(); j++) { sc.len[j] = len[j]; sc.stride[j] = str[j]; }
+                if (p.beta == 0.0) l1_set<double>(static_cast<double*>(p.r->C.data), sc, 0.0, st);
+                else l1_scale<double>(static_cast<double*>(p.r->C.data), sc, p.beta, st);
+                continue;
+            }
+            bs.resize(std::max({v.m, v.n, v.k, v.l}) + 1);
+            auto put = [&](const ivec& lens, const ivec& strides, i64 n, bool p3) -> const i64*
+            {
+                i64* h = htab + pos;
+                fill_block_scatter(lens, strides, 1, 0, n, h, bs.data(), p3);
+                const i64* d = dtab + pos;
+                pos += n;
+                return d;
+            };
+            const i64* a_m = put(v.lenM, v.aM, v.m, v.pack_m_3d);
+            const i64* c_m = put(v.lenM, v.cM, v.m, v.pack_m_3d);
+            const i64* b_n = put(v.lenN, v.bN, v.n, v.pack_n_3d);
+            const i64* c_n = put(v.lenN, v.cN, v.n, v.pack_n_3d);
+            i64* ha_k = htab + pos;
+            const i64* a_k = put(v.lenK, v.aK, v.k, v.pack_k_3d);
+            i64* hb_k = htab + pos;
+            const i64* b_k = put(v.lenK, v.bK, v.k, v.pack_k_3d);
+            const i64 nkb = (v.k + BK - 1)/BK;
+            auto kbs = [&](const i64* k) -> const i64*
+            {
+                i64* h = htab + pos;
+                for (i64 b = 0; b < nkb; b++)
+                {
+                    const i64 i0 = b*BK, bl = std::min(v.k - i0, BK);
+                    i64 sv = bl > 1 ? k[i0 + 1] - k[i0] : 1;
+                    for (i64 j = i0 + 1; j + 1 < i0 + bl; j++) if (k[j + 1] - k[j] != sv) sv = 0;
+                    h[b] = sv;
+                }
+                const i64* d = dtab + pos;
+                pos += nkb;
+                return d;
+            };
+            const i64* a_kbs = kbs(ha_k);
+            const i64* b_kbs = kbs(hb_k);
+            std::vector<i64> al(v.l), bl(v.l), cl(v.l);
+            fill_block_scatter(v.lenL, v.aL, 1, 0, v.l, al.data(), bs.data(), false);
+            fill_block_scatter(v.lenL, v.bL, 1, 0, v.l, bl.data(), bs.data(), false);
+            fill_block_scatter(v.lenL, v.cL, 1, 0, v.l, cl.data(), bs.data(), false);
+            for (i64 l = 0; l < v.l; l++)
+            {
+                GroupDesc& d = hdesc[g];
+                d.A = static_cast<const double*>(p.r->A.data) + al[l];
+                d.B = static_cast<const double*>(p.r->B.data) + bl[l];
+                d.C = static_cast<double*>(p.r->C.data) + cl[l];
+                d.a_m = a_m; d.a_k = a_k; d.b_k = b_k; d.b_n = b_n; d.c_m = c_m; d.c_n = c_n;
+                d.a_kbs = a_kbs; d.b_kbs = b_kbs;
+                d.M = v.m; d.N = v.n; d.K = v.k;
+                d.alpha = p.alpha; d.beta = p.beta;
+                d.amode = v.amode; d.bmode = v.bmode;
+                d.nseg = 0; d.segs = nullptr;
+                htb[g] = tiles;
+                tiles += ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn);
+                g++;
+            }
+        }
+        if (g > 0)
+        {
+            TB_CUDA(cudaMemcpyAsync(s.dbuf_, s.hbuf, need, cudaMemcpyHostToDevice, st));
+            gemm_f64_grouped_launch(ddesc, dtb, (int)g, tiles, kVariant, st);
+        }
+        TB_CUDA(cudaEventRecord(s.done, st));
+    }
+
+    void loop()
+    {
+        cudaSetDevice(device);
+        while (true)
+        {
+            std::vector<Request*> batch;
+            Slot* slot = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mtx);
+                // completions
+                for (auto& s : slots)
+                {
+                    if (!s.busy) continue;
+                    cudaError_t q = cudaEventQuery(s.done);
+                    if (q == cudaErrorNotReady) continue;
+                    const auto now = clk::now();
+                    for (int64_t id : s.reqs)
+                    {
+                        auto it = reqs.find(id);
+                        if (it == reqs.end()) continue;
+                        Request& r = *it->second;
+                        if (r.state == 1)
+                        {
+                            if (q == cudaSuccess) { r.state = 2; n_done++; }
+                            else { r.state = 3; r.err = TB_ERR_CUDA; r.msg = cudaGetErrorString(q); n_failed++; }
+                            r.t_done = now;
+                            latencies.push_back(std::chrono::duration<double, std::milli>(now - r.t_submit).count());
+                        }
+                        else if (r.state == 3) { r.t_done = now; n_failed++; }
+                    }
+                    s.reqs.clear();
+                    s.busy = false;
+                    in_use -= s.footprint;
+                    s.footprint = 0;
+                    done_cv.notify_all();
+                }
+                int running = 0;
+                for (auto& s : slots) running += s.busy;
+                max_running = std::max(max_running, running);
+                if (stop && queue.empty() && running == 0) break;
+                // admission: arrival order, while the budget allows
+                for (auto& s : slots) if (!s.busy) { slot = &s; break; }
+                if (slot && !queue.empty())
+                {
+                    while (!queue.empty() && (int)batch.size() < max_batch)
+                    {
+                        Request& r = *reqs[queue.front()];
+                        if (in_use + r.footprint > budget) break;
+                        in_use += r.footprint;
+                        slot->footprint += r.footprint;
+                        r.state = 1;
+                        batch.push_back(&r);
+                        slot->reqs.push_back(r.id);
+                        queue.pop_front();
+                    }
+                }
+                if (batch.empty())
+                {
+                    if (running == 0) cv.wait_for(lk, std::chrono::milliseconds(1));
+                    else
+                    {
+                        lk.unlock();
+                        std::this_thread::sleep_for(std::chrono::microseconds(20));
+                    }
+                    continue;
+                }
+                slot->busy = true;
+            }
+            try
+            {
+                launch(*slot, batch);
+                std::lock_guard<std::mutex> lk(mtx);
+                n_batches++;
+                batched_requests += (int64_t)batch.size();
+            }
+            catch (const std::exception& e)
+            {
+                std::lock_guard<std::mutex> lk(mtx);
+                fatal = e.what();
+                for (Request* r : batch) { r->state = 3; r->err = TB_ERR_CUDA; r->msg = e.what(); }
+                cudaEventRecord(slot->done, slot->stream);
+                done_cv.notify_all();
+            }
+        }
+    }
+};
+
+} // namespace tb
+
+using namespace tb;
+
+extern "C" {
+
+struct tblis_b200_server { Server* s; };
+
+tblis_b200_server* tblis_b200_server_create(size_t hbm_budget_bytes, int slots)
+{
+    tblis_b200_server* out = nullptr;
+    guarded([&]
+    {
+        ensure_device();
+        out = new tblis_b200_server{new Server(hbm_budget_bytes, slots)};
+    });
+    return out;
+}
+
+void tblis_b200_server_destroy(tblis_b200_server* srv)
+{
+    if (!srv) return;
+    delete srv->s;
+    delete srv;
+}
+
+int64_t tblis_b200_server_submit(tblis_b200_server* srv, const tblis_tensor* A, const label_type* idx_A,
+                                 const tblis_tensor* B, const label_type* idx_B,
+                                 const tblis_tensor* C, const label_type* idx_C, double tolerance)
+{
+    int64_t id = -1;
+    guarded([&]
+    {
+        TB_CHECK(srv, TB_ERR_ARG, "null server");
+        id = srv->s->submit(A, idx_A, B, idx_B, C, idx_C, tolerance);
+    });
+    return id;
+}
+
+int tblis_b200_server_poll(tblis_b200_server* srv, int64_t id, double* latency_ms)
+{
+    int r = -1;
+    int e = guarded([&] { TB_CHECK(srv, TB_ERR_ARG, "null server"); r = srv->s->status(id, latency_ms, false); });
+    return e ? e : r;
+}
+
+int tblis_b200_server_wait(tblis_b200_server* srv, int64_t id, double* latency_ms)
+{
+    int r = -1;
+    int e = guarded([&] { TB_CHECK(srv, TB_ERR_ARG, "null server"); r = srv->s->status(id, latency_ms, true); });
+    return e ? e : r;
+}
+
+int tblis_b200_server_get_stats(tblis_b200_server* srv, tblis_b200_server_stats* out)
+{
+    return guarded([&]
+    {
+        TB_CHECK(srv && out, TB_ERR_ARG, "null argument");
+        Server& s = *srv->s;
+        std::lock_guard<std::mutex> lk(s.mtx);
+        memset(out, 0, sizeof(*out));
+        out->completed = s.n_done;
+        out->failed = s.n_failed;
+        out->batches = s.n_batches;
+        out->mean_batch = s.n_batches ? (double)s.batched_requests/s.n_batches : 0.0;
+        out->max_concurrent_batches = s.max_running;
+        out->queued = (int64_t)s.queue.size();
+        std::vector<double> l = s.latencies;
+        if (!l.empty())
+        {
+            std::sort(l.begin(), l.end());
+            auto pct = [&](double q) { return l[std::min(l.size() - 1, (size_t)(q*(l.size() - 1) + 0.5))]; };
+            out->p50_ms = pct(0.50);
+            out->p99_ms = pct(0.99);
+            out->max_ms = l.back();
+        }
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,141 @@
+"""GPU tests of the continuous-batching server: results against the oracle,
+each result bit-identical alone and in a mix, HBM-budget admission, batches
+overlapping on the device, and a failing request not disturbing others."""
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import random_contraction, make_operand, normwise_rel, to_device, view_of
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+
+
+def _requests(torch, cuda, seeds, max_len=10):
+    out = []
+    for s in seeds:
+        rng = np.random.default_rng(s)
+        idx_A, idx_B, idx_C, lens = random_contraction(rng, max_len=max_len)
+        A = make_operand(idx_A, lens, rng)
+        B = make_operand(idx_B, lens, rng)
+        C = make_operand(idx_C, lens, rng)
+        alpha, beta = float(rng.choice([1.0, 0.5])), float(rng.choice([0.0, 1.0]))
+        ref = C[1].copy()
+        oracle.orc_mult(alpha, A[1], idx_A, B[1], idx_B, beta, ref, idx_C)
+        _, dA = to_device(*A, torch, cuda)
+        _, dB = to_device(*B, torch, cuda)
+        dCb, dC = to_device(*C, torch, cuda)
+        out.append(dict(args=(alpha, dA, idx_A, dB, idx_B, beta, dC, idx_C), ref=ref, Cb=dCb, C=C))
+    return out
+
+
+def test_results_match_oracle(cuda):
+    import torch
+    import tblis_b200 as tb
+    srv = tb.Server(hbm_budget_bytes=8 << 30, slots=4)
+    reqs = _requests(torch, cuda, range(8000, 8060))
+    ids = [srv.submit(*r["args"]) for r in reqs]
+    lats = [srv.wait(i) for i in ids]
+    torch.cuda.synchronize()
+    for r in reqs:
+        got = view_of(r["Cb"].cpu().numpy(), r["C"][1].shape, r["C"][2])
+        assert normwise_rel(got, r["ref"]) <= TOL
+    st = srv.stats()
+    assert st["completed"] == 60 and st["failed"] == 0 and min(lats) >= 0
+    srv.close()
+
+
+def test_same_result_alone_and_in_the_mix(cuda):
+    import torch
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(1)
+    A = torch.empty((48, 40, 36), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    B = torch.empty((36, 52, 40), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    C0 = torch.empty((52, 48), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    srv = tb.Server(slots=4)
+    alone = C0.clone()
+    srv.wait(srv.submit(1.0, A, "abc", B, "cdb", 0.5, alone, "da"))
+    others = _requests(torch, cuda, range(9000, 9040))
+    mixed = C0.clone()
+    ids = [srv.submit(*r["args"]) for r in others[:20]]
+    mid = srv.submit(1.0, A, "abc", B, "cdb", 0.5, mixed, "da")
+    ids += [srv.submit(*r["args"]) for r in others[20:]]
+    srv.wait(mid)
+    for i in ids:
+        srv.wait(i)
+    torch.cuda.synchronize()
+    assert torch.equal(alone, mixed)
+    srv.close()
+
+
+def test_budget_admission(cuda):
+    import torch
+    import tblis_b200 as tb
+    # each request holds 3 x 8 MB; a 40 MB budget admits one at a time
+    srv = tb.Server(hbm_budget_bytes=40 << 20, slots=4)
+    n = 1024
+    mats = [(torch.rand((n, n), dtype=torch.float64, device=cuda), torch.rand((n, n), dtype=torch.float64, device=cuda),
+             torch.zeros((n, n), dtype=torch.float64, device=cuda)) for _ in range(6)]
+    ids = [srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij") for a, b, c in mats]
+    for i in ids:
+        srv.wait(i)
+    torch.cuda.synchronize()
+    for a, b, c in mats:
+        assert torch.allclose(c, a @ b, rtol=1e-12, atol=1e-12)
+    st = srv.stats()
+    assert st["batches"] == 6 and st["mean_batch"] == 1.0
+    big = torch.zeros((2048, 2048), dtype=torch.float64, device=cuda)
+    with pytest.raises(tb.TblisError) as e:
+        srv.submit(1.0, big, "ik", big, "kj", 0.0, big, "ij")
+    assert e.value.code == 7
+    srv.close()
+
+
+def test_batches_overlap_on_device(cuda):
+    """Requests arriving while a long batch runs are admitted into another
+    slot instead of waiting for it (continuous batching)."""
+    import torch
+    import tblis_b200 as tb
+    srv = tb.Server(slots=4)
+    n = 6144
+    a = torch.rand((n, n), dtype=torch.float64, device=cuda)
+    b = torch.rand((n, n), dtype=torch.float64, device=cuda)
+    c = torch.zeros((n, n), dtype=torch.float64, device=cuda)
+    big = srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij")      # ~20 ms on the GPU
+    time.sleep(0.003)
+    small = _requests(torch, cuda, range(9500, 9508), max_len=6)
+    ids = [srv.submit(*r["args"]) for r in small]
+    lat_small = [srv.wait(i) for i in ids]
+    lat_big = srv.wait(big)
+    torch.cuda.synchronize()
+    st = srv.stats()
+    assert st["max_concurrent_batches"] >= 2
+    for r in small:
+        got = view_of(r["Cb"].cpu().numpy(), r["C"][1].shape, r["C"][2])
+        assert normwise_rel(got, r["ref"]) <= TOL
+    srv.close()
+
+
+def test_failed_request_is_isolated(cuda):
+    import torch
+    import tblis_b200 as tb
+    srv = tb.Server(slots=2)
+    good = _requests(torch, cuda, range(9700, 9705))
+    A = torch.ones((3, 4), dtype=torch.float64, device=cuda)
+    B = torch.ones((5, 2), dtype=torch.float64, device=cuda)   # k lengths differ: 4 vs 5
+    C = torch.ones((3, 2), dtype=torch.float64, device=cuda)
+    ids = [srv.submit(*r["args"]) for r in good[:2]]
+    bad = srv.submit(1.0, A, "ik", B, "kj", 0.0, C, "ij")
+    ids += [srv.submit(*r["args"]) for r in good[2:]]
+    with pytest.raises(tb.TblisError):
+        srv.wait(bad)
+    for i in ids:
+        srv.wait(i)
+    torch.cuda.synchronize()
+    for r in good:
+        got = view_of(r["Cb"].cpu().numpy(), r["C"][1].shape, r["C"][2])
+        assert normwise_rel(got, r["ref"]) <= TOL
+    srv.close()
