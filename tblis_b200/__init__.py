@@ -342,9 +342,45 @@ def dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
 
 
+class PreparedBatch:
+    """The C-ABI arrays of a batch built once, so repeated runs of the same
+    tensors (an iterative solver's step) cost one library call."""
+
+    def __init__(self, items):
+        n = len(items)
+        self.views = []
+        self.TA = (tblis_tensor * n)()
+        self.TB = (tblis_tensor * n)()
+        self.TC = (tblis_tensor * n)()
+        self.IA = (ctypes.c_char_p * n)()
+        self.IB = (ctypes.c_char_p * n)()
+        self.IC = (ctypes.c_char_p * n)()
+        for i, (alpha, A, ia, B, ib, beta, C, ic) in enumerate(items):
+            va, vb, vc = _View(A, alpha), _View(B), _View(C, beta)
+            self.views.append((va, vb, vc))
+            self.TA[i], self.TB[i], self.TC[i] = va.t, vb.t, vc.t
+            self.IA[i], self.IB[i], self.IC[i] = _labels(ia), _labels(ib), _labels(ic)
+        self.betas = [float(it[5]) for it in items]
+        self.n = n
+
+    def run(self):
+        # the library resets C's scalar after each call: restore beta
+        for i, b in enumerate(self.betas):
+            self.TC[i].scalar.data[0] = b
+        r = tblis_b200_report()
+        lib.tblis_b200_tensor_mult_batch(self.n, self.TA, self.IA, self.TB, self.IB, self.TC, self.IC,
+                                         ctypes.byref(r))
+        _check()
+        return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
 def mult_batch(items):
     """items: list of (alpha, A, idx_A, B, idx_B, beta, C, idx_C) with device
     tensors; all run in one grouped launch."""
+    return PreparedBatch(items).run()
+
+
+def _mult_batch_unprepared(items):
     n = len(items)
     views = []
     TA = (tblis_tensor * n)()

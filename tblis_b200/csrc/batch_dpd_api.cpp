@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace tb
 {
@@ -83,6 +85,41 @@ void run_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
     }
 }
 
+// everything a batch plan depends on, straight from the caller's descriptors
+// (lengths, strides, labels, and whether alpha is zero): a cache hit skips
+// all planning
+std::string batch_key(int count, const tblis_tensor* A, const label_type* const* idx_A,
+                      const tblis_tensor* B, const label_type* const* idx_B,
+                      const tblis_tensor* C, const label_type* const* idx_C)
+{
+    std::string key;
+    key.reserve((size_t)count*160);
+    for (int i = 0; i < count; i++)
+    {
+        const tblis_tensor* ts[3] = {&A[i], &B[i], &C[i]};
+        const label_type* ix[3] = {idx_A[i], idx_B[i], idx_C[i]};
+        for (int t = 0; t < 3; t++)
+        {
+            const unsigned nd = ts[t]->ndim;
+            key.push_back((char)nd);
+            key.append(reinterpret_cast<const char*>(ts[t]->len), nd*sizeof(len_type));
+            key.append(reinterpret_cast<const char*>(ts[t]->stride), nd*sizeof(stride_type));
+            if (nd) key.append(ix[t], nd);
+        }
+        key.push_back(A[i].scalar.data.d*B[i].scalar.data.d == 0.0 ? 'z' : 'n');
+    }
+    return key;
+}
+
+struct BatchPlanExtra
+{
+    // members that need no GEMM (alpha == 0 or an empty contracted extent)
+    std::vector<std::pair<int, Strided>> trivial;
+};
+
+std::mutex g_extra_mtx;
+std::map<const GroupedPlan*, BatchPlanExtra> g_extra;
+
 void run_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
                const tblis_tensor* B, const label_type* const* idx_B,
                tblis_tensor* C, const label_type* const* idx_C, tblis_b200_report* report)
@@ -93,68 +130,48 @@ void run_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
     TB_CHECK(count >= 0, TB_ERR_ARG, "batch: negative count");
     std::vector<const double*> ptrs(3*(size_t)count);
     std::vector<double> alphas(count), betas(count);
-    std::string key;
-    std::vector<GemmView> views(count);
-    std::vector<char> trivial(count, 0);
     for (int i = 0; i < count; i++)
     {
         TB_CHECK(A[i].type == TYPE_DOUBLE && B[i].type == TYPE_DOUBLE && C[i].type == TYPE_DOUBLE, TB_ERR_TYPE,
                  "batch: only double tensors");
-        for (const tblis_tensor* t : {&A[i], &B[i], (const tblis_tensor*)&C[i]})
-        {
-            i64 lo, hi;
-            tensor_extent(t->ndim, t->len, t->stride, lo, hi);
-            TB_CHECK(hi < lo || !t->data || pointer_kind(t->data) == MEM_DEVICE, TB_ERR_ARG,
-                     "batch: tensors must be in device memory");
-        }
-        views[i] = gemm_view(mult_groups(&A[i], idx_A[i], &B[i], idx_B[i], &C[i], idx_C[i]));
         ptrs[3*i] = static_cast<const double*>(A[i].data);
         ptrs[3*i + 1] = static_cast<const double*>(B[i].data);
         ptrs[3*i + 2] = static_cast<const double*>(C[i].data);
         alphas[i] = A[i].scalar.data.d*B[i].scalar.data.d;
         betas[i] = C[i].scalar.data.d;
-        const GemmView& v = views[i];
-        trivial[i] = alphas[i] == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
-        // the plan depends on shapes and strides only
-        for (const ivec* p : {&v.lenM, &v.lenN, &v.lenK, &v.lenL, &v.aM, &v.cM, &v.aK, &v.bK, &v.bN, &v.cN,
-                              &v.aL, &v.bL, &v.cL})
-        {
-            key.append(reinterpret_cast<const char*>(p->data()), p->size()*sizeof(i64));
-            key.push_back('|');
-        }
-        key.push_back(trivial[i] ? 't' : 'n');
-        key.push_back(v.pack_m_3d ? '1' : '0');
-        key.push_back(v.pack_n_3d ? '1' : '0');
-        key.push_back(v.pack_k_3d ? '1' : '0');
-        key.push_back(';');
     }
-
-    // trivial members: alpha == 0 or empty contracted extent -> set/scale C
-    for (int i = 0; i < count; i++)
-    {
-        const GemmView& v = views[i];
-        if (!trivial[i] || v.m*v.n*v.l == 0 || betas[i] == 1.0) continue;
-        Strided s;
-        ivec len, str;
-        for (size_t j = 0; j < v.lenM.size(); j++) { len.push_back(v.lenM[j]); str.push_back(v.cM[j]); }
-        for (size_t j = 0; j < v.lenN.size(); j++) { len.push_back(v.lenN[j]); str.push_back(v.cN[j]); }
-        for (size_t j = 0; j < v.lenL.size(); j++) { len.push_back(v.lenL[j]); str.push_back(v.cL[j]); }
-        TB_CHECK(len.size() <= (size_t)L1_MAX_DIM, TB_ERR_SIZE, "too many dimensions");
-        s.ndim = (int)len.size();
-        for (size_t j = 0; j < len.size(); j++) { s.len[j] = len[j]; s.stride[j] = str[j]; }
-        if (betas[i] == 0.0) l1_set<double>(static_cast<double*>(C[i].data), s, 0.0, st);
-        else l1_scale<double>(static_cast<double*>(C[i].data), s, betas[i], st);
-    }
-
+    const std::string key = batch_key(count, A, idx_A, B, idx_B, C, idx_C);
     auto plan = grouped_plan_cache().find(key);
     if (!plan)
     {
         auto p = std::make_shared<GroupedPlan>();
+        BatchPlanExtra extra;
         double flops = 0;
         for (int i = 0; i < count; i++)
         {
-            if (trivial[i]) continue;
-            const GemmView& v = views[i];
+            for (const tblis_tensor* t : {&A[i], &B[i], (const tblis_tensor*)&C[i]})
+            {
+                i64 lo, hi;
+                tensor_extent(t->ndim, t->len, t->stride, lo, hi);
+                TB_CHECK(hi < lo || !t->data || pointer_kind(t->data) == MEM_DEVICE, TB_ERR_ARG,
+                         "batch: tensors must be in device memory");
+            }
+            const GemmView v = gemm_view(mult_groups(&A[i], idx_A[i], &B[i], idx_B[i], &C[i], idx_C[i]));
+            const bool trivial = alphas[i] == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
+            if (trivial)
+            {
+                if (v.m*v.n*v.l == 0) continue;
+                Strided s;
+                ivec len, str;
+                for (size_t j = 0; j < v.lenM.size(); j++) { len.push_back(v.lenM[j]); str.push_back(v.cM[j]); }
+                for (size_t j = 0; j < v.lenN.size(); j++) { len.push_back(v.lenN[j]); str.push_back(v.cN[j]); }
+                for (size_t j = 0; j < v.lenL.size(); j++) { len.push_back(v.lenL[j]); str.push_back(v.cL[j]); }
+                TB_CHECK(len.size() <= (size_t)L1_MAX_DIM, TB_ERR_SIZE, "too many dimensions");
+                s.ndim = (int)len.size();
+                for (size_t j = 0; j < len.size(); j++) { s.len[j] = len[j]; s.stride[j] = str[j]; }
+                extra.trivial.push_back({i, s});
+                continue;
+            }
             GroupTables base;
             base.M = v.m; base.N = v.n; base.K = v.k;
             base.a_m.resize(v.m); base.c_m.resize(v.m); base.a_k.resize(v.k); base.b_k.resize(v.k);
@@ -184,7 +201,23 @@ void run_batch(int count, const tblis_tensor* A, const label_type* const* idx_A,
         p->flops = flops;
         p->nslots = 3*count;
         p->finalize(st);
+        {
+            std::lock_guard<std::mutex> lk(g_extra_mtx);
+            g_extra[p.get()] = std::move(extra);
+        }
         plan = grouped_plan_cache().insert(key, p);
+    }
+
+    // trivial members: set/scale C
+    {
+        std::lock_guard<std::mutex> lk(g_extra_mtx);
+        for (auto& t : g_extra[plan.get()].trivial)
+        {
+            const int i = t.first;
+            if (betas[i] == 1.0) continue;
+            if (betas[i] == 0.0) l1_set<double>(static_cast<double*>(C[i].data), t.second, 0.0, st);
+            else l1_scale<double>(static_cast<double*>(C[i].data), t.second, betas[i], st);
+        }
     }
     grouped_run(*plan, ptrs.data(), alphas.data(), betas.data(), st);
     for (int i = 0; i < count; i++)

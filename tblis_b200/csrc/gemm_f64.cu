@@ -345,14 +345,26 @@ gemm_f64_kernel(const GemmF64Args p)
 template <int BM, int BN, int WM, int WN, int STAGES, int MINB>
 __global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
 gemm_f64_grouped_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__ tile_begin,
-                        int ngroups, i64 total_tiles)
+                        int ngroups, i64 total_tiles, unsigned long long* __restrict__ counter)
 {
     extern __shared__ __align__(16) double smem[];
     i64* sAm = reinterpret_cast<i64*>(smem + tile_smem_doubles<BM, BN>(STAGES));
     i64* sBn = sAm + BM;
     i64* sCm = sBn + BN;
     i64* sCn = sCm + BM;
-    for (i64 tile = blockIdx.x; tile < total_tiles; tile += gridDim.x)
+    __shared__ i64 s_next;
+    // tiles come from a global counter (groups are ordered longest K first,
+    // so the longest tiles start first and the short ones fill in behind);
+    // without a counter, static striding by the grid size
+    auto next_tile = [&](i64 cur) -> i64
+    {
+        if (!counter) return cur < 0 ? (i64)blockIdx.x : cur + gridDim.x;
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = (i64)atomicAdd(counter, 1ull);
+        __syncthreads();
+        return s_next;
+    };
+    for (i64 tile = next_tile(-1); tile < total_tiles; tile = next_tile(tile))
     {
         int lo = 0, hi = ngroups - 1;
         while (lo < hi)
@@ -412,7 +424,7 @@ struct Variant
 {
     int bm, bn;
     void (*launch)(const GemmF64Args&, dim3, cudaStream_t, int amode, int bmode);
-    void (*grouped)(const GroupDesc*, const i64*, int, i64, cudaStream_t);
+    void (*grouped)(const GroupDesc*, const i64*, int, i64, unsigned long long*, cudaStream_t);
 };
 
 template <int BM_, int BN_, int WM, int WN, int STAGES, int MINB>
@@ -434,7 +446,8 @@ struct Config
         kern<<<grid, NT, bytes, s>>>(a);
         check_launch("gemm_f64_kernel");
     }
-    static void grouped(const GroupDesc* g, const i64* tb, int ngroups, i64 total, cudaStream_t s)
+    static void grouped(const GroupDesc* g, const i64* tb, int ngroups, i64 total, unsigned long long* ctr,
+                        cudaStream_t s)
     {
         auto kern = gemm_f64_grouped_kernel<BM_, BN_, WM, WN, STAGES, MINB>;
         const size_t bytes = (size_t)tile_smem_doubles<BM_, BN_>(STAGES)*sizeof(double) +
@@ -445,7 +458,7 @@ struct Config
         TB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         const i64 grid = std::min<i64>(total, (i64)sms*MINB);
         if (grid <= 0) return;
-        kern<<<(unsigned)grid, NT, bytes, s>>>(g, tb, ngroups, total);
+        kern<<<(unsigned)grid, NT, bytes, s>>>(g, tb, ngroups, total, ctr);
         check_launch("gemm_f64_grouped_kernel");
     }
     static void launch(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
@@ -500,11 +513,12 @@ void gemm_f64_variant_tile(int variant, int& bm, int& bn)
 }
 
 void gemm_f64_grouped_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups,
-                             i64 total_tiles, int variant, cudaStream_t stream)
+                             i64 total_tiles, int variant, cudaStream_t stream, unsigned long long* d_counter)
 {
     if (ngroups <= 0 || total_tiles <= 0) return;
     const Variant& v = kVariants[std::max(1, std::min(variant, kNumVariants)) - 1];
-    v.grouped(d_groups, d_tile_begin, ngroups, total_tiles, stream);
+    if (d_counter) TB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), stream));
+    v.grouped(d_groups, d_tile_begin, ngroups, total_tiles, d_counter, stream);
 }
 
 i64 gemm_f64_tile_m() { return 128; }

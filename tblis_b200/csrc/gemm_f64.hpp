@@ -50,9 +50,12 @@ struct GroupDesc
 
 int gemm_f64_num_variants();
 void gemm_f64_variant_tile(int variant, int& bm, int& bn);
-// tile_begin[g] = first global tile of group g (tiles of BM x BN of the variant)
+// tile_begin[g] = first global tile of group g (tiles of BM x BN of the variant).
+// d_counter (optional, one 64-bit word of device memory, zeroed by the launch)
+// turns the static tile striding into a dynamic queue.
 void gemm_f64_grouped_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups,
-                             i64 total_tiles, int variant, cudaStream_t stream);
+                             i64 total_tiles, int variant, cudaStream_t stream,
+                             unsigned long long* d_counter = nullptr);
 
 i64 gemm_f64_tile_m();
 i64 gemm_f64_tile_n();

@@ -74,6 +74,9 @@ bool grouped_use_graphs()
 void GroupedPlan::finalize(cudaStream_t st)
 {
     const i64 BK = gemm_f64_tile_k();
+    // longest K first: with the dynamic tile queue the longest tiles start first
+    std::stable_sort(groups.begin(), groups.end(),
+                     [](const GroupTables& a, const GroupTables& b) { return a.K > b.K; });
     // device tables: for each group a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs,
     // then for each segment a_m, a_k, b_k, b_n, a_kbs, b_kbs
     std::vector<i64> host;
@@ -165,6 +168,7 @@ void GroupedPlan::finalize(cudaStream_t st)
         TB_CUDA(cudaMalloc(&d_tile_begin, all.size()*sizeof(i64)));
         TB_CUDA(cudaMemcpy(d_tile_begin, all.data(), all.size()*sizeof(i64), cudaMemcpyHostToDevice));
     }
+    TB_CUDA(cudaMalloc(&d_counter, sizeof(unsigned long long)));
     if (!groups.empty())
     {
         TB_CUDA(cudaMalloc(&d_descs, groups.size()*sizeof(GroupDesc)));
@@ -183,6 +187,7 @@ GroupedPlan::~GroupedPlan()
     if (d_segs) cudaFree(d_segs);
     if (d_tile_begin) cudaFree(d_tile_begin);
     if (d_descs) cudaFree(d_descs);
+    if (d_counter) cudaFree(d_counter);
     if (h_descs) cudaFreeHost(h_descs);
 }
 
@@ -266,10 +271,10 @@ static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* 
     for (int v = 1; v <= gemm_f64_num_variants(); v++)
     {
         gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st);     // warm-up
+                                plan.total_tiles[v - 1], v, st, plan.d_counter);     // warm-up
         TB_CUDA(cudaEventRecord(e0, st));
         gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st);
+                                plan.total_tiles[v - 1], v, st, plan.d_counter);
         TB_CUDA(cudaEventRecord(e1, st));
         TB_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
@@ -310,7 +315,7 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
                 try
                 {
                     gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                            plan.total_tiles[v - 1], v, cs);
+                                            plan.total_tiles[v - 1], v, cs, plan.d_counter);
                 }
                 catch (const error&) { ok = false; }
             }
@@ -338,7 +343,7 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
         TB_CUDA(cudaMemcpyAsync(plan.d_descs, plan.h_descs, plan.groups.size()*sizeof(GroupDesc),
                                 cudaMemcpyHostToDevice, st));
         gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st);
+                                plan.total_tiles[v - 1], v, st, plan.d_counter);
     }
     TB_CUDA(cudaEventRecord(plan.last_use, st));
 }

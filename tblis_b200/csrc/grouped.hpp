@@ -48,6 +48,7 @@ struct GroupedPlan
     std::vector<i64> total_tiles;
     i64* d_tile_begin = nullptr;              // all variants, concatenated
     GroupDesc* d_descs = nullptr;
+    unsigned long long* d_counter = nullptr;  // dynamic tile queue
     GroupDesc* h_descs = nullptr;             // pinned
     int variant = 0;                          // tuned tile configuration
     cudaGraphExec_t graph = nullptr;

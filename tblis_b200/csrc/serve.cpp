@@ -63,9 +63,11 @@ struct Slot
     std::vector<int64_t> reqs;
     bool busy = false;
     i64 footprint = 0;
+    unsigned long long* counter = nullptr;   // dynamic tile queue of the grouped launch
 };
 
 constexpr int kVariant = 4;          // 64 x 64 tiles: every batch uses the same tile shape
+constexpr i64 kDenseTiles = 2*148;   // requests with this many 64x64 tiles run as their own launch
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -99,6 +101,7 @@ struct Server
         {
             TB_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
             TB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+            TB_CUDA(cudaMalloc(&s.counter, sizeof(unsigned long long)));
         }
         worker = std::thread([this] { loop(); });
     }
@@ -117,6 +120,7 @@ struct Server
             if (s.hbuf) cudaFreeHost(s.hbuf);
             if (s.dbuf_) cudaFree(s.dbuf_);
             if (s.done) cudaEventDestroy(s.done);
+            if (s.counter) cudaFree(s.counter);
             if (s.stream) cudaStreamDestroy(s.stream);
         }
     }
@@ -183,7 +187,10 @@ struct Server
         return e;
     }
 
-    // builds one batch into a slot's staging buffer and launches it
+    // builds one batch into a slot's staging buffer and launches it: requests
+    // large enough to fill the GPU run as their own dense launch (with split-K
+    // where it pays), the rest are folded into one grouped launch whose tiles
+    // are handed out longest-K first
     void launch(Slot& s, std::vector<Request*>& batch)
     {
         cudaStream_t st = s.stream;
@@ -191,13 +198,15 @@ struct Server
         {
             Request* r;
             GemmView v;
-            bool trivial;
+            bool trivial, dense;
             double alpha, beta;
         };
         std::vector<Prep> prep;
         size_t table_elems = 0;
         size_t ngroups = 0;
         const i64 BK = gemm_f64_tile_k();
+        int bm, bn;
+        gemm_f64_variant_tile(kVariant, bm, bn);
         for (Request* r : batch)
         {
             try
@@ -206,18 +215,22 @@ struct Server
                                                    &r->C, r->idx[2].c_str()));
                 const double alpha = r->A.scalar.data.d*r->B.scalar.data.d, beta = r->C.scalar.data.d;
                 const bool trivial = alpha == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
+                const bool dense = !trivial && ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn)*v.l >= kDenseTiles;
                 if (!trivial)
                 {
-                    table_elems += 2*v.m + 2*v.n + 2*v.k + 2*((v.k + BK - 1)/BK) + 8;
-                    ngroups += v.l;
+                    table_elems += 2*v.m + 2*v.n + 2*v.k + 2*((v.k + BK - 1)/BK) + 3*v.l + 8;
+                    if (!dense) ngroups += v.l;
                 }
-                prep.push_back({r, v, trivial, alpha, beta});
+                prep.push_back({r, v, trivial, dense, alpha, beta});
             }
             catch (const error& e)
             {
                 r->state = 3; r->err = e.code; r->msg = e.what();
             }
         }
+        // longest K first in the grouped launch
+        std::stable_sort(prep.begin(), prep.end(), [](const Prep& a, const Prep& b) { return a.v.k > b.v.k; });
+
         const size_t tab_bytes = align_up(table_elems*sizeof(i64));
         const size_t desc_bytes = align_up(ngroups*sizeof(GroupDesc));
         const size_t tb_bytes = align_up((ngroups + 1)*sizeof(i64));
@@ -243,12 +256,12 @@ struct Server
 
         size_t pos = 0, g = 0;
         i64 tiles = 0;
-        int bm, bn;
-        gemm_f64_variant_tile(kVariant, bm, bn);
         std::vector<i64> bs;
+        std::vector<GemmF64Args> dense;
         for (Prep& p : prep)
         {
             const GemmView& v = p.v;
+            if (p.r->state == 3) continue;
             if (p.trivial)
             {
                 if (v.m*v.n*v.l == 0 || p.beta == 1.0) continue;
@@ -297,16 +310,33 @@ struct Server
             };
             const i64* a_kbs = kbs(ha_k);
             const i64* b_kbs = kbs(hb_k);
-            std::vector<i64> al(v.l), bl(v.l), cl(v.l);
-            fill_block_scatter(v.lenL, v.aL, 1, 0, v.l, al.data(), bs.data(), false);
-            fill_block_scatter(v.lenL, v.bL, 1, 0, v.l, bl.data(), bs.data(), false);
-            fill_block_scatter(v.lenL, v.cL, 1, 0, v.l, cl.data(), bs.data(), false);
+            i64* hal = htab + pos;
+            const i64* a_l = put(v.lenL, v.aL, v.l, false);
+            i64* hbl = htab + pos;
+            const i64* b_l = put(v.lenL, v.bL, v.l, false);
+            i64* hcl = htab + pos;
+            const i64* c_l = put(v.lenL, v.cL, v.l, false);
+            if (p.dense)
+            {
+                GemmF64Args a = {};
+                a.A = static_cast<const double*>(p.r->A.data);
+                a.B = static_cast<const double*>(p.r->B.data);
+                a.C = static_cast<double*>(p.r->C.data);
+                a.a_m = a_m; a.a_k = a_k; a.b_k = b_k; a.b_n = b_n; a.c_m = c_m; a.c_n = c_n;
+                a.a_l = a_l; a.b_l = b_l; a.c_l = c_l; a.a_kbs = a_kbs; a.b_kbs = b_kbs;
+                a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;
+                a.alpha = p.alpha; a.beta = p.beta;
+                a.amode = v.amode; a.bmode = v.bmode;
+                a.variant = kVariant;
+                dense.push_back(a);
+                continue;
+            }
             for (i64 l = 0; l < v.l; l++)
             {
                 GroupDesc& d = hdesc[g];
-                d.A = static_cast<const double*>(p.r->A.data) + al[l];
-                d.B = static_cast<const double*>(p.r->B.data) + bl[l];
-                d.C = static_cast<double*>(p.r->C.data) + cl[l];
+                d.A = static_cast<const double*>(p.r->A.data) + hal[l];
+                d.B = static_cast<const double*>(p.r->B.data) + hbl[l];
+                d.C = static_cast<double*>(p.r->C.data) + hcl[l];
                 d.a_m = a_m; d.a_k = a_k; d.b_k = b_k; d.b_n = b_n; d.c_m = c_m; d.c_n = c_n;
                 d.a_kbs = a_kbs; d.b_kbs = b_kbs;
                 d.M = v.m; d.N = v.n; d.K = v.k;
@@ -318,10 +348,16 @@ struct Server
                 g++;
             }
         }
-        if (g > 0)
-        {
+        if (pos > 0 || g > 0)
             TB_CUDA(cudaMemcpyAsync(s.dbuf_, s.hbuf, need, cudaMemcpyHostToDevice, st));
-            gemm_f64_grouped_launch(ddesc, dtb, (int)g, tiles, kVariant, st);
+        if (g > 0)
+            gemm_f64_grouped_launch(ddesc, dtb, (int)g, tiles, kVariant, st, s.counter);
+        for (GemmF64Args& a : dense)
+        {
+            a.splits = gemm_f64_choose_splits(a.M, a.N, a.K, a.L, device_sm_count());
+            dbuf ws(gemm_f64_workspace_bytes(a.M, a.N, a.L, a.splits), st);
+            a.partial = ws.as<double>();
+            gemm_f64_launch(a, st);
         }
         TB_CUDA(cudaEventRecord(s.done, st));
     }
