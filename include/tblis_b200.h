@@ -282,7 +282,9 @@ int tblis_b200_tensor_mult_batch(int count, const tblis_tensor* A, const label_t
  * thread admits them while their operand footprint (A, B and C extents) fits
  * the HBM budget, folds every admitted request into one grouped launch and
  * keeps up to `slots` launches in flight on separate streams, so requests that
- * arrive while others run start as soon as a slot and budget free up. A
+ * arrive while others run start as soon as a slot and budget free up. Large
+ * requests whose tolerance is at least 1e-13 run on the Ozaki INT8 path with
+ * the slice count chosen from that tolerance; the rest run in FP64. A
  * request's result is the same alone and in any mix (every output tile is
  * computed by one CTA with a fixed k order). Tensors must be in device memory
  * and stay valid until the request completes; the tensor descriptors are
@@ -298,6 +300,7 @@ typedef struct tblis_b200_server_stats
     double mean_batch;               /* requests per launch */
     int max_concurrent_batches;      /* most launches seen in flight at once */
     double p50_ms, p99_ms, max_ms;   /* submit-to-completion latency */
+    int64_t ozaki;                   /* requests run on the INT8 Ozaki path */
 } tblis_b200_server_stats;
 
 tblis_b200_server* tblis_b200_server_create(size_t hbm_budget_bytes, int slots);

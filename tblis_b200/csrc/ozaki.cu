@@ -658,49 +658,65 @@ int ozaki_error_flag()
     return v;
 }
 
-OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
-                       double alpha, double beta, double tol, int slices, cudaStream_t st)
+void ozaki_begin(OzakiJob& j, cudaStream_t st)
 {
-    OzakiResult res;
-    const i64 BMt = 128, BNt = 128, BKt = 16;
-    auto tab = gemm_tables(v, BMt, BNt, BKt, st);
+    const GemmView& v = j.v;
+    j.tab = gemm_tables(v, 128, 128, 16, st);
     TB_CHECK(v.m < (1ll << 31) && v.n < (1ll << 31) && v.k < (1ll << 31), TB_ERR_SIZE,
              "Ozaki path: extents beyond 2^31");
     TB_CHECK(v.l*OZ_SMAX < (1ll << 31), TB_ERR_SIZE, "Ozaki path: batch too large");
+    j.eA = dbuf((size_t)v.l*v.m*sizeof(int), st);
+    j.eB = dbuf((size_t)v.l*v.n*sizeof(int), st);
+    j.sA = dbuf((size_t)v.l*v.m*sizeof(double), st);
+    j.sB = dbuf((size_t)v.l*v.n*sizeof(double), st);
+    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode};
+    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode};
+    stats(oa, j.eA.as<int>(), j.sA.as<double>(), st);
+    stats(ob, j.eB.as<int>(), j.sB.as<double>(), st);
+}
 
-    OzOperand oa = {A, tab->a_m, tab->a_k, tab->a_l, v.m, v.k, v.l, v.amode};
-    OzOperand ob = {B, tab->b_n, tab->b_k, tab->b_l, v.n, v.k, v.l, v.bmode};
-
-    dbuf eA((size_t)v.l*v.m*sizeof(int), st), eB((size_t)v.l*v.n*sizeof(int), st);
-    dbuf sA((size_t)v.l*v.m*sizeof(double), st), sB((size_t)v.l*v.n*sizeof(double), st);
-    stats(oa, eA.as<int>(), sA.as<double>(), st);
-    stats(ob, eB.as<int>(), sB.as<double>(), st);
-
-    int S = slices;
+void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
+{
+    const GemmView& v = j.v;
+    int S = j.slices;
     if (S <= 0)
     {
         std::vector<int> heA(v.l*v.m), heB(v.l*v.n);
         std::vector<double> hsA(v.l*v.m), hsB(v.l*v.n);
-        TB_CUDA(cudaMemcpyAsync(heA.data(), eA.ptr, heA.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
-        TB_CUDA(cudaMemcpyAsync(heB.data(), eB.ptr, heB.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
-        TB_CUDA(cudaMemcpyAsync(hsA.data(), sA.ptr, hsA.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
-        TB_CUDA(cudaMemcpyAsync(hsB.data(), sB.ptr, hsB.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
-        TB_CUDA(cudaStreamSynchronize(st));
+        if (stats_ready)
+        {
+            // the statistics are complete: copy them without queueing behind
+            // the caller's stream
+            TB_CUDA(cudaMemcpy(heA.data(), j.eA.ptr, heA.size()*sizeof(int), cudaMemcpyDeviceToHost));
+            TB_CUDA(cudaMemcpy(heB.data(), j.eB.ptr, heB.size()*sizeof(int), cudaMemcpyDeviceToHost));
+            TB_CUDA(cudaMemcpy(hsA.data(), j.sA.ptr, hsA.size()*sizeof(double), cudaMemcpyDeviceToHost));
+            TB_CUDA(cudaMemcpy(hsB.data(), j.sB.ptr, hsB.size()*sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        else
+        {
+            TB_CUDA(cudaMemcpyAsync(heA.data(), j.eA.ptr, heA.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
+            TB_CUDA(cudaMemcpyAsync(heB.data(), j.eB.ptr, heB.size()*sizeof(int), cudaMemcpyDeviceToHost, st));
+            TB_CUDA(cudaMemcpyAsync(hsA.data(), j.sA.ptr, hsA.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
+            TB_CUDA(cudaMemcpyAsync(hsB.data(), j.sB.ptr, hsB.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
+            TB_CUDA(cudaStreamSynchronize(st));
+        }
         S = OZ_SMAX;
         for (int s = 1; s <= OZ_SMAX; s++)
         {
             // safety factor 4 between the estimate and the target
-            if (estimate_error(s, heA, hsA, v.k, heB, hsB, v.k)*4.0 <= tol) { S = s; break; }
+            if (estimate_error(s, heA, hsA, v.k, heB, hsB, v.k)*4.0 <= j.tol) { S = s; break; }
         }
-        res.est_error = estimate_error(S, heA, hsA, v.k, heB, hsB, v.k);
+        j.res.est_error = estimate_error(S, heA, hsA, v.k, heB, hsB, v.k);
     }
     TB_CHECK(S >= 1 && S <= OZ_SMAX, TB_ERR_ARG, "Ozaki slice count must be 1..8");
-    res.slices = S;
+    j.res.slices = S;
 
+    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode};
+    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode};
     const i64 kp = (v.k + 63)/64*64;       // row pitch: TMA strides and 16-byte digit stores
     dbuf pa((size_t)v.l*S*v.m*kp, st), pb((size_t)v.l*S*v.n*kp, st);
-    slice_dispatch(S, oa, eA.as<int>(), pa.as<signed char>(), kp, st);
-    slice_dispatch(S, ob, eB.as<int>(), pb.as<signed char>(), kp, st);
+    slice_dispatch(S, oa, j.eA.as<int>(), pa.as<signed char>(), kp, st);
+    slice_dispatch(S, ob, j.eB.as<int>(), pb.as<signed char>(), kp, st);
 
     const CUtensorMap ta = make_map(pa.as<signed char>(), v.k, v.m, v.l*S, kp, OZ_BM);
     const CUtensorMap tbm = make_map(pb.as<signed char>(), v.k, v.n, v.l*S, kp, OZ_BN);
@@ -710,17 +726,27 @@ OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, doub
     for (i64 k0 = 0; k0 < v.k; k0 += klimit)
     {
         OzGemmArgs g;
-        g.C = C;
-        g.c_m = tab->c_m; g.c_n = tab->c_n; g.c_l = tab->c_l;
-        g.eA = eA.as<int>(); g.eB = eB.as<int>();
+        g.C = j.C;
+        g.c_m = j.tab->c_m; g.c_n = j.tab->c_n; g.c_l = j.tab->c_l;
+        g.eA = j.eA.as<int>(); g.eB = j.eB.as<int>();
         g.M = v.m; g.N = v.n; g.K = v.k; g.L = v.l;
         g.k_begin = (int)k0;
         g.k_count = (int)std::min(klimit, v.k - k0);
-        g.alpha = alpha;
-        g.beta = k0 == 0 ? beta : 1.0;
+        g.alpha = j.alpha;
+        g.beta = k0 == 0 ? j.beta : 1.0;
         gemm_dispatch(S, ta, tbm, g, st);
     }
-    return res;
+}
+
+OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
+                       double alpha, double beta, double tol, int slices, cudaStream_t st)
+{
+    OzakiJob j;
+    j.v = v; j.A = A; j.B = B; j.C = C;
+    j.alpha = alpha; j.beta = beta; j.tol = tol; j.slices = slices;
+    ozaki_begin(j, st);
+    ozaki_end(j, st, false);
+    return j.res;
 }
 
 } // namespace tb

@@ -19,6 +19,7 @@
 #include "gemm_f64.hpp"
 #include "level1.hpp"
 #include "mult.hpp"
+#include "ozaki.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -56,6 +57,7 @@ struct Slot
 {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t stats = nullptr;     // Ozaki statistics of the current batch done
     char* hbuf = nullptr;            // pinned staging
     size_t hcap = 0;
     char* dbuf_ = nullptr;           // device copy
@@ -68,6 +70,14 @@ struct Slot
 
 constexpr int kVariant = 4;          // 64 x 64 tiles: every batch uses the same tile shape
 constexpr i64 kDenseTiles = 2*148;   // requests with this many 64x64 tiles run as their own launch
+
+// large contractions whose requested tolerance allows it run on the INT8
+// tensor cores (Ozaki slices, slice count chosen from the tolerance)
+bool use_ozaki(const GemmView& v, double tol)
+{
+    return tol >= 1e-13 && v.m >= 256 && v.n >= 256 && v.k >= 512 &&
+           2.0*(double)v.m*(double)v.n*(double)v.k*(double)v.l >= 4e9;
+}
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -87,7 +97,7 @@ struct Server
     int device = 0;
     int max_batch = 256;
     // statistics
-    int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_requests = 0;
+    int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_requests = 0, n_ozaki = 0;
     int max_running = 0;
     std::vector<double> latencies;
     std::string fatal;
@@ -102,6 +112,7 @@ struct Server
             TB_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
             TB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
             TB_CUDA(cudaMalloc(&s.counter, sizeof(unsigned long long)));
+            TB_CUDA(cudaEventCreateWithFlags(&s.stats, cudaEventDisableTiming));
         }
         worker = std::thread([this] { loop(); });
     }
@@ -121,6 +132,7 @@ struct Server
             if (s.dbuf_) cudaFree(s.dbuf_);
             if (s.done) cudaEventDestroy(s.done);
             if (s.counter) cudaFree(s.counter);
+            if (s.stats) cudaEventDestroy(s.stats);
             if (s.stream) cudaStreamDestroy(s.stream);
         }
     }
@@ -198,7 +210,7 @@ struct Server
         {
             Request* r;
             GemmView v;
-            bool trivial, dense;
+            bool trivial, dense, ozaki;
             double alpha, beta;
         };
         std::vector<Prep> prep;
@@ -215,13 +227,15 @@ struct Server
                                                    &r->C, r->idx[2].c_str()));
                 const double alpha = r->A.scalar.data.d*r->B.scalar.data.d, beta = r->C.scalar.data.d;
                 const bool trivial = alpha == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
-                const bool dense = !trivial && ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn)*v.l >= kDenseTiles;
-                if (!trivial)
+                const bool ozaki = !trivial && use_ozaki(v, r->tol);
+                const bool dense = !trivial && !ozaki &&
+                                   ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn)*v.l >= kDenseTiles;
+                if (!trivial && !ozaki)
                 {
                     table_elems += 2*v.m + 2*v.n + 2*v.k + 2*((v.k + BK - 1)/BK) + 3*v.l + 8;
                     if (!dense) ngroups += v.l;
                 }
-                prep.push_back({r, v, trivial, dense, alpha, beta});
+                prep.push_back({r, v, trivial, dense, ozaki, alpha, beta});
             }
             catch (const error& e)
             {
@@ -262,6 +276,7 @@ struct Server
         {
             const GemmView& v = p.v;
             if (p.r->state == 3) continue;
+            if (p.ozaki) continue;
             if (p.trivial)
             {
                 if (v.m*v.n*v.l == 0 || p.beta == 1.0) continue;
@@ -348,6 +363,21 @@ struct Server
                 g++;
             }
         }
+        // Ozaki members: statistics first, so the wait below covers only them
+        std::vector<std::unique_ptr<OzakiJob>> jobs;
+        for (Prep& p : prep)
+        {
+            if (!p.ozaki || p.r->state == 3) continue;
+            auto j = std::make_unique<OzakiJob>();
+            j->v = p.v;
+            j->A = static_cast<const double*>(p.r->A.data);
+            j->B = static_cast<const double*>(p.r->B.data);
+            j->C = static_cast<double*>(p.r->C.data);
+            j->alpha = p.alpha; j->beta = p.beta; j->tol = p.r->tol;
+            ozaki_begin(*j, st);
+            jobs.push_back(std::move(j));
+        }
+        if (!jobs.empty()) TB_CUDA(cudaEventRecord(s.stats, st));
         if (pos > 0 || g > 0)
             TB_CUDA(cudaMemcpyAsync(s.dbuf_, s.hbuf, need, cudaMemcpyHostToDevice, st));
         if (g > 0)
@@ -358,6 +388,13 @@ struct Server
             dbuf ws(gemm_f64_workspace_bytes(a.M, a.N, a.L, a.splits), st);
             a.partial = ws.as<double>();
             gemm_f64_launch(a, st);
+        }
+        if (!jobs.empty())
+        {
+            TB_CUDA(cudaEventSynchronize(s.stats));
+            for (auto& j : jobs) ozaki_end(*j, st, true);
+            std::lock_guard<std::mutex> lk(mtx);
+            n_ozaki += (int64_t)jobs.size();
         }
         TB_CUDA(cudaEventRecord(s.done, st));
     }
@@ -516,6 +553,7 @@ int tblis_b200_server_get_stats(tblis_b200_server* srv, tblis_b200_server_stats*
         out->mean_batch = s.n_batches ? (double)s.batched_requests/s.n_batches : 0.0;
         out->max_concurrent_batches = s.max_running;
         out->queued = (int64_t)s.queue.size();
+        out->ozaki = s.n_ozaki;
         std::vector<double> l = s.latencies;
         if (!l.empty())
         {

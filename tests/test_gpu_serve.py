@@ -139,3 +139,44 @@ def test_failed_request_is_isolated(cuda):
         got = view_of(r["Cb"].cpu().numpy(), r["C"][1].shape, r["C"][2])
         assert normwise_rel(got, r["ref"]) <= TOL
     srv.close()
+
+
+def test_tolerant_requests_use_int8_slices(cuda):
+    """Large requests whose tolerance allows it run as Ozaki INT8 slices: the
+    result meets each request's tolerance, is the same alone and in a mix,
+    and a zero tolerance keeps the plain FP64 path."""
+    import torch
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(7)
+    m, n, k = 1024, 768, 4096
+    a = torch.empty((m, k), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    b = torch.empty((k, n), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    exact = a @ b
+    srv = tb.Server(slots=3)
+    outs = {}
+    for tol in (1e-10, 1e-13, 0.0):
+        c = torch.zeros((m, n), dtype=torch.float64, device=cuda)
+        srv.wait(srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij", tolerance=tol))
+        outs[tol] = c
+    torch.cuda.synchronize()
+    assert srv.stats()["ozaki"] == 2
+    for tol in (1e-10, 1e-13):
+        err = (torch.linalg.norm(outs[tol] - exact)/torch.linalg.norm(exact)).item()
+        assert err <= tol
+    assert (torch.linalg.norm(outs[0.0] - exact)/torch.linalg.norm(exact)).item() <= 1e-14
+    # the same request among small ones
+    small = _requests(torch, cuda, range(9800, 9830), max_len=8)
+    c = torch.zeros((m, n), dtype=torch.float64, device=cuda)
+    ids = [srv.submit(*r["args"]) for r in small[:15]]
+    mid = srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij", tolerance=1e-13)
+    ids += [srv.submit(*r["args"]) for r in small[15:]]
+    for i in ids + [mid]:
+        srv.wait(i)
+    torch.cuda.synchronize()
+    assert torch.equal(c, outs[1e-13])
+    for r in small:
+        got = view_of(r["Cb"].cpu().numpy(), r["C"][1].shape, r["C"][2])
+        assert normwise_rel(got, r["ref"]) <= TOL
+    assert srv.stats()["ozaki"] == 3
+    srv.close()
