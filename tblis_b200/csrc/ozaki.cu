@@ -12,9 +12,11 @@
 //     the strided tensor through the GEMM view's scatter vectors;
 //  3. one fused tcgen05 kernel per 128x64 output tile: for every k block,
 //     TMA brings the S planes of A and B into shared memory and one thread
-//     issues tcgen05.mma.kind::i8 for every slice pair (p, q) with
+//     issues tcgen05.mma.kind::i8 for the slice pairs (p, q) with
 //     p + q <= S + 1, accumulating pairs of equal p + q ("diagonal" d) in
-//     their own INT32 accumulator in tensor memory (exact: |sum| <=
+//     their own INT32 accumulator in tensor memory (slice p of A meets
+//     B slices 1..S+1-p in one wide MMA, the B planes and the diagonals
+//     being adjacent in shared and tensor memory) (exact: |sum| <=
 //     (d-1)*K*64^2 < 2^31 for the K of one launch); the epilogue sums the
 //     diagonals in FP64 with weights 2^(2-7d), applies 2^(e_m + f_n),
 //     alpha and beta, and scatters into C through C's scatter vectors.
@@ -165,9 +167,13 @@ __device__ __forceinline__ uint64_t sdesc_sw32(const void* p)
          | (6ull << 61);                       // SWIZZLE_32B
 }
 
-// instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = 64
-constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
-                              ((uint32_t)(OZ_BM >> 4) << 24);
+// instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = n
+// (a multiple of 16 up to 256)
+__host__ __device__ constexpr uint32_t idesc_i8(int n)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+}
+static_assert(idesc_i8(256) >> 17 == ((256u >> 3) | ((OZ_BM >> 4) << 7)), "N field is 6 bits wide");
 
 struct OzGemmArgs
 {
@@ -278,19 +284,22 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 if (!mbar_wait(&full[s], (kt/STAGES) & 1, abort_flag)) break;
                 tc_fence_after();
                 const unsigned char* st = smem + s*STAGE_BYTES;
+                // slice pa of A against B slices 1..S+1-pa at once: the B
+                // tiles sit back to back in shared memory and the diagonals
+                // pa+1..S+1 they feed are adjacent accumulators, so one MMA
+                // of N = 64*(S+1-pa) columns (split at 256) covers the row
                 #pragma unroll
-                for (int d = 2; d <= S + 1; d++)
+                for (int pa = 1; pa <= S; pa++)
                 {
-                    const uint32_t acc_addr = tmem_base + (uint32_t)((d - 2)*OZ_BN);
+                    const uint64_t ad = sdesc_sw32(st + (pa - 1)*A_TILE);
                     #pragma unroll
-                    for (int pa = 1; pa <= S; pa++)
+                    for (int n0c = 0; n0c < (S + 1 - pa)*OZ_BN; n0c += 256)
                     {
-                        const int qb = d - pa;
-                        if (qb < 1 || qb > S) continue;
-                        const uint64_t ad = sdesc_sw32(st + (pa - 1)*A_TILE);
-                        const uint64_t bd = sdesc_sw32(st + S*A_TILE + (qb - 1)*B_TILE);
-                        const bool first = kt == 0 && pa == max(1, d - S);
-                        mma_i8(acc_addr, ad, bd, IDESC_I8, first ? 0u : 1u);
+                        const int nc = min(256, (S + 1 - pa)*OZ_BN - n0c);
+                        const uint64_t bd = sdesc_sw32(st + S*A_TILE + n0c*OZ_BK);
+                        const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*OZ_BN + n0c);
+                        // the pa = 1 row spans every diagonal: it starts the sums
+                        mma_i8(acc_addr, ad, bd, idesc_i8(nc), (kt == 0 && pa == 1) ? 0u : 1u);
                     }
                 }
                 mma_commit(&empty[s]);
