@@ -43,6 +43,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
     p.add_argument("--o", type=int, default=48, help="occupied extent (profiling runs use a smaller case)")
     p.add_argument("--v", type=int, default=160, help="virtual extent")
+    p.add_argument("--case", default=None, choices=["ring", "transpose"],
+                   help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
     a = p.parse_args()
     global O, V, FLOPS_LADDER, WORKLOAD
     if (a.o, a.v) != (O, V):
@@ -287,6 +289,10 @@ def main():
     stream = torch.cuda.current_stream()
     tb.set_stream(stream.cuda_stream)
 
+    if args.case:
+        print(json.dumps(single_case(torch, tb, dev, stream, args)))
+        return
+
     # --- headline workload: ladder with exponent spread --------------------------------
     A = spread_tensor(torch, [V, V, V, V], 1001 + rank, dev)
     B = spread_tensor(torch, [V, V, O, O], 1002 + rank, dev)
@@ -322,8 +328,12 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     k0 = tb.kernel_count()
+    tb.kernel_timer(True)
     total_ms, per = time_steps(torch, step, args.steps, stream)
     launches = tb.kernel_count() - k0
+    kname = "ozaki_gemm_kernel" if method == 2 else "gemm_f64_kernel"
+    k_total_ms, k_launches = tb.kernel_time(kname)
+    tb.kernel_timer(False)
     clocks = sampler.stop()
     if dist:
         t = torch.tensor([total_ms], device=dev)
@@ -358,19 +368,23 @@ def main():
         fp64_gflops = FLOPS_LADDER / (fp_kernel_ms * 1e-3) / 1e9
         extra["fp64_dmma_gflops"] = fp64_gflops
         extra["speedup_vs_fp64_path"] = value / world / fp64_gflops
-        kernel_ms = statistics.mean(per)
+        # the dominant kernel's own device time: CUDA events around each of its
+        # launches on the launching stream, inside the timed steps
+        launch_ms = k_total_ms / max(1, k_launches)
+        units_per_launch = args.steps / max(1, k_launches)    # ladder contractions per launch
         if method == 1:
-            achieved = FLOPS_LADDER / (kernel_ms * 1e-3) / 1e12
+            achieved = FLOPS_LADDER * units_per_launch / (launch_ms * 1e-3) / 1e12
             result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                                   "frac": achieved / fp64_peak, "traffic": None,
                                   "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor cores)",
-                                  "kernel": "gemm_f64_kernel"}
+                                  "kernel": "gemm_f64_kernel", "launch_ms": launch_ms,
+                                  "share_of_step": k_total_ms / total_ms}
         else:
             # the dominant kernel is the fused INT8 slice-pair GEMM: its work is
             # S(S+1)/2 INT8 GEMMs of m x n x k (2 ops per MAC)
             S = int(method_name.split("_")[2])
-            int8_ops = S * (S + 1) / 2 * FLOPS_LADDER
-            achieved = int8_ops / (kernel_ms * 1e-3) / 1e12
+            int8_ops = S * (S + 1) / 2 * FLOPS_LADDER * units_per_launch
+            achieved = int8_ops / (launch_ms * 1e-3) / 1e12
             i8peak = measure_int8_peak(torch, dev)
             src = "cuBLAS int8 GEMM 8192^3 (torch._int_mm) measured in this run"
             if not i8peak:
@@ -378,8 +392,12 @@ def main():
                 src = "2 x measured bf16 dense GEMM (MEASURED_PEAKS.json)"
             result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": i8peak, "unit": "TOP/s (int8)",
                                   "frac": achieved / i8peak, "traffic": None, "peak_source": src,
-                                  "kernel": "ozaki_gemm_kernel (whole step incl. slicing)",
-                                  "fp64_equivalent_tflops": FLOPS_LADDER / (kernel_ms * 1e-3) / 1e12}
+                                  "kernel": "ozaki_gemm_kernel", "launch_ms": launch_ms,
+                                  "share_of_step": k_total_ms / total_ms,
+                                  "fp64_equivalent_tflops_kernel": FLOPS_LADDER * units_per_launch /
+                                                                   (launch_ms * 1e-3) / 1e12}
+        if not args.no_extra:
+            extra["precision_variants"] = precision_variants(torch, tb, A, B, C, stream)
         del A, B, C
         torch.cuda.empty_cache()
 
@@ -401,6 +419,33 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def precision_variants(torch, tb, A, B, C, stream):
+    """The ladder under every arithmetic the library offers: plain FP64 DMMA,
+    Ozaki INT8 and BF16 slices with 3..8 slices, one TF32 and one BF16 pass.
+    Error = normwise relative difference to the FP64 DMMA result (which the
+    GPU tests pin to the FP64 oracle within 1e-13); rate = FP64-equivalent
+    GFLOP/s of the whole call (statistics, slicing and GEMM), mean of 2."""
+    Cref = torch.zeros_like(C)
+    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cref, "abij", method=1)
+    nref = torch.linalg.vector_norm(Cref).item()
+    runs = [("fp64_dmma", 1, 0)]
+    runs += [("ozaki_int8", 2, s) for s in range(3, 9)]
+    runs += [("ozaki_bf16", 3, s) for s in range(3, 9)]
+    runs += [("tf32_single_pass", 4, 1), ("bf16_single_pass", 5, 1)]
+    out = []
+    for name, method, slices in runs:
+        def call():
+            tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, slices=slices, tolerance=1e-12)
+        call()
+        torch.cuda.synchronize()
+        err = (torch.linalg.vector_norm(C - Cref) / nref).item()
+        total, _ = time_steps(torch, call, 2, stream)
+        out.append({"variant": name, "slices": slices, "normwise_rel_err": err,
+                    "gflops_fp64_equiv": FLOPS_LADDER * 2 / (total * 1e-3) / 1e9})
+    del Cref
+    return out
 
 
 def e2e_ladder(torch, tb, method, steps):
@@ -592,6 +637,36 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
             "arrival_window_s": arrivals_s,
             "serial_req_s": nreq / serial_s, "serial_gflops": total_flops / serial_s / 1e9,
             "throughput_vs_serial": serial_s / served_s}
+
+
+def single_case(torch, tb, dev, stream, args):
+    """One secondary kernel alone at extents o, v (for profiling captures):
+    ring C[aibj] += A[aeim]*B[mbej] (FP64 DMMA) or transpose D[ijab] = C[abij]."""
+    o, v = args.o, args.v
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+
+    def cm(shape):
+        return torch.empty(list(reversed(shape)), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g) \
+            .permute(*reversed(range(len(shape))))
+    if args.case == "ring":
+        A, B, C = cm([v, v, o, o]), cm([o, v, v, o]), cm([v, o, v, o])
+
+        def fn():
+            tb.mult_ex(1.0, A, "aeim", B, "mbej", 1.0, C, "aibj", method=1)
+        work, unit = 2.0 * v ** 3 * o ** 3 / 1e9, "GFLOP/s"
+    else:
+        C = cm([v, v, o, o])
+        D = torch.zeros((v, v, o, o), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
+
+        def fn():
+            tb.add(1.0, C, "abij", 0.0, D, "ijab")
+        work, unit = 2 * C.numel() * 8 / 1e9, "GB/s"
+    for _ in range(args.warmup):
+        fn()
+    total, _ = time_steps(torch, fn, args.steps, stream)
+    return {"case": args.case, "o": o, "v": v, "value": work * args.steps / (total * 1e-3), "unit": unit,
+            "ms_per_step": total / args.steps}
 
 
 def extra_workloads(torch, tb, dev, stream, peaks):

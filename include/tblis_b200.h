@@ -149,8 +149,10 @@ unsigned tblis_get_num_threads(void);
 void tblis_set_num_threads(unsigned num_threads);
 
 /* src/util/configs.h:11: returns a GPU configuration by name, or NULL.
- * Names: "b200_fp64" (default; FP64 DMMA), "b200_ozaki_i8" (INT8 Ozaki
- * slices on tcgen05, slice count chosen from the tolerance). */
+ * Names: "b200_fp64" (default; FP64 DMMA), "b200_ozaki_i8" and
+ * "b200_ozaki_bf16" (Ozaki INT8 / BF16 slices on tcgen05, slice count chosen
+ * from the tolerance), "b200_tf32" and "b200_bf16" (one low-precision pass
+ * with FP32 accumulation). */
 const tblis_config* tblis_get_config(const char* name);
 
 /* ---- extensions (no counterpart in the reference) ------------------------ */
@@ -176,7 +178,9 @@ double tblis_b200_config_get_tolerance(const tblis_config* cfg);
 /* Per-call options and report of the extended contraction entry point. */
 typedef struct tblis_b200_opts
 {
-    int method;          /* 0 = from cfg, 1 = FP64 DMMA, 2 = Ozaki INT8 */
+    int method;          /* 0 = from cfg, 1 = FP64 DMMA, 2 = Ozaki INT8 slices,
+                            3 = Ozaki BF16 slices, 4 = one TF32 pass, 5 = one
+                            BF16 pass (FP32 accumulation; no tolerance) */
     int slices;          /* Ozaki slice count; 0 = choose from tolerance */
     double tolerance;    /* normwise relative target; 0 = from cfg */
 } tblis_b200_opts;
@@ -218,6 +222,15 @@ int tblis_b200_mult_groups(const tblis_tensor* A, const label_type* idx_A,
 
 /* Number of kernels this library launched since the process started. */
 int64_t tblis_b200_kernel_count(void);
+
+/* Per-kernel device timing (no reference counterpart). While enabled, the
+ * library brackets each launch of its contraction and transpose kernels
+ * (gemm_f64_kernel, gemm_f64_grouped_kernel, ozaki_gemm_kernel, k_transpose,
+ * k_add_rows) with a CUDA event pair on the launching stream. Enabling or
+ * disabling clears the records; reading waits for the recorded launches and
+ * returns their summed device time and count for one kernel name. */
+int tblis_b200_kernel_timer(int enable);
+int tblis_b200_kernel_timer_read(const char* kernel, double* total_ms, int64_t* launches);
 
 /* ---- DPD (irrep block-sparse) tensors ------------------------------------ */
 

@@ -87,6 +87,8 @@ lib.tblis_b200_mult_groups.argtypes = [_P(tblis_tensor), ctypes.c_char_p, _P(tbl
                                        ctypes.c_char_p, _P(ctypes.c_int64)]
 lib.tblis_b200_mult_groups.restype = ctypes.c_int
 lib.tblis_b200_kernel_count.restype = ctypes.c_int64
+lib.tblis_b200_kernel_timer.argtypes = [ctypes.c_int]
+lib.tblis_b200_kernel_timer_read.argtypes = [ctypes.c_char_p, _P(ctypes.c_double), _P(ctypes.c_int64)]
 lib.tblis_b200_set_stream.argtypes = [ctypes.c_void_p]
 lib.tblis_b200_get_stream.restype = ctypes.c_void_p
 lib.tblis_b200_config_set_tolerance.argtypes = [ctypes.c_void_p, ctypes.c_double]
@@ -171,7 +173,9 @@ def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, cfg=None):
 
 
 def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, tolerance=0.0, cfg=None):
-    """mult with an explicit method (1 = FP64 DMMA, 2 = Ozaki INT8) and a report dict."""
+    """mult with an explicit method and a report dict. Methods: 1 = FP64 DMMA,
+    2 = Ozaki INT8 slices, 3 = Ozaki BF16 slices (slice count from the
+    tolerance unless given), 4 = one TF32 pass, 5 = one BF16 pass."""
     a, b, c = _View(A, alpha), _View(B), _View(C, beta)
     o = tblis_b200_opts(method, slices, tolerance)
     r = tblis_b200_report()
@@ -250,6 +254,20 @@ def _scalar_value(s, code):
 def kernel_count():
     """Kernels this library launched in this process."""
     return lib.tblis_b200_kernel_count()
+
+
+def kernel_timer(enable):
+    """Start (True) or stop (False) per-launch device timing of the contraction
+    and transpose kernels; either call clears the records."""
+    lib.tblis_b200_kernel_timer(1 if enable else 0)
+
+
+def kernel_time(kernel):
+    """(total device ms, launches) of one kernel name since kernel_timer(True)."""
+    ms, n = ctypes.c_double(0), ctypes.c_int64(0)
+    if lib.tblis_b200_kernel_timer_read(kernel.encode(), ctypes.byref(ms), ctypes.byref(n)):
+        _check()
+    return ms.value, n.value
 
 
 def set_stream(stream_handle):

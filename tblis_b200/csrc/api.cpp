@@ -21,6 +21,20 @@ namespace tb
 {
 
 std::atomic<int64_t> g_kernel_count{0};
+std::atomic<bool> g_ktimer_on{false};
+
+namespace
+{
+struct KtRecord { std::string name; cudaEvent_t a, b; };
+std::mutex g_kt_mtx;
+std::vector<KtRecord> g_kt;
+}
+
+void ktimer_push(const char* name, cudaEvent_t a, cudaEvent_t b)
+{
+    std::lock_guard<std::mutex> lk(g_kt_mtx);
+    g_kt.push_back({name, a, b});
+}
 
 namespace
 {
@@ -29,8 +43,13 @@ thread_local std::string t_err_msg;
 thread_local cudaStream_t t_stream = 0;
 unsigned g_num_threads = 1;
 
-tblis_config_s g_cfg_fp64 = {"b200_fp64", 1, 1e-12};
-tblis_config_s g_cfg_ozaki = {"b200_ozaki_i8", 2, 1e-12};
+tblis_config_s g_cfgs[] = {
+    {"b200_fp64", 1, 1e-12},
+    {"b200_ozaki_i8", 2, 1e-12},
+    {"b200_ozaki_bf16", 3, 1e-12},
+    {"b200_tf32", 4, 1e-12},
+    {"b200_bf16", 5, 1e-12},
+};
 }
 
 void set_last_error(int code, const char* msg)
@@ -500,8 +519,8 @@ void tblis_set_num_threads(unsigned n) { g_num_threads = n ? n : 1; }
 const tblis_config* tblis_get_config(const char* name)
 {
     if (!name) return nullptr;
-    if (!strcmp(name, g_cfg_fp64.name)) return &g_cfg_fp64;
-    if (!strcmp(name, g_cfg_ozaki.name)) return &g_cfg_ozaki;
+    for (auto& c : g_cfgs)
+        if (!strcmp(name, c.name)) return &c;
     return nullptr;
 }
 
@@ -560,5 +579,36 @@ int tblis_b200_mult_groups(const tblis_tensor* A, const label_type* idx_A,
 }
 
 int64_t tblis_b200_kernel_count(void) { return g_kernel_count.load(); }
+
+int tblis_b200_kernel_timer(int enable)
+{
+    std::lock_guard<std::mutex> lk(g_kt_mtx);
+    for (auto& r : g_kt) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    g_kt.clear();
+    g_ktimer_on.store(enable != 0);
+    return 0;
+}
+
+int tblis_b200_kernel_timer_read(const char* name, double* total_ms, int64_t* launches)
+{
+    return guarded([&]
+    {
+        TB_CHECK(name && total_ms && launches, TB_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(g_kt_mtx);
+        double t = 0.0;
+        int64_t n = 0;
+        for (auto& r : g_kt)
+        {
+            if (r.name != name) continue;
+            TB_CUDA(cudaEventSynchronize(r.b));
+            float ms = 0.f;
+            TB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+            t += ms;
+            n++;
+        }
+        *total_ms = t;
+        *launches = n;
+    });
+}
 
 } // extern "C"

@@ -19,7 +19,7 @@
 struct tblis_config_s
 {
     const char* name;
-    int method;        // 1 = FP64 DMMA, 2 = Ozaki INT8
+    int method;        // 1 = FP64 DMMA, 2 = Ozaki INT8, 3 = Ozaki BF16, 4 = TF32 pass, 5 = BF16 pass
     double tolerance;  // normwise relative target
 };
 
@@ -88,6 +88,30 @@ void ensure_device();
 // kernel launch accounting (every launch of this library's kernels)
 extern std::atomic<int64_t> g_kernel_count;
 inline void count_launch(int n = 1) { g_kernel_count.fetch_add(n, std::memory_order_relaxed); }
+
+// optional per-kernel device timing: while enabled, a TimedLaunch scope
+// around a launch records a CUDA event pair on the launching stream; the
+// pairs are read back (and the stream waited for) only on request
+extern std::atomic<bool> g_ktimer_on;
+void ktimer_push(const char* name, cudaEvent_t a, cudaEvent_t b);
+struct TimedLaunch
+{
+    const char* name;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    TimedLaunch(const char* n, cudaStream_t s) : name(n), st(s)
+    {
+        if (g_ktimer_on.load(std::memory_order_relaxed) && cudaEventCreate(&a) == cudaSuccess)
+            cudaEventRecord(a, st);
+    }
+    ~TimedLaunch()
+    {
+        if (!a) return;
+        cudaEvent_t b = nullptr;
+        if (cudaEventCreate(&b) == cudaSuccess && cudaEventRecord(b, st) == cudaSuccess) ktimer_push(name, a, b);
+        else { cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+    }
+};
 
 // checks the launch status right after a kernel launch
 inline void check_launch(const char* what)

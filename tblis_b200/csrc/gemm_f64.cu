@@ -443,6 +443,7 @@ struct Config
         auto kern = gemm_f64_kernel<BM_, BN_, WM, WN, STAGES, AM, BMd, MINB>;
         const size_t bytes = smem_bytes(AM, BMd);
         TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        TimedLaunch t("gemm_f64_kernel", s);
         kern<<<grid, NT, bytes, s>>>(a);
         check_launch("gemm_f64_kernel");
     }
@@ -458,6 +459,7 @@ struct Config
         TB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         const i64 grid = std::min<i64>(total, (i64)sms*MINB);
         if (grid <= 0) return;
+        TimedLaunch t("gemm_f64_grouped_kernel", s);
         kern<<<(unsigned)grid, NT, bytes, s>>>(g, tb, ngroups, total, ctr);
         check_launch("gemm_f64_grouped_kernel");
     }

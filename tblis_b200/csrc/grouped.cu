@@ -335,6 +335,7 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
     }
     if (plan.graph)
     {
+        TimedLaunch t("gemm_f64_grouped_kernel", st);
         TB_CUDA(cudaGraphLaunch(plan.graph, st));
         count_launch();
     }

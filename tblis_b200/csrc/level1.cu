@@ -471,6 +471,7 @@ void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strid
             i64 n0 = s.len[0];
             i64 segs = (nab/n0)*((n0 + SEG - 1)/SEG);
             int grid = l1_grid(segs, L1_THREADS/32);
+            TimedLaunch t("k_add_rows", st);
             if (b0) k_add_rows<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
             else k_add_rows<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
             check_launch("k_add_rows");
@@ -480,6 +481,7 @@ void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strid
         i64 outer = nab/(ab.len[pa]*ab.len[pb]);
         i64 ntiles = tp*tq*outer;
         int grid = (int)std::min<i64>(ntiles, 148*16);
+        TimedLaunch t("k_transpose", st);
         if (b0) k_transpose<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
         else k_transpose<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
         check_launch("k_transpose");

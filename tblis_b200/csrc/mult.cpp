@@ -130,11 +130,15 @@ void mult_dispatch(const tblis_config* cfg,
         {
             stage(sa, A, true, st);
             stage(sb, B, true, st);
-            if (method == 2)
+            TB_CHECK(method >= 1 && method <= 5, TB_ERR_ARG, "unknown contraction method");
+            if (method >= 2)
             {
+                // 2: Ozaki INT8 slices, 3: Ozaki BF16 slices, 4: one TF32 pass, 5: one BF16 pass
+                const int kind = method == 2 ? OZ_I8 : method == 4 ? OZ_TF32 : OZ_BF16;
                 OzakiResult r = ozaki_mult(v, static_cast<const double*>(sa.dptr),
                                            static_cast<const double*>(sb.dptr),
-                                           static_cast<double*>(sc.dptr), alpha, beta, tol, slices, st);
+                                           static_cast<double*>(sc.dptr), alpha, beta, tol, slices, st,
+                                           kind, method >= 4);
                 if (report) { report->slices = r.slices; report->est_error = r.est_error; }
             }
             else

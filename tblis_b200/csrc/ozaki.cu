@@ -25,10 +25,18 @@
 // digit extraction, the cross-diagonal summation and the alpha/beta update.
 // The slice count S is chosen per call from an a-priori estimate of the
 // normwise error (row maxima and norms of A and B) to meet the tolerance.
+//
+// The same kernel runs two more plane formats: BF16 planes holding the same
+// integer digits (tcgen05.mma.kind::f16, FP32 accumulators, exact while a
+// diagonal's sum stays below 2^24, so K is split over launches of at most
+// 2^24/(S*64^2) each), and a single low-precision pass (S = 1) whose plane
+// holds x' itself rounded to BF16 or TF32 (kind::f16 / kind::tf32, FP32
+// accumulation over the whole K) for callers who accept that error.
 #include "ozaki.hpp"
 #include "mult.hpp"
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -43,7 +51,7 @@ namespace
 
 constexpr int OZ_BM = 128;           // tile rows (TMEM lanes)
 constexpr int OZ_BN = 64;            // tile columns per diagonal accumulator
-constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step)
+constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step of any kind)
 constexpr int OZ_SMAX = 8;           // 8 diagonals x 64 columns = all 512 TMEM columns
 constexpr int OZ_THREADS = 192;      // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr int A_TILE = OZ_BM*OZ_BK;  // bytes of one A slice tile
@@ -131,12 +139,26 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+// one tcgen05.mma of the given kind (OZ_I8: s8 x s8 -> s32, OZ_BF16:
+// bf16 x bf16 -> f32, OZ_TF32: tf32 x tf32 -> f32), A and B in shared memory
+template <int KIND>
+__device__ __forceinline__ void mma_op(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
 {
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "setp.ne.b32 p, %4, 0;\n\t"
-                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-                 :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+    if constexpr (KIND == OZ_I8)
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+    else if constexpr (KIND == OZ_BF16)
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+    else
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "setp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
@@ -167,13 +189,20 @@ __device__ __forceinline__ uint64_t sdesc_sw32(const void* p)
          | (6ull << 61);                       // SWIZZLE_32B
 }
 
-// instruction descriptor: s8 x s8 -> s32, K-major A and B, M = 128, N = n
-// (a multiple of 16 up to 256)
-__host__ __device__ constexpr uint32_t idesc_i8(int n)
+// instruction descriptor, K-major A and B, M = 128, N = n (a multiple of 16
+// up to 256): accumulator format at bits 4-5 (s32 = 2, f32 = 1), A and B
+// formats at bits 7-9 and 10-12 (s8 = 1; bf16 = 1, tf32 = 2)
+__host__ __device__ constexpr uint32_t idesc_mma(int kind, int n)
 {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+    return (kind == OZ_I8 ? (2u << 4) | (1u << 7) | (1u << 10)
+          : kind == OZ_BF16 ? (1u << 4) | (1u << 7) | (1u << 10)
+          : (1u << 4) | (2u << 7) | (2u << 10)) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
 }
-static_assert(idesc_i8(256) >> 17 == ((256u >> 3) | ((OZ_BM >> 4) << 7)), "N field is 6 bits wide");
+static_assert(idesc_mma(OZ_I8, 256) >> 17 == ((256u >> 3) | ((OZ_BM >> 4) << 7)), "N field is 6 bits wide");
+
+// bytes of one element of the slice planes
+__host__ __device__ constexpr int elem_bytes(int kind) { return kind == OZ_I8 ? 1 : kind == OZ_BF16 ? 2 : 4; }
 
 struct OzGemmArgs
 {
@@ -181,8 +210,9 @@ struct OzGemmArgs
     const i64 *c_m, *c_n, *c_l;
     const int *eA, *eB;          // [l][m], [l][n] exponents
     i64 M, N, K, L;
-    int k_begin, k_count;        // k range of this launch (multiples of OZ_BK except the tail)
+    int k_begin, k_count;        // k range of this launch, in elements (multiples of the k step)
     double alpha, beta;
+    int wbase;                   // diagonal d carries weight 2^(wbase - 7d)
 };
 
 // TMEM columns for S diagonal accumulators of OZ_BN columns (a power of two >= 32)
@@ -193,12 +223,13 @@ struct TmemCols
     static constexpr uint32_t value = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 };
 
-template <int S, int STAGES>
+template <int S, int STAGES, int KIND>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   const OzGemmArgs p)
 {
     constexpr int STAGE_BYTES = S*(A_TILE + B_TILE);
+    constexpr int KE = OZ_BK/elem_bytes(KIND);       // k elements per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned base for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -217,7 +248,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     const i64 tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
     const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*OZ_BN);
     const int l = blockIdx.y;
-    const int kt_count = (p.k_count + OZ_BK - 1)/OZ_BK;
+    const int kt_count = (p.k_count + KE - 1)/KE;
 
     if (threadIdx.x == 0)
     {
@@ -256,7 +287,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 if (kt >= STAGES && !mbar_wait(&empty[s], ((kt/STAGES) & 1) ^ 1, abort_flag)) break;
                 unsigned char* st = smem + s*STAGE_BYTES;
                 mbar_expect_tx(&full[s], STAGE_BYTES);
-                const int kx = p.k_begin + kt*OZ_BK;
+                const int kx = (p.k_begin + kt*KE)*elem_bytes(KIND);     // byte coordinate
                 #pragma unroll
                 for (int q = 0; q < S; q++)
                     tma_load_3d(st + q*A_TILE, &tmA, &full[s], kx, m0, l*S + q);
@@ -299,7 +330,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         const uint64_t bd = sdesc_sw32(st + S*A_TILE + n0c*OZ_BK);
                         const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*OZ_BN + n0c);
                         // the pa = 1 row spans every diagonal: it starts the sums
-                        mma_i8(acc_addr, ad, bd, idesc_i8(nc), (kt == 0 && pa == 1) ? 0u : 1u);
+                        mma_op<KIND>(acc_addr, ad, bd, idesc_mma(KIND, nc), (kt == 0 && pa == 1) ? 0u : 1u);
                     }
                 }
                 mma_commit(&empty[s]);
@@ -332,9 +363,10 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             {
                 int r[16];
                 tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*OZ_BN + c*16), r);
-                const double w = ldexp(1.0, 2 - 7*d);
+                const double w = ldexp(1.0, p.wbase - 7*d);
                 #pragma unroll
-                for (int j = 0; j < 16; j++) v[j] += (double)r[j]*w;
+                for (int j = 0; j < 16; j++)
+                    v[j] += (KIND == OZ_I8 ? (double)r[j] : (double)__int_as_float(r[j]))*w;
             }
             if (rc >= 0 && ok)
             {
@@ -467,11 +499,45 @@ __device__ __forceinline__ void digits(double xs, signed char (&d)[S])
 
 constexpr int SL_T = 64;     // 64 rows x 64 k per block
 
-// writes the S digit planes of a 64x64 tile, out[(l*S + p)][r][k], pitch kp
-template <int S>
-__global__ void __launch_bounds__(256)
-oz_slice(const OzOperand o, const int* e_rows, signed char* out, i64 kp)
+// x' rounded to the nearest TF32 value (10 fraction bits), as FP32 bits
+__device__ __forceinline__ uint32_t to_tf32_bits(double xs)
 {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(__double2float_rn(xs)));
+    return r;
+}
+
+// plane element types: digits as integers (INT8, or BF16 holding the same
+// integers exactly) or, for a single pass, x' itself rounded to BF16 / TF32
+template <int KIND>
+struct PlaneElem;
+template <> struct PlaneElem<OZ_I8> { using T = signed char; };
+template <> struct PlaneElem<OZ_BF16> { using T = unsigned short; };
+template <> struct PlaneElem<OZ_TF32> { using T = uint32_t; };
+
+template <int KIND>
+__device__ __forceinline__ typename PlaneElem<KIND>::T digit_elem(int d)
+{
+    if constexpr (KIND == OZ_I8) return (signed char)d;
+    else if constexpr (KIND == OZ_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn((float)d));  // exact: |d| <= 64
+    else return __float_as_uint((float)d);
+}
+
+template <int KIND>
+__device__ __forceinline__ typename PlaneElem<KIND>::T single_elem(double xs)
+{
+    if constexpr (KIND == OZ_BF16) return __bfloat16_as_ushort(__double2bfloat16(xs));
+    else return to_tf32_bits(xs);
+}
+
+// writes the S planes of a 64x64 tile, out[(l*S + p)][r][k] (pitch kp
+// elements): digit planes, or (SINGLE, S = 1) x' rounded to the plane type
+template <int S, int KIND, bool SINGLE>
+__global__ void __launch_bounds__(256)
+oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp)
+{
+    using T = typename PlaneElem<KIND>::T;
+    T* out = static_cast<T*>(out_);
     __shared__ double tile[SL_T][SL_T + 1];
     const i64 r0 = blockIdx.x*(i64)SL_T, k0 = blockIdx.y*(i64)SL_T;
     const int l = blockIdx.z;
@@ -492,49 +558,69 @@ oz_slice(const OzOperand o, const int* e_rows, signed char* out, i64 kp)
     const i64 r = r0 + rl;
     if (r >= o.R) return;
     const double sc = ldexp(1.0, -e_rows[(i64)l*o.R + r]);
-    signed char dg[16][S];
+    alignas(16) T dg[S][16];
     #pragma unroll
     for (int j = 0; j < 16; j++)
     {
-        signed char d[S];
-        digits<S>(tile[rl][seg + j]*sc, d);
-        #pragma unroll
-        for (int q = 0; q < S; q++) dg[j][q] = d[q];
+        const double xs = tile[rl][seg + j]*sc;
+        if constexpr (SINGLE)
+            dg[0][j] = single_elem<KIND>(xs);
+        else
+        {
+            signed char d[S];
+            digits<S>(xs, d);
+            #pragma unroll
+            for (int q = 0; q < S; q++) dg[q][j] = digit_elem<KIND>(d[q]);
+        }
     }
     const i64 kk = k0 + seg;
     if (kk >= kp) return;
+    constexpr int VEC = 16*sizeof(T)/16;     // 16-byte stores per row segment
     #pragma unroll
     for (int q = 0; q < S; q++)
     {
-        uint4 v;
-        unsigned char* b = reinterpret_cast<unsigned char*>(&v);
+        uint4* dst = reinterpret_cast<uint4*>(out + (((i64)l*S + q)*o.R + r)*kp + kk);
+        const uint4* src = reinterpret_cast<const uint4*>(&dg[q][0]);
         #pragma unroll
-        for (int j = 0; j < 16; j++) b[j] = (unsigned char)dg[j][q];
-        *reinterpret_cast<uint4*>(out + (((i64)l*S + q)*o.R + r)*kp + kk) = v;
+        for (int v = 0; v < VEC; v++) dst[v] = src[v];
     }
 }
 
-template <int S>
-void launch_slice(const OzOperand& o, const int* e, signed char* out, i64 kp, cudaStream_t st)
+template <int S, int KIND, bool SINGLE>
+void launch_slice(const OzOperand& o, const int* e, void* out, i64 kp, cudaStream_t st)
 {
     dim3 grid((unsigned)((o.R + SL_T - 1)/SL_T), (unsigned)((o.K + SL_T - 1)/SL_T), (unsigned)o.L);
-    oz_slice<S><<<grid, 256, 0, st>>>(o, e, out, kp);
+    oz_slice<S, KIND, SINGLE><<<grid, 256, 0, st>>>(o, e, out, kp);
     check_launch("oz_slice");
 }
 
-void slice_dispatch(int S, const OzOperand& o, const int* e, signed char* out, i64 kp, cudaStream_t st)
+template <int KIND>
+void slice_dispatch_kind(int S, const OzOperand& o, const int* e, void* out, i64 kp, cudaStream_t st)
 {
     switch (S)
     {
-        case 1: launch_slice<1>(o, e, out, kp, st); break;
-        case 2: launch_slice<2>(o, e, out, kp, st); break;
-        case 3: launch_slice<3>(o, e, out, kp, st); break;
-        case 4: launch_slice<4>(o, e, out, kp, st); break;
-        case 5: launch_slice<5>(o, e, out, kp, st); break;
-        case 6: launch_slice<6>(o, e, out, kp, st); break;
-        case 7: launch_slice<7>(o, e, out, kp, st); break;
-        default: launch_slice<8>(o, e, out, kp, st); break;
+        case 1: launch_slice<1, KIND, false>(o, e, out, kp, st); break;
+        case 2: launch_slice<2, KIND, false>(o, e, out, kp, st); break;
+        case 3: launch_slice<3, KIND, false>(o, e, out, kp, st); break;
+        case 4: launch_slice<4, KIND, false>(o, e, out, kp, st); break;
+        case 5: launch_slice<5, KIND, false>(o, e, out, kp, st); break;
+        case 6: launch_slice<6, KIND, false>(o, e, out, kp, st); break;
+        case 7: launch_slice<7, KIND, false>(o, e, out, kp, st); break;
+        default: launch_slice<8, KIND, false>(o, e, out, kp, st); break;
     }
+}
+
+void slice_dispatch(int kind, bool single, int S, const OzOperand& o, const int* e, void* out, i64 kp,
+                    cudaStream_t st)
+{
+    if (single)
+    {
+        if (kind == OZ_BF16) launch_slice<1, OZ_BF16, true>(o, e, out, kp, st);
+        else launch_slice<1, OZ_TF32, true>(o, e, out, kp, st);
+        return;
+    }
+    if (kind == OZ_I8) slice_dispatch_kind<OZ_I8>(S, o, e, out, kp, st);
+    else slice_dispatch_kind<OZ_BF16>(S, o, e, out, kp, st);
 }
 
 void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
@@ -582,15 +668,16 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// 3-D map over the digit planes [L*S][R][kp] (bytes), box 32 x rows x 1
-CUtensorMap make_map(const signed char* base, i64 K, i64 R, i64 planes, i64 kp, int box_rows)
+// 3-D map over the slice planes [L*S][R][kp] as bytes (K and kp in
+// elements of esz bytes), box 32 bytes x rows x 1
+CUtensorMap make_map(const void* base, i64 K, i64 R, i64 planes, i64 kp, int esz, int box_rows)
 {
     CUtensorMap m;
-    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)R, (cuuint64_t)planes};
-    cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)(kp*R)};
+    cuuint64_t dims[3] = {(cuuint64_t)(K*esz), (cuuint64_t)R, (cuuint64_t)planes};
+    cuuint64_t strides[2] = {(cuuint64_t)(kp*esz), (cuuint64_t)(kp*esz*R)};
     cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<signed char*>(base), dims, strides,
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides,
                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     TB_CHECK(r == CUDA_SUCCESS, TB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
@@ -610,11 +697,11 @@ size_t gemm_smem_bytes()
            (2*stages_for<S>() + 2)*8 + 16 + (OZ_BM + OZ_BN)*8 + OZ_BN*8;
 }
 
-template <int S>
+template <int S, int KIND>
 void launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb_, const OzGemmArgs& a, cudaStream_t st)
 {
     constexpr int STG = stages_for<S>();
-    auto kern = ozaki_gemm_kernel<S, STG>;
+    auto kern = ozaki_gemm_kernel<S, STG, KIND>;
     const size_t bytes = gemm_smem_bytes<S>();
     TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     const i64 tiles = ((a.M + OZ_BM - 1)/OZ_BM)*((a.N + OZ_BN - 1)/OZ_BN);
@@ -623,40 +710,68 @@ void launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb_, const OzGemmArgs
     check_launch("ozaki_gemm_kernel");
 }
 
-void gemm_dispatch(int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a, cudaStream_t st)
+template <int KIND>
+void gemm_dispatch_kind(int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a, cudaStream_t st)
 {
     switch (S)
     {
-        case 1: launch_gemm<1>(ta, tbm, a, st); break;
-        case 2: launch_gemm<2>(ta, tbm, a, st); break;
-        case 3: launch_gemm<3>(ta, tbm, a, st); break;
-        case 4: launch_gemm<4>(ta, tbm, a, st); break;
-        case 5: launch_gemm<5>(ta, tbm, a, st); break;
-        case 6: launch_gemm<6>(ta, tbm, a, st); break;
-        case 7: launch_gemm<7>(ta, tbm, a, st); break;
-        default: launch_gemm<8>(ta, tbm, a, st); break;
+        case 1: launch_gemm<1, KIND>(ta, tbm, a, st); break;
+        case 2: launch_gemm<2, KIND>(ta, tbm, a, st); break;
+        case 3: launch_gemm<3, KIND>(ta, tbm, a, st); break;
+        case 4: launch_gemm<4, KIND>(ta, tbm, a, st); break;
+        case 5: launch_gemm<5, KIND>(ta, tbm, a, st); break;
+        case 6: launch_gemm<6, KIND>(ta, tbm, a, st); break;
+        case 7: launch_gemm<7, KIND>(ta, tbm, a, st); break;
+        default: launch_gemm<8, KIND>(ta, tbm, a, st); break;
     }
 }
 
-// a-priori normwise error estimate for S slices (rounding of both operands
-// to S digits plus the dropped cross terms), from per-row maxima and norms
-double estimate_error(int S, const std::vector<int>& eA, const std::vector<double>& ssA, i64 KA,
-                      const std::vector<int>& eB, const std::vector<double>& ssB, i64 KB)
+void gemm_dispatch(int kind, int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a,
+                   cudaStream_t st)
 {
-    auto rel = [&](const std::vector<int>& e, const std::vector<double>& ss, i64 K)
+    TimedLaunch t("ozaki_gemm_kernel", st);
+    if (kind == OZ_I8) gemm_dispatch_kind<OZ_I8>(S, ta, tbm, a, st);
+    else if (kind == OZ_BF16) gemm_dispatch_kind<OZ_BF16>(S, ta, tbm, a, st);
+    else launch_gemm<1, OZ_TF32>(ta, tbm, a, st);
+}
+
+// a-priori normwise error estimate for S slices (rounding of both operands
+// to S digits plus the dropped cross terms), from per-row maxima and norms:
+// rounding row i to S digits leaves an error of about 2^(e_i - 7S) per
+// element (uniform, variance 1/3), so the squared relative error of the
+// operand is K/3 * sum_i 4^(e_i - 7S) / sum_i ss_i
+struct ErrorModel
+{
+    double ra2 = 0, rb2 = 0;      // squared relative error at S = 0: mantissa ...
+    int ea = 0, eb = 0;           // ... and binary exponent
+    static void build(const std::vector<int>& e, const std::vector<double>& ss, i64 K, double& m, int& ex)
     {
+        int emax = -100000;
+        for (int v : e) emax = std::max(emax, v);
         double num = 0.0, den = 0.0;
         for (size_t i = 0; i < e.size(); i++)
         {
-            num += (double)K*std::ldexp(1.0, 2*(e[i] - 7*S))/3.0;
+            num += std::ldexp(1.0, 2*(e[i] - emax));
             den += ss[i];
         }
-        return den > 0 ? std::sqrt(num/den) : 0.0;
-    };
-    const double ra = rel(eA, ssA, KA), rb = rel(eB, ssB, KB);
-    // dropped pairs p + q > S + 1 are below the rounding terms by ~2^-7
-    return (ra + rb)*(1.0 + 2.0*S*std::ldexp(1.0, -7));
-}
+        if (den <= 0.0 || num == 0.0) { m = 0.0; ex = 0; return; }
+        m = (double)K/3.0*num/den;
+        ex = 2*emax;
+    }
+    ErrorModel(const std::vector<int>& eA, const std::vector<double>& ssA,
+               const std::vector<int>& eB, const std::vector<double>& ssB, i64 K)
+    {
+        build(eA, ssA, K, ra2, ea);
+        build(eB, ssB, K, rb2, eb);
+    }
+    double operator()(int S) const
+    {
+        const double ra = ra2 > 0 ? std::sqrt(std::ldexp(ra2, ea - 14*S)) : 0.0;
+        const double rb = rb2 > 0 ? std::sqrt(std::ldexp(rb2, eb - 14*S)) : 0.0;
+        // dropped pairs p + q > S + 1 are below the rounding terms by ~2^-7
+        return (ra + rb)*(1.0 + 2.0*S*std::ldexp(1.0, -7));
+    }
+};
 
 } // namespace
 
@@ -687,8 +802,17 @@ void ozaki_begin(OzakiJob& j, cudaStream_t st)
 void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
 {
     const GemmView& v = j.v;
-    int S = j.slices;
-    if (S <= 0)
+    const int kind = j.kind;
+    TB_CHECK(kind == OZ_I8 || kind == OZ_BF16 || (kind == OZ_TF32 && j.single), TB_ERR_ARG,
+             "split-precision kind must be INT8 or BF16 slices, or a single TF32/BF16 pass");
+    int S = j.single ? 1 : j.slices;
+    if (j.single)
+    {
+        // one pass in the low precision: x' rounded to 8 (BF16) or 11 (TF32)
+        // significant bits in both operands, FP32 accumulation
+        j.res.est_error = std::sqrt(2.0)*(kind == OZ_BF16 ? std::ldexp(1.0, -9) : std::ldexp(1.0, -11));
+    }
+    else if (S <= 0)
     {
         std::vector<int> heA(v.l*v.m), heB(v.l*v.n);
         std::vector<double> hsA(v.l*v.m), hsB(v.l*v.n);
@@ -709,29 +833,35 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
             TB_CUDA(cudaMemcpyAsync(hsB.data(), j.sB.ptr, hsB.size()*sizeof(double), cudaMemcpyDeviceToHost, st));
             TB_CUDA(cudaStreamSynchronize(st));
         }
+        const ErrorModel est(heA, hsA, heB, hsB, v.k);
         S = OZ_SMAX;
         for (int s = 1; s <= OZ_SMAX; s++)
         {
             // safety factor 4 between the estimate and the target
-            if (estimate_error(s, heA, hsA, v.k, heB, hsB, v.k)*4.0 <= j.tol) { S = s; break; }
+            if (est(s)*4.0 <= j.tol) { S = s; break; }
         }
-        j.res.est_error = estimate_error(S, heA, hsA, v.k, heB, hsB, v.k);
+        j.res.est_error = est(S);
     }
     TB_CHECK(S >= 1 && S <= OZ_SMAX, TB_ERR_ARG, "Ozaki slice count must be 1..8");
     j.res.slices = S;
 
     OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode};
     OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode};
-    const i64 kp = (v.k + 63)/64*64;       // row pitch: TMA strides and 16-byte digit stores
-    dbuf pa((size_t)v.l*S*v.m*kp, st), pb((size_t)v.l*S*v.n*kp, st);
-    slice_dispatch(S, oa, j.eA.as<int>(), pa.as<signed char>(), kp, st);
-    slice_dispatch(S, ob, j.eB.as<int>(), pb.as<signed char>(), kp, st);
+    const int esz = elem_bytes(kind);
+    const i64 ke = OZ_BK/esz;              // k elements per MMA step
+    const i64 kp = (v.k + 63)/64*64;       // row pitch (elements): TMA strides and 16-byte stores
+    dbuf pa((size_t)v.l*S*v.m*kp*esz, st), pb((size_t)v.l*S*v.n*kp*esz, st);
+    slice_dispatch(kind, j.single, S, oa, j.eA.as<int>(), pa.ptr, kp, st);
+    slice_dispatch(kind, j.single, S, ob, j.eB.as<int>(), pb.ptr, kp, st);
 
-    const CUtensorMap ta = make_map(pa.as<signed char>(), v.k, v.m, v.l*S, kp, OZ_BM);
-    const CUtensorMap tbm = make_map(pb.as<signed char>(), v.k, v.n, v.l*S, kp, OZ_BN);
+    const CUtensorMap ta = make_map(pa.ptr, v.k, v.m, v.l*S, kp, esz, OZ_BM);
+    const CUtensorMap tbm = make_map(pb.ptr, v.k, v.n, v.l*S, kp, esz, OZ_BN);
 
-    // INT32 exactness: (#pairs on a diagonal) * K_launch * 64^2 < 2^31
-    const i64 klimit = ((i64)0x7fffffff/((i64)S*64*64))/OZ_BK*OZ_BK;
+    // exact accumulation of the digit products, (#pairs on a diagonal) *
+    // K_launch * 64^2 below 2^31 (INT32) or 2^24 (FP32 holds integers
+    // exactly up to there); a single pass runs the whole K at once
+    const i64 acc_limit = kind == OZ_I8 ? (i64)0x7fffffff : ((i64)1 << 24);
+    const i64 klimit = j.single ? std::max<i64>(v.k, 1) : (acc_limit/((i64)S*64*64))/ke*ke;
     for (i64 k0 = 0; k0 < v.k; k0 += klimit)
     {
         OzGemmArgs g;
@@ -743,16 +873,19 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
         g.k_count = (int)std::min(klimit, v.k - k0);
         g.alpha = j.alpha;
         g.beta = k0 == 0 ? j.beta : 1.0;
-        gemm_dispatch(S, ta, tbm, g, st);
+        g.wbase = j.single ? 14 : 2;       // digits: 2^(2-7d); a single pass: weight 1
+        gemm_dispatch(kind, S, ta, tbm, g, st);
     }
 }
 
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
-                       double alpha, double beta, double tol, int slices, cudaStream_t st)
+                       double alpha, double beta, double tol, int slices, cudaStream_t st,
+                       int kind, bool single)
 {
     OzakiJob j;
     j.v = v; j.A = A; j.B = B; j.C = C;
     j.alpha = alpha; j.beta = beta; j.tol = tol; j.slices = slices;
+    j.kind = kind; j.single = single;
     ozaki_begin(j, st);
     ozaki_end(j, st, false);
     return j.res;

@@ -1,4 +1,5 @@
-// ozaki.hpp -- Ozaki split-precision contraction (INT8 slices on tcgen05)
+// ozaki.hpp -- split-precision contraction on tcgen05: Ozaki INT8 or BF16
+// slices, or a single TF32 / BF16 pass
 #pragma once
 
 #include "planner.hpp"
@@ -6,14 +7,20 @@
 namespace tb
 {
 
+// element kind of the slice planes and of the tensor-core MMA
+enum OzKind { OZ_I8 = 0, OZ_BF16 = 1, OZ_TF32 = 2 };
+
 struct OzakiResult
 {
     int slices = 0;
     double est_error = 0;
 };
 
+// kind OZ_I8 / OZ_BF16 with single = false: Ozaki slices (slices = 0
+// chooses the count from tol); single = true: one BF16 or TF32 pass
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
-                       double alpha, double beta, double tol, int slices, cudaStream_t st);
+                       double alpha, double beta, double tol, int slices, cudaStream_t st,
+                       int kind = OZ_I8, bool single = false);
 
 // the same contraction in two phases, so a caller can queue the statistics
 // of several contractions, do other work, and wait only for the statistics
@@ -25,6 +32,8 @@ struct OzakiJob
     double* C = nullptr;
     double alpha = 1, beta = 0, tol = 1e-12;
     int slices = 0;
+    int kind = OZ_I8;
+    bool single = false;
     std::shared_ptr<GemmTables> tab;
     dbuf eA, eB, sA, sB;             // row exponents and sums of squares
     OzakiResult res;
@@ -32,7 +41,7 @@ struct OzakiJob
 // queues the row statistics of A and B on st
 void ozaki_begin(OzakiJob& j, cudaStream_t st);
 // picks the slice count (reads the statistics: stats_ready = they are
-// complete, else this waits for st) and queues slicing and the INT8 GEMM
+// complete, else this waits for st) and queues slicing and the slice GEMM
 void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready);
 
 } // namespace tb

@@ -123,3 +123,78 @@ def test_config_selects_ozaki(cuda):
     torch.cuda.synchronize()
     ref = A.cpu().numpy() @ B.cpu().numpy()
     assert normwise_rel(C.cpu().numpy(), ref) <= 1e-12
+
+
+def _gpu_method(torch, dev, method, alpha, A, idx_A, B, idx_B, beta, C, idx_C, slices=0, tol=1e-12):
+    import tblis_b200 as tb
+    dA = torch.from_numpy(np.ascontiguousarray(A)).to(dev)
+    dB = torch.from_numpy(np.ascontiguousarray(B)).to(dev)
+    dC = torch.from_numpy(np.ascontiguousarray(C)).to(dev)
+    rep = tb.mult_ex(alpha, dA, idx_A, dB, idx_B, beta, dC, idx_C, method=method, slices=slices, tolerance=tol)
+    tb.synchronize()
+    return dC.cpu().numpy(), rep
+
+
+@pytest.mark.parametrize("tol", [1e-8, 1e-12])
+def test_bf16_slices_meet_tolerance(cuda, tol):
+    """Ozaki with BF16 digit planes (exact FP32 accumulation over K chunks of
+    the launch) on the ladder's exponent-spread inputs; K = 1600 spans
+    several exactness chunks."""
+    import torch
+    rng = np.random.default_rng(11)
+    A = _spread(rng, (96, 40, 40))
+    B = _spread(rng, (40, 40, 72))
+    C = rng.uniform(-1, 1, (96, 72))
+    ref = C.copy()
+    oracle.orc_mult(1.5, A, "aef", B, "efb", 0.5, ref, "ab")
+    got, rep = _gpu_method(torch, cuda, 3, 1.5, A, "aef", B, "efb", 0.5, C, "ab", tol=tol)
+    assert rep["method"] == 3 and 1 <= rep["slices"] <= 8
+    assert normwise_rel(got, ref) <= tol
+
+
+def test_bf16_and_int8_slices_agree(cuda):
+    """Both digit formats carry the same integers; with identical slice
+    counts the two methods differ only by FP64 rounding of the sums."""
+    import torch
+    rng = np.random.default_rng(12)
+    A = rng.uniform(-1, 1, (200, 300))
+    B = rng.uniform(-1, 1, (300, 130))
+    C = np.zeros((200, 130))
+    i8, _ = _gpu_method(torch, cuda, 2, 1.0, A, "ik", B, "kj", 0.0, C, "ij", slices=5)
+    bf, _ = _gpu_method(torch, cuda, 3, 1.0, A, "ik", B, "kj", 0.0, C, "ij", slices=5)
+    assert normwise_rel(bf, i8) <= 1e-15
+
+
+@pytest.mark.parametrize("method,bound", [(4, 2e-3), (5, 1.5e-2)])
+def test_single_pass_low_precision(cuda, method, bound):
+    """One TF32 (method 4) or BF16 (method 5) pass with FP32 accumulation:
+    error of the order of the input rounding, reported as such."""
+    import torch
+    rng = np.random.default_rng(13)
+    A = _spread(rng, (64, 30, 30), -6, 6)
+    B = _spread(rng, (30, 30, 80), -6, 6)
+    C = np.zeros((64, 80))
+    ref = C.copy()
+    oracle.orc_mult(1.0, A, "aef", B, "efb", 0.0, ref, "ab")
+    got, rep = _gpu_method(torch, cuda, method, 1.0, A, "aef", B, "efb", 0.0, C, "ab")
+    err = normwise_rel(got, ref)
+    assert rep["method"] == method and rep["slices"] == 1
+    assert err <= bound, err
+    assert err >= 1e-9      # a genuine low-precision pass, not an FP64 one
+
+
+def test_named_configs_select_methods(cuda):
+    import ctypes
+    import torch
+    import tblis_b200 as tb
+    for name, method in [("b200_fp64", 1), ("b200_ozaki_i8", 2), ("b200_ozaki_bf16", 3),
+                         ("b200_tf32", 4), ("b200_bf16", 5)]:
+        cfg = tb.lib.tblis_get_config(name.encode())
+        assert cfg
+        a = torch.rand((40, 50), dtype=torch.float64, device=cuda)
+        b = torch.rand((50, 30), dtype=torch.float64, device=cuda)
+        c = torch.zeros((40, 30), dtype=torch.float64, device=cuda)
+        rep = tb.mult_ex(1.0, a, "ik", b, "kj", 0.0, c, "ij", cfg=ctypes.c_void_p(cfg))
+        assert rep["method"] == method
+        err = (torch.linalg.norm(c - a @ b) / torch.linalg.norm(a @ b)).item()
+        assert err <= (1e-12 if method <= 3 else 2e-2)
