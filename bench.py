@@ -367,6 +367,8 @@ def main():
         fp_kernel_ms = statistics.mean(fp_per)
         fp64_gflops = FLOPS_LADDER / (fp_kernel_ms * 1e-3) / 1e9
         extra["fp64_dmma_gflops"] = fp64_gflops
+        extra["cublas_dgemm_8192_tflops"] = fp64_peak
+        extra["fp64_path_frac_of_cublas_dgemm"] = fp64_gflops / 1e3 / fp64_peak
         extra["speedup_vs_fp64_path"] = value / world / fp64_gflops
         # the dominant kernel's own device time: CUDA events around each of its
         # launches on the launching stream, inside the timed steps
@@ -611,6 +613,23 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
     torch.cuda.synchronize()
     serial_s = time.perf_counter() - t0
 
+    # serial plain calls under the same arrivals: each request waits for its
+    # predecessor and for its own result (a plain caller's latency)
+    lat_serial = []
+    t0 = time.perf_counter()
+    due = t0
+    for j, i in enumerate(picks):
+        due += gaps[j]
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        p = pool[i]
+        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"])
+        torch.cuda.synchronize()
+        lat_serial.append((time.perf_counter() - due) * 1e3)
+    serial_arr_s = time.perf_counter() - t0
+    lat_serial.sort()
+
     srv = tb.Server(hbm_budget_bytes=150 << 30, slots=4)
     ids = []
     t0 = time.perf_counter()
@@ -636,7 +655,11 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
             "served_req_s": nreq / served_s, "served_gflops": total_flops / served_s / 1e9,
             "arrival_window_s": arrivals_s,
             "serial_req_s": nreq / serial_s, "serial_gflops": total_flops / serial_s / 1e9,
-            "throughput_vs_serial": serial_s / served_s}
+            "throughput_vs_serial": serial_s / served_s,
+            "serial_same_arrivals": {"req_s": nreq / serial_arr_s,
+                                     "p50_ms": lat_serial[len(lat_serial) // 2],
+                                     "p99_ms": lat_serial[min(len(lat_serial) - 1, int(0.99 * len(lat_serial)))]},
+            "throughput_vs_serial_same_arrivals": serial_arr_s / served_s}
 
 
 def single_case(torch, tb, dev, stream, args):
