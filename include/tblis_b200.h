@@ -267,6 +267,76 @@ int tblis_b200_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
                               tblis_b200_dpd_tensor* C, const label_type* idx_C,
                         tblis_b200_report* report);
 
+/* A DPD tensor given by the geometry of its stored blocks rather than by one
+ * of MArray's storage layouts: what a dpd_varray_view reports for each block
+ * through operator()(irreps) (dpd_varray_base.hpp:482-508), which also covers
+ * permuted views. len is [ndim][nirrep]; offset[t] and stride[t*ndim + d]
+ * describe the block whose irreps are (i_0, ..., i_{ndim-1}) at
+ * t = sum_d i_d*nirrep^d (dimension 0 fastest); offset -1 marks tuples that
+ * are not stored. Offsets and strides are in elements, non-negative. */
+typedef struct tblis_b200_dpd_block_table
+{
+    type_t type;
+    int conj;
+    tblis_scalar scalar;
+    void* data;
+    unsigned ndim;
+    unsigned nirrep;
+    unsigned irrep;
+    const len_type* len;
+    const stride_type* offset;
+    const stride_type* stride;
+} tblis_b200_dpd_block_table;
+
+/* tblis_b200_dpd_mult over block tables: the entry the C++ overload
+ * tblis::mult(comm, alpha, dpd_varray_view<const T> A, ...) of
+ * src/iface/3t/mult.h:56-60 reaches (libtblis_b200_cxx.so). */
+int tblis_b200_dpd_mult_blocks(const tblis_b200_dpd_block_table* A, const label_type* idx_A,
+                               const tblis_b200_dpd_block_table* B, const label_type* idx_B,
+                                     tblis_b200_dpd_block_table* C, const label_type* idx_C,
+                               tblis_b200_report* report);
+
+/* An indexed DPD tensor as MArray's indexed_dpd_varray holds it
+ * (indexed_dpd_varray_base.hpp, indexed_dpd_varray.hpp:309-370): the first
+ * dense_ndim dimensions are DPD dimensions; each of the other (indexed)
+ * dimensions has one fixed irrep, and the tensor stores nidx entries, each a
+ * DPD tensor over the dense dimensions (irrep dense_irrep) at data[i] with an
+ * index tuple indices[i][...] and a scalar factor[i] (NULL = all 1). len is
+ * [ndim][nirrep]; the dense blocks of every entry share one block table
+ * (offset/stride relative to the entry's data, as tblis_b200_dpd_block_table). */
+typedef struct tblis_b200_indexed_dpd_tensor
+{
+    type_t type;
+    tblis_scalar scalar;
+    unsigned ndim;
+    unsigned dense_ndim;
+    unsigned nirrep;
+    unsigned dense_irrep;
+    const len_type* len;
+    const unsigned* idx_irrep;
+    len_type nidx;
+    const len_type* indices;
+    double* const* data;
+    const double* factor;
+    const stride_type* offset;
+    const stride_type* stride;
+} tblis_b200_indexed_dpd_tensor;
+
+/* C = alpha*A*B + beta*C over indexed DPD tensors (alpha = A.scalar*B.scalar,
+ * beta = C.scalar), the entry of tblis::mult over indexed_dpd_varray_view
+ * (src/iface/3t/mult.cxx:412-533): C entry i is first scaled by f_C[i]*beta
+ * (beta == 1: untouched; beta == 0 or f_C[i] == 0: zeroed), then it
+ * receives alpha*f_C[i]*f_A[j]*f_B[k]*(A_j . B_k) from every pair of
+ * A and B entries whose index values agree with it and with each other; a
+ * label indexed in one tensor and dense in another selects that slice. Each
+ * consistent triple runs as one grouped launch of the FP64 kernel. Labels
+ * dense in all three tensors are not supported. report->m = triples launched.
+ * Returns 0 or an error code. */
+int tblis_b200_indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                                const tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B,
+                                      tblis_b200_indexed_dpd_tensor* C, const label_type* idx_C,
+                                tblis_b200_report* report);
+
 /* Offset (from data), lengths and strides of one block (one irrep per
  * dimension), as dpd_varray_view::operator()(irreps) gives them
  * (dpd_marray_base.hpp:171-228). Returns 0 or an error code. */

@@ -315,3 +315,30 @@ def ref_dpd_mult(nirrep, alpha, irrep_A, lens_A, A, idx_A, irrep_B, lens_B, B, i
         ctypes.c_double(beta), irrep_C, len(lens_C), flat(lens_C), ctypes.c_void_p(C.ctypes.data), _lab(idx_C))
     if rc:
         raise ValueError("reference dpd mult failed")
+
+
+def ref_indexed_dpd_mult(nirrep, alpha, A, idx_A, B, idx_B, beta, C, idx_C, impl=2):
+    """The reference's own indexed-DPD contraction (tblis::mult over
+    indexed_dpd_varray_view). Each tensor is a dict: irrep (overall), lens
+    [ndim][nirrep], idx_irreps, indices [nidx][nidim], data (numpy, nidx x
+    dense size, default layout), factors. C's data is updated in place.
+    impl: 0 = the reference's default block path, 1 = BLOCKED, 2 = FULL (the
+    dense round trip its own tests take as the answer, test/3t/mult.cxx:176-232)."""
+    def args(T):
+        ndim = len(T["lens"])
+        nidim = len(T["idx_irreps"])
+        flat = (_sz * (ndim * nirrep))(*[x for row in T["lens"] for x in row])
+        irr = (ctypes.c_uint * max(1, nidim))(*T["idx_irreps"])
+        idx = [x for t in T["indices"] for x in t]
+        nidx = max(1, len(T["indices"])) if nidim else 1
+        ix = (_sz * max(1, len(idx)))(*idx)
+        f = (ctypes.c_double * nidx)(*T["factors"])
+        return [ctypes.c_uint(T["irrep"]), ctypes.c_uint(ndim), flat, ctypes.c_uint(nidim), irr, ctypes.c_long(nidx),
+                ix, ctypes.c_void_p(T["data"].ctypes.data), f]
+    a = args(A) + [_lab(idx_A)]
+    b = args(B) + [_lab(idx_B)]
+    c = args(C) + [_lab(idx_C)]
+    rc = shim().refshim_indexed_dpd_mult(ctypes.c_uint(nirrep), ctypes.c_double(alpha), *a, *b,
+                                         ctypes.c_double(beta), *c, ctypes.c_int(impl))
+    if rc:
+        raise ValueError("reference indexed dpd mult failed")

@@ -6,7 +6,8 @@
  * library. It exposes internals that the reference's C ABI does not: the
  * block-scatter vector builder (src/matrix/block_scatter_matrix.hpp:249-258),
  * the MArray DPD block layout (src/external/marray/include/dpd_marray_base.hpp)
- * and the C++ DPD contraction entry point (src/iface/3t/mult.cxx:170-298), so
+ * and the C++ DPD and indexed-DPD contraction entry points
+ * (src/iface/3t/mult.cxx:170-298, 412-541), so
  * that the tests can pin the oracle restatement and the product's planner
  * against the reference bit for bit.
  */
@@ -15,6 +16,7 @@
 #include "matrix/block_scatter_matrix.hpp"
 #include "iface/3t/mult.h"
 #include "iface/1t/add.h"
+#include "internal/3t/dpd/mult.hpp"
 
 using namespace tblis;
 
@@ -108,6 +110,64 @@ int refshim_dpd_mult(unsigned nirrep,
     MArray::dpd_varray_view<double> C(irrep_C, nirrep, mk(ndim_C, lens_C), data_C);
 
     tblis::mult<double>(alpha, A, idx_A, B, idx_B, beta, C, idx_C);
+    return 0;
+}
+
+/*
+ * The reference's indexed-DPD contraction (tblis::mult over
+ * indexed_dpd_varray_view, src/iface/3t/mult.cxx:412-541). Each tensor is
+ * given by its overall irrep, ndim, lens [ndim][nirrep], the irreps of its
+ * last nidx_dim (indexed) dimensions, nidx index tuples [nidx][nidx_dim], the
+ * storage of its entries back to back (nidx x dense size, MArray's default
+ * layout, as indexed_dpd_varray allocates it) and the entry factors. C's
+ * storage is updated in place. impl selects the reference's implementation
+ * (0 default, 1 BLOCKED, 2 FULL). Returns 0 on success.
+ */
+int refshim_indexed_dpd_mult(unsigned nirrep, double alpha,
+                             unsigned irrep_A, unsigned ndim_A, const len_type* lens_A, unsigned nidim_A,
+                             const unsigned* irr_A, long nidx_A, const len_type* idx_A_, const double* data_A,
+                             const double* f_A, const char* lab_A,
+                             unsigned irrep_B, unsigned ndim_B, const len_type* lens_B, unsigned nidim_B,
+                             const unsigned* irr_B, long nidx_B, const len_type* idx_B_, const double* data_B,
+                             const double* f_B, const char* lab_B,
+                             double beta,
+                             unsigned irrep_C, unsigned ndim_C, const len_type* lens_C, unsigned nidim_C,
+                             const unsigned* irr_C, long nidx_C, const len_type* idx_C_, double* data_C,
+                             const double* f_C, const char* lab_C, int impl)
+{
+    // filled in place (MArray's owning containers are not returned by value)
+    auto fill = [&](MArray::indexed_dpd_varray<double>& T, unsigned irrep, unsigned ndim, const len_type* lens,
+                    unsigned nidim, const unsigned* irr, long nidx, const len_type* idx, const double* data,
+                    const double* f)
+    {
+        MArray::matrix<len_type> len({ndim, nirrep}, MArray::ROW_MAJOR);
+        for (unsigned i = 0; i < ndim; i++)
+            for (unsigned j = 0; j < nirrep; j++) len[i][j] = lens[i*nirrep+j];
+        std::vector<unsigned> ir(irr, irr + nidim);
+        MArray::matrix<len_type> ix({(len_type)nidx, (len_type)nidim}, MArray::ROW_MAJOR);
+        for (long e = 0; e < nidx; e++)
+            for (unsigned d = 0; d < nidim; d++) ix[e][d] = idx[e*nidim+d];
+        T.reset(irrep, nirrep, len, ir, ix);
+        const len_type n = T.dense_size();
+        for (long e = 0; e < nidx; e++)
+        {
+            std::copy_n(data + e*n, n, T.data(e));
+            T.factor(e) = f[e];
+        }
+    };
+    MArray::indexed_dpd_varray<double> A, B, C;
+    fill(A, irrep_A, ndim_A, lens_A, nidim_A, irr_A, nidx_A, idx_A_, data_A, f_A);
+    fill(B, irrep_B, ndim_B, lens_B, nidim_B, irr_B, nidx_B, idx_B_, data_B, f_B);
+    fill(C, irrep_C, ndim_C, lens_C, nidim_C, irr_C, nidx_C, idx_C_, data_C, f_C);
+    // impl: 0 = the default block path, 1 = BLOCKED, 2 = FULL (dense round
+    // trip, src/internal/3t/indexed_dpd/mult.cxx:68-114)
+    const auto saved = tblis::internal::dpd_impl;
+    tblis::internal::dpd_impl = impl == 2 ? tblis::internal::FULL : impl == 1 ? tblis::internal::BLOCKED
+                                                                            : tblis::internal::BLIS;
+    tblis::mult<double>(alpha, A, lab_A, B, lab_B, beta, C, lab_C);
+    tblis::internal::dpd_impl = saved;
+    const len_type n = C.dense_size();
+    for (long e = 0; e < nidx_C; e++) std::copy_n(C.data(e), n, data_C + e*n);
     return 0;
 }
 

@@ -360,6 +360,106 @@ def dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
 
 
+class tblis_b200_indexed_dpd_tensor(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("scalar", tblis_scalar), ("ndim", ctypes.c_uint),
+                ("dense_ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint), ("dense_irrep", ctypes.c_uint),
+                ("len", _P(ctypes.c_ssize_t)), ("idx_irrep", _P(ctypes.c_uint)), ("nidx", ctypes.c_ssize_t),
+                ("indices", _P(ctypes.c_ssize_t)), ("data", _P(ctypes.c_void_p)), ("factor", _P(ctypes.c_double)),
+                ("offset", _P(ctypes.c_ssize_t)), ("stride", _P(ctypes.c_ssize_t))]
+
+
+lib.tblis_b200_indexed_dpd_mult.argtypes = [_P(tblis_b200_indexed_dpd_tensor), ctypes.c_char_p,
+                                            _P(tblis_b200_indexed_dpd_tensor), ctypes.c_char_p,
+                                            _P(tblis_b200_indexed_dpd_tensor), ctypes.c_char_p,
+                                            _P(tblis_b200_report)]
+lib.tblis_b200_indexed_dpd_mult.restype = ctypes.c_int
+
+
+class IndexedDpdTensor:
+    """An indexed DPD tensor as MArray's indexed_dpd_varray holds it: the
+    first ndim - len(idx_irreps) dimensions are dense DPD dimensions, the
+    others are indexed with fixed irreps; `indices` lists the index tuples of
+    the stored entries, `data` holds their dense storage back to back (entry
+    size = dense_size(), MArray layout `layout`), `factors` their scalars.
+
+    irrep: the overall irrep (dense irrep XOR the indexed irreps), as
+    indexed_dpd_varray(irrep, nirrep, len, idx_irrep, idx) takes it."""
+
+    def __init__(self, irrep, nirrep, lens, idx_irreps, indices, data=None, factors=None, layout=5):
+        self.nirrep = int(nirrep)
+        self.lens = [list(map(int, r)) for r in lens]
+        self.idx_irreps = [int(x) for x in idx_irreps]
+        self.ndim = len(self.lens)
+        self.dense_ndim = self.ndim - len(self.idx_irreps)
+        self.irrep = int(irrep)
+        self.dense_irrep = self.irrep
+        for r in self.idx_irreps:
+            self.dense_irrep ^= r
+        self.indices = [list(map(int, t)) for t in indices] if self.idx_irreps else [[]]
+        self.nidx = max(1, len(self.indices))
+        self.factors = [1.0] * self.nidx if factors is None else [float(f) for f in factors]
+        self.layout = int(layout)
+        self.data = data
+        dense = DpdTensor(self.dense_irrep, self.nirrep, self.lens[:self.dense_ndim], layout=self.layout)
+        self._dense_size = dense.size()
+        # block table of one entry: every irrep tuple of the dense dims, dim 0 fastest
+        nt = self.nirrep ** self.dense_ndim
+        off = [-1] * nt
+        strides = [0] * (nt * self.dense_ndim)
+        for t in range(nt):
+            irr = [(t // self.nirrep ** d) % self.nirrep for d in range(self.dense_ndim)]
+            x = 0
+            for r in irr:
+                x ^= r
+            ext = 1
+            for d in range(self.dense_ndim):
+                ext *= self.lens[d][irr[d]]
+            if x != self.dense_irrep or ext == 0:
+                continue
+            o, _, st = dense.block(irr)
+            off[t] = o
+            strides[t * self.dense_ndim:(t + 1) * self.dense_ndim] = st
+        self._len = (ctypes.c_ssize_t * (self.ndim * self.nirrep))(*[x for r in self.lens for x in r])
+        self._irr = (ctypes.c_uint * max(1, len(self.idx_irreps)))(*self.idx_irreps)
+        flat_idx = [x for t in self.indices for x in t]
+        self._idx = (ctypes.c_ssize_t * max(1, len(flat_idx)))(*flat_idx)
+        self._off = (ctypes.c_ssize_t * nt)(*off)
+        self._str = (ctypes.c_ssize_t * max(1, len(strides)))(*strides)
+
+    def dense_size(self):
+        """Stored elements of one entry."""
+        return self._dense_size
+
+    def struct(self, scalar=1.0):
+        t = tblis_b200_indexed_dpd_tensor()
+        t.type = TYPE_DOUBLE
+        t.scalar.type = TYPE_DOUBLE
+        t.scalar.data[0] = float(scalar)
+        t.ndim, t.dense_ndim, t.nirrep, t.dense_irrep = self.ndim, self.dense_ndim, self.nirrep, self.dense_irrep
+        t.len = ctypes.cast(self._len, _P(ctypes.c_ssize_t))
+        t.idx_irrep = ctypes.cast(self._irr, _P(ctypes.c_uint))
+        t.nidx = self.nidx
+        t.indices = ctypes.cast(self._idx, _P(ctypes.c_ssize_t))
+        base = self.data.data_ptr() if hasattr(self.data, "data_ptr") else self.data.ctypes.data
+        self._ptrs = (ctypes.c_void_p * self.nidx)(*[base + 8 * e * self._dense_size for e in range(self.nidx)])
+        t.data = ctypes.cast(self._ptrs, _P(ctypes.c_void_p))
+        self._fac = (ctypes.c_double * self.nidx)(*self.factors)
+        t.factor = ctypes.cast(self._fac, _P(ctypes.c_double))
+        t.offset = ctypes.cast(self._off, _P(ctypes.c_ssize_t))
+        t.stride = ctypes.cast(self._str, _P(ctypes.c_ssize_t))
+        return t
+
+
+def indexed_dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
+    """C = alpha*A*B + beta*C over indexed DPD tensors (src/iface/3t/mult.h:92-110)."""
+    a, b, c = A.struct(alpha), B.struct(), C.struct(beta)
+    r = tblis_b200_report()
+    lib.tblis_b200_indexed_dpd_mult(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B),
+                                    ctypes.byref(c), _labels(idx_C), ctypes.byref(r))
+    _check()
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
 class PreparedBatch:
     """The C-ABI arrays of a batch built once, so repeated runs of the same
     tensors (an iterative solver's step) cost one library call."""

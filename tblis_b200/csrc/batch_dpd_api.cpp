@@ -50,9 +50,19 @@ struct DpdStage
     }
 };
 
-void run_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
-                  const tblis_b200_dpd_tensor* B, const label_type* idx_B,
-                  tblis_b200_dpd_tensor* C, const label_type* idx_C, tblis_b200_report* report)
+void to_layout(const tblis_b200_dpd_block_table* t, DpdLayout& lay)
+{
+    TB_CHECK(t, TB_ERR_ARG, "null DPD tensor");
+    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "DPD: only double is supported");
+    TB_CHECK(t->len, TB_ERR_ARG, "DPD: null lengths");
+    std::vector<i64> lens(t->len, t->len + (size_t)t->ndim*t->nirrep);
+    lay.init_explicit(t->irrep, t->nirrep, t->ndim, lens.data(), t->offset, t->stride);
+}
+
+// both descriptor kinds carry the same header fields
+template <typename Desc>
+void run_dpd_mult(const Desc* A, const label_type* idx_A, const Desc* B, const label_type* idx_B,
+                  Desc* C, const label_type* idx_C, tblis_b200_report* report)
 {
     ensure_device();
     cudaStream_t st = current_stream();
@@ -249,6 +259,14 @@ int tblis_b200_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
                         const tblis_b200_dpd_tensor* B, const label_type* idx_B,
                               tblis_b200_dpd_tensor* C, const label_type* idx_C,
                         tblis_b200_report* report)
+{
+    return guarded([&] { run_dpd_mult(A, idx_A, B, idx_B, C, idx_C, report); });
+}
+
+int tblis_b200_dpd_mult_blocks(const tblis_b200_dpd_block_table* A, const label_type* idx_A,
+                               const tblis_b200_dpd_block_table* B, const label_type* idx_B,
+                                     tblis_b200_dpd_block_table* C, const label_type* idx_C,
+                               tblis_b200_report* report)
 {
     return guarded([&] { run_dpd_mult(A, idx_A, B, idx_B, C, idx_C, report); });
 }

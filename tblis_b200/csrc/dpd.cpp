@@ -135,9 +135,64 @@ void DpdLayout::init(unsigned irrep_, unsigned nirrep_, unsigned ndim_, const i6
     }
 }
 
+void DpdLayout::init_explicit(unsigned irrep_, unsigned nirrep_, unsigned ndim_, const i64* lens,
+                              const i64* offsets, const i64* strides)
+{
+    TB_CHECK(ndim_ >= 1 && ndim_ <= 16, TB_ERR_ARG, "DPD: 1..16 dimensions");
+    TB_CHECK(nirrep_ == 1 || nirrep_ == 2 || nirrep_ == 4 || nirrep_ == 8, TB_ERR_ARG, "DPD: nirrep must be 1, 2, 4 or 8");
+    TB_CHECK(irrep_ < nirrep_, TB_ERR_ARG, "DPD: irrep out of range");
+    TB_CHECK(offsets && strides, TB_ERR_ARG, "DPD: null block table");
+    ndim = ndim_; nirrep = nirrep_; irrep = irrep_; layout = -1;
+    len.assign(ndim, std::vector<i64>(nirrep));
+    for (unsigned d = 0; d < ndim; d++)
+        for (unsigned r = 0; r < nirrep; r++)
+        {
+            len[d][r] = lens[(size_t)d*nirrep + r];
+            TB_CHECK(len[d][r] >= 0, TB_ERR_ARG, "DPD: negative length");
+        }
+    size_t nt = 1;
+    for (unsigned d = 0; d < ndim; d++) nt *= nirrep;
+    TB_CHECK(nt <= ((size_t)1 << 24), TB_ERR_SIZE, "DPD: block table too large");
+    xoff.assign(offsets, offsets + nt);
+    xstride.assign(strides, strides + nt*ndim);
+    xextent = 0;
+    // every stored block must be given, with non-negative geometry
+    std::vector<unsigned> irr(ndim, 0);
+    for (size_t t = 0; t < nt; t++)
+    {
+        unsigned x = 0;
+        i64 ext = 1, last = 0;
+        for (unsigned d = 0; d < ndim; d++) { x ^= irr[d]; ext *= len[d][irr[d]]; }
+        if (x == irrep && ext > 0)
+        {
+            TB_CHECK(xoff[t] >= 0, TB_ERR_ARG, "DPD: block table lacks a stored block");
+            for (unsigned d = 0; d < ndim; d++)
+            {
+                TB_CHECK(xstride[t*ndim + d] >= 0, TB_ERR_ARG, "DPD: negative block stride");
+                last += (len[d][irr[d]] - 1)*xstride[t*ndim + d];
+            }
+            xextent = std::max(xextent, xoff[t] + last + 1);
+        }
+        unsigned d = 0;
+        while (d < ndim && ++irr[d] == nirrep) { irr[d] = 0; d++; }
+    }
+}
+
 // get_block (dpd_marray_base.hpp:171-228) for a full (unsliced) tensor
 void DpdLayout::block(const unsigned* irreps, i64* blen, i64* bstride, i64& offset) const
 {
+    if (is_explicit())
+    {
+        size_t t = 0;
+        for (unsigned d = ndim; d-- > 0;) t = t*nirrep + irreps[d];
+        offset = xoff[t];
+        for (unsigned d = 0; d < ndim; d++)
+        {
+            blen[d] = len[d][irreps[d]];
+            bstride[d] = xstride[t*ndim + d];
+        }
+        return;
+    }
     std::vector<unsigned> dirrep(2*ndim - 1, 0);
     std::vector<i64> dstride(2*ndim - 1, 0);
     dstride[2*ndim - 2] = 1;
@@ -306,6 +361,11 @@ static std::string dpd_key(const DpdTensor& A, const char* ia, const DpdTensor& 
         k += std::to_string(l.ndim) + "," + std::to_string(l.nirrep) + "," + std::to_string(l.irrep) + "," +
              std::to_string(l.layout) + ":";
         for (auto& r : l.len) for (i64 x : r) k += std::to_string(x) + ",";
+        if (l.is_explicit())
+        {
+            k.append(reinterpret_cast<const char*>(l.xoff.data()), l.xoff.size()*sizeof(i64));
+            k.append(reinterpret_cast<const char*>(l.xstride.data()), l.xstride.size()*sizeof(i64));
+        }
         k += "|";
     }
     k += std::string(ia) + "|" + ib + "|" + ic;
@@ -314,7 +374,7 @@ static std::string dpd_key(const DpdTensor& A, const char* ia, const DpdTensor& 
 
 void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
-              DpdMultReport* rep)
+              DpdMultReport* rep, bool reference_irrep_check)
 {
     const unsigned nirrep = A.lay.nirrep;
     TB_CHECK(B.lay.nirrep == nirrep && C.lay.nirrep == nirrep, TB_ERR_ARG, "DPD: nirrep differs");
@@ -355,16 +415,30 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
     // src/iface/3t/mult.cxx:270: "A.irrep()^B.irrep() != C.irrep()" parses as
     // A.irrep() ^ (B.irrep() != C.irrep()); kept as is
     const unsigned irrA = A.lay.irrep, irrB = B.lay.irrep, irrC = C.lay.irrep;
-    const bool mismatch = (irrA ^ (unsigned)(irrB != irrC)) != 0;
+    const bool mismatch = reference_irrep_check ? (irrA ^ (unsigned)(irrB != irrC)) != 0
+                                                : (irrA ^ irrB) != irrC;
     const i64 ctotal = C.lay.total();
     if (alpha == 0.0 || (ABC.empty() && mismatch))
     {
-        Strided s; s.ndim = 1; s.len[0] = ctotal; s.stride[0] = 1;
-        if (ctotal > 0)
+        if (beta == 1.0 || ctotal == 0) return;
+        if (C.lay.is_explicit())
         {
-            if (beta == 0.0) l1_set<double>(C.data, s, 0.0, st);
-            else if (beta != 1.0) l1_scale<double>(C.data, s, beta, st);
+            // a view's blocks need not fill [0, extent): scale block by block
+            C.lay.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
+                                     const std::vector<i64>& bs, i64 off)
+            {
+                TB_CHECK(C.lay.ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "DPD: too many dimensions");
+                Strided s;
+                s.ndim = (int)C.lay.ndim;
+                for (unsigned d = 0; d < C.lay.ndim; d++) { s.len[d] = bl[d]; s.stride[d] = bs[d]; }
+                if (beta == 0.0) l1_set<double>(C.data + off, s, 0.0, st);
+                else l1_scale<double>(C.data + off, s, beta, st);
+            });
+            return;
         }
+        Strided s; s.ndim = 1; s.len[0] = ctotal; s.stride[0] = 1;
+        if (beta == 0.0) l1_set<double>(C.data, s, 0.0, st);
+        else l1_scale<double>(C.data, s, beta, st);
         return;
     }
     TB_CHECK(ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
@@ -374,6 +448,18 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
     // (BC), A then B (AB)
     auto dense_stride = [](const DpdTensor& X, unsigned d)
     {
+        if (X.lay.is_explicit())
+        {
+            // a view's own strides, taken from its first stored block
+            i64 s = 0;
+            bool found = false;
+            X.lay.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>&,
+                                     const std::vector<i64>& bs, i64)
+            {
+                if (!found) { s = bs[d]; found = true; }
+            });
+            return s;
+        }
         // row-major layouts: last dimension fastest
         const bool cm = X.lay.layout == 0 || X.lay.layout == 2 || X.lay.layout == 4;
         i64 s = 1;

@@ -18,10 +18,41 @@ struct DpdLayout
     std::vector<std::vector<i64>> size;           // [2*ndim-1][nirrep] subtree sizes
     std::vector<unsigned> leaf, parent, perm;
 
+    // explicit block table (layout = -1): the geometry of every stored block
+    // as the caller's view reports it, for views that are not one of the six
+    // MArray storage layouts (permuted or sliced views)
+    std::vector<i64> xoff;                        // [nirrep^ndim] offset per irrep tuple (dim 0 fastest), -1 = none
+    std::vector<i64> xstride;                     // [nirrep^ndim][ndim]
+    i64 xextent = 0;                              // elements from the data base past the last stored element
+
     void init(unsigned irrep, unsigned nirrep, unsigned ndim, const i64* lens, int layout);
+    void init_explicit(unsigned irrep, unsigned nirrep, unsigned ndim, const i64* lens, const i64* offsets,
+                       const i64* strides);
+    bool is_explicit() const { return !xoff.empty(); }
     // block (one irrep per dimension): lengths, strides, offset from the data base
     void block(const unsigned* irreps, i64* blen, i64* bstride, i64& offset) const;
-    i64 total() const { return size.empty() ? 0 : size[2*ndim - 2][irrep]; }
+    i64 total() const { return is_explicit() ? xextent : size.empty() ? 0 : size[2*ndim - 2][irrep]; }
+    // every stored block with a non-zero extent: irreps, lengths, strides, offset
+    template <typename F> void for_each_block(F&& f) const
+    {
+        std::vector<unsigned> irr(ndim, 0);
+        std::vector<i64> bl(ndim), bs(ndim);
+        while (true)
+        {
+            unsigned x = 0;
+            i64 ext = 1;
+            for (unsigned d = 0; d < ndim; d++) { x ^= irr[d]; ext *= len[d][irr[d]]; }
+            if (x == irrep && ext > 0)
+            {
+                i64 off;
+                block(irr.data(), bl.data(), bs.data(), off);
+                f(irr, bl, bs, off);
+            }
+            unsigned d = 0;
+            while (d < ndim && ++irr[d] == nirrep) { irr[d] = 0; d++; }
+            if (d == ndim) break;
+        }
+    }
 };
 
 // src/external/marray/include/dpd_marray_base.hpp:34-67
@@ -41,8 +72,12 @@ struct DpdMultReport
     int variant = 0;              // tile configuration picked by the tuner
 };
 
+// reference_irrep_check: skip the contraction as src/iface/3t/mult.cxx:270
+// does (its operator precedence included); false: skip only when
+// irrep(A) ^ irrep(B) != irrep(C), as the internal block loops of the
+// indexed-DPD contraction see it
 void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
-              DpdMultReport* rep);
+              DpdMultReport* rep, bool reference_irrep_check = true);
 
 } // namespace tb

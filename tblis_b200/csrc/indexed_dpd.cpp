@@ -1,0 +1,394 @@
+// indexed_dpd.cpp -- contraction of indexed DPD tensors (MArray's
+// indexed_dpd_varray: a list of DPD tensors over the "dense" dimensions, one
+// per index tuple of the "indexed" dimensions, each with a scalar factor).
+//
+// Semantics (src/iface/3t/mult.cxx:412-533 and the FULL form of
+// src/internal/3t/indexed_dpd/mult.cxx:68-114 with
+// src/internal/1t/indexed_dpd/util.hpp:14-113): every entry i of C is first
+// scaled by f^C_i*beta (beta == 1: untouched; beta == 0 or f^C_i == 0: set
+// to zero), then
+//     C_i += alpha * f^C_i * sum_{j,k} f^A_j f^B_k (A_j . B_k)
+// over the entries j of A and k of B whose index values agree with C_i's and
+// with each other on every shared indexed label. A label indexed in one tensor
+// and dense in another selects one slice (the indexed irrep, the index value)
+// of the dense dimension.
+//
+// GPU form: each consistent (i, j, k) triple is a DPD contraction over the
+// labels that are dense everywhere. Its operands are the entries' storage
+// with the selected slices folded into per-block offsets (an explicit block
+// table), so no dense copy of any tensor is made; every triple runs through
+// the grouped persistent FP64 kernel with the factor-weighted alpha and
+// beta = 1 on top of the initial scaling.
+#include "common.hpp"
+#include "dpd.hpp"
+#include "level1.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+
+namespace tb
+{
+
+namespace
+{
+
+struct IdxTensor
+{
+    unsigned ndim = 0, dense_ndim = 0, nirrep = 1, dense_irrep = 0;
+    std::vector<std::vector<i64>> len;          // [ndim][nirrep]
+    std::vector<unsigned> idx_irrep;            // [ndim - dense_ndim]
+    i64 nidx = 0;
+    std::vector<i64> indices;                   // [nidx][ndim - dense_ndim]
+    std::vector<double*> data;                  // per entry (device after staging)
+    std::vector<double> factor;
+    DpdLayout dense;                            // block table of one entry, relative to its data
+    unsigned irrep() const
+    {
+        unsigned x = dense_irrep;
+        for (unsigned r : idx_irrep) x ^= r;
+        return x;
+    }
+    unsigned nindexed() const { return ndim - dense_ndim; }
+    i64 index(i64 entry, unsigned d) const { return indices[(size_t)entry*nindexed() + d]; }
+};
+
+void parse(const tblis_b200_indexed_dpd_tensor* t, IdxTensor& x)
+{
+    TB_CHECK(t, TB_ERR_ARG, "null indexed DPD tensor");
+    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "indexed DPD: only double is supported");
+    TB_CHECK(t->dense_ndim >= 1 && t->dense_ndim <= t->ndim, TB_ERR_ARG, "indexed DPD: needs 1..ndim dense dimensions");
+    TB_CHECK(t->nidx >= 1, TB_ERR_ARG, "indexed DPD: needs at least one index entry");
+    TB_CHECK(t->len && t->data && t->offset && t->stride, TB_ERR_ARG, "indexed DPD: null array");
+    x.ndim = t->ndim; x.dense_ndim = t->dense_ndim; x.nirrep = t->nirrep; x.dense_irrep = t->dense_irrep;
+    const unsigned ni = t->ndim - t->dense_ndim;
+    TB_CHECK(ni == 0 || (t->idx_irrep && t->indices), TB_ERR_ARG, "indexed DPD: null index arrays");
+    TB_CHECK(ni > 0 || t->nidx == 1, TB_ERR_ARG, "indexed DPD: several entries need indexed dimensions");
+    x.len.assign(x.ndim, std::vector<i64>(x.nirrep));
+    for (unsigned d = 0; d < x.ndim; d++)
+        for (unsigned r = 0; r < x.nirrep; r++) x.len[d][r] = t->len[(size_t)d*x.nirrep + r];
+    x.idx_irrep.assign(t->idx_irrep, t->idx_irrep + ni);
+    for (unsigned d = 0; d < ni; d++) TB_CHECK(x.idx_irrep[d] < x.nirrep, TB_ERR_ARG, "indexed DPD: bad indexed irrep");
+    x.nidx = t->nidx;
+    x.indices.assign(t->indices, t->indices + (size_t)t->nidx*ni);
+    for (i64 e = 0; e < x.nidx; e++)
+        for (unsigned d = 0; d < ni; d++)
+        {
+            const i64 v = x.index(e, d);
+            TB_CHECK(v >= 0 && v < x.len[t->dense_ndim + d][x.idx_irrep[d]], TB_ERR_ARG,
+                     "indexed DPD: index value out of range");
+        }
+    x.data.assign(t->data, t->data + t->nidx);
+    x.factor.assign(t->factor ? t->factor : nullptr, t->factor ? t->factor + t->nidx : nullptr);
+    if (!t->factor) x.factor.assign(t->nidx, 1.0);
+    std::vector<i64> dl((size_t)x.dense_ndim*x.nirrep);
+    for (unsigned d = 0; d < x.dense_ndim; d++)
+        for (unsigned r = 0; r < x.nirrep; r++) dl[(size_t)d*x.nirrep + r] = x.len[d][r];
+    x.dense.init_explicit(x.dense_irrep, x.nirrep, x.dense_ndim, dl.data(), t->offset, t->stride);
+}
+
+// device copies of host-resident entries
+struct EntryStage
+{
+    std::vector<dbuf> bufs;
+    std::vector<std::pair<double*, double*>> back;      // (host, device) to copy out
+    void init(IdxTensor& x, bool copy_in, bool copy_out, cudaStream_t st)
+    {
+        const i64 n = x.dense.total();
+        for (auto& p : x.data)
+        {
+            if (!p || n == 0 || pointer_kind(p) == MEM_DEVICE) continue;
+            bufs.emplace_back((size_t)n*sizeof(double), st);
+            double* d = bufs.back().as<double>();
+            if (copy_in) TB_CUDA(cudaMemcpyAsync(d, p, (size_t)n*sizeof(double), cudaMemcpyHostToDevice, st));
+            if (copy_out) back.push_back({p, d});
+            p = d;
+        }
+    }
+    void out(i64 n, cudaStream_t st)
+    {
+        for (auto& hd : back)
+            TB_CUDA(cudaMemcpyAsync(hd.first, hd.second, (size_t)n*sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    bool staged() const { return !bufs.empty(); }
+};
+
+// one operand of a triple: which dense dims stay, which are sliced
+struct Slicing
+{
+    std::vector<unsigned> keep;                     // dense dims that stay (in order)
+    std::vector<unsigned> cut;                      // dense dims fixed to one (irrep, value)
+    std::vector<unsigned> cut_irrep;
+    std::vector<int> cut_label;                     // label of each cut dim
+    std::string labels;                             // labels of the kept dims
+};
+
+// the DPD tensor of entry `e` of x with the cut dims fixed to `values`
+// (parallel to s.cut); false when a cut value lies outside its block
+bool slice_entry(const IdxTensor& x, i64 e, const Slicing& s, const std::vector<i64>& values,
+                 unsigned ndummy, DpdTensor& out)
+{
+    const unsigned nk = (unsigned)s.keep.size();
+    const unsigned nd = nk + ndummy;
+    const unsigned nirrep = x.nirrep;
+    unsigned irrep = x.dense_irrep;
+    for (size_t c = 0; c < s.cut.size(); c++)
+    {
+        irrep ^= s.cut_irrep[c];
+        if (values[c] < 0 || values[c] >= x.len[s.cut[c]][s.cut_irrep[c]]) return false;
+    }
+    std::vector<i64> lens((size_t)nd*nirrep, 0);
+    for (unsigned k = 0; k < nk; k++)
+        for (unsigned r = 0; r < nirrep; r++) lens[(size_t)k*nirrep + r] = x.len[s.keep[k]][r];
+    for (unsigned u = 0; u < ndummy; u++) lens[(size_t)(nk + u)*nirrep + 0] = 1;     // one element, irrep 0
+    size_t nt = 1;
+    for (unsigned d = 0; d < nd; d++) nt *= nirrep;
+    std::vector<i64> off(nt, -1), str(nt*nd, 0);
+    std::vector<unsigned> sub(nd, 0), full(x.dense_ndim, 0);
+    std::vector<i64> bl(x.dense_ndim), bs(x.dense_ndim);
+    for (size_t t = 0; t < nt; t++)
+    {
+        unsigned xr = 0;
+        i64 ext = 1;
+        for (unsigned d = 0; d < nd; d++)
+        {
+            xr ^= sub[d];
+            ext *= lens[(size_t)d*nirrep + sub[d]];
+        }
+        if (xr == irrep && ext > 0)
+        {
+            for (unsigned k = 0; k < nk; k++) full[s.keep[k]] = sub[k];
+            for (size_t c = 0; c < s.cut.size(); c++) full[s.cut[c]] = s.cut_irrep[c];
+            i64 o;
+            x.dense.block(full.data(), bl.data(), bs.data(), o);
+            for (size_t c = 0; c < s.cut.size(); c++) o += values[c]*bs[s.cut[c]];
+            off[t] = o;
+            for (unsigned k = 0; k < nk; k++) str[t*nd + k] = bs[s.keep[k]];
+            for (unsigned u = 0; u < ndummy; u++) str[t*nd + nk + u] = 1;
+        }
+        unsigned d = 0;
+        while (d < nd && ++sub[d] == nirrep) { sub[d] = 0; d++; }
+    }
+    out.lay = DpdLayout();
+    out.lay.init_explicit(irrep, nirrep, nd, lens.data(), off.data(), str.data());
+    out.data = x.data[e];
+    return true;
+}
+
+} // namespace
+
+void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
+                      const tblis_b200_indexed_dpd_tensor* B_, const label_type* idx_B,
+                      tblis_b200_indexed_dpd_tensor* C_, const label_type* idx_C,
+                      tblis_b200_report* report)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    const int k0 = (int)g_kernel_count.load();
+    IdxTensor A, B, C;
+    parse(A_, A); parse(B_, B); parse(C_, C);
+    TB_CHECK(B.nirrep == A.nirrep && C.nirrep == A.nirrep, TB_ERR_ARG, "indexed DPD: nirrep differs");
+    const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim), iC(idx_C, C.ndim);
+    for (const std::string* s : {&iA, &iB, &iC})
+        for (size_t i = 0; i < s->size(); i++)
+            for (size_t j = 0; j < i; j++)
+                TB_CHECK((*s)[i] != (*s)[j], TB_ERR_ARG, "indexed DPD: repeated label in one tensor");
+    // every label in exactly two or three tensors, equal per-irrep lengths
+    const IdxTensor* T[3] = {&A, &B, &C};
+    const std::string* I[3] = {&iA, &iB, &iC};
+    for (int t = 0; t < 3; t++)
+        for (size_t p = 0; p < I[t]->size(); p++)
+        {
+            const char c = (*I[t])[p];
+            int n = 0;
+            for (int u = 0; u < 3; u++)
+            {
+                const size_t q = I[u]->find(c);
+                if (q == std::string::npos) continue;
+                n++;
+                TB_CHECK(T[u]->len[q] == T[t]->len[p], TB_ERR_ARG, "indexed DPD: per-irrep lengths differ");
+            }
+            TB_CHECK(n >= 2, TB_ERR_ARG, "indexed DPD: a label appears in one tensor only");
+        }
+
+    const double alpha = A_->scalar.data.d*B_->scalar.data.d, beta = C_->scalar.data.d;
+
+    EntryStage sa, sb, sc;
+    sa.init(A, true, false, st);
+    sb.init(B, true, false, st);
+    sc.init(C, beta != 0.0, true, st);
+
+    // beta through the entries' factors (src/internal/3t/indexed_dpd/mult.cxx:1217-1224
+    // with src/internal/1t/indexed_dpd/scale.cxx and set.cxx): beta == 1
+    // leaves C, beta == 0 or a zero factor sets the entry to 0, otherwise
+    // entry e is scaled by f_e*beta
+    if (beta != 1.0)
+        for (i64 e = 0; e < C.nidx; e++)
+            C.dense.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
+                                       const std::vector<i64>& bs, i64 off)
+            {
+                TB_CHECK(C.dense_ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "indexed DPD: too many dimensions");
+                Strided s;
+                s.ndim = (int)C.dense_ndim;
+                for (unsigned d = 0; d < C.dense_ndim; d++) { s.len[d] = bl[d]; s.stride[d] = bs[d]; }
+                if (beta == 0.0 || C.factor[e] == 0.0) l1_set<double>(C.data[e] + off, s, 0.0, st);
+                else l1_scale<double>(C.data[e] + off, s, C.factor[e]*beta, st);
+            });
+
+    // labels shared by all three tensors must not be dense in all of them
+    // (batch labels are not supported, as in the DPD contraction)
+    auto indexed_in = [&](int t, char c, unsigned& slot)
+    {
+        const size_t p = I[t]->find(c);
+        if (p == std::string::npos || p < T[t]->dense_ndim) return false;
+        slot = (unsigned)(p - T[t]->dense_ndim);
+        return true;
+    };
+
+    // src/iface/3t/mult.cxx:514 (with its operator precedence) and the
+    // indexed-irrep agreement of src/internal/3t/indexed_dpd/mult.cxx:1226-1280
+    bool has_abc = false;
+    for (char c : iA) if (iB.find(c) != std::string::npos && iC.find(c) != std::string::npos) has_abc = true;
+    bool skip = alpha == 0.0 || (!has_abc && (A.irrep() ^ (unsigned)(B.irrep() != C.irrep())) != 0);
+    // fixed (irrep) of every label indexed somewhere; they must agree
+    std::map<char, unsigned> fixed_irrep;
+    for (int t = 0; t < 3 && !skip; t++)
+        for (unsigned d = 0; d < T[t]->nindexed(); d++)
+        {
+            const char c = (*I[t])[T[t]->dense_ndim + d];
+            auto it = fixed_irrep.find(c);
+            if (it == fixed_irrep.end()) fixed_irrep[c] = T[t]->idx_irrep[d];
+            else if (it->second != T[t]->idx_irrep[d]) skip = true;
+        }
+
+    int launches = 0;
+    double flops = 0;
+    if (!skip)
+    {
+        for (char c : iA)
+        {
+            if (iB.find(c) == std::string::npos || iC.find(c) == std::string::npos) continue;
+            TB_CHECK(fixed_irrep.count(c), TB_ERR_ARG,
+                     "indexed DPD: labels dense in all three tensors are not supported on the GPU path");
+        }
+        // per tensor: dense dims kept (label dense everywhere) or cut (label indexed elsewhere)
+        Slicing S[3];
+        for (int t = 0; t < 3; t++)
+            for (unsigned d = 0; d < T[t]->dense_ndim; d++)
+            {
+                const char c = (*I[t])[d];
+                auto it = fixed_irrep.find(c);
+                if (it == fixed_irrep.end()) { S[t].keep.push_back(d); S[t].labels.push_back(c); }
+                else { S[t].cut.push_back(d); S[t].cut_irrep.push_back(it->second); S[t].cut_label.push_back(c); }
+            }
+        // labels for tensors left without dims: a length-1 dimension shared
+        // with a partner (AB for A or B, AC for C)
+        std::string used = iA + iB + iC;
+        auto fresh = [&]()
+        {
+            for (int c = 33; c < 127; c++)
+                if (used.find((char)c) == std::string::npos) { used.push_back((char)c); return (char)c; }
+            throw error(TB_ERR_ARG, "indexed DPD: no free label");
+        };
+        unsigned dumA = 0, dumB = 0, dumC = 0;
+        std::string lA = S[0].labels, lB = S[1].labels, lC = S[2].labels;
+        if (lA.empty() || lB.empty())
+        {
+            const char k = fresh();               // contracted, length 1
+            lA.push_back(k); lB.push_back(k); dumA++; dumB++;
+        }
+        if (lC.empty())
+        {
+            const char m = fresh();               // A and C, length 1
+            lA.push_back(m); lC.push_back(m); dumA++; dumC++;
+        }
+
+        // value of every fixed label for a given entry of a tensor
+        auto value_of = [&](int t, i64 e, char c, i64& v)
+        {
+            unsigned slot;
+            if (!indexed_in(t, c, slot)) return false;
+            v = T[t]->index(e, slot);
+            return true;
+        };
+        // entries of A and B keyed by the values of the fixed labels they index
+        for (i64 ec = 0; ec < C.nidx; ec++)
+        {
+            for (i64 ea = 0; ea < A.nidx; ea++)
+            {
+                // A and C agree on labels indexed in both
+                bool ok = true;
+                for (unsigned d = 0; d < A.nindexed() && ok; d++)
+                {
+                    const char c = iA[A.dense_ndim + d];
+                    i64 v;
+                    if (value_of(2, ec, c, v) && v != A.index(ea, d)) ok = false;
+                }
+                if (!ok) continue;
+                for (i64 eb = 0; eb < B.nidx; eb++)
+                {
+                    bool okb = true;
+                    for (unsigned d = 0; d < B.nindexed() && okb; d++)
+                    {
+                        const char c = iB[B.dense_ndim + d];
+                        i64 v;
+                        if (value_of(0, ea, c, v) && v != B.index(eb, d)) okb = false;
+                        if (value_of(2, ec, c, v) && v != B.index(eb, d)) okb = false;
+                    }
+                    if (!okb) continue;
+                    // the value of every cut label, from whichever tensor indexes it
+                    auto cut_values = [&](int t, std::vector<i64>& vals)
+                    {
+                        vals.clear();
+                        for (char c : S[t].cut_label)
+                        {
+                            i64 v = -1;
+                            if (!value_of(0, ea, c, v) && !value_of(1, eb, c, v)) value_of(2, ec, c, v);
+                            vals.push_back(v);
+                        }
+                    };
+                    std::vector<i64> vA, vB, vC;
+                    cut_values(0, vA); cut_values(1, vB); cut_values(2, vC);
+                    DpdTensor a, b, c;
+                    if (!slice_entry(A, ea, S[0], vA, dumA, a) || !slice_entry(B, eb, S[1], vB, dumB, b) ||
+                        !slice_entry(C, ec, S[2], vC, dumC, c))
+                        continue;
+                    const double w = alpha*A.factor[ea]*B.factor[eb]*C.factor[ec];
+                    if (w == 0.0) continue;
+                    DpdMultReport r;
+                    dpd_mult(a, lA.c_str(), b, lB.c_str(), c, lC.c_str(), w, 1.0, st, &r, false);
+                    launches += r.groups > 0;
+                    flops += r.flops;
+                }
+            }
+        }
+    }
+
+    sc.out(C.dense.total(), st);
+    if (sa.staged() || sb.staged() || sc.staged()) TB_CUDA(cudaStreamSynchronize(st));
+    C_->scalar.data.d = 1.0;
+    C_->scalar.type = TYPE_DOUBLE;
+    if (report)
+    {
+        memset(report, 0, sizeof(*report));
+        report->method = 1;
+        report->flops = flops;
+        report->m = launches;            // triples that ran a grouped launch
+        report->kernels = (int)(g_kernel_count.load() - k0);
+    }
+}
+
+} // namespace tb
+
+extern "C" {
+
+int tblis_b200_indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                                const tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B,
+                                      tblis_b200_indexed_dpd_tensor* C, const label_type* idx_C,
+                                tblis_b200_report* report)
+{
+    return tb::guarded([&] { tb::indexed_dpd_mult(A, idx_A, B, idx_B, C, idx_C, report); });
+}
+
+}

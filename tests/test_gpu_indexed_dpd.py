@@ -1,0 +1,106 @@
+"""GPU parity of the indexed-DPD contraction (tblis_b200_indexed_dpd_mult,
+the entry of tblis::mult over indexed_dpd_varray_view) against the
+reference's own indexed-DPD contraction on the same storage: label mixes with
+indexed labels in the output, contracted over, or slicing a dense dimension,
+entry factors including zero, and every kind of beta."""
+import copy
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.idx_dpd_helpers import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu(torch, dev, nirrep, alpha, A, iA, B, iB, beta, C, iC):
+    import tblis_b200 as tb
+
+    def wrap(T):
+        data = torch.from_numpy(T["data"]).to(dev)
+        t = tb.IndexedDpdTensor(T["irrep"], nirrep, T["lens"], T["idx_irreps"], T["indices"], data, T["factors"])
+        assert t.dense_size() * t.nidx == len(T["data"])
+        return t, data
+    a, _ = wrap(A)
+    b, _ = wrap(B)
+    c, dc = wrap(C)
+    rep = tb.indexed_dpd_mult(alpha, a, iA, b, iB, beta, c, iC)
+    torch.cuda.synchronize()
+    return dc.cpu().numpy(), rep
+
+
+@pytest.mark.parametrize("name,build", cases())
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.5])
+def test_matches_reference(cuda, name, build, beta):
+    import torch
+    rng = np.random.default_rng(sum(map(ord, name)) + 7)
+    n, A, iA, B, iB, C, iC = build(rng)
+    want = copy.deepcopy(C)
+    oracle.ref_indexed_dpd_mult(n, 0.7, A, iA, B, iB, beta, want, iC, impl=0)
+    got, rep = _gpu(torch, cuda, n, 0.7, A, iA, B, iB, beta, C, iC)
+    scale = max(1.0, np.linalg.norm(want["data"]))
+    assert np.linalg.norm(got - want["data"]) <= 1e-13 * scale, name
+
+
+def test_zero_factor_and_host_storage(cuda):
+    """A zero C factor clears its entry; host (numpy) storage is staged."""
+    import tblis_b200 as tb
+    rng = np.random.default_rng(5)
+    n, A, iA, B, iB, C, iC = dict(cases())["ladder_indexed_j"](rng)
+    C["factors"] = [0.0, 1.0, 2.0]
+    want = copy.deepcopy(C)
+    oracle.ref_indexed_dpd_mult(n, 1.0, A, iA, B, iB, 0.25, want, iC, impl=0)
+    mk = lambda T: tb.IndexedDpdTensor(T["irrep"], n, T["lens"], T["idx_irreps"], T["indices"], T["data"],
+                                       T["factors"])
+    c = mk(C)
+    tb.indexed_dpd_mult(1.0, mk(A), iA, mk(B), iB, 0.25, c, iC)
+    assert np.linalg.norm(C["data"] - want["data"]) <= 1e-13 * max(1.0, np.linalg.norm(want["data"]))
+
+
+def test_mismatched_indexed_irreps_only_scale(cuda):
+    """Labels indexed with different irreps in two tensors contribute
+    nothing: C is only scaled (src/internal/3t/indexed_dpd/mult.cxx:1226-1280)."""
+    import torch
+    from tests.idx_dpd_helpers import make
+    rng = np.random.default_rng(9)
+    n, A, iA, B, iB, _, iC = dict(cases())["ladder_indexed_j"](rng)
+    v, o = [3, 2], [2, 3]
+    # j indexed with irrep 1 in B but irrep 0 in C
+    C = make(rng, n, 0, [v, v, o, o], [0], [[0], [1]], factors=[1.0, 3.0])
+    want = copy.deepcopy(C)
+    oracle.ref_indexed_dpd_mult(n, 1.0, A, iA, B, iB, 0.5, want, iC, impl=0)
+    got, rep = _gpu(torch, cuda, n, 1.0, A, iA, B, iB, 0.5, C, iC)
+    assert np.linalg.norm(got - want["data"]) <= 1e-14 * max(1.0, np.linalg.norm(want["data"]))
+    assert rep["m"] == 0
+
+
+def test_cxx_overload_matches_reference(cuda):
+    """tblis::mult over indexed_dpd_varray_view through its mangled C++ name
+    (libtblis_b200_cxx.so), on owning MArray tensors as a TBLIS program has."""
+    import ctypes
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "cxx", "_bin",
+                        "libdpd_driver.so")
+    assert os.path.exists(path), "C++ test driver not built (make -C tests/cxx MARRAY=...)"
+    drv = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+    sz = ctypes.c_ssize_t
+    for name, build in cases():
+        rng = np.random.default_rng(sum(map(ord, name)) + 11)
+        n, A, iA, B, iB, C, iC = build(rng)
+        want = copy.deepcopy(C)
+        oracle.ref_indexed_dpd_mult(n, 1.25, A, iA, B, iB, 0.5, want, iC, impl=0)
+
+        def args(T, lab):
+            nidim = len(T["idx_irreps"])
+            idx = [x for t in T["indices"] for x in t]
+            nidx = max(1, len(T["indices"])) if nidim else 1
+            return [ctypes.c_uint(T["irrep"]), ctypes.c_uint(len(T["lens"])),
+                    (sz * (len(T["lens"]) * n))(*[x for r in T["lens"] for x in r]), ctypes.c_uint(nidim),
+                    (ctypes.c_uint * max(1, nidim))(*T["idx_irreps"]), ctypes.c_long(nidx),
+                    (sz * max(1, len(idx)))(*idx), ctypes.c_void_p(T["data"].ctypes.data),
+                    (ctypes.c_double * nidx)(*T["factors"]), lab.encode()]
+        rc = drv.driver_indexed_dpd_mult(ctypes.c_uint(n), ctypes.c_double(1.25), *args(A, iA), *args(B, iB),
+                                         ctypes.c_double(0.5), *args(C, iC))
+        assert rc == 0, name
+        assert np.linalg.norm(C["data"] - want["data"]) <= 1e-13 * max(1.0, np.linalg.norm(want["data"])), name
