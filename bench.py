@@ -32,7 +32,7 @@ FLOPS_LADDER = 2.0 * V * V * V * V * O * O
 WORKLOAD = "ladder C[abij]=A[abef]*B[efij] o=48 v=160 fp64 exponent spread 2^[-20,20]"
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=10)
@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--v", type=int, default=160, help="virtual extent")
     p.add_argument("--case", default=None, choices=["ring", "transpose"],
                    help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
-    a = p.parse_args()
+    a = p.parse_args(argv)
     global O, V, FLOPS_LADDER, WORKLOAD
     if (a.o, a.v) != (O, V):
         O, V = a.o, a.v
@@ -335,13 +335,22 @@ def main():
     k_total_ms, k_launches = tb.kernel_time(kname)
     tb.kernel_timer(False)
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = t.item()
-        dist.barrier()
+    total_ms = max_over_ranks(dist, torch, total_ms, dev)
     ms_per_step = total_ms / args.steps
-    value = world * FLOPS_LADDER * args.steps / (total_ms * 1e-3) / 1e9
+    value = job_value(world, args.steps, total_ms)
+
+    # end to end through the C ABI with pinned host buffers (copies inside the
+    # timed region), on every rank, max over ranks; del the device copies first
+    e2e = None
+    if not args.no_e2e:
+        del A, B, C
+        torch.cuda.empty_cache()
+        if dist:
+            dist.barrier()
+        e2e = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)), rank)
+        e2e_ms = max_over_ranks(dist, torch, e2e["ms_per_step"], dev)
+        e2e["ms_per_step"] = e2e_ms
+        e2e["value"] = job_value(world, 1, e2e_ms)
 
     result = {
         "metric": "contraction GFLOP/s at <=1e-12 normwise rel err",
@@ -355,8 +364,14 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if e2e:
+        result["e2e"] = e2e
 
     if rank == 0:
+        if e2e:
+            A = spread_tensor(torch, [V, V, V, V], 1001, dev)
+            B = spread_tensor(torch, [V, V, O, O], 1002, dev)
+            C = torch.zeros((O, O, V, V), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
         peaks = load_peaks()
         extra = {}
         # plain FP64 rate on the same workload and the roofline of its kernel
@@ -398,17 +413,15 @@ def main():
                                   "share_of_step": k_total_ms / total_ms,
                                   "fp64_equivalent_tflops_kernel": FLOPS_LADDER * units_per_launch /
                                                                    (launch_ms * 1e-3) / 1e12}
-        if not args.no_extra:
+        if not args.no_extra and world == 1:
             extra["precision_variants"] = precision_variants(torch, tb, A, B, C, stream)
         del A, B, C
         torch.cuda.empty_cache()
 
-        if not args.no_extra:
+        # the secondary workloads are single-GPU; with several ranks the others
+        # would wait at the closing barrier for minutes
+        if not args.no_extra and world == 1:
             extra.update(extra_workloads(torch, tb, dev, stream, peaks))
-
-        # end-to-end through the C ABI with pinned host buffers (copies inside the timed region)
-        if not args.no_e2e:
-            result["e2e"] = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)))
 
         if world == 1 and not args.no_cpu:
             cb = cpu_reference_sample()
@@ -450,9 +463,25 @@ def precision_variants(torch, tb, A, B, C, stream):
     return out
 
 
-def e2e_ladder(torch, tb, method, steps):
-    A = spread_tensor(torch, [V, V, V, V], 1001, torch.device("cuda")).cpu().pin_memory()
-    B = spread_tensor(torch, [V, V, O, O], 1002, torch.device("cuda")).cpu().pin_memory()
+def max_over_ranks(dist, torch, value, dev):
+    """The largest of one scalar over all ranks (the job's time is its
+    slowest rank's); the value itself with one process."""
+    if not dist:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return t.item()
+
+
+def job_value(world, steps, total_ms):
+    """Whole-job GFLOP/s: every rank contracts its own ladder per step."""
+    return world * FLOPS_LADDER * steps / (total_ms * 1e-3) / 1e9
+
+
+def e2e_ladder(torch, tb, method, steps, rank=0):
+    A = spread_tensor(torch, [V, V, V, V], 1001 + rank, torch.device("cuda")).cpu().pin_memory()
+    B = spread_tensor(torch, [V, V, O, O], 1002 + rank, torch.device("cuda")).cpu().pin_memory()
     C = torch.zeros((O, O, V, V), dtype=torch.float64).pin_memory().permute(3, 2, 1, 0)
     h2d = (A.numel() + B.numel()) * 8
     d2h = C.numel() * 8
