@@ -12,6 +12,7 @@
 #include "level1.hpp"
 #include "ozaki.hpp"
 
+#include <algorithm>
 #include <cmath>
 
 namespace tb
@@ -56,11 +57,108 @@ static void stage(StagedOp& o, const tblis_tensor* t, bool copy_in, cudaStream_t
     o.dptr = o.buf.as<double>() - lo;
 }
 
+// A host-resident A is copied in slices on a copy stream while the slices
+// already on the device are contracted. The cut label is A's label of
+// largest stride, when that stride spans everything else A holds, so the
+// slices of A are disjoint, ordered ranges of host memory. A label A shares
+// with C cuts A and C (independent row slices); a label A shares with B (a
+// contracted one) cuts A and B, and the slices accumulate into C (beta for
+// the first, 1 after). Each slice is an ordinary contraction of sub-tensors
+// (shorter extent of the label, data offset to the slice).
+struct Slices
+{
+    int dim_A = -1, dim_C = -1, dim_B = -1;    // the cut label's dimension in A and in C or B
+    std::vector<std::pair<i64, i64>> range;    // [q0, q1) of the label
+    std::vector<std::pair<i64, i64>> fp;       // A footprint [lo, hi] of each slice (elements)
+};
+
+static bool plan_slices(const tblis_tensor* A, const label_type* idx_A, const tblis_tensor* B,
+                        const label_type* idx_B, const tblis_tensor* C, const label_type* idx_C, Slices& sl)
+{
+    constexpr i64 kSliceBytes = (i64)384 << 20;
+    i64 lo, hi;
+    tensor_extent(A->ndim, A->len, A->stride, lo, hi);
+    const i64 bytes = (hi - lo + 1)*8;
+    if (bytes < 2*kSliceBytes) return false;
+    for (unsigned d = 0; d < A->ndim; d++)
+        if (A->stride[d] < 0) return false;
+    // A's dimension of largest stride
+    int q = -1;
+    for (unsigned d = 0; d < A->ndim; d++)
+        if (A->len[d] > 1 && (q < 0 || A->stride[d] > A->stride[q])) q = (int)d;
+    if (q < 0) return false;
+    const label_type c = idx_A[q];
+    int nA = 0, nB = 0, nC = 0, qc = -1, qb = -1;
+    for (unsigned d = 0; d < A->ndim; d++) nA += idx_A[d] == c;
+    for (unsigned d = 0; d < B->ndim; d++) if (idx_B[d] == c) { nB++; qb = (int)d; }
+    for (unsigned d = 0; d < C->ndim; d++) if (idx_C[d] == c) { nC++; qc = (int)d; }
+    if (nA != 1 || nB + nC != 1) return false;
+    // everything else of A fits below one step of the label
+    i64 rest = 0;
+    for (unsigned d = 0; d < A->ndim; d++)
+        if ((int)d != q) rest += (A->len[d] - 1)*A->stride[d];
+    const i64 s = A->stride[q], L = A->len[q];
+    if (s <= rest) return false;
+    const i64 n = std::min<i64>({16, L, std::max<i64>(2, bytes/kSliceBytes)});
+    if (n < 2) return false;
+    const i64 per = (L + n - 1)/n;
+    sl.dim_A = q; sl.dim_C = qc; sl.dim_B = qb;
+    for (i64 q0 = 0; q0 < L; q0 += per)
+    {
+        const i64 q1 = std::min(L, q0 + per);
+        sl.range.push_back({q0, q1});
+        sl.fp.push_back({q0*s, (q1 - 1)*s + rest});
+    }
+    return sl.range.size() >= 2;
+}
+
+static cudaStream_t copy_stream()
+{
+    static cudaStream_t s[64] = {};
+    int dev = 0;
+    TB_CUDA(cudaGetDevice(&dev));
+    TB_CHECK(dev < 64, TB_ERR_ARG, "device index");
+    if (!s[dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
+    return s[dev];
+}
+
 static void unstage(StagedOp& o, cudaStream_t s)
 {
     if (!o.staged) return;
     TB_CUDA(cudaMemcpyAsync(static_cast<double*>(o.host) + o.lo, o.buf.ptr, (size_t)o.n*sizeof(double),
                             cudaMemcpyDeviceToHost, s));
+}
+
+// one contraction on device data (a GEMM view of device-resident operands)
+static void contract_device(const GemmView& v, const double* A, const double* B, double* C, double alpha,
+                            double beta, int method, double tol, int slices, cudaStream_t st,
+                            int& used_slices, double& est_error)
+{
+    if (method >= 2)
+    {
+        // 2: Ozaki INT8 slices, 3: Ozaki BF16 slices, 4: one TF32 pass, 5: one BF16 pass
+        const int kind = method == 2 ? OZ_I8 : method == 4 ? OZ_TF32 : OZ_BF16;
+        OzakiResult r = ozaki_mult(v, A, B, C, alpha, beta, tol, slices, st, kind, method >= 4);
+        used_slices = r.slices;
+        est_error = r.est_error;
+        return;
+    }
+    const i64 BMt = gemm_f64_tile_m(), BNt = gemm_f64_tile_n(), BKt = gemm_f64_tile_k();
+    auto tab = gemm_tables(v, BMt, BNt, BKt, st);
+    GemmF64Args a = {};
+    a.A = A; a.B = B; a.C = C;
+    a.a_m = tab->a_m; a.a_k = tab->a_k; a.b_k = tab->b_k; a.b_n = tab->b_n;
+    a.c_m = tab->c_m; a.c_n = tab->c_n; a.a_l = tab->a_l; a.b_l = tab->b_l; a.c_l = tab->c_l;
+    a.a_kbs = tab->a_kbs; a.b_kbs = tab->b_kbs;
+    a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;
+    a.alpha = alpha; a.beta = beta;
+    a.amode = v.amode; a.bmode = v.bmode;
+    a.splits = gemm_f64_choose_splits(v.m, v.n, v.k, v.l, device_sm_count());
+    dbuf ws(gemm_f64_workspace_bytes(v.m, v.n, v.l, a.splits), st);
+    a.partial = ws.as<double>();
+    gemm_f64_launch(a, st);
+    used_slices = 0;
+    est_error = 1.1e-16*std::sqrt((double)v.k);
 }
 
 void mult_dispatch(const tblis_config* cfg,
@@ -128,39 +226,77 @@ void mult_dispatch(const tblis_config* cfg,
         }
         else
         {
-            stage(sa, A, true, st);
-            stage(sb, B, true, st);
             TB_CHECK(method >= 1 && method <= 5, TB_ERR_ARG, "unknown contraction method");
-            if (method >= 2)
+            stage(sb, B, true, st);
+            Slices sl;
+            const bool sliced = A->data && pointer_kind(A->data) == MEM_HOST &&
+                                plan_slices(A, idx_A, B, idx_B, C, idx_C, sl);
+            stage(sa, A, !sliced, st);
+            int used = 0;
+            double est = 0;
+            if (sliced)
             {
-                // 2: Ozaki INT8 slices, 3: Ozaki BF16 slices, 4: one TF32 pass, 5: one BF16 pass
-                const int kind = method == 2 ? OZ_I8 : method == 4 ? OZ_TF32 : OZ_BF16;
-                OzakiResult r = ozaki_mult(v, static_cast<const double*>(sa.dptr),
-                                           static_cast<const double*>(sb.dptr),
-                                           static_cast<double*>(sc.dptr), alpha, beta, tol, slices, st,
-                                           kind, method >= 4);
-                if (report) { report->slices = r.slices; report->est_error = r.est_error; }
+                // copies on the copy stream (once the buffer exists), each
+                // slice's contraction on st after its copy
+                cudaStream_t cs = copy_stream();
+                cudaEvent_t ready;
+                TB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+                TB_CUDA(cudaEventRecord(ready, st));
+                TB_CUDA(cudaStreamWaitEvent(cs, ready, 0));
+                std::vector<cudaEvent_t> ev(sl.range.size());
+                for (size_t c = 0; c < sl.range.size(); c++)
+                {
+                    const i64 a = sl.fp[c].first, b = sl.fp[c].second;
+                    TB_CUDA(cudaMemcpyAsync(static_cast<double*>(sa.dptr) + a, static_cast<const double*>(A->data) + a,
+                                            (size_t)(b - a + 1)*sizeof(double), cudaMemcpyHostToDevice, cs));
+                    TB_CUDA(cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming));
+                    TB_CUDA(cudaEventRecord(ev[c], cs));
+                }
+                std::vector<len_type> lenA(A->len, A->len + A->ndim), lenB(B->len, B->len + B->ndim),
+                                      lenC(C->len, C->len + C->ndim);
+                const bool over_k = sl.dim_B >= 0;
+                // slices that accumulate: each meets tol/n, so their sum meets tol
+                const double tol_slice = over_k ? tol/(double)sl.range.size() : tol;
+                for (size_t c = 0; c < sl.range.size(); c++)
+                {
+                    TB_CUDA(cudaStreamWaitEvent(st, ev[c], 0));
+                    const i64 q0 = sl.range[c].first, nq = sl.range[c].second - q0;
+                    tblis_tensor a = *A, b = *B, cc = *C;
+                    lenA[sl.dim_A] = nq;
+                    a.len = lenA.data();
+                    a.data = static_cast<double*>(sa.dptr) + q0*A->stride[sl.dim_A];
+                    b.data = sb.dptr;
+                    cc.data = sc.dptr;
+                    if (over_k)
+                    {
+                        lenB[sl.dim_B] = nq;
+                        b.len = lenB.data();
+                        b.data = static_cast<double*>(sb.dptr) + q0*B->stride[sl.dim_B];
+                    }
+                    else
+                    {
+                        lenC[sl.dim_C] = nq;
+                        cc.len = lenC.data();
+                        cc.data = static_cast<double*>(sc.dptr) + q0*C->stride[sl.dim_C];
+                    }
+                    const GemmView vs = gemm_view(mult_groups(&a, idx_A, &b, idx_B, &cc, idx_C));
+                    int u = 0;
+                    double e = 0;
+                    contract_device(vs, static_cast<const double*>(a.data), static_cast<const double*>(b.data),
+                                    static_cast<double*>(cc.data), alpha, over_k && c > 0 ? 1.0 : beta, method,
+                                    tol_slice, slices, st, u, e);
+                    used = std::max(used, u);
+                    est = over_k ? est + e : std::max(est, e);
+                }
+                for (auto e : ev) cudaEventDestroy(e);
+                cudaEventDestroy(ready);
             }
             else
             {
-                const i64 BMt = gemm_f64_tile_m(), BNt = gemm_f64_tile_n(), BKt = gemm_f64_tile_k();
-                auto tab = gemm_tables(v, BMt, BNt, BKt, st);
-                GemmF64Args a = {};
-                a.A = static_cast<const double*>(sa.dptr);
-                a.B = static_cast<const double*>(sb.dptr);
-                a.C = static_cast<double*>(sc.dptr);
-                a.a_m = tab->a_m; a.a_k = tab->a_k; a.b_k = tab->b_k; a.b_n = tab->b_n;
-                a.c_m = tab->c_m; a.c_n = tab->c_n; a.a_l = tab->a_l; a.b_l = tab->b_l; a.c_l = tab->c_l;
-                a.a_kbs = tab->a_kbs; a.b_kbs = tab->b_kbs;
-                a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;
-                a.alpha = alpha; a.beta = beta;
-                a.amode = v.amode; a.bmode = v.bmode;
-                a.splits = gemm_f64_choose_splits(v.m, v.n, v.k, v.l, device_sm_count());
-                dbuf ws(gemm_f64_workspace_bytes(v.m, v.n, v.l, a.splits), st);
-                a.partial = ws.as<double>();
-                gemm_f64_launch(a, st);
-                if (report) report->est_error = 1.1e-16*std::sqrt((double)v.k);
+                contract_device(v, static_cast<const double*>(sa.dptr), static_cast<const double*>(sb.dptr),
+                                static_cast<double*>(sc.dptr), alpha, beta, method, tol, slices, st, used, est);
             }
+            if (report) { report->slices = used; report->est_error = est; }
         }
     }
 

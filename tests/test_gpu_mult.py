@@ -215,3 +215,32 @@ def test_bad_labels_raise(cuda):
     B5 = torch.ones((5, 2), dtype=torch.float64, device=cuda)
     with pytest.raises(tb.TblisError):
         tb.mult(1.0, A, "ik", B5, "kj", 0.0, C, "ij")  # mismatched k lengths
+
+
+@pytest.mark.parametrize("method,tol", [(1, 1e-13), (2, 1e-12)])
+def test_large_host_operand_pipelined(cuda, method, tol):
+    """A host-resident A of 800 MB is copied in row chunks overlapped with the
+    contraction of the chunks already on the device; the result matches the
+    device-resident call (FP64) or meets the tolerance (Ozaki). A second
+    layout whose row chunks overlap in memory takes the one-copy path."""
+    import torch
+    import tblis_b200 as tb
+    v, o = 100, 8
+    g = torch.Generator(device=cuda)
+    g.manual_seed(3)
+    dA = torch.empty((v, v, v, v), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    dB = torch.empty((v, v, o, o), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    dC = torch.zeros((v, v, o, o), dtype=torch.float64, device=cuda)
+    tb.mult_ex(1.0, dA, "abef", dB, "efij", 0.0, dC, "abij", method=1)
+    torch.cuda.synchronize()
+    want = dC.cpu()
+    hA = dA.cpu().pin_memory()
+    hB = dB.cpu()
+    # the same tensor stored with its rows (a, b) fastest: row chunks overlap
+    for A, lab in ((hA, "abef"), (hA.permute(2, 3, 0, 1).contiguous(), "efab")):
+        C = torch.full((v, v, o, o), 7.0, dtype=torch.float64)
+        rep = tb.mult_ex(1.0, A, lab, hB, "efij", 0.0, C, "abij", method=method, tolerance=tol)
+        err = (torch.linalg.norm(C - want) / torch.linalg.norm(want)).item()
+        assert err <= tol, (lab, err, rep)
+    del dA, dB, dC
+    torch.cuda.empty_cache()
