@@ -87,13 +87,15 @@ def _lab(s):
     return s.encode() if isinstance(s, str) else s
 
 
-def _tensor(a, alpha=1.0, keep=None):
+def _tensor(a, alpha=1.0, keep=None, conj=False):
     L, S = _lens_strides(a)
     t = Tensor()
-    t.type = 1
-    t.conj = 0
-    t.scalar.data[0] = alpha
-    t.scalar.type = 1
+    cplx = a.dtype == np.complex128
+    t.type = 3 if cplx else 1
+    t.conj = 1 if conj else 0
+    t.scalar.data[0] = complex(alpha).real
+    t.scalar.data[1] = complex(alpha).imag if cplx else 0.0
+    t.scalar.type = t.type
     t.data = a.ctypes.data
     t.ndim = a.ndim
     t.len = ctypes.cast(L, _P(_sz))
@@ -214,13 +216,14 @@ def orc_mult_groups(A, idx_A, B, idx_B, C, idx_C):
 
 # ---- the reference itself -----------------------------------------------------------------
 
-def ref_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, threads=None):
+def ref_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, threads=None, conj_A=False, conj_B=False):
+    """The reference's tblis_tensor_mult (double or dcomplex numpy arrays)."""
     keep = []
     r = ref()
     if threads:
         r.tblis_set_num_threads(int(threads))
-    tA = _tensor(A, alpha, keep)
-    tB = _tensor(B, 1.0, keep)
+    tA = _tensor(A, alpha, keep, conj_A)
+    tB = _tensor(B, 1.0, keep, conj_B)
     tC = _tensor(C, beta, keep)
     r.tblis_tensor_mult(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B),
                         ctypes.byref(tC), _lab(idx_C))
@@ -342,3 +345,11 @@ def ref_indexed_dpd_mult(nirrep, alpha, A, idx_A, B, idx_B, beta, C, idx_C, impl
                                          ctypes.c_double(beta), *c, ctypes.c_int(impl))
     if rc:
         raise ValueError("reference indexed dpd mult failed")
+
+
+def ref_dense_impl(impl):
+    """Selects the reference's dense contraction implementation: 0 = its
+    default BLIS-based path, 2 = REFERENCE (mult_ref,
+    src/internal/3t/dense/mult.cxx:653-720), which applies conjugation flags
+    (the default path asserts them off). Returns the previous value."""
+    return shim().refshim_set_dense_impl(int(impl))

@@ -17,6 +17,7 @@
 #include "iface/3t/mult.h"
 #include "iface/1t/add.h"
 #include "internal/3t/dpd/mult.hpp"
+#include "internal/3t/dense/mult.hpp"
 
 using namespace tblis;
 
@@ -32,6 +33,17 @@ extern "C"
 {
 
 int refshim_version() { return 1; }
+
+/* Selects the reference's dense contraction implementation
+ * (src/internal/3t/dense/mult.cxx:24): 0 = BLIS_BASED (default),
+ * 2 = REFERENCE (mult_ref, the one that applies conjugation flags).
+ * Returns the previous value. */
+int refshim_set_dense_impl(int impl)
+{
+    const int old = (int)tblis::internal::impl;
+    tblis::internal::impl = impl == 2 ? tblis::internal::REFERENCE : tblis::internal::BLIS_BASED;
+    return old;
+}
 
 void refshim_fill_block_scatter(unsigned ndim, const len_type* len, const stride_type* stride,
                                 len_type BS, stride_type off, stride_type size,

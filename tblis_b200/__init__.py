@@ -120,6 +120,8 @@ def _dtype_code(x):
         return TYPE_DOUBLE, 8
     if name.endswith("float32"):
         return TYPE_FLOAT, 4
+    if name.endswith("complex128"):
+        return TYPE_DCOMPLEX, 16
     raise TypeError("tblis_b200: unsupported dtype %s" % name)
 
 
@@ -146,6 +148,9 @@ class _View:
         t.scalar.type = code
         if code == TYPE_DOUBLE:
             t.scalar.data[0] = float(scalar)
+        elif code == TYPE_DCOMPLEX:
+            t.scalar.data[0] = complex(scalar).real
+            t.scalar.data[1] = complex(scalar).imag
         else:
             ctypes.cast(ctypes.byref(t.scalar), _P(ctypes.c_float))[0] = float(scalar)
         t.data = ptr

@@ -161,6 +161,167 @@ static void contract_device(const GemmView& v, const double* A, const double* B,
     est_error = 1.1e-16*std::sqrt((double)v.k);
 }
 
+// runs one of this library's C entry points from inside another call and
+// turns its recorded error into an exception
+template <typename F>
+static void checked(F&& f)
+{
+    tblis_b200_clear_error();
+    f();
+    const int c = tblis_b200_last_error();
+    if (c) throw error(c, tblis_b200_last_error_string());
+}
+
+// the double view of a dcomplex tensor: every dimension with twice the
+// stride, plus the real/imaginary dimension (length 2, stride 1) last
+struct ComplexParts
+{
+    std::vector<len_type> len, len2;
+    std::vector<stride_type> stride, stride2;
+    tblis_tensor whole = {}, re = {}, im = {};
+    explicit ComplexParts(const tblis_tensor* X)
+    {
+        for (unsigned d = 0; d < X->ndim; d++) { len.push_back(X->len[d]); stride.push_back(2*X->stride[d]); }
+        len2 = len; stride2 = stride;
+        len2.push_back(2); stride2.push_back(1);
+        whole.type = TYPE_DOUBLE;
+        whole.ndim = X->ndim + 1;
+        whole.len = len2.data();
+        whole.stride = stride2.data();
+        whole.data = X->data;
+        re = whole;
+        re.ndim = X->ndim;
+        re.len = len.data();
+        re.stride = stride.data();
+        im = re;
+    }
+    void place(void* dptr)                      // device pointer of element 0 (real part)
+    {
+        re.data = dptr;
+        im.data = static_cast<double*>(dptr) + 1;
+    }
+};
+
+// C = alpha*op(A)*op(B) + beta*op(C) over dcomplex tensors (op = conjugate
+// when the tensor's conj flag is set), as four real contractions per
+// product on the FP64 (or configured) path: with A = Ar + i sa Ai and
+// B = Br + i sb Bi, A*B = (Ar Br - sa sb Ai Bi) + i (sb Ar Bi + sa Ai Br).
+// A complex beta first scales C in place; a complex alpha doubles the
+// product terms.
+static void mult_complex(const tblis_config* cfg,
+                         const tblis_tensor* A, const label_type* idx_A,
+                         const tblis_tensor* B, const label_type* idx_B,
+                         tblis_tensor* C, const label_type* idx_C,
+                         const tblis_b200_opts* opts, tblis_b200_report* report)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    const int kernels_before = (int)g_kernel_count.load();
+    // alpha = alpha_A*alpha_B (complex), beta = C's scalar (complex)
+    const double ar0 = A->scalar.data.z[0], ai0 = A->scalar.data.z[1];
+    const double br0 = B->scalar.data.z[0], bi0 = B->scalar.data.z[1];
+    const double alr = ar0*br0 - ai0*bi0, ali = ar0*bi0 + ai0*br0;
+    const double ber = C->scalar.data.z[0], bei = C->scalar.data.z[1];
+    const double sa = A->conj ? -1.0 : 1.0, sb = B->conj ? -1.0 : 1.0;
+
+    ComplexParts pa(A), pb(B), pc(C);
+    StagedOp sA, sB, sC;
+    const bool read_c = ber != 0.0 || bei != 0.0;
+    stage(sC, &pc.whole, read_c, st);
+    stage(sA, &pa.whole, true, st);
+    stage(sB, &pb.whole, true, st);
+    pa.place(sA.dptr); pb.place(sB.dptr); pc.place(sC.dptr);
+
+    auto real_add = [&](double alpha, tblis_tensor X, double beta, tblis_tensor Y)
+    {
+        X.scalar.type = TYPE_DOUBLE; X.scalar.data.d = alpha;
+        Y.scalar.type = TYPE_DOUBLE; Y.scalar.data.d = beta;
+        checked([&] { tblis_tensor_add(nullptr, cfg, &X, idx_C, &Y, idx_C); });
+    };
+    // beta: C <- beta*op(C); conj(C) flips the imaginary part first
+    double beta_eff = 1.0;
+    const double ci_sign = C->conj ? -1.0 : 1.0;
+    if (!read_c)
+        beta_eff = 0.0;
+    else if (bei == 0.0 && ci_sign == 1.0)
+        beta_eff = ber;
+    else
+    {
+        // (ber + i bei)(Cr + i s Ci) = (ber Cr - bei s Ci) + i (ber s Ci + bei Cr)
+        std::vector<len_type> dl(pc.len);
+        std::vector<stride_type> ds(pc.len.size());
+        i64 cnt = 1;
+        for (size_t d = 0; d < dl.size(); d++) { ds[d] = cnt; cnt *= dl[d]; }
+        dbuf tmp((size_t)std::max<i64>(cnt, 1)*sizeof(double), st);
+        tblis_tensor T = pc.re;
+        T.data = tmp.ptr;
+        T.stride = ds.data();
+        real_add(1.0, pc.re, 0.0, T);                         // T = Cr
+        real_add(-bei*ci_sign, pc.im, ber, pc.re);            // Cr = ber Cr - bei s Ci
+        real_add(bei, T, ber*ci_sign, pc.im);                 // Ci = ber s Ci + bei T
+        beta_eff = 1.0;
+    }
+
+    // the real products: (X part, Y part, coefficient into Cr, coefficient into Ci)
+    struct Term { const tblis_tensor* x; const tblis_tensor* y; double cr, ci; };
+    const Term terms[4] = {
+        {&pa.re, &pb.re, alr, ali},                       // Ar Br
+        {&pa.im, &pb.im, -alr*sa*sb, -ali*sa*sb},         // Ai Bi
+        {&pa.re, &pb.im, -ali*sb, alr*sb},                // Ar Bi
+        {&pa.im, &pb.re, -ali*sa, alr*sa},                // Ai Br
+    };
+    bool first_r = true, first_i = true;
+    int slices_max = 0;
+    double flops = 0, est = 0;
+    for (const Term& t : terms)
+        for (int part = 0; part < 2; part++)
+        {
+            const double coef = part == 0 ? t.cr : t.ci;
+            if (coef == 0.0) continue;
+            bool& first = part == 0 ? first_r : first_i;
+            tblis_tensor x = *t.x, y = *t.y, z = part == 0 ? pc.re : pc.im;
+            x.scalar.type = y.scalar.type = z.scalar.type = TYPE_DOUBLE;
+            x.scalar.data.d = coef;
+            y.scalar.data.d = 1.0;
+            z.scalar.data.d = first ? beta_eff : 1.0;
+            x.conj = y.conj = z.conj = 0;
+            tblis_b200_report r = {};
+            mult_dispatch(cfg, &x, idx_A, &y, idx_B, &z, idx_C, opts, &r);
+            first = false;
+            slices_max = std::max(slices_max, r.slices);
+            flops += r.flops;
+            est += r.est_error;
+        }
+    // parts that received no product (alpha == 0): beta only
+    for (int part = 0; part < 2; part++)
+    {
+        const bool untouched = part == 0 ? first_r : first_i;
+        if (!untouched || beta_eff == 1.0) continue;
+        tblis_tensor z = part == 0 ? pc.re : pc.im;
+        z.scalar.type = TYPE_DOUBLE; z.scalar.data.d = beta_eff;
+        // beta == 0 overwrites (NaN-safe), as the real path does
+        tblis_scalar zero;
+        zero.type = TYPE_DOUBLE;
+        zero.data.d = 0.0;
+        if (beta_eff == 0.0) checked([&] { tblis_tensor_set(nullptr, cfg, &zero, &z, idx_C); });
+        else checked([&] { tblis_tensor_scale(nullptr, cfg, &z, idx_C); });
+    }
+    unstage(sC, st);
+    if (sA.staged || sB.staged || sC.staged) TB_CUDA(cudaStreamSynchronize(st));
+    C->scalar.type = TYPE_DCOMPLEX;
+    C->scalar.data.z[0] = 1.0;
+    C->scalar.data.z[1] = 0.0;
+    C->conj = 0;
+    if (report)
+    {
+        report->method = opts && opts->method ? opts->method : (cfg ? cfg->method : 1);
+        report->slices = slices_max;
+        report->est_error = est;
+        report->flops = flops;
+        report->kernels = (int)(g_kernel_count.load() - kernels_before);
+    }
+}
+
 void mult_dispatch(const tblis_config* cfg,
                    const tblis_tensor* A, const label_type* idx_A,
                    const tblis_tensor* B, const label_type* idx_B,
@@ -169,8 +330,13 @@ void mult_dispatch(const tblis_config* cfg,
 {
     TB_CHECK(A && B && C, TB_ERR_ARG, "null tensor");
     TB_CHECK(A->type == B->type && A->type == C->type, TB_ERR_TYPE, "mult: operand types differ");
+    if (A->type == TYPE_DCOMPLEX)
+    {
+        mult_complex(cfg, A, idx_A, B, idx_B, C, idx_C, opts, report);
+        return;
+    }
     TB_CHECK(A->type == TYPE_DOUBLE, TB_ERR_TYPE,
-             "mult: only double is supported on the GPU path");
+             "mult: double and dcomplex are supported on the GPU path");
     ensure_device();
     cudaStream_t st = current_stream();
     const int kernels_before = (int)g_kernel_count.load();
