@@ -296,6 +296,25 @@ int tblis_b200_dpd_mult_blocks(const tblis_b200_dpd_block_table* A, const label_
                                      tblis_b200_dpd_block_table* C, const label_type* idx_C,
                                tblis_b200_report* report);
 
+/* Level-1 operations over DPD tensors given by block tables: the C entries
+ * of tblis::add / dot / reduce / scale / set / shift over dpd_varray_view
+ * (src/iface/1t/{add,dot,reduce,scale,set,shift}.cxx). add: B = alpha*A +
+ * beta*B (alpha = A.scalar, beta = B.scalar) with A-only labels traced and
+ * B-only labels replicated per block; dot: alpha_A*alpha_B*sum A*B over the
+ * blocks (labels must match); reduce: reduce_t over every stored element,
+ * idx = the element's offset from data; scale: A *= A.scalar; set: A =
+ * alpha; shift: A = alpha + A.scalar*A. Each runs the dense kernel of the
+ * operation on every stored block in place. Return 0 or an error code. */
+int tblis_b200_dpd_add(const tblis_b200_dpd_block_table* A, const label_type* idx_A,
+                       tblis_b200_dpd_block_table* B, const label_type* idx_B);
+int tblis_b200_dpd_dot(const tblis_b200_dpd_block_table* A, const label_type* idx_A,
+                       const tblis_b200_dpd_block_table* B, const label_type* idx_B, tblis_scalar* result);
+int tblis_b200_dpd_reduce(reduce_t op, const tblis_b200_dpd_block_table* A, const label_type* idx_A,
+                          tblis_scalar* result, len_type* idx);
+int tblis_b200_dpd_scale(tblis_b200_dpd_block_table* A, const label_type* idx_A);
+int tblis_b200_dpd_set(const tblis_scalar* alpha, tblis_b200_dpd_block_table* A, const label_type* idx_A);
+int tblis_b200_dpd_shift(const tblis_scalar* alpha, tblis_b200_dpd_block_table* A, const label_type* idx_A);
+
 /* An indexed DPD tensor as MArray's indexed_dpd_varray holds it
  * (indexed_dpd_varray_base.hpp, indexed_dpd_varray.hpp:309-370): the first
  * dense_ndim dimensions are DPD dimensions; each of the other (indexed)

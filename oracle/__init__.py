@@ -353,3 +353,37 @@ def ref_dense_impl(impl):
     src/internal/3t/dense/mult.cxx:653-720), which applies conjugation flags
     (the default path asserts them off). Returns the previous value."""
     return shim().refshim_set_dense_impl(int(impl))
+
+
+def _dpd_flat(nirrep, lens):
+    return (_sz * (len(lens) * nirrep))(*[x for row in lens for x in row])
+
+
+def ref_dpd_add(nirrep, alpha, irrep_A, lens_A, A, idx_A, beta, irrep_B, lens_B, B, idx_B):
+    """The reference's tblis::add over dpd_varray_view (default layout storage)."""
+    rc = shim().refshim_dpd_add(nirrep, ctypes.c_double(alpha), irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A),
+                                ctypes.c_void_p(A.ctypes.data), _lab(idx_A), ctypes.c_double(beta), irrep_B,
+                                len(lens_B), _dpd_flat(nirrep, lens_B), ctypes.c_void_p(B.ctypes.data), _lab(idx_B))
+    if rc:
+        raise ValueError("reference dpd add failed")
+
+
+def ref_dpd_dot(nirrep, irrep_A, lens_A, A, idx_A, irrep_B, lens_B, B, idx_B):
+    f = shim().refshim_dpd_dot
+    f.restype = ctypes.c_double
+    return f(nirrep, irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A), ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+             irrep_B, len(lens_B), _dpd_flat(nirrep, lens_B), ctypes.c_void_p(B.ctypes.data), _lab(idx_B))
+
+
+def ref_dpd_reduce(op, nirrep, irrep_A, lens_A, A, idx_A):
+    r = ctypes.c_double()
+    i = ctypes.c_long()
+    shim().refshim_dpd_reduce(int(op), nirrep, irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A),
+                              ctypes.c_void_p(A.ctypes.data), _lab(idx_A), ctypes.byref(r), ctypes.byref(i))
+    return r.value, i.value
+
+
+def ref_dpd_unary(kind, alpha, beta, nirrep, irrep_A, lens_A, A, idx_A):
+    """kind 0: A *= alpha; 1: A = alpha; 2: A = alpha + beta*A (reference, in place)."""
+    shim().refshim_dpd_unary(int(kind), ctypes.c_double(alpha), ctypes.c_double(beta), nirrep, irrep_A,
+                             len(lens_A), _dpd_flat(nirrep, lens_A), ctypes.c_void_p(A.ctypes.data), _lab(idx_A))

@@ -16,6 +16,11 @@
 #include "matrix/block_scatter_matrix.hpp"
 #include "iface/3t/mult.h"
 #include "iface/1t/add.h"
+#include "iface/1t/shift.h"
+#include "iface/1t/set.h"
+#include "iface/1t/scale.h"
+#include "iface/1t/reduce.h"
+#include "iface/1t/dot.h"
 #include "internal/3t/dpd/mult.hpp"
 #include "internal/3t/dense/mult.hpp"
 
@@ -122,6 +127,59 @@ int refshim_dpd_mult(unsigned nirrep,
     MArray::dpd_varray_view<double> C(irrep_C, nirrep, mk(ndim_C, lens_C), data_C);
 
     tblis::mult<double>(alpha, A, idx_A, B, idx_B, beta, C, idx_C);
+    return 0;
+}
+
+/*
+ * The reference's DPD level-1 operations (tblis::add / dot / reduce / scale /
+ * set / shift over dpd_varray_view, src/iface/1t/*.cxx) on default-layout
+ * storage. kind for the unary entry: 0 scale (A *= alpha), 1 set (A = alpha),
+ * 2 shift (A = alpha + beta*A). Return 0 on success.
+ */
+static std::vector<std::vector<len_type>> dpd_lens(unsigned ndim, unsigned nirrep, const len_type* lens)
+{
+    std::vector<std::vector<len_type>> len(ndim, std::vector<len_type>(nirrep));
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++) len[i][j] = lens[i*nirrep+j];
+    return len;
+}
+
+int refshim_dpd_add(unsigned nirrep, double alpha, unsigned irrep_A, unsigned ndim_A, const len_type* lens_A,
+                    const double* data_A, const char* idx_A, double beta, unsigned irrep_B, unsigned ndim_B,
+                    const len_type* lens_B, double* data_B, const char* idx_B)
+{
+    MArray::dpd_varray_view<const double> A(irrep_A, nirrep, dpd_lens(ndim_A, nirrep, lens_A), data_A);
+    MArray::dpd_varray_view<double> B(irrep_B, nirrep, dpd_lens(ndim_B, nirrep, lens_B), data_B);
+    tblis::add<double>(alpha, A, idx_A, beta, B, idx_B);
+    return 0;
+}
+
+double refshim_dpd_dot(unsigned nirrep, unsigned irrep_A, unsigned ndim_A, const len_type* lens_A,
+                       const double* data_A, const char* idx_A, unsigned irrep_B, unsigned ndim_B,
+                       const len_type* lens_B, const double* data_B, const char* idx_B)
+{
+    MArray::dpd_varray_view<const double> A(irrep_A, nirrep, dpd_lens(ndim_A, nirrep, lens_A), data_A);
+    MArray::dpd_varray_view<const double> B(irrep_B, nirrep, dpd_lens(ndim_B, nirrep, lens_B), data_B);
+    return tblis::dot<double>(A, idx_A, B, idx_B);
+}
+
+int refshim_dpd_reduce(int op, unsigned nirrep, unsigned irrep_A, unsigned ndim_A, const len_type* lens_A,
+                       const double* data_A, const char* idx_A, double* result, long* idx)
+{
+    MArray::dpd_varray_view<const double> A(irrep_A, nirrep, dpd_lens(ndim_A, nirrep, lens_A), data_A);
+    auto r = tblis::reduce<double>((tblis::reduce_t)op, A, idx_A);
+    *result = r.first;
+    *idx = r.second;
+    return 0;
+}
+
+int refshim_dpd_unary(int kind, double alpha, double beta, unsigned nirrep, unsigned irrep_A, unsigned ndim_A,
+                      const len_type* lens_A, double* data_A, const char* idx_A)
+{
+    MArray::dpd_varray_view<double> A(irrep_A, nirrep, dpd_lens(ndim_A, nirrep, lens_A), data_A);
+    if (kind == 0) tblis::scale<double>(alpha, A, idx_A);
+    else if (kind == 1) tblis::set<double>(alpha, A, idx_A);
+    else tblis::shift<double>(alpha, beta, A, idx_A);
     return 0;
 }
 

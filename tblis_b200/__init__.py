@@ -365,6 +365,109 @@ def dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
 
 
+class tblis_b200_dpd_block_table(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("conj", ctypes.c_int), ("scalar", tblis_scalar),
+                ("data", ctypes.c_void_p), ("ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint),
+                ("irrep", ctypes.c_uint), ("len", _P(ctypes.c_ssize_t)), ("offset", _P(ctypes.c_ssize_t)),
+                ("stride", _P(ctypes.c_ssize_t))]
+
+
+_DT = _P(tblis_b200_dpd_block_table)
+lib.tblis_b200_dpd_add.argtypes = [_DT, ctypes.c_char_p, _DT, ctypes.c_char_p]
+lib.tblis_b200_dpd_dot.argtypes = [_DT, ctypes.c_char_p, _DT, ctypes.c_char_p, _P(tblis_scalar)]
+lib.tblis_b200_dpd_reduce.argtypes = [ctypes.c_int, _DT, ctypes.c_char_p, _P(tblis_scalar),
+                                      _P(ctypes.c_ssize_t)]
+lib.tblis_b200_dpd_scale.argtypes = [_DT, ctypes.c_char_p]
+lib.tblis_b200_dpd_set.argtypes = [_P(tblis_scalar), _DT, ctypes.c_char_p]
+lib.tblis_b200_dpd_shift.argtypes = [_P(tblis_scalar), _DT, ctypes.c_char_p]
+
+
+def _dpd_table(T, scalar=1.0):
+    """The block table of a DpdTensor (every stored block's offset and
+    strides, irrep tuples numbered with dimension 0 fastest)."""
+    nd, n = len(T.lens), T.nirrep
+    nt = n ** nd
+    off = [-1] * nt
+    st = [0] * (nt * nd)
+    for t in range(nt):
+        irr = [(t // n ** d) % n for d in range(nd)]
+        x = 0
+        ext = 1
+        for d in range(nd):
+            x ^= irr[d]
+            ext *= T.lens[d][irr[d]]
+        if x != T.irrep or ext == 0:
+            continue
+        o, _, strides = T.block(irr)
+        off[t] = o
+        st[t * nd:(t + 1) * nd] = strides
+    keep = [(ctypes.c_ssize_t * (nd * n))(*[x for r in T.lens for x in r]), (ctypes.c_ssize_t * nt)(*off),
+            (ctypes.c_ssize_t * max(1, len(st)))(*st)]
+    b = tblis_b200_dpd_block_table()
+    b.type = TYPE_DOUBLE
+    b.conj = 0
+    b.scalar.type = TYPE_DOUBLE
+    b.scalar.data[0] = float(scalar)
+    b.data = T.data.data_ptr() if hasattr(T.data, "data_ptr") else T.data.ctypes.data
+    b.ndim, b.nirrep, b.irrep = nd, n, T.irrep
+    b.len = ctypes.cast(keep[0], _P(ctypes.c_ssize_t))
+    b.offset = ctypes.cast(keep[1], _P(ctypes.c_ssize_t))
+    b.stride = ctypes.cast(keep[2], _P(ctypes.c_ssize_t))
+    return b, keep
+
+
+def dpd_add(alpha, A, idx_A, beta, B, idx_B):
+    """B = alpha*A + beta*B over DPD tensors (tblis::add over dpd_varray_view)."""
+    a, ka = _dpd_table(A, alpha)
+    b, kb = _dpd_table(B, beta)
+    lib.tblis_b200_dpd_add(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B))
+    _check()
+
+
+def dpd_dot(A, idx_A, B, idx_B):
+    a, ka = _dpd_table(A)
+    b, kb = _dpd_table(B)
+    r = tblis_scalar()
+    lib.tblis_b200_dpd_dot(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B), ctypes.byref(r))
+    _check()
+    return r.data[0]
+
+
+def dpd_reduce(op, A, idx_A):
+    """(value, offset from the data) of a reduction over the stored elements."""
+    a, ka = _dpd_table(A)
+    r = tblis_scalar()
+    i = ctypes.c_ssize_t(-1)
+    lib.tblis_b200_dpd_reduce(int(op), ctypes.byref(a), _labels(idx_A), ctypes.byref(r), ctypes.byref(i))
+    _check()
+    return r.data[0], i.value
+
+
+def dpd_scale(alpha, A, idx_A):
+    a, ka = _dpd_table(A, alpha)
+    lib.tblis_b200_dpd_scale(ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
+def dpd_set(alpha, A, idx_A):
+    a, ka = _dpd_table(A)
+    s = tblis_scalar()
+    s.type = TYPE_DOUBLE
+    s.data[0] = float(alpha)
+    lib.tblis_b200_dpd_set(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
+def dpd_shift(alpha, beta, A, idx_A):
+    """A = alpha + beta*A over the stored elements."""
+    a, ka = _dpd_table(A, beta)
+    s = tblis_scalar()
+    s.type = TYPE_DOUBLE
+    s.data[0] = float(alpha)
+    lib.tblis_b200_dpd_shift(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
 class tblis_b200_indexed_dpd_tensor(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("scalar", tblis_scalar), ("ndim", ctypes.c_uint),
                 ("dense_ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint), ("dense_irrep", ctypes.c_uint),

@@ -82,6 +82,17 @@ int guarded(F&& f)
     }
 }
 
+// runs one of this library's C entry points from inside another call and
+// turns its recorded error into an exception
+template <typename F>
+void checked(F&& f)
+{
+    tblis_b200_clear_error();
+    f();
+    const int c = tblis_b200_last_error();
+    if (c) throw error(c, tblis_b200_last_error_string());
+}
+
 cudaStream_t current_stream();
 void ensure_device();
 

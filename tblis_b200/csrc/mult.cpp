@@ -161,17 +161,6 @@ static void contract_device(const GemmView& v, const double* A, const double* B,
     est_error = 1.1e-16*std::sqrt((double)v.k);
 }
 
-// runs one of this library's C entry points from inside another call and
-// turns its recorded error into an exception
-template <typename F>
-static void checked(F&& f)
-{
-    tblis_b200_clear_error();
-    f();
-    const int c = tblis_b200_last_error();
-    if (c) throw error(c, tblis_b200_last_error_string());
-}
-
 // the double view of a dcomplex tensor: every dimension with twice the
 // stride, plus the real/imaginary dimension (length 2, stride 1) last
 struct ComplexParts

@@ -1,9 +1,10 @@
 // tblis_mult_dpd.cxx -- TBLIS's compiled C++ overloads of tblis::mult over
 // MArray's DPD views, reaching the GPU library through its C ABI.
 //
-// TBLIS declares these overloads in src/iface/3t/mult.h:56-60 and 92-96 and
-// instantiates them in its library (src/iface/3t/mult.cxx:292-298 and
-// 535-541) for float, double, scomplex and dcomplex, so a C++ program links
+// TBLIS declares these overloads in src/iface/3t/mult.h:56-60 and 92-96 (and
+// the level-1 ones in src/iface/1t/*.h) and instantiates them in its library
+// (src/iface/3t/mult.cxx:292-298, 535-541; src/iface/1t/*.cxx) for float,
+// double, scomplex and dcomplex, so a C++ program links
 // against their mangled names. This file defines the same templates with the
 // same instantiations; compiled against the caller's MArray headers (the
 // views' layout must match the caller's, so the same MARRAY_* configuration
@@ -193,6 +194,117 @@ void mult(const tci::communicator& comm,
     }
     wait_all(comm);
 }
+
+// the reference's reduce_t lives in namespace tblis (src/util/basic_types.h:53-64)
+typedef enum
+{
+    REDUCE_SUM_ = 0, REDUCE_SUM_ABS_ = 1, REDUCE_MAX_ = 2, REDUCE_MAX_ABS_ = 3,
+    REDUCE_MIN_ = 4, REDUCE_MIN_ABS_ = 5, REDUCE_NORM_2_ = 6
+} reduce_t;
+
+namespace
+{
+template <typename T> T from_double(double v) { return T(v); }
+}
+
+// level-1 operations over DPD views (src/iface/1t/{add,dot,reduce,scale,set,
+// shift}.cxx, instantiated there for the same four types)
+template <typename T>
+void add(const tci::communicator& comm,
+         T alpha, dpd_varray_view<const T> A, const label_type* idx_A,
+         T  beta, dpd_varray_view<      T> B, const label_type* idx_B)
+{
+    if (is_master(comm))
+    {
+        Table a(A, alpha), b(B, beta);
+        tblis_b200_dpd_add(&a.t, idx_A, &b.t, idx_B);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void dot(const tci::communicator& comm,
+         dpd_varray_view<const T> A, const label_type* idx_A,
+         dpd_varray_view<const T> B, const label_type* idx_B, T& result)
+{
+    if (is_master(comm))
+    {
+        Table a(A, T(1)), b(B, T(1));
+        tblis_scalar r;
+        if (tblis_b200_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = from_double<T>(r.data.d);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void reduce(const tci::communicator& comm, reduce_t op,
+            dpd_varray_view<const T> A, const label_type* idx_A, T& result, len_type& idx)
+{
+    if (is_master(comm))
+    {
+        Table a(A, T(1));
+        tblis_scalar r;
+        len_type i = -1;
+        if (tblis_b200_dpd_reduce((::reduce_t)op, &a.t, idx_A, &r, &i) == 0)
+        {
+            result = from_double<T>(r.data.d);
+            idx = i;
+        }
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void scale(const tci::communicator& comm, T alpha, dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        Table a(A, alpha);
+        tblis_b200_dpd_scale(&a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void set(const tci::communicator& comm, T alpha, dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        Table a(A, T(1));
+        tblis_scalar s;
+        set_scalar(s, alpha);
+        tblis_b200_dpd_set(&s, &a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void shift(const tci::communicator& comm, T alpha, T beta, dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        Table a(A, beta);
+        tblis_scalar s;
+        set_scalar(s, alpha);
+        tblis_b200_dpd_shift(&s, &a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+#define TBLIS_B200_DPD_LEVEL1(T) \
+template void add(const tci::communicator&, T, dpd_varray_view<const T>, const label_type*, \
+                  T, dpd_varray_view<T>, const label_type*); \
+template void dot(const tci::communicator&, dpd_varray_view<const T>, const label_type*, \
+                  dpd_varray_view<const T>, const label_type*, T&); \
+template void reduce(const tci::communicator&, reduce_t, dpd_varray_view<const T>, const label_type*, \
+                     T&, len_type&); \
+template void scale(const tci::communicator&, T, dpd_varray_view<T>, const label_type*); \
+template void set(const tci::communicator&, T, dpd_varray_view<T>, const label_type*); \
+template void shift(const tci::communicator&, T, T, dpd_varray_view<T>, const label_type*);
+TBLIS_B200_DPD_LEVEL1(float)
+TBLIS_B200_DPD_LEVEL1(double)
+TBLIS_B200_DPD_LEVEL1(std::complex<float>)
+TBLIS_B200_DPD_LEVEL1(std::complex<double>)
 
 #define TBLIS_B200_DPD_MULT(T) \
 template void mult(const tci::communicator& comm, \

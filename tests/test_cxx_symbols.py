@@ -26,6 +26,17 @@ DPD_MULT = [
 INDEXED_DPD_MULT = [n.replace("15dpd_varray_view", "23indexed_dpd_varray_view") for n in DPD_MULT]
 
 
+# the DPD level-1 overloads (src/iface/1t/{add,dot,reduce,scale,set,shift}.cxx), double
+DPD_LEVEL1 = [
+    "_ZN5tblis3addIdEEvRKN3tci12communicatorET_N6MArray15dpd_varray_viewIKS5_EEPKcS5_NS7_IS5_EESB_",
+    "_ZN5tblis3dotIdEEvRKN3tci12communicatorEN6MArray15dpd_varray_viewIKT_EEPKcS9_SB_RS7_",
+    "_ZN5tblis6reduceIdEEvRKN3tci12communicatorENS_8reduce_tEN6MArray15dpd_varray_viewIKT_EEPKcRS8_Rl",
+    "_ZN5tblis5scaleIdEEvRKN3tci12communicatorET_N6MArray15dpd_varray_viewIS5_EEPKc",
+    "_ZN5tblis3setIdEEvRKN3tci12communicatorET_N6MArray15dpd_varray_viewIS5_EEPKc",
+    "_ZN5tblis5shiftIdEEvRKN3tci12communicatorET_S5_N6MArray15dpd_varray_viewIS5_EEPKc",
+]
+
+
 def _has(lib, name):
     try:
         getattr(lib, name)
@@ -37,7 +48,7 @@ def _has(lib, name):
 def test_cxx_library_exports_the_dpd_overloads():
     assert os.path.exists(CXX_LIB), "libtblis_b200_cxx.so not built (make -C tblis_b200 cxx MARRAY=...)"
     lib = ctypes.CDLL(CXX_LIB, mode=ctypes.RTLD_LOCAL)
-    missing = [n for n in DPD_MULT + INDEXED_DPD_MULT if not _has(lib, n)]
+    missing = [n for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1 if not _has(lib, n)]
     assert not missing, missing
 
 
@@ -45,4 +56,4 @@ def test_names_match_the_reference_library():
     if not os.path.exists(REF_LIB):
         pytest.skip("reference library not built here")
     ref = ctypes.CDLL(REF_LIB, mode=ctypes.RTLD_LOCAL)
-    assert all(_has(ref, n) for n in DPD_MULT + INDEXED_DPD_MULT)
+    assert all(_has(ref, n) for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1)
