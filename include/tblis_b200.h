@@ -356,6 +356,30 @@ int tblis_b200_indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A, const la
                                       tblis_b200_indexed_dpd_tensor* C, const label_type* idx_C,
                                 tblis_b200_report* report);
 
+/* Level-1 operations over indexed DPD tensors, the C entries of tblis::add /
+ * dot / reduce / scale / set / shift over indexed_dpd_varray_view
+ * (src/iface/1t/{add,dot,reduce,scale,set,shift}.cxx and src/internal/1t/indexed_dpd/). Entries act through
+ * their factors as the reference's do: add scales B's entries by f*beta then
+ * adds alpha*f_A*f_B*A_i to every B entry whose index values agree (a label
+ * indexed in one tensor selects that slice of the other); dot sums
+ * f_A*f_B*(A_i . B_j) over agreeing pairs; reduce combines the entries'
+ * reductions scaled by their factors, idx counted from entry 0's data; scale
+ * multiplies entry e by f_e*A.scalar, set writes f_e*alpha, shift writes
+ * f_e*alpha + A.scalar*A (A.scalar*A only, when f_e == 0). Return 0 or an
+ * error code. */
+int tblis_b200_indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                               tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B);
+int tblis_b200_indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                               const tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B,
+                               tblis_scalar* result);
+int tblis_b200_indexed_dpd_reduce(reduce_t op, const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                                  tblis_scalar* result, len_type* idx);
+int tblis_b200_indexed_dpd_scale(tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A);
+int tblis_b200_indexed_dpd_set(const tblis_scalar* alpha, tblis_b200_indexed_dpd_tensor* A,
+                               const label_type* idx_A);
+int tblis_b200_indexed_dpd_shift(const tblis_scalar* alpha, tblis_b200_indexed_dpd_tensor* A,
+                                 const label_type* idx_A);
+
 /* Offset (from data), lengths and strides of one block (one irrep per
  * dimension), as dpd_varray_view::operator()(irreps) gives them
  * (dpd_marray_base.hpp:171-228). Returns 0 or an error code. */

@@ -320,6 +320,44 @@ def ref_dpd_mult(nirrep, alpha, irrep_A, lens_A, A, idx_A, irrep_B, lens_B, B, i
         raise ValueError("reference dpd mult failed")
 
 
+def _idx_args(nirrep, T, lab):
+    ndim = len(T["lens"])
+    nidim = len(T["idx_irreps"])
+    flat = (_sz * (ndim * nirrep))(*[x for row in T["lens"] for x in row])
+    irr = (ctypes.c_uint * max(1, nidim))(*T["idx_irreps"])
+    idx = [x for t in T["indices"] for x in t]
+    nidx = max(1, len(T["indices"])) if nidim else 1
+    ix = (_sz * max(1, len(idx)))(*idx)
+    f = (ctypes.c_double * nidx)(*T["factors"])
+    return [ctypes.c_uint(T["irrep"]), ctypes.c_uint(ndim), flat, ctypes.c_uint(nidim), irr, ctypes.c_long(nidx),
+            ix, ctypes.c_void_p(T["data"].ctypes.data), f, _lab(lab)]
+
+
+def ref_indexed_dpd_add(nirrep, alpha, A, idx_A, beta, B, idx_B):
+    """The reference's tblis::add over indexed_dpd_varray_view; B's data updated."""
+    shim().refshim_indexed_dpd_add(ctypes.c_uint(nirrep), ctypes.c_double(alpha), *_idx_args(nirrep, A, idx_A),
+                                   ctypes.c_double(beta), *_idx_args(nirrep, B, idx_B))
+
+
+def ref_indexed_dpd_dot(nirrep, A, idx_A, B, idx_B):
+    f = shim().refshim_indexed_dpd_dot
+    f.restype = ctypes.c_double
+    return f(ctypes.c_uint(nirrep), *_idx_args(nirrep, A, idx_A), *_idx_args(nirrep, B, idx_B))
+
+
+def ref_indexed_dpd_reduce(op, nirrep, A, idx_A):
+    r = ctypes.c_double()
+    i = ctypes.c_long()
+    shim().refshim_indexed_dpd_reduce(ctypes.c_int(op), ctypes.c_uint(nirrep), *_idx_args(nirrep, A, idx_A),
+                                      ctypes.byref(r), ctypes.byref(i))
+    return r.value, i.value
+
+
+def ref_indexed_dpd_unary(kind, alpha, beta, nirrep, A, idx_A):
+    shim().refshim_indexed_dpd_unary(ctypes.c_int(kind), ctypes.c_double(alpha), ctypes.c_double(beta),
+                                     ctypes.c_uint(nirrep), *_idx_args(nirrep, A, idx_A))
+
+
 def ref_indexed_dpd_mult(nirrep, alpha, A, idx_A, B, idx_B, beta, C, idx_C, impl=2):
     """The reference's own indexed-DPD contraction (tblis::mult over
     indexed_dpd_varray_view). Each tensor is a dict: irrep (overall), lens

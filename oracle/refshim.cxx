@@ -184,6 +184,87 @@ int refshim_dpd_unary(int kind, double alpha, double beta, unsigned nirrep, unsi
 }
 
 /*
+ * An owning MArray indexed DPD tensor filled from flat storage (entries back
+ * to back, default layout) and factors; and its storage copied back.
+ */
+static void fill_indexed(MArray::indexed_dpd_varray<double>& T, unsigned nirrep, unsigned irrep, unsigned ndim,
+                         const len_type* lens, unsigned nidim, const unsigned* irr, long nidx,
+                         const len_type* idx, const double* data, const double* f)
+{
+    MArray::matrix<len_type> len({ndim, nirrep}, MArray::ROW_MAJOR);
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++) len[i][j] = lens[i*nirrep+j];
+    std::vector<unsigned> ir(irr, irr + nidim);
+    MArray::matrix<len_type> ix({(len_type)nidx, (len_type)nidim}, MArray::ROW_MAJOR);
+    for (long e = 0; e < nidx; e++)
+        for (unsigned d = 0; d < nidim; d++) ix[e][d] = idx[e*nidim+d];
+    T.reset(irrep, nirrep, len, ir, ix);
+    const len_type n = T.dense_size();
+    for (long e = 0; e < nidx; e++)
+    {
+        std::copy_n(data + e*n, n, T.data(e));
+        T.factor(e) = f[e];
+    }
+}
+
+static void copy_out(const MArray::indexed_dpd_varray<double>& T, long nidx, double* data)
+{
+    const len_type n = T.dense_size();
+    for (long e = 0; e < nidx; e++) std::copy_n(T.data(e), n, data + e*n);
+}
+
+#define IDX_ARGS(X) unsigned irrep_##X, unsigned ndim_##X, const len_type* lens_##X, unsigned nidim_##X, \
+                    const unsigned* irr_##X, long nidx_##X, const len_type* idx_##X, double* data_##X, \
+                    const double* f_##X, const char* lab_##X
+#define IDX_FILL(T, X) fill_indexed(T, nirrep, irrep_##X, ndim_##X, lens_##X, nidim_##X, irr_##X, nidx_##X, \
+                                    idx_##X, data_##X, f_##X)
+
+/*
+ * The reference's indexed-DPD level-1 operations (tblis::add / dot / reduce /
+ * scale / set / shift over indexed_dpd_varray_view). unary kind: 0 scale
+ * (A *= alpha), 1 set (A = alpha), 2 shift (A = alpha + beta*A).
+ */
+int refshim_indexed_dpd_add(unsigned nirrep, double alpha, IDX_ARGS(A), double beta, IDX_ARGS(B))
+{
+    MArray::indexed_dpd_varray<double> A, B;
+    IDX_FILL(A, A);
+    IDX_FILL(B, B);
+    tblis::add<double>(alpha, A, lab_A, beta, B, lab_B);
+    copy_out(B, nidx_B, data_B);
+    return 0;
+}
+
+double refshim_indexed_dpd_dot(unsigned nirrep, IDX_ARGS(A), IDX_ARGS(B))
+{
+    MArray::indexed_dpd_varray<double> A, B;
+    IDX_FILL(A, A);
+    IDX_FILL(B, B);
+    return tblis::dot<double>(A, lab_A, B, lab_B);
+}
+
+int refshim_indexed_dpd_reduce(int op, unsigned nirrep, IDX_ARGS(A), double* result, long* idx)
+{
+    MArray::indexed_dpd_varray<double> A;
+    IDX_FILL(A, A);
+    auto r = tblis::reduce<double>((tblis::reduce_t)op, A, lab_A);
+    *result = r.first;
+    // offsets are counted from entry 0's data, which is where the flat copy starts too
+    *idx = r.second;
+    return 0;
+}
+
+int refshim_indexed_dpd_unary(int kind, double alpha, double beta, unsigned nirrep, IDX_ARGS(A))
+{
+    MArray::indexed_dpd_varray<double> A;
+    IDX_FILL(A, A);
+    if (kind == 0) tblis::scale<double>(alpha, A, lab_A);
+    else if (kind == 1) tblis::set<double>(alpha, A, lab_A);
+    else tblis::shift<double>(alpha, beta, A, lab_A);
+    copy_out(A, nidx_A, data_A);
+    return 0;
+}
+
+/*
  * The reference's indexed-DPD contraction (tblis::mult over
  * indexed_dpd_varray_view, src/iface/3t/mult.cxx:412-541). Each tensor is
  * given by its overall irrep, ndim, lens [ndim][nirrep], the irreps of its

@@ -558,6 +558,68 @@ class IndexedDpdTensor:
         return t
 
 
+_IT = _P(tblis_b200_indexed_dpd_tensor)
+lib.tblis_b200_indexed_dpd_add.argtypes = [_IT, ctypes.c_char_p, _IT, ctypes.c_char_p]
+lib.tblis_b200_indexed_dpd_dot.argtypes = [_IT, ctypes.c_char_p, _IT, ctypes.c_char_p, _P(tblis_scalar)]
+lib.tblis_b200_indexed_dpd_reduce.argtypes = [ctypes.c_int, _IT, ctypes.c_char_p, _P(tblis_scalar),
+                                              _P(ctypes.c_ssize_t)]
+lib.tblis_b200_indexed_dpd_scale.argtypes = [_IT, ctypes.c_char_p]
+lib.tblis_b200_indexed_dpd_set.argtypes = [_P(tblis_scalar), _IT, ctypes.c_char_p]
+lib.tblis_b200_indexed_dpd_shift.argtypes = [_P(tblis_scalar), _IT, ctypes.c_char_p]
+
+
+def _dscalar(v):
+    s = tblis_scalar()
+    s.type = TYPE_DOUBLE
+    s.data[0] = float(v)
+    return s
+
+
+def indexed_dpd_add(alpha, A, idx_A, beta, B, idx_B):
+    """B = alpha*A + beta*B over indexed DPD tensors (tblis::add over indexed_dpd_varray_view)."""
+    a, b = A.struct(alpha), B.struct(beta)
+    lib.tblis_b200_indexed_dpd_add(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B))
+    _check()
+
+
+def indexed_dpd_dot(A, idx_A, B, idx_B):
+    a, b = A.struct(), B.struct()
+    r = tblis_scalar()
+    lib.tblis_b200_indexed_dpd_dot(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B),
+                                   ctypes.byref(r))
+    _check()
+    return r.data[0]
+
+
+def indexed_dpd_reduce(op, A, idx_A):
+    a = A.struct()
+    r = tblis_scalar()
+    i = ctypes.c_ssize_t(-1)
+    lib.tblis_b200_indexed_dpd_reduce(int(op), ctypes.byref(a), _labels(idx_A), ctypes.byref(r), ctypes.byref(i))
+    _check()
+    return r.data[0], i.value
+
+
+def indexed_dpd_scale(alpha, A, idx_A):
+    a = A.struct(alpha)
+    lib.tblis_b200_indexed_dpd_scale(ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
+def indexed_dpd_set(alpha, A, idx_A):
+    a = A.struct()
+    s = _dscalar(alpha)
+    lib.tblis_b200_indexed_dpd_set(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
+def indexed_dpd_shift(alpha, beta, A, idx_A):
+    a = A.struct(beta)
+    s = _dscalar(alpha)
+    lib.tblis_b200_indexed_dpd_shift(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
+    _check()
+
+
 def indexed_dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     """C = alpha*A*B + beta*C over indexed DPD tensors (src/iface/3t/mult.h:92-110)."""
     a, b, c = A.struct(alpha), B.struct(), C.struct(beta)

@@ -80,4 +80,15 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
               DpdMultReport* rep, bool reference_irrep_check = true);
 
+// level-1 operations on device-resident DPD storage (dpd_level1.cpp):
+// B = alpha*A + beta*B (trace / replicate per block), sum A*B, a reduction
+// with the offset of its extreme element, and the unary updates (kind 0:
+// A *= scal, 1: A = alpha, 2: A = alpha + scal*A)
+void dpd_add_dev(double alpha, const DpdLayout& A, const double* a, const std::string& iA, double beta,
+                 const DpdLayout& B, double* b, const std::string& iB);
+double dpd_dot_dev(const DpdLayout& A, const double* a, const std::string& iA,
+                   const DpdLayout& B, const double* b, const std::string& iB);
+void dpd_reduce_dev(int op, const DpdLayout& A, const double* a, const std::string& iA, double& result, i64& idx);
+void dpd_unary_dev(int kind, double alpha, double scal, const DpdLayout& A, double* a, const std::string& iA);
+
 } // namespace tb

@@ -103,7 +103,7 @@ struct BlockView
     tblis_tensor t = {};
     i64 offset = 0;
     bool empty = true;
-    BlockView(const DpdLayout& X, double* base, const std::vector<unsigned>& irr, double scalar)
+    BlockView(const DpdLayout& X, const double* base, const std::vector<unsigned>& irr, double scalar)
     {
         len.resize(X.ndim);
         stride.resize(X.ndim);
@@ -118,7 +118,7 @@ struct BlockView
         t.conj = 0;
         t.scalar.type = TYPE_DOUBLE;
         t.scalar.data.d = scalar;
-        t.data = base + offset;
+        t.data = const_cast<double*>(base) + offset;
         t.ndim = X.ndim;
         t.len = len.data();
         t.stride = stride.data();
@@ -151,16 +151,10 @@ std::vector<unsigned> positions(const std::string& labels, const std::string& of
 
 } // namespace
 
-void dpd_add(const tblis_b200_dpd_block_table* A_, const label_type* idx_A,
-             tblis_b200_dpd_block_table* B_, const label_type* idx_B)
+void dpd_add_dev(double alpha, const DpdLayout& A, const double* a, const std::string& iA, double beta,
+                 const DpdLayout& B, double* b, const std::string& iB)
 {
-    ensure_device();
-    cudaStream_t st = current_stream();
-    DpdLayout A, B;
-    to_layout(A_, A);
-    to_layout(B_, B);
     TB_CHECK(A.nirrep == B.nirrep, TB_ERR_ARG, "DPD add: nirrep differs");
-    const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim);
     for (const std::string* s : {&iA, &iB})
         for (size_t i = 0; i < s->size(); i++)
             for (size_t j = 0; j < i; j++)
@@ -172,53 +166,90 @@ void dpd_add(const tblis_b200_dpd_block_table* A_, const label_type* idx_A,
     TB_CHECK(!AB.empty(), TB_ERR_ARG, "DPD add: no shared label");
     for (char c : AB)
         TB_CHECK(A.len[iA.find(c)] == B.len[iB.find(c)], TB_ERR_ARG, "DPD add: per-irrep lengths differ");
-    const double alpha = A_->scalar.data.d, beta = B_->scalar.data.d;
+    cudaStream_t st = current_stream();
+    if (alpha == 0.0 || (Aonly.empty() && Bonly.empty() && A.irrep != B.irrep))
+    {
+        scale_all(B, b, beta, iB.c_str(), st);
+        return;
+    }
+    const auto pA_AB = positions(AB, iA), pB_AB = positions(AB, iB), pA_only = positions(Aonly, iA);
+    std::vector<unsigned> irrA(A.ndim, 0);
+    B.for_each_block([&](const std::vector<unsigned>& irrB, const std::vector<i64>&, const std::vector<i64>&, i64)
+    {
+        BlockView bb(B, b, irrB, beta);
+        unsigned x = A.irrep;
+        for (size_t i = 0; i < AB.size(); i++) { irrA[pA_AB[i]] = irrB[pB_AB[i]]; x ^= irrB[pB_AB[i]]; }
+        double local_beta = beta;
+        // the A blocks reaching this B block: the A-only irreps close A's XOR
+        for_each_combo(pA_only, x, A.nirrep, irrA, [&]
+        {
+            BlockView ab(A, a, irrA, alpha);
+            if (ab.empty) return;
+            bb.t.scalar.data.d = local_beta;
+            checked([&] { tblis_tensor_add(nullptr, nullptr, &ab.t, iA.c_str(), &bb.t, iB.c_str()); });
+            local_beta = 1.0;
+        });
+        if (local_beta == 0.0)
+        {
+            tblis_scalar z;
+            z.type = TYPE_DOUBLE;
+            z.data.d = 0.0;
+            checked([&] { tblis_tensor_set(nullptr, nullptr, &z, &bb.t, iB.c_str()); });
+        }
+        else if (local_beta != 1.0)
+        {
+            bb.t.scalar.data.d = local_beta;
+            checked([&] { tblis_tensor_scale(nullptr, nullptr, &bb.t, iB.c_str()); });
+        }
+    });
+}
 
+void dpd_add(const tblis_b200_dpd_block_table* A_, const label_type* idx_A,
+             tblis_b200_dpd_block_table* B_, const label_type* idx_B)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    DpdLayout A, B;
+    to_layout(A_, A);
+    to_layout(B_, B);
+    const double alpha = A_->scalar.data.d, beta = B_->scalar.data.d;
     Storage sa, sb;
     sa.init(A_->data, A.total(), true, st);
     sb.init(B_->data, B.total(), beta != 0.0, st);
-
-    if (alpha == 0.0 || (Aonly.empty() && Bonly.empty() && A.irrep != B.irrep))
-        scale_all(B, sb.dev, beta, idx_B, st);
-    else
-    {
-        const auto pA_AB = positions(AB, iA), pB_AB = positions(AB, iB), pA_only = positions(Aonly, iA);
-        std::vector<unsigned> irrA(A.ndim, 0);
-        B.for_each_block([&](const std::vector<unsigned>& irrB, const std::vector<i64>&, const std::vector<i64>&, i64)
-        {
-            BlockView bb(B, sb.dev, irrB, beta);
-            unsigned x = A.irrep;
-            for (size_t i = 0; i < AB.size(); i++) { irrA[pA_AB[i]] = irrB[pB_AB[i]]; x ^= irrB[pB_AB[i]]; }
-            double local_beta = beta;
-            // the A blocks reaching this B block: the A-only irreps close A's XOR
-            for_each_combo(pA_only, x, A.nirrep, irrA, [&]
-            {
-                BlockView ab(A, sa.dev, irrA, alpha);
-                if (ab.empty) return;
-                bb.t.scalar.data.d = local_beta;
-                checked([&] { tblis_tensor_add(nullptr, nullptr, &ab.t, idx_A, &bb.t, idx_B); });
-                local_beta = 1.0;
-            });
-            if (local_beta == 0.0)
-            {
-                tblis_scalar z;
-                z.type = TYPE_DOUBLE;
-                z.data.d = 0.0;
-                checked([&] { tblis_tensor_set(nullptr, nullptr, &z, &bb.t, idx_B); });
-            }
-            else if (local_beta != 1.0)
-            {
-                bb.t.scalar.data.d = local_beta;
-                checked([&] { tblis_tensor_scale(nullptr, nullptr, &bb.t, idx_B); });
-            }
-        });
-    }
+    dpd_add_dev(alpha, A, sa.dev, std::string(idx_A, A.ndim), beta, B, sb.dev, std::string(idx_B, B.ndim));
     sb.out(st);
     sb.finish(st);
     sa.finish(st);
     B_->scalar.data.d = 1.0;
     B_->scalar.type = TYPE_DOUBLE;
     B_->conj = 0;
+}
+
+double dpd_dot_dev(const DpdLayout& A, const double* a, const std::string& iA,
+                   const DpdLayout& B, const double* b, const std::string& iB)
+{
+    TB_CHECK(A.nirrep == B.nirrep && A.ndim == B.ndim, TB_ERR_ARG, "DPD dot: shapes differ");
+    for (char c : iA)
+    {
+        const size_t p = iB.find(c);
+        TB_CHECK(p != std::string::npos, TB_ERR_ARG, "DPD dot: labels must match");
+        TB_CHECK(A.len[iA.find(c)] == B.len[p], TB_ERR_ARG, "DPD dot: per-irrep lengths differ");
+    }
+    double sum = 0.0;
+    if (A.irrep != B.irrep) return sum;
+    const auto pB = positions(iA, iB);
+    std::vector<unsigned> irrB(B.ndim), all(A.ndim), irrA(A.ndim, 0);
+    for (unsigned d = 0; d < A.ndim; d++) all[d] = d;
+    for_each_combo(all, A.irrep, A.nirrep, irrA, [&]
+    {
+        for (unsigned d = 0; d < A.ndim; d++) irrB[pB[d]] = irrA[d];
+        BlockView ab(A, a, irrA, 1.0), bb(B, b, irrB, 1.0);
+        if (ab.empty || bb.empty) return;
+        tblis_scalar r;
+        checked([&] { tblis_tensor_dot(nullptr, nullptr, &ab.t, iA.c_str(), &bb.t, iB.c_str(), &r); });
+        sum += r.data.d;
+    });
+    return sum;
 }
 
 double dpd_dot(const tblis_b200_dpd_block_table* A_, const label_type* idx_A,
@@ -229,46 +260,17 @@ double dpd_dot(const tblis_b200_dpd_block_table* A_, const label_type* idx_A,
     DpdLayout A, B;
     to_layout(A_, A);
     to_layout(B_, B);
-    TB_CHECK(A.nirrep == B.nirrep && A.ndim == B.ndim, TB_ERR_ARG, "DPD dot: shapes differ");
-    const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim);
-    for (char c : iA)
-    {
-        const size_t p = iB.find(c);
-        TB_CHECK(p != std::string::npos, TB_ERR_ARG, "DPD dot: labels must match");
-        TB_CHECK(A.len[iA.find(c)] == B.len[p], TB_ERR_ARG, "DPD dot: per-irrep lengths differ");
-    }
     Storage sa, sb;
     sa.init(A_->data, A.total(), true, st);
     sb.init(B_->data, B.total(), true, st);
-    double sum = 0.0;
-    if (A.irrep == B.irrep)
-    {
-        const auto pB = positions(iA, iB);
-        std::vector<unsigned> irrB(B.ndim), all(A.ndim), irrA(A.ndim, 0);
-        for (unsigned d = 0; d < A.ndim; d++) all[d] = d;
-        for_each_combo(all, A.irrep, A.nirrep, irrA, [&]
-        {
-            for (unsigned d = 0; d < A.ndim; d++) irrB[pB[d]] = irrA[d];
-            BlockView ab(A, sa.dev, irrA, 1.0), bb(B, sb.dev, irrB, 1.0);
-            if (ab.empty || bb.empty) return;
-            tblis_scalar r;
-            checked([&] { tblis_tensor_dot(nullptr, nullptr, &ab.t, idx_A, &bb.t, idx_B, &r); });
-            sum += r.data.d;
-        });
-    }
+    const double sum = dpd_dot_dev(A, sa.dev, std::string(idx_A, A.ndim), B, sb.dev, std::string(idx_B, B.ndim));
     sa.finish(st);
     sb.finish(st);
     return A_->scalar.data.d*B_->scalar.data.d*sum;
 }
 
-void dpd_reduce(int op, const tblis_b200_dpd_block_table* A_, const label_type* idx_A, double& result, i64& idx)
+void dpd_reduce_dev(int op, const DpdLayout& A, const double* a, const std::string& iA, double& result, i64& idx)
 {
-    ensure_device();
-    cudaStream_t st = current_stream();
-    DpdLayout A;
-    to_layout(A_, A);
-    Storage sa;
-    sa.init(A_->data, A.total(), true, st);
     // reduce_init (src/util/thread.h:160-182)
     using lim = std::numeric_limits<double>;
     double acc = op == REDUCE_MAX ? lim::lowest() : (op == REDUCE_MIN || op == REDUCE_MIN_ABS) ? lim::max() : 0.0;
@@ -279,11 +281,11 @@ void dpd_reduce(int op, const tblis_b200_dpd_block_table* A_, const label_type* 
     for (unsigned d = 0; d < A.ndim; d++) all[d] = d;
     for_each_combo(all, A.irrep, A.nirrep, irr, [&]
     {
-        BlockView ab(A, sa.dev, irr, 1.0);
+        BlockView ab(A, a, irr, 1.0);
         if (ab.empty) return;
         tblis_scalar r;
         len_type bi = 0;
-        checked([&] { tblis_tensor_reduce(nullptr, nullptr, (reduce_t)op, &ab.t, idx_A, &r, &bi); });
+        checked([&] { tblis_tensor_reduce(nullptr, nullptr, (reduce_t)op, &ab.t, iA.c_str(), &r, &bi); });
         const double v = r.data.d;
         const i64 gi = bi + ab.offset;
         switch (op)
@@ -297,33 +299,48 @@ void dpd_reduce(int op, const tblis_b200_dpd_block_table* A_, const label_type* 
             default: throw error(TB_ERR_ARG, "DPD reduce: unknown operation");
         }
     });
-    sa.finish(st);
     if (op == REDUCE_NORM_2) acc = std::sqrt(acc);
     result = acc;
     idx = at;
 }
 
-// kind: 0 scale, 1 set, 2 shift (A = alpha + scalar*A)
+void dpd_reduce(int op, const tblis_b200_dpd_block_table* A_, const label_type* idx_A, double& result, i64& idx)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    DpdLayout A;
+    to_layout(A_, A);
+    Storage sa;
+    sa.init(A_->data, A.total(), true, st);
+    dpd_reduce_dev(op, A, sa.dev, std::string(idx_A, A.ndim), result, idx);
+    sa.finish(st);
+}
+
+// kind: 0 scale (A *= scal), 1 set (A = alpha), 2 shift (A = alpha + scal*A)
+void dpd_unary_dev(int kind, double alpha, double scal, const DpdLayout& A, double* a, const std::string& iA)
+{
+    A.for_each_block([&](const std::vector<unsigned>& irr, const std::vector<i64>&, const std::vector<i64>&, i64)
+    {
+        BlockView ab(A, a, irr, scal);
+        if (ab.empty) return;
+        tblis_scalar s;
+        s.type = TYPE_DOUBLE;
+        s.data.d = alpha;
+        if (kind == 0) checked([&] { tblis_tensor_scale(nullptr, nullptr, &ab.t, iA.c_str()); });
+        else if (kind == 1) checked([&] { tblis_tensor_set(nullptr, nullptr, &s, &ab.t, iA.c_str()); });
+        else checked([&] { tblis_tensor_shift(nullptr, nullptr, &s, &ab.t, iA.c_str()); });
+    });
+}
+
 void dpd_unary(int kind, double alpha, tblis_b200_dpd_block_table* A_, const label_type* idx_A)
 {
     ensure_device();
     cudaStream_t st = current_stream();
     DpdLayout A;
     to_layout(A_, A);
-    const double scal = A_->scalar.data.d;
     Storage sa;
     sa.init(A_->data, A.total(), kind != 1, st);
-    A.for_each_block([&](const std::vector<unsigned>& irr, const std::vector<i64>&, const std::vector<i64>&, i64)
-    {
-        BlockView ab(A, sa.dev, irr, scal);
-        if (ab.empty) return;
-        tblis_scalar a;
-        a.type = TYPE_DOUBLE;
-        a.data.d = alpha;
-        if (kind == 0) checked([&] { tblis_tensor_scale(nullptr, nullptr, &ab.t, idx_A); });
-        else if (kind == 1) checked([&] { tblis_tensor_set(nullptr, nullptr, &a, &ab.t, idx_A); });
-        else checked([&] { tblis_tensor_shift(nullptr, nullptr, &a, &ab.t, idx_A); });
-    });
+    dpd_unary_dev(kind, alpha, A_->scalar.data.d, A, sa.dev, std::string(idx_A, A.ndim));
     sa.out(st);
     sa.finish(st);
     A_->scalar.data.d = 1.0;

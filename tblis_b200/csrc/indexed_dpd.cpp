@@ -24,7 +24,9 @@
 #include "level1.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <string>
 
@@ -379,9 +381,311 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
     }
 }
 
+namespace
+{
+
+// scales every entry's blocks by f_e*beta (set when beta == 0 or f_e == 0),
+// as src/internal/1t/indexed_dpd/scale.cxx and set.cxx do
+void scale_entries(const IdxTensor& X, double beta, const std::string& labels)
+{
+    const std::string dl = labels.substr(0, X.dense_ndim);
+    for (i64 e = 0; e < X.nidx; e++)
+    {
+        if (beta == 0.0 || X.factor[e] == 0.0) dpd_unary_dev(1, 0.0, 1.0, X.dense, X.data[e], dl);
+        else dpd_unary_dev(0, 0.0, X.factor[e]*beta, X.dense, X.data[e], dl);
+    }
+}
+
+// the pairs (entry of X, entry of Y) that agree on the labels both index, as
+// DPD tensors over the labels dense in both with the other labels fixed
+// (slices); a shared length-1 label stands in when none is left
+template <typename F>
+void for_each_pair(const IdxTensor& X, const std::string& iX, const IdxTensor& Y, const std::string& iY, F&& f)
+{
+    const IdxTensor* T[2] = {&X, &Y};
+    const std::string* I[2] = {&iX, &iY};
+    std::map<char, unsigned> fixed;
+    for (int t = 0; t < 2; t++)
+        for (unsigned d = 0; d < T[t]->nindexed(); d++) fixed[(*I[t])[T[t]->dense_ndim + d]] = T[t]->idx_irrep[d];
+    Slicing S[2];
+    for (int t = 0; t < 2; t++)
+        for (unsigned d = 0; d < T[t]->dense_ndim; d++)
+        {
+            const char c = (*I[t])[d];
+            auto it = fixed.find(c);
+            if (it == fixed.end()) { S[t].keep.push_back(d); S[t].labels.push_back(c); }
+            else { S[t].cut.push_back(d); S[t].cut_irrep.push_back(it->second); S[t].cut_label.push_back(c); }
+        }
+    bool shared = false;
+    for (char c : S[0].labels) if (S[1].labels.find(c) != std::string::npos) shared = true;
+    std::string lX = S[0].labels, lY = S[1].labels;
+    unsigned dum = 0;
+    if (!shared)
+    {
+        std::string used = iX + iY;
+        for (int c = 33; c < 127 && !dum; c++)
+            if (used.find((char)c) == std::string::npos) { lX.push_back((char)c); lY.push_back((char)c); dum = 1; }
+        TB_CHECK(dum, TB_ERR_ARG, "indexed DPD: no free label");
+    }
+    auto value_of = [&](int t, i64 e, char c, i64& v)
+    {
+        const size_t p = I[t]->find(c);
+        if (p == std::string::npos || p < T[t]->dense_ndim) return false;
+        v = T[t]->index(e, (unsigned)(p - T[t]->dense_ndim));
+        return true;
+    };
+    for (i64 ex = 0; ex < X.nidx; ex++)
+        for (i64 ey = 0; ey < Y.nidx; ey++)
+        {
+            bool ok = true;
+            for (unsigned d = 0; d < Y.nindexed() && ok; d++)
+            {
+                i64 v;
+                if (value_of(0, ex, iY[Y.dense_ndim + d], v) && v != Y.index(ey, d)) ok = false;
+            }
+            if (!ok) continue;
+            std::vector<i64> vals[2];
+            for (int t = 0; t < 2; t++)
+                for (char c : S[t].cut_label)
+                {
+                    i64 v = -1;
+                    if (!value_of(0, ex, c, v)) value_of(1, ey, c, v);
+                    vals[t].push_back(v);
+                }
+            DpdTensor x, y;
+            if (!slice_entry(X, ex, S[0], vals[0], dum, x) || !slice_entry(Y, ey, S[1], vals[1], dum, y)) continue;
+            f(ex, ey, x, lX, y, lY);
+        }
+}
+
+bool indexed_irreps_agree(const IdxTensor& X, const std::string& iX, const IdxTensor& Y, const std::string& iY)
+{
+    for (unsigned d = 0; d < X.nindexed(); d++)
+    {
+        const size_t p = iY.find(iX[X.dense_ndim + d]);
+        if (p != std::string::npos && p >= Y.dense_ndim && Y.idx_irrep[p - Y.dense_ndim] != X.idx_irrep[d])
+            return false;
+    }
+    return true;
+}
+
+struct IdxCall
+{
+    IdxTensor A, B;
+    EntryStage sa, sb;
+};
+
+} // namespace
+
+void indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
+                     tblis_b200_indexed_dpd_tensor* B_, const label_type* idx_B)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    IdxTensor A, B;
+    parse(A_, A); parse(B_, B);
+    TB_CHECK(A.nirrep == B.nirrep, TB_ERR_ARG, "indexed DPD add: nirrep differs");
+    const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim);
+    std::string Aonly, Bonly;
+    for (char c : iA) if (iB.find(c) == std::string::npos) Aonly.push_back(c);
+    for (char c : iB) if (iA.find(c) == std::string::npos) Bonly.push_back(c);
+    const double alpha = A_->scalar.data.d, beta = B_->scalar.data.d;
+    EntryStage sa, sb;
+    sa.init(A, true, false, st);
+    sb.init(B, beta != 0.0, true, st);
+    // src/iface/1t/add.cxx:312-325: alpha == 0 or an irrep mismatch only
+    // scales (through the factors, beta == 1 included)
+    if (alpha == 0.0 || (Aonly.empty() && Bonly.empty() && A.irrep() != B.irrep()))
+    {
+        for (i64 e = 0; e < B.nidx; e++)
+        {
+            const std::string dl = iB.substr(0, B.dense_ndim);
+            if (beta == 0.0 || B.factor[e] == 0.0) dpd_unary_dev(1, 0.0, 1.0, B.dense, B.data[e], dl);
+            else dpd_unary_dev(0, 0.0, B.factor[e]*beta, B.dense, B.data[e], dl);
+        }
+    }
+    else
+    {
+        if (beta != 1.0) scale_entries(B, beta, iB);
+        if (indexed_irreps_agree(A, iA, B, iB))
+            for_each_pair(A, iA, B, iB, [&](i64 ea, i64 eb, const DpdTensor& a, const std::string& la,
+                                            const DpdTensor& b, const std::string& lb)
+            {
+                const double w = alpha*A.factor[ea]*B.factor[eb];
+                if (w == 0.0) return;
+                dpd_add_dev(w, a.lay, a.data, la, 1.0, b.lay, b.data, lb);
+            });
+    }
+    sb.out(B.dense.total(), st);
+    if (sa.staged() || sb.staged()) TB_CUDA(cudaStreamSynchronize(st));
+    B_->scalar.data.d = 1.0;
+    B_->scalar.type = TYPE_DOUBLE;
+}
+
+double indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
+                       const tblis_b200_indexed_dpd_tensor* B_, const label_type* idx_B)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    IdxTensor A, B;
+    parse(A_, A); parse(B_, B);
+    TB_CHECK(A.nirrep == B.nirrep && A.ndim == B.ndim, TB_ERR_ARG, "indexed DPD dot: shapes differ");
+    const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim);
+    for (char c : iA) TB_CHECK(iB.find(c) != std::string::npos, TB_ERR_ARG, "indexed DPD dot: labels must match");
+    EntryStage sa, sb;
+    sa.init(A, true, false, st);
+    sb.init(B, true, false, st);
+    double sum = 0.0;
+    if (indexed_irreps_agree(A, iA, B, iB))
+        for_each_pair(A, iA, B, iB, [&](i64 ea, i64 eb, const DpdTensor& a, const std::string& la,
+                                        const DpdTensor& b, const std::string& lb)
+        {
+            const double w = A.factor[ea]*B.factor[eb];
+            if (w == 0.0) return;
+            sum += w*dpd_dot_dev(a.lay, a.data, la, b.lay, b.data, lb);
+        });
+    if (sa.staged() || sb.staged()) TB_CUDA(cudaStreamSynchronize(st));
+    return A_->scalar.data.d*B_->scalar.data.d*sum;
+}
+
+// src/internal/1t/indexed_dpd/reduce.cxx: each entry's reduction scaled by
+// its factor, combined in entry order; idx counts from entry 0's data
+void indexed_dpd_reduce(int op, const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
+                        double& result, i64& idx)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    IdxTensor A;
+    parse(A_, A);
+    const std::vector<double*> orig = A.data;
+    EntryStage sa;
+    sa.init(A, true, false, st);
+    const std::string dl(idx_A, A.dense_ndim);
+    using lim = std::numeric_limits<double>;
+    double acc = op == REDUCE_MAX ? lim::lowest() : (op == REDUCE_MIN || op == REDUCE_MIN_ABS) ? lim::max() : 0.0;
+    i64 at = -1;
+    for (i64 e = 0; e < A.nidx; e++)
+    {
+        double v;
+        i64 bi;
+        dpd_reduce_dev(op == REDUCE_NORM_2 ? REDUCE_NORM_2 : op, A.dense, A.data[e], dl, v, bi);
+        const double f = A.factor[e], fv = f*v;
+        const i64 gi = bi + (i64)(orig[e] - orig[0]);
+        switch (op)
+        {
+            case REDUCE_SUM: case REDUCE_SUM_ABS: acc += fv; break;
+            case REDUCE_NORM_2: acc += fv*fv; break;
+            case REDUCE_MAX: if (fv > acc) { acc = fv; at = gi; } break;
+            case REDUCE_MAX_ABS: if (std::fabs(fv) > acc) { acc = std::fabs(fv); at = gi; } break;
+            case REDUCE_MIN: if (fv < acc) { acc = fv; at = gi; } break;
+            case REDUCE_MIN_ABS: if (std::fabs(fv) < acc) { acc = std::fabs(fv); at = gi; } break;
+            default: throw error(TB_ERR_ARG, "indexed DPD reduce: unknown operation");
+        }
+    }
+    if (sa.staged()) TB_CUDA(cudaStreamSynchronize(st));
+    if (op == REDUCE_NORM_2) acc = std::sqrt(acc);
+    result = acc;
+    idx = at;
+}
+
+// kind 0: scale by A.scalar, 1: set to alpha, 2: shift (alpha + A.scalar*A),
+// each entry through its factor (src/internal/1t/indexed_dpd/{scale,set,shift}.cxx)
+void indexed_dpd_unary(int kind, double alpha, tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    IdxTensor A;
+    parse(A_, A);
+    EntryStage sa;
+    sa.init(A, kind != 1, true, st);
+    const std::string dl(idx_A, A.dense_ndim);
+    const double scal = A_->scalar.data.d;
+    for (i64 e = 0; e < A.nidx; e++)
+    {
+        const double f = A.factor[e];
+        if (kind == 0)
+        {
+            if (scal == 0.0 || f == 0.0) dpd_unary_dev(1, 0.0, 1.0, A.dense, A.data[e], dl);
+            else dpd_unary_dev(0, 0.0, f*scal, A.dense, A.data[e], dl);
+        }
+        else if (kind == 1)
+            dpd_unary_dev(1, f*alpha, 1.0, A.dense, A.data[e], dl);
+        else if (f == 0.0)
+        {
+            if (scal == 0.0) dpd_unary_dev(1, 0.0, 1.0, A.dense, A.data[e], dl);
+            else if (scal != 1.0) dpd_unary_dev(0, 0.0, scal, A.dense, A.data[e], dl);
+        }
+        else
+            dpd_unary_dev(2, f*alpha, scal, A.dense, A.data[e], dl);
+    }
+    sa.out(A.dense.total(), st);
+    if (sa.staged()) TB_CUDA(cudaStreamSynchronize(st));
+    A_->scalar.data.d = 1.0;
+    A_->scalar.type = TYPE_DOUBLE;
+}
+
 } // namespace tb
 
 extern "C" {
+
+int tblis_b200_indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                               tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B)
+{
+    return tb::guarded([&] { tb::indexed_dpd_add(A, idx_A, B, idx_B); });
+}
+
+int tblis_b200_indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                               const tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B,
+                               tblis_scalar* result)
+{
+    return tb::guarded([&]
+    {
+        TB_CHECK(result, tb::TB_ERR_ARG, "null result");
+        result->type = TYPE_DOUBLE;
+        result->data.d = tb::indexed_dpd_dot(A, idx_A, B, idx_B);
+    });
+}
+
+int tblis_b200_indexed_dpd_reduce(reduce_t op, const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
+                                  tblis_scalar* result, len_type* idx)
+{
+    return tb::guarded([&]
+    {
+        TB_CHECK(result && idx, tb::TB_ERR_ARG, "null result");
+        double r = 0;
+        tb::i64 i = -1;
+        tb::indexed_dpd_reduce((int)op, A, idx_A, r, i);
+        result->type = TYPE_DOUBLE;
+        result->data.d = r;
+        *idx = i;
+    });
+}
+
+int tblis_b200_indexed_dpd_scale(tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A)
+{
+    return tb::guarded([&] { tb::indexed_dpd_unary(0, 0.0, A, idx_A); });
+}
+
+int tblis_b200_indexed_dpd_set(const tblis_scalar* alpha, tblis_b200_indexed_dpd_tensor* A,
+                               const label_type* idx_A)
+{
+    return tb::guarded([&]
+    {
+        TB_CHECK(alpha, tb::TB_ERR_ARG, "null alpha");
+        tb::indexed_dpd_unary(1, alpha->data.d, A, idx_A);
+    });
+}
+
+int tblis_b200_indexed_dpd_shift(const tblis_scalar* alpha, tblis_b200_indexed_dpd_tensor* A,
+                                 const label_type* idx_A)
+{
+    return tb::guarded([&]
+    {
+        TB_CHECK(alpha, tb::TB_ERR_ARG, "null alpha");
+        tb::indexed_dpd_unary(2, alpha->data.d, A, idx_A);
+    });
+}
+
 
 int tblis_b200_indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A,
                                 const tblis_b200_indexed_dpd_tensor* B, const label_type* idx_B,

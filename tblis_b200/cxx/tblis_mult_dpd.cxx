@@ -306,6 +306,104 @@ TBLIS_B200_DPD_LEVEL1(double)
 TBLIS_B200_DPD_LEVEL1(std::complex<float>)
 TBLIS_B200_DPD_LEVEL1(std::complex<double>)
 
+// the same over indexed DPD views (instantiated in src/iface/1t/*.cxx)
+template <typename T>
+void add(const tci::communicator& comm,
+         T alpha, indexed_dpd_varray_view<const T> A, const label_type* idx_A,
+         T  beta, indexed_dpd_varray_view<      T> B, const label_type* idx_B)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, alpha), b(B, beta);
+        tblis_b200_indexed_dpd_add(&a.t, idx_A, &b.t, idx_B);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void dot(const tci::communicator& comm,
+         indexed_dpd_varray_view<const T> A, const label_type* idx_A,
+         indexed_dpd_varray_view<const T> B, const label_type* idx_B, T& result)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, T(1)), b(B, T(1));
+        tblis_scalar r;
+        if (tblis_b200_indexed_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = from_double<T>(r.data.d);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void reduce(const tci::communicator& comm, reduce_t op,
+            indexed_dpd_varray_view<const T> A, const label_type* idx_A, T& result, len_type& idx)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, T(1));
+        tblis_scalar r;
+        len_type i = -1;
+        if (tblis_b200_indexed_dpd_reduce((::reduce_t)op, &a.t, idx_A, &r, &i) == 0)
+        {
+            result = from_double<T>(r.data.d);
+            idx = i;
+        }
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void scale(const tci::communicator& comm, T alpha, indexed_dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, alpha);
+        tblis_b200_indexed_dpd_scale(&a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void set(const tci::communicator& comm, T alpha, indexed_dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, T(1));
+        tblis_scalar s;
+        set_scalar(s, alpha);
+        tblis_b200_indexed_dpd_set(&s, &a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+template <typename T>
+void shift(const tci::communicator& comm, T alpha, T beta, indexed_dpd_varray_view<T> A, const label_type* idx_A)
+{
+    if (is_master(comm))
+    {
+        IdxTable a(A, beta);
+        tblis_scalar s;
+        set_scalar(s, alpha);
+        tblis_b200_indexed_dpd_shift(&s, &a.t, idx_A);
+    }
+    wait_all(comm);
+}
+
+#define TBLIS_B200_INDEXED_DPD_LEVEL1(T) \
+template void add(const tci::communicator&, T, indexed_dpd_varray_view<const T>, const label_type*, \
+                  T, indexed_dpd_varray_view<T>, const label_type*); \
+template void dot(const tci::communicator&, indexed_dpd_varray_view<const T>, const label_type*, \
+                  indexed_dpd_varray_view<const T>, const label_type*, T&); \
+template void reduce(const tci::communicator&, reduce_t, indexed_dpd_varray_view<const T>, const label_type*, \
+                     T&, len_type&); \
+template void scale(const tci::communicator&, T, indexed_dpd_varray_view<T>, const label_type*); \
+template void set(const tci::communicator&, T, indexed_dpd_varray_view<T>, const label_type*); \
+template void shift(const tci::communicator&, T, T, indexed_dpd_varray_view<T>, const label_type*);
+TBLIS_B200_INDEXED_DPD_LEVEL1(float)
+TBLIS_B200_INDEXED_DPD_LEVEL1(double)
+TBLIS_B200_INDEXED_DPD_LEVEL1(std::complex<float>)
+TBLIS_B200_INDEXED_DPD_LEVEL1(std::complex<double>)
+
 #define TBLIS_B200_DPD_MULT(T) \
 template void mult(const tci::communicator& comm, \
                    T alpha, dpd_varray_view<const T> A, const label_type* idx_A, \

@@ -37,6 +37,9 @@ DPD_LEVEL1 = [
 ]
 
 
+INDEXED_DPD_LEVEL1 = [n.replace("15dpd_varray_view", "23indexed_dpd_varray_view") for n in DPD_LEVEL1]
+
+
 def _has(lib, name):
     try:
         getattr(lib, name)
@@ -48,7 +51,7 @@ def _has(lib, name):
 def test_cxx_library_exports_the_dpd_overloads():
     assert os.path.exists(CXX_LIB), "libtblis_b200_cxx.so not built (make -C tblis_b200 cxx MARRAY=...)"
     lib = ctypes.CDLL(CXX_LIB, mode=ctypes.RTLD_LOCAL)
-    missing = [n for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1 if not _has(lib, n)]
+    missing = [n for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1 + INDEXED_DPD_LEVEL1 if not _has(lib, n)]
     assert not missing, missing
 
 
@@ -56,4 +59,4 @@ def test_names_match_the_reference_library():
     if not os.path.exists(REF_LIB):
         pytest.skip("reference library not built here")
     ref = ctypes.CDLL(REF_LIB, mode=ctypes.RTLD_LOCAL)
-    assert all(_has(ref, n) for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1)
+    assert all(_has(ref, n) for n in DPD_MULT + INDEXED_DPD_MULT + DPD_LEVEL1 + INDEXED_DPD_LEVEL1)

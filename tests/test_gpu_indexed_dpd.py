@@ -104,3 +104,105 @@ def test_cxx_overload_matches_reference(cuda):
                                          ctypes.c_double(0.5), *args(C, iC))
         assert rc == 0, name
         assert np.linalg.norm(C["data"] - want["data"]) <= 1e-13 * max(1.0, np.linalg.norm(want["data"])), name
+
+
+# ---- level-1 ------------------------------------------------------------------------
+
+def _wrap(tb, torch, dev, n, T):
+    data = torch.from_numpy(T["data"]).to(dev)
+    return tb.IndexedDpdTensor(T["irrep"], n, T["lens"], T["idx_irreps"], T["indices"], data, T["factors"]), data
+
+
+def _l1_cases():
+    from tests.idx_dpd_helpers import make
+
+    def transpose(rng):
+        # B[jba] (j indexed in both) = A[abj]
+        n = 2
+        a, b, j = [2, 3], [3, 1], [2, 2]
+        A = make(rng, n, 1, [a, b, j], [1], [[0], [1]], factors=[1.0, -0.5])
+        B = make(rng, n, 1, [b, a, j], [1], [[1], [0]], factors=[2.0, 0.0])
+        return n, A, "abj", B, "baj"
+
+    def sliced(rng):
+        # j indexed in A, dense in B: each A entry adds into one slice of B
+        n = 2
+        a, j = [2, 3], [2, 2]
+        A = make(rng, n, 1, [a, j], [1], [[0], [1]], factors=[1.5, 1.0])
+        B = make(rng, n, 1, [a, j], [], [])
+        return n, A, "aj", B, "aj"
+
+    def trace(rng):
+        # B[a] = sum_c A[ac], c indexed in A
+        n = 2
+        a, c = [3, 2], [2, 1]
+        A = make(rng, n, 0, [a, c], [0], [[0], [1]], factors=[1.0, 2.0])
+        B = make(rng, n, 0, [a], [], [])
+        return n, A, "ac", B, "a"
+    return [("transpose", transpose), ("sliced", sliced), ("trace", trace)]
+
+
+@pytest.mark.parametrize("name,build", _l1_cases())
+@pytest.mark.parametrize("beta", [0.0, 1.0, -0.5])
+def test_level1_add(cuda, name, build, beta):
+    import torch
+    import tblis_b200 as tb
+    rng = np.random.default_rng(sum(map(ord, name)))
+    n, A, iA, B, iB = build(rng)
+    want = copy.deepcopy(B)
+    oracle.ref_indexed_dpd_add(n, 0.75, A, iA, beta, want, iB)
+    a, _ = _wrap(tb, torch, cuda, n, A)
+    b, db = _wrap(tb, torch, cuda, n, B)
+    tb.indexed_dpd_add(0.75, a, iA, beta, b, iB)
+    got = db.cpu().numpy()
+    assert np.linalg.norm(got - want["data"]) <= 1e-14 * max(1.0, np.linalg.norm(want["data"])), name
+
+
+@pytest.mark.parametrize("name,build", _l1_cases()[:2])
+def test_level1_dot(cuda, name, build):
+    import torch
+    import tblis_b200 as tb
+    rng = np.random.default_rng(3 + sum(map(ord, name)))
+    n, A, iA, B, iB = build(rng)
+    want = oracle.ref_indexed_dpd_dot(n, A, iA, B, iB)
+    a, _ = _wrap(tb, torch, cuda, n, A)
+    b, _ = _wrap(tb, torch, cuda, n, B)
+    got = tb.indexed_dpd_dot(a, iA, b, iB)
+    assert abs(got - want) <= 1e-13 * max(1.0, abs(want))
+
+
+@pytest.mark.parametrize("op", range(7))
+def test_level1_reduce(cuda, op):
+    import torch
+    import tblis_b200 as tb
+    from tests.idx_dpd_helpers import make
+    rng = np.random.default_rng(40 + op)
+    n = 4
+    A = make(rng, n, 3, [[2, 1, 3, 2], [1, 2, 2, 1], [2, 2, 1, 3]], [3], [[0], [2]], factors=[-0.5, 1.5])
+    want, wi = oracle.ref_indexed_dpd_reduce(op, n, A, "abc")
+    a, _ = _wrap(tb, torch, cuda, n, A)
+    got, gi = tb.indexed_dpd_reduce(op, a, "abc")
+    assert abs(got - want) <= 1e-13 * max(1.0, abs(want)), op
+    if op not in (0, 1, 6):
+        assert gi == wi
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_level1_unary(cuda, kind):
+    import torch
+    import tblis_b200 as tb
+    from tests.idx_dpd_helpers import make
+    rng = np.random.default_rng(50 + kind)
+    n = 2
+    A = make(rng, n, 1, [[2, 3], [3, 1], [2, 2]], [1], [[0], [1]], factors=[0.0, 1.5])
+    want = copy.deepcopy(A)
+    oracle.ref_indexed_dpd_unary(kind, 0.3, -2.0, n, want, "abc")
+    a, da = _wrap(tb, torch, cuda, n, A)
+    if kind == 0:
+        tb.indexed_dpd_scale(0.3, a, "abc")
+    elif kind == 1:
+        tb.indexed_dpd_set(0.3, a, "abc")
+    else:
+        tb.indexed_dpd_shift(0.3, -2.0, a, "abc")
+    got = da.cpu().numpy()
+    assert np.linalg.norm(got - want["data"]) <= 1e-14 * max(1.0, np.linalg.norm(want["data"]))
