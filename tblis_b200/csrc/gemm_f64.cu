@@ -177,31 +177,89 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
 
         const i64 kt_count = (k_end - k_begin + BK - 1)/BK;
 
+        // Per-thread gather geometry, fixed for the whole tile: in the
+        // rows-contiguous layout (mode 0) a thread always copies the same row
+        // at k = k0 + j*KSTEP; in the k-contiguous layout (mode 1) the same k
+        // of rows r0 + j*RSTEP. Row offsets are read from shared memory once
+        // per tile, k offsets once per stage (stride arithmetic when the
+        // 16-block of k is regular).
+        constexpr int AJ = BK*BM/NT, BJ = BK*BN/NT;
+        static_assert(NT % BM == 0 && NT % BN == 0 && NT % BK == 0, "gather geometry");
+        i64 a_ro[AMODE == 0 ? 1 : AJ], b_ro[BMODE == 0 ? 1 : BJ];
+        if (AMODE == 0) a_ro[0] = sAm[tid % BM];
+        else
+        {
+            #pragma unroll
+            for (int j = 0; j < (AMODE == 0 ? 1 : AJ); j++) a_ro[j] = sAm[tid/BK + j*(NT/BK)];
+        }
+        if (BMODE == 0) b_ro[0] = sBn[tid % BN];
+        else
+        {
+            #pragma unroll
+            for (int j = 0; j < (BMODE == 0 ? 1 : BJ); j++) b_ro[j] = sBn[tid/BK + j*(NT/BK)];
+        }
+
         auto load_tile = [&](int stage, i64 kt, const KInfo& ka, const KInfo& kb)
         {
             double* As = smem + stage*STAGE;
             double* Bs = As + TA::SIZE;
             const i64 k0 = k_begin + kt*BK;
             const int kvalid = (int)min((i64)BK, k_end - k0);
-            #pragma unroll
-            for (int e = tid; e < BK*BM; e += NT)
+            if (AMODE == 0)
             {
-                const int ml = AMODE == 0 ? e % BM : e / BK;
-                const int kl = AMODE == 0 ? e / BM : e % BK;
-                const i64 ro = sAm[ml];
-                const bool ok = ro >= 0 && kl < kvalid;
-                const i64 ko = ok ? koff(a_k, ka, k0, kl) : 0;
-                cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
+                const int ml = tid % BM, kl0 = tid / BM;
+                constexpr int KS = NT/BM;
+                const i64 ro = a_ro[0];
+                #pragma unroll
+                for (int j = 0; j < AJ; j++)
+                {
+                    const int kl = kl0 + j*KS;
+                    const bool ok = ro >= 0 && kl < kvalid;
+                    const i64 ko = ok ? koff(a_k, ka, k0, kl) : 0;
+                    cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
+                }
             }
-            #pragma unroll
-            for (int e = tid; e < BK*BN; e += NT)
+            else
             {
-                const int nl = BMODE == 0 ? e % BN : e / BK;
-                const int kl = BMODE == 0 ? e / BN : e % BK;
-                const i64 co = sBn[nl];
-                const bool ok = co >= 0 && kl < kvalid;
-                const i64 ko = ok ? koff(b_k, kb, k0, kl) : 0;
-                cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
+                const int kl = tid % BK, ml0 = tid / BK;
+                constexpr int RS = NT/BK;
+                const bool kok = kl < kvalid;
+                const i64 ko = kok ? koff(a_k, ka, k0, kl) : 0;
+                #pragma unroll
+                for (int j = 0; j < AJ; j++)
+                {
+                    const i64 ro = a_ro[AMODE == 0 ? 0 : j];
+                    const bool ok = kok && ro >= 0;
+                    cp_async8(As + TA::idx(ml0 + j*RS, kl), ok ? A + ro + ko : p.A, ok);
+                }
+            }
+            if (BMODE == 0)
+            {
+                const int nl = tid % BN, kl0 = tid / BN;
+                constexpr int KS = NT/BN;
+                const i64 co = b_ro[0];
+                #pragma unroll
+                for (int j = 0; j < BJ; j++)
+                {
+                    const int kl = kl0 + j*KS;
+                    const bool ok = co >= 0 && kl < kvalid;
+                    const i64 ko = ok ? koff(b_k, kb, k0, kl) : 0;
+                    cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
+                }
+            }
+            else
+            {
+                const int kl = tid % BK, nl0 = tid / BK;
+                constexpr int RS = NT/BK;
+                const bool kok = kl < kvalid;
+                const i64 ko = kok ? koff(b_k, kb, k0, kl) : 0;
+                #pragma unroll
+                for (int j = 0; j < BJ; j++)
+                {
+                    const i64 co = b_ro[BMODE == 0 ? 0 : j];
+                    const bool ok = kok && co >= 0;
+                    cp_async8(Bs + TB::idx(nl0 + j*RS, kl), ok ? B + co + ko : p.B, ok);
+                }
             }
         };
 
