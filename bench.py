@@ -333,6 +333,9 @@ def main():
     launches = tb.kernel_count() - k0
     kname = "ozaki_gemm_kernel" if method == 2 else "gemm_f64_kernel"
     k_total_ms, k_launches = tb.kernel_time(kname)
+    # device time per step of each stage of the contraction
+    stage_ms = {n: tb.kernel_time(n)[0] / args.steps
+                for n in (("oz_stats", "oz_slice", kname) if method == 2 else (kname,))}
     tb.kernel_timer(False)
     clocks = sampler.stop()
     total_ms = max_over_ranks(dist, torch, total_ms, dev)
@@ -385,6 +388,7 @@ def main():
         extra["cublas_dgemm_8192_tflops"] = fp64_peak
         extra["fp64_path_frac_of_cublas_dgemm"] = fp64_gflops / 1e3 / fp64_peak
         extra["speedup_vs_fp64_path"] = value / world / fp64_gflops
+        extra["stage_ms_per_step"] = stage_ms
         # the dominant kernel's own device time: CUDA events around each of its
         # launches on the launching stream, inside the timed steps
         launch_ms = k_total_ms / max(1, k_launches)

@@ -6,29 +6,32 @@
 //  1. row statistics: e_r = max exponent of row r of A (of column n of B) so
 //     that |x| < 2^e_r, plus the row's sum of squares for the error estimate;
 //  2. slicing: x' = x*2^-e_r in (-1,1) is split into S signed digits
-//     d_p in [-64, 64] by round-to-nearest, x' = sum_p d_p*2^(1-7p) + r_S,
-//     |r_S| <= 2^-7S, every step exact in FP64. Digits are written as INT8
-//     planes [l][p][row][k] (k contiguous, 16-byte row pitch) straight from
-//     the strided tensor through the GEMM view's scatter vectors;
+//     in [-127, 127] by round-to-nearest in base 254 (d_1 = rint(127 x'),
+//     then d_(p+1) = rint(254 r_p)), about 8 bits per slice, so
+//     x' = (sum_p d_p 254^(1-p) + r_S 254^(1-S))/127 with |r_S| <= 1/2.
+//     Digits are written as INT8 planes [l][p][row][k] (k contiguous, row
+//     pitch rounded to 64) straight from the strided tensor through the
+//     GEMM view's scatter vectors;
 //  3. one fused tcgen05 kernel per 128x64 output tile: for every k block,
 //     TMA brings the S planes of A and B into shared memory and one thread
 //     issues tcgen05.mma.kind::i8 for the slice pairs (p, q) with
 //     p + q <= S + 1, accumulating pairs of equal p + q ("diagonal" d) in
 //     their own INT32 accumulator in tensor memory (slice p of A meets
 //     B slices 1..S+1-p in one wide MMA, the B planes and the diagonals
-//     being adjacent in shared and tensor memory) (exact: |sum| <=
-//     (d-1)*K*64^2 < 2^31 for the K of one launch); the epilogue sums the
-//     diagonals in FP64 with weights 2^(2-7d), applies 2^(e_m + f_n),
-//     alpha and beta, and scatters into C through C's scatter vectors.
+//     being adjacent in shared and tensor memory). The sums are exact while
+//     (pairs on a diagonal) * K * 127^2 < 2^31, so K is split over launches
+//     beyond that; the epilogue sums the diagonals in FP64 with weights
+//     254^(2-d)/127^2, applies 2^(e_m + f_n), alpha and beta, and scatters
+//     into C through C's scatter vectors.
 //
 // FP64 arithmetic is used only for the exponent extraction and scaling, the
 // digit extraction, the cross-diagonal summation and the alpha/beta update.
 // The slice count S is chosen per call from an a-priori estimate of the
 // normwise error (row maxima and norms of A and B) to meet the tolerance.
 //
-// The same kernel runs two more plane formats: BF16 planes holding the same
-// integer digits (tcgen05.mma.kind::f16, FP32 accumulators, exact while a
-// diagonal's sum stays below 2^24, so K is split over launches of at most
+// The same kernel runs two more plane formats: BF16 planes holding base-128
+// digits in [-64, 64] (tcgen05.mma.kind::f16, FP32 accumulators, exact while
+// a diagonal's sum stays below 2^24, so K is split over launches of at most
 // 2^24/(S*64^2) each), and a single low-precision pass (S = 1) whose plane
 // holds x' itself rounded to BF16 or TF32 (kind::f16 / kind::tf32, FP32
 // accumulation over the whole K) for callers who accept that error.
@@ -76,6 +79,11 @@ __device__ __forceinline__ unsigned long long globaltimer()
 __device__ __forceinline__ void mbar_init(uint64_t* bar, int count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
@@ -211,8 +219,10 @@ struct OzGemmArgs
     const int *eA, *eB;          // [l][m], [l][n] exponents
     i64 M, N, K, L;
     int k_begin, k_count;        // k range of this launch, in elements (multiples of the k step)
+    int kt_flush;                // k steps whose digit sums stay exact; the accumulators are
+                                 // flushed into C after each such run of steps
     double alpha, beta;
-    int wbase;                   // diagonal d carries weight 2^(wbase - 7d)
+    double w[OZ_SMAX];           // weight of diagonal d = p + q at w[d - 2]
 };
 
 // TMEM columns for S diagonal accumulators of OZ_BN columns (a power of two >= 32)
@@ -237,7 +247,8 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     uint64_t* empty = full + STAGES;
     uint64_t* accum = empty + STAGES;
     uint64_t* done = accum + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* drained = done + 1;      // the epilogue has read a flushed chunk out of TMEM
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     i64* sCm = reinterpret_cast<i64*>(tmem_slot + 4);
     i64* sCn = sCm + OZ_BM;
@@ -249,12 +260,15 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*OZ_BN);
     const int l = blockIdx.y;
     const int kt_count = (p.k_count + KE - 1)/KE;
+    const int kt_flush = p.kt_flush > 0 ? p.kt_flush : kt_count;
+    const int nchunks = (kt_count + kt_flush - 1)/kt_flush;
 
     if (threadIdx.x == 0)
     {
         for (int s = 0; s < STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(accum, 1);
         mbar_init(done, 1);
+        mbar_init(drained, 4);             // one arrival per epilogue warp
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -309,8 +323,18 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         // ---- MMA issuer ----------------------------------------------------------
         if (lane == 0)
         {
+            int chunk = 0;
             for (int kt = 0; kt < kt_count; kt++)
             {
+                if (kt > 0 && kt % kt_flush == 0)
+                {
+                    // the sums of this run of k steps are complete: hand them to
+                    // the epilogue and restart once it has read them out
+                    mma_commit(accum);
+                    if (!mbar_wait(drained, chunk & 1, abort_flag)) break;
+                    tc_fence_after();
+                    chunk++;
+                }
                 const int s = kt % STAGES;
                 if (!mbar_wait(&full[s], (kt/STAGES) & 1, abort_flag)) break;
                 tc_fence_after();
@@ -330,7 +354,8 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         const uint64_t bd = sdesc_sw32(st + S*A_TILE + n0c*OZ_BK);
                         const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*OZ_BN + n0c);
                         // the pa = 1 row spans every diagonal: it starts the sums
-                        mma_op<KIND>(acc_addr, ad, bd, idesc_mma(KIND, nc), (kt == 0 && pa == 1) ? 0u : 1u);
+                        mma_op<KIND>(acc_addr, ad, bd, idesc_mma(KIND, nc),
+                                     (kt % kt_flush == 0 && pa == 1) ? 0u : 1u);
                     }
                 }
                 mma_commit(&empty[s]);
@@ -345,40 +370,54 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         // ---- epilogue: warps 2..5, one TMEM lane quarter each --------------------
         const int quarter = warp & 3;
         const int row = quarter*32 + lane;
-        const bool ok = mbar_wait(accum, 0, abort_flag);
-        tc_fence_after();
         const i64 rc = sCm[row];
         const i64 m = (i64)m0 + row;
-        const double rscale = (rc >= 0 && ok) ? p.alpha*ldexp(1.0, p.eA[(i64)l*p.M + m]) : 0.0;
         double* C = p.C + p.c_l[l];
+        // one pass per flushed chunk: the first applies beta, later ones add
         #pragma unroll 1
-        for (int c = 0; c < OZ_BN/16; c++)
+        for (int chunk = 0; chunk < nchunks; chunk++)
         {
-            double v[16];
-            #pragma unroll
-            for (int j = 0; j < 16; j++) v[j] = 0.0;
-            // smallest weights first
-            #pragma unroll
-            for (int d = S + 1; d >= 2; d--)
+            const bool ok = mbar_wait(accum, chunk & 1, abort_flag);
+            tc_fence_after();
+            const double rscale = (rc >= 0 && ok) ? p.alpha*ldexp(1.0, p.eA[(i64)l*p.M + m]) : 0.0;
+            const double beta = chunk == 0 ? p.beta : 1.0;
+            #pragma unroll 1
+            for (int c = 0; c < OZ_BN/16; c++)
             {
-                int r[16];
-                tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*OZ_BN + c*16), r);
-                const double w = ldexp(1.0, p.wbase - 7*d);
+                double v[16];
                 #pragma unroll
-                for (int j = 0; j < 16; j++)
-                    v[j] += (KIND == OZ_I8 ? (double)r[j] : (double)__int_as_float(r[j]))*w;
-            }
-            if (rc >= 0 && ok)
-            {
+                for (int j = 0; j < 16; j++) v[j] = 0.0;
+                // smallest weights first
                 #pragma unroll
-                for (int j = 0; j < 16; j++)
+                for (int d = S + 1; d >= 2; d--)
                 {
-                    const i64 cc = sCn[c*16 + j];
-                    if (cc < 0) continue;
-                    double* dst = C + rc + cc;
-                    const double val = rscale*sScaleN[c*16 + j]*v[j];
-                    *dst = p.beta == 0.0 ? val : val + p.beta*(*dst);
+                    int r[16];
+                    tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*OZ_BN + c*16), r);
+                    const double w = p.w[d - 2];
+                    #pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        v[j] += (KIND == OZ_I8 ? (double)r[j] : (double)__int_as_float(r[j]))*w;
                 }
+                if (rc >= 0 && ok)
+                {
+                    #pragma unroll
+                    for (int j = 0; j < 16; j++)
+                    {
+                        const i64 cc = sCn[c*16 + j];
+                        if (cc < 0) continue;
+                        double* dst = C + rc + cc;
+                        const double val = rscale*sScaleN[c*16 + j]*v[j];
+                        *dst = beta == 0.0 ? val : val + beta*(*dst);
+                    }
+                }
+            }
+            if (!ok) break;
+            if (chunk + 1 < nchunks)
+            {
+                // this warp's TMEM reads are done: the MMA thread may reuse the accumulators
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(drained);
             }
         }
     }
@@ -403,6 +442,7 @@ struct OzOperand
     const i64 *r_off, *k_off, *l_off;
     i64 R, K, L;
     int rmode;                     // 0: gather along rows (rows contiguous), 1: along k
+    i64 r_step, k_step;            // r_off[i] == i*r_step (k alike) for every i, or -1
 };
 
 constexpr int ST_THREADS = 256;
@@ -413,6 +453,20 @@ __device__ __forceinline__ int exp_of(double x)
     if (x != 0.0) frexp(x, &e);
     return x != 0.0 ? e : -100000;
 }
+
+// |x| as ordered integer bits: the largest |x| of a row has the largest
+// frexp exponent, so the row maximum is taken on the bits and converted once
+__device__ __forceinline__ unsigned long long abs_bits(double x)
+{
+    return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+}
+
+__device__ __forceinline__ int exp_of_bits(unsigned long long b)
+{
+    return exp_of(__longlong_as_double((long long)b));
+}
+
+constexpr int ST_UNROLL = 8;     // independent loads in flight per thread
 
 // rows contiguous: a thread per row, k split over blockIdx.y; partial
 // (max exponent, sum of squares) per split
@@ -426,16 +480,26 @@ oz_stats_rows(const OzOperand o, int ksplit, int* pexp, double* pss)
     const i64 kchunk = (o.K + ksplit - 1)/ksplit;
     const i64 k0 = sp*kchunk, k1 = min(o.K, k0 + kchunk);
     const double* X = o.X + o.l_off[l] + o.r_off[r];
-    int e = -100000;
+    unsigned long long mb = 0;
     double ss = 0.0;
-    for (i64 k = k0; k < k1; k++)
+    i64 k = k0;
+    const i64 ks = o.k_step;
+    for (; k + ST_UNROLL <= k1; k += ST_UNROLL)
+    {
+        double x[ST_UNROLL];
+        #pragma unroll
+        for (int u = 0; u < ST_UNROLL; u++) x[u] = X[ks >= 0 ? (k + u)*ks : o.k_off[k + u]];
+        #pragma unroll
+        for (int u = 0; u < ST_UNROLL; u++) { mb = max(mb, abs_bits(x[u])); ss += x[u]*x[u]; }
+    }
+    for (; k < k1; k++)
     {
         const double x = X[o.k_off[k]];
-        e = max(e, exp_of(x));
+        mb = max(mb, abs_bits(x));
         ss += x*x;
     }
     const i64 idx = ((i64)l*ksplit + sp)*o.R + r;
-    pexp[idx] = e;
+    pexp[idx] = exp_of_bits(mb);
     pss[idx] = ss;
 }
 
@@ -448,20 +512,30 @@ oz_stats_k(const OzOperand o, int* pexp, double* pss)
     const int l = blockIdx.z;
     if (r >= o.R) return;
     const double* X = o.X + o.l_off[l] + o.r_off[r];
-    int e = -100000;
+    unsigned long long mb = 0;
     double ss = 0.0;
-    for (i64 k = lane; k < o.K; k += 32)
+    i64 k = lane;
+    const i64 ks = o.k_step;
+    for (; k + 32*(ST_UNROLL - 1) < o.K; k += 32*ST_UNROLL)
+    {
+        double x[ST_UNROLL];
+        #pragma unroll
+        for (int u = 0; u < ST_UNROLL; u++) x[u] = X[ks >= 0 ? (k + 32*u)*ks : o.k_off[k + 32*u]];
+        #pragma unroll
+        for (int u = 0; u < ST_UNROLL; u++) { mb = max(mb, abs_bits(x[u])); ss += x[u]*x[u]; }
+    }
+    for (; k < o.K; k += 32)
     {
         const double x = X[o.k_off[k]];
-        e = max(e, exp_of(x));
+        mb = max(mb, abs_bits(x));
         ss += x*x;
     }
     for (int s = 16; s > 0; s >>= 1)
     {
-        e = max(e, __shfl_xor_sync(0xffffffffu, e, s));
+        mb = max(mb, (unsigned long long)__shfl_xor_sync(0xffffffffu, (long long)mb, s));
         ss += __shfl_xor_sync(0xffffffffu, ss, s);
     }
-    if (lane == 0) { pexp[(i64)l*o.R + r] = e; pss[(i64)l*o.R + r] = ss; }
+    if (lane == 0) { pexp[(i64)l*o.R + r] = exp_of_bits(mb); pss[(i64)l*o.R + r] = ss; }
 }
 
 // combines the per-split partials in split order
@@ -483,18 +557,41 @@ __global__ void oz_stats_final(i64 R, i64 L, int ksplit, const int* pexp, const 
     ss_out[i] = ss;
 }
 
-// digits of one value: x' = x*2^-e, d_1 = rint(64 x'), then 7 bits per digit
-template <int S>
-__device__ __forceinline__ void digits(double xs, signed char (&d)[S])
+// digits of one value x' = x*2^-e in (-1, 1). INT8 planes: base 254,
+// d_1 = rint(127 x') and d_(p+1) = rint(254 r_p) with r_p the remainder in
+// [-1/2, 1/2], so every digit lies in [-127, 127] and a slice carries ~8 bits:
+// x' = (d_1 + d_2/254 + ... + d_S/254^(S-1) + r_S/254^(S-1))/127. BF16 planes:
+// base 128, d_1 = rint(64 x'), then 7 bits per digit (products stay exact in
+// FP32 over longer K). Each step is y - rint(y), exact in FP64; the scaling
+// by 127 / 254 rounds at 2^-53 relative, far below any tolerance the slices
+// serve.
+template <int KIND>
+constexpr double first_digit_scale() { return KIND == OZ_I8 ? 127.0 : 64.0; }
+
+// digits of y = x'*first_digit_scale<KIND>()
+template <int S, int KIND>
+__device__ __forceinline__ void digit_words(double y, int (&d)[S])
 {
-    double y = xs*64.0;
+    constexpr double base = KIND == OZ_I8 ? 254.0 : 128.0;
+    // rounding to the nearest integer (ties to even, as rint) by adding and
+    // subtracting 1.5*2^52: exact for |y| < 2^51, and the integer sits in the
+    // low word of the sum, which saves the FP64 round and convert units
+    constexpr double shifter = 6755399441055744.0;
+    // (the _rn intrinsics keep the compiler from fusing a product into the
+    // shifter add, which would round the unrounded product instead)
     #pragma unroll
     for (int p = 0; p < S; p++)
     {
-        const double t = rint(y);
-        d[p] = (signed char)(int)t;
-        y = (y - t)*128.0;
+        const double sh = __dadd_rn(y, shifter);
+        d[p] = __double2loint(sh);      // the digit, two's complement
+        if (p + 1 < S) y = __dmul_rn(__dsub_rn(y, __dsub_rn(sh, shifter)), base);
     }
+}
+
+// 2^n, directly from the exponent field where 2^n is a normal number
+__device__ __forceinline__ double pow2i(int n)
+{
+    return (n >= -1022 && n <= 1023) ? __longlong_as_double((long long)(n + 1023) << 52) : ldexp(1.0, n);
 }
 
 constexpr int SL_T = 64;     // 64 rows x 64 k per block
@@ -530,67 +627,171 @@ __device__ __forceinline__ typename PlaneElem<KIND>::T single_elem(double xs)
     else return to_tf32_bits(xs);
 }
 
-// writes the S planes of a 64x64 tile, out[(l*S + p)][r][k] (pitch kp
-// elements): digit planes, or (SINGLE, S = 1) x' rounded to the plane type
+__device__ __forceinline__ void sl_cp_async8(double* smem, const double* gmem, bool valid)
+{
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
+                 :: "r"(saddr), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+
+constexpr int SL_LD = SL_T + 1;            // padded smem row (doubles)
+constexpr int SL_BLOCKS_PER_SM = 3;
+constexpr size_t SL_SMEM = 2*SL_T*SL_LD*sizeof(double);
+
+// writes the S planes of 64x64 tiles, out[(l*S + p)][r][k] (pitch kp
+// elements): digit planes, or (SINGLE, S = 1) x' rounded to the plane type.
+// Persistent blocks walk the tiles; the gather of the next tile (cp.async,
+// zero-filled outside the operand) runs while the current one is converted.
 template <int S, int KIND, bool SINGLE>
-__global__ void __launch_bounds__(256)
-oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp)
+__global__ void __launch_bounds__(256, SL_BLOCKS_PER_SM)
+oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tiles_r, unsigned tiles_k)
 {
     using T = typename PlaneElem<KIND>::T;
     T* out = static_cast<T*>(out_);
-    __shared__ double tile[SL_T][SL_T + 1];
-    const i64 r0 = blockIdx.x*(i64)SL_T, k0 = blockIdx.y*(i64)SL_T;
-    const int l = blockIdx.z;
-    const double* X = o.X + o.l_off[l];
+    extern __shared__ double sl_smem[];    // two [SL_T][SL_LD] buffers
+    const unsigned per_l = tiles_r*tiles_k, ntiles = per_l*(unsigned)o.L;   // below 2^31 (host check)
     const int t = threadIdx.x;
-    #pragma unroll
-    for (int j = 0; j < SL_T*SL_T/256; j++)
-    {
-        const int e = t + j*256;
-        const int rl = o.rmode == 0 ? e % SL_T : e / SL_T;
-        const int kl = o.rmode == 0 ? e / SL_T : e % SL_T;
-        const i64 r = r0 + rl, k = k0 + kl;
-        tile[rl][kl] = (r < o.R && k < o.K) ? X[o.r_off[r] + o.k_off[k]] : 0.0;
-    }
-    __syncthreads();
-    // 4 threads per row, 16 consecutive k each
-    const int rl = t >> 2, seg = (t & 3)*16;
-    const i64 r = r0 + rl;
-    if (r >= o.R) return;
-    const double sc = ldexp(1.0, -e_rows[(i64)l*o.R + r]);
-    alignas(16) T dg[S][16];
-    #pragma unroll
-    for (int j = 0; j < 16; j++)
-    {
-        const double xs = tile[rl][seg + j]*sc;
-        if constexpr (SINGLE)
-            dg[0][j] = single_elem<KIND>(xs);
+
+    // each thread gathers one fixed row (rows contiguous) or one fixed k (k
+    // contiguous) of the tile and 16 positions along the other index, which
+    // are the same across the warp
+    const bool by_rows = o.rmode == 0;
+    const int fixed = t & (SL_T - 1), vary0 = t >> 6;
+    const i64* fixed_off = by_rows ? o.r_off : o.k_off;
+    const i64* vary_off = by_rows ? o.k_off : o.r_off;
+    const i64 vary_step = by_rows ? o.k_step : o.r_step;     // -1: read the table
+    const i64 fixed_n = by_rows ? o.R : o.K, vary_n = by_rows ? o.K : o.R;
+    // smem position of element (fixed, vary0 + 4j): row-major [r][k] tile
+    const int s_base = by_rows ? fixed*SL_LD + vary0 : vary0*SL_LD + fixed;
+    const int s_step = by_rows ? 4 : 4*SL_LD;
+
+    struct At { int l; i64 r0, k0; };
+    auto where = [&](unsigned tile) {
+        const unsigned l = tile/per_l, rem = tile - l*per_l;
+        const unsigned tr = rem/tiles_k;
+        return At{(int)l, (i64)tr*SL_T, (i64)(rem - tr*tiles_k)*SL_T};
+    };
+    auto load = [&](const At& w, double* buf) {
+        const i64 f = (by_rows ? w.r0 : w.k0) + fixed;
+        const i64 v0 = (by_rows ? w.k0 : w.r0) + vary0;
+        const bool fok = f < fixed_n;
+        const double* Xf = o.X + o.l_off[w.l] + (fok ? fixed_off[f] : 0);
+        if (vary_step >= 0)
+        {
+            // a single stride: the addresses need no table reads
+            const double* Xv = Xf + v0*vary_step;
+            #pragma unroll
+            for (int j = 0; j < SL_T*SL_T/256; j++)
+            {
+                const bool ok = fok && v0 + 4*j < vary_n;
+                sl_cp_async8(buf + s_base + j*s_step, ok ? Xv + 4*j*vary_step : o.X, ok);
+            }
+        }
         else
         {
-            signed char d[S];
-            digits<S>(xs, d);
             #pragma unroll
-            for (int q = 0; q < S; q++) dg[q][j] = digit_elem<KIND>(d[q]);
+            for (int j = 0; j < SL_T*SL_T/256; j++)
+            {
+                const i64 v = v0 + 4*j;
+                const bool ok = fok && v < vary_n;
+                sl_cp_async8(buf + s_base + j*s_step, ok ? Xf + vary_off[v] : o.X, ok);
+            }
         }
-    }
-    const i64 kk = k0 + seg;
-    if (kk >= kp) return;
-    constexpr int VEC = 16*sizeof(T)/16;     // 16-byte stores per row segment
-    #pragma unroll
-    for (int q = 0; q < S; q++)
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    // 4 threads per row of a tile, 16 consecutive k each
+    const int rl = t >> 2, seg = (t & 3)*16;
+    const i64 plane = o.R*kp;              // elements between two planes
+    unsigned tile = blockIdx.x;
+    At at{0, 0, 0};
+    if (tile < ntiles) { at = where(tile); load(at, sl_smem); }
+    for (int it = 0; tile < ntiles; tile += gridDim.x, it++)
     {
-        uint4* dst = reinterpret_cast<uint4*>(out + (((i64)l*S + q)*o.R + r)*kp + kk);
-        const uint4* src = reinterpret_cast<const uint4*>(&dg[q][0]);
-        #pragma unroll
-        for (int v = 0; v < VEC; v++) dst[v] = src[v];
+        const double* cur = sl_smem + (it & 1)*SL_T*SL_LD;
+        const unsigned nxt = tile + gridDim.x;
+        At nat = at;
+        if (nxt < ntiles) { nat = where(nxt); load(nat, sl_smem + ((it + 1) & 1)*SL_T*SL_LD); }
+        else asm volatile("cp.async.commit_group;" ::: "memory");   // keeps the group count uniform
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+
+        const i64 r = at.r0 + rl, kk = at.k0 + seg;
+        if (r < o.R && kk < kp)
+        {
+            const int e = e_rows[(i64)at.l*o.R + r];
+            const double* src = cur + rl*SL_LD + seg;
+            T* dst = out + ((i64)at.l*S*o.R + r)*kp + kk;
+            if constexpr (KIND == OZ_I8 && !SINGLE)
+            {
+                // 2^-e*127 is exact: x*(2^-e*127) rounds once, as x'*127 does
+                const double sc = pow2i(-e)*first_digit_scale<KIND>();
+                // four digits to a word: the integers sit in the low words of
+                // the shifted sums, and two byte permutes interleave four of them
+                uint32_t w[S][4];
+                #pragma unroll
+                for (int g = 0; g < 4; g++)
+                {
+                    int lo[4][S];
+                    #pragma unroll
+                    for (int u = 0; u < 4; u++) digit_words<S, KIND>(src[g*4 + u]*sc, lo[u]);
+                    #pragma unroll
+                    for (int q = 0; q < S; q++)
+                        w[q][g] = __byte_perm(__byte_perm(lo[0][q], lo[1][q], 0x0040),
+                                              __byte_perm(lo[2][q], lo[3][q], 0x0040), 0x5410);
+                }
+                #pragma unroll
+                for (int q = 0; q < S; q++)
+                    *reinterpret_cast<uint4*>(dst + q*plane) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+            }
+            else
+            {
+                const double sc = pow2i(-e)*(SINGLE ? 1.0 : first_digit_scale<KIND>());
+                alignas(16) T dg[S][16];
+                #pragma unroll
+                for (int j = 0; j < 16; j++)
+                {
+                    const double xs = src[j]*sc;
+                    if constexpr (SINGLE)
+                        dg[0][j] = single_elem<KIND>(xs);
+                    else
+                    {
+                        int d[S];
+                        digit_words<S, KIND>(xs, d);
+                        #pragma unroll
+                        for (int q = 0; q < S; q++) dg[q][j] = digit_elem<KIND>(d[q]);
+                    }
+                }
+                constexpr int VEC = 16*sizeof(T)/16;     // 16-byte stores per row segment
+                #pragma unroll
+                for (int q = 0; q < S; q++)
+                {
+                    uint4* dq = reinterpret_cast<uint4*>(dst + q*plane);
+                    const uint4* sv = reinterpret_cast<const uint4*>(&dg[q][0]);
+                    #pragma unroll
+                    for (int v = 0; v < VEC; v++) dq[v] = sv[v];
+                }
+            }
+        }
+        at = nat;
+        __syncthreads();      // the buffer is refilled two tiles later
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 template <int S, int KIND, bool SINGLE>
 void launch_slice(const OzOperand& o, const int* e, void* out, i64 kp, cudaStream_t st)
 {
-    dim3 grid((unsigned)((o.R + SL_T - 1)/SL_T), (unsigned)((o.K + SL_T - 1)/SL_T), (unsigned)o.L);
-    oz_slice<S, KIND, SINGLE><<<grid, 256, 0, st>>>(o, e, out, kp);
+    const i64 tiles_r = (o.R + SL_T - 1)/SL_T, tiles_k = (o.K + SL_T - 1)/SL_T;
+    const i64 ntiles = tiles_r*tiles_k*o.L;
+    if (ntiles == 0) return;
+    TB_CHECK(ntiles < ((i64)1 << 31), TB_ERR_SIZE, "Ozaki operand above 2^31 tiles of 64x64");
+    const i64 grid = std::min<i64>(ntiles, (i64)device_sm_count()*SL_BLOCKS_PER_SM);
+    TB_CUDA(cudaFuncSetAttribute(oz_slice<S, KIND, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SL_SMEM));
+    TimedLaunch t("oz_slice", st);
+    oz_slice<S, KIND, SINGLE><<<(unsigned)grid, 256, SL_SMEM, st>>>(o, e, out, kp, (unsigned)tiles_r,
+                                                                     (unsigned)tiles_k);
     check_launch("oz_slice");
 }
 
@@ -625,6 +826,7 @@ void slice_dispatch(int kind, bool single, int S, const OzOperand& o, const int*
 
 void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
 {
+    TimedLaunch t("oz_stats", st);
     if (o.rmode == 0)
     {
         const int ksplit = (int)std::min<i64>(32, std::max<i64>(1, o.K/256));
@@ -694,7 +896,7 @@ template <int S>
 size_t gemm_smem_bytes()
 {
     return (size_t)stages_for<S>()*S*(A_TILE + B_TILE) + 1024 /* alignment */ +
-           (2*stages_for<S>() + 2)*8 + 16 + (OZ_BM + OZ_BN)*8 + OZ_BN*8;
+           (2*stages_for<S>() + 3)*8 + 16 + (OZ_BM + OZ_BN)*8 + OZ_BN*8;
 }
 
 template <int S, int KIND>
@@ -764,14 +966,27 @@ struct ErrorModel
         build(eA, ssA, K, ra2, ea);
         build(eB, ssB, K, rb2, eb);
     }
-    double operator()(int S) const
+    // residual bound of S digits relative to 2^e: base 254 (INT8):
+    // 1/(2*127*254^(S-1)); base 128 (BF16): 2^-7S
+    static double resolution(int kind, int S)
     {
-        const double ra = ra2 > 0 ? std::sqrt(std::ldexp(ra2, ea - 14*S)) : 0.0;
-        const double rb = rb2 > 0 ? std::sqrt(std::ldexp(rb2, eb - 14*S)) : 0.0;
-        // dropped pairs p + q > S + 1 are below the rounding terms by ~2^-7
-        return (ra + rb)*(1.0 + 2.0*S*std::ldexp(1.0, -7));
+        return kind == OZ_I8 ? 0.5/(127.0*std::pow(254.0, S - 1)) : std::ldexp(1.0, -7*S);
+    }
+    double operator()(int S, int kind) const
+    {
+        const double r = resolution(kind, S);
+        const double ra = ra2 > 0 ? std::sqrt(std::ldexp(ra2, ea))*r : 0.0;
+        const double rb = rb2 > 0 ? std::sqrt(std::ldexp(rb2, eb))*r : 0.0;
+        // dropped pairs p + q > S + 1 are below the rounding terms by ~1/base
+        return (ra + rb)*(1.0 + 2.0*S*(kind == OZ_I8 ? 1.0/127.0 : std::ldexp(1.0, -7)));
     }
 };
+
+// weight of diagonal d = p + q (p, q >= 1) in the epilogue's FP64 sum
+double diagonal_weight(int kind, int d)
+{
+    return kind == OZ_I8 ? 1.0/(127.0*127.0*std::pow(254.0, d - 2)) : std::ldexp(1.0, 2 - 7*d);
+}
 
 } // namespace
 
@@ -793,8 +1008,10 @@ void ozaki_begin(OzakiJob& j, cudaStream_t st)
     j.eB = dbuf((size_t)v.l*v.n*sizeof(int), st);
     j.sA = dbuf((size_t)v.l*v.m*sizeof(double), st);
     j.sB = dbuf((size_t)v.l*v.n*sizeof(double), st);
-    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode};
-    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode};
+    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode,
+                    j.tab->a_m_step, j.tab->a_k_step};
+    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode,
+                    j.tab->b_n_step, j.tab->b_k_step};
     stats(oa, j.eA.as<int>(), j.sA.as<double>(), st);
     stats(ob, j.eB.as<int>(), j.sB.as<double>(), st);
 }
@@ -812,8 +1029,9 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
         // significant bits in both operands, FP32 accumulation
         j.res.est_error = std::sqrt(2.0)*(kind == OZ_BF16 ? std::ldexp(1.0, -9) : std::ldexp(1.0, -11));
     }
-    else if (S <= 0)
+    else
     {
+        // the error model (and, without an explicit count, the slice count)
         std::vector<int> heA(v.l*v.m), heB(v.l*v.n);
         std::vector<double> hsA(v.l*v.m), hsB(v.l*v.n);
         if (stats_ready)
@@ -834,19 +1052,24 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
             TB_CUDA(cudaStreamSynchronize(st));
         }
         const ErrorModel est(heA, hsA, heB, hsB, v.k);
-        S = OZ_SMAX;
-        for (int s = 1; s <= OZ_SMAX; s++)
+        if (S <= 0)
         {
-            // safety factor 4 between the estimate and the target
-            if (est(s)*4.0 <= j.tol) { S = s; break; }
+            S = OZ_SMAX;
+            for (int s = 1; s <= OZ_SMAX; s++)
+            {
+                // safety factor 4 between the estimate and the target
+                if (est(s, kind)*4.0 <= j.tol) { S = s; break; }
+            }
         }
-        j.res.est_error = est(S);
+        if (S >= 1 && S <= OZ_SMAX) j.res.est_error = est(S, kind);
     }
     TB_CHECK(S >= 1 && S <= OZ_SMAX, TB_ERR_ARG, "Ozaki slice count must be 1..8");
     j.res.slices = S;
 
-    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode};
-    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode};
+    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode,
+                    j.tab->a_m_step, j.tab->a_k_step};
+    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode,
+                    j.tab->b_n_step, j.tab->b_k_step};
     const int esz = elem_bytes(kind);
     const i64 ke = OZ_BK/esz;              // k elements per MMA step
     const i64 kp = (v.k + 63)/64*64;       // row pitch (elements): TMA strides and 16-byte stores
@@ -858,24 +1081,28 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
     const CUtensorMap tbm = make_map(pb.ptr, v.k, v.n, v.l*S, kp, esz, OZ_BN);
 
     // exact accumulation of the digit products, (#pairs on a diagonal) *
-    // K_launch * 64^2 below 2^31 (INT32) or 2^24 (FP32 holds integers
-    // exactly up to there); a single pass runs the whole K at once
+    // (k run) * max|digit|^2 below 2^31 (INT32, digits up to 127) or 2^24
+    // (FP32 holds integers exactly up to there; digits up to 64): the kernel
+    // flushes the accumulators into C after each such run of k steps; a
+    // single pass runs the whole K at once
     const i64 acc_limit = kind == OZ_I8 ? (i64)0x7fffffff : ((i64)1 << 24);
-    const i64 klimit = j.single ? std::max<i64>(v.k, 1) : (acc_limit/((i64)S*64*64))/ke*ke;
-    for (i64 k0 = 0; k0 < v.k; k0 += klimit)
-    {
-        OzGemmArgs g;
-        g.C = j.C;
-        g.c_m = j.tab->c_m; g.c_n = j.tab->c_n; g.c_l = j.tab->c_l;
-        g.eA = j.eA.as<int>(); g.eB = j.eB.as<int>();
-        g.M = v.m; g.N = v.n; g.K = v.k; g.L = v.l;
-        g.k_begin = (int)k0;
-        g.k_count = (int)std::min(klimit, v.k - k0);
-        g.alpha = j.alpha;
-        g.beta = k0 == 0 ? j.beta : 1.0;
-        g.wbase = j.single ? 14 : 2;       // digits: 2^(2-7d); a single pass: weight 1
-        gemm_dispatch(kind, S, ta, tbm, g, st);
-    }
+    const i64 dmax = kind == OZ_I8 ? 127 : 64;
+    const i64 krun = j.single ? 0 : (acc_limit/((i64)S*dmax*dmax))/ke*ke;
+    TB_CHECK(j.single || krun >= ke, TB_ERR_SIZE, "Ozaki exactness run below one k step");
+    TB_CHECK(v.k <= (i64)0x7fffffff, TB_ERR_SIZE, "Ozaki contraction length above 2^31");
+    OzGemmArgs g;
+    g.C = j.C;
+    g.c_m = j.tab->c_m; g.c_n = j.tab->c_n; g.c_l = j.tab->c_l;
+    g.eA = j.eA.as<int>(); g.eB = j.eB.as<int>();
+    g.M = v.m; g.N = v.n; g.K = v.k; g.L = v.l;
+    g.k_begin = 0;
+    g.k_count = (int)v.k;
+    g.kt_flush = (int)(krun/ke);
+    g.alpha = j.alpha;
+    g.beta = j.beta;
+    for (int d = 2; d < OZ_SMAX + 2; d++)
+        g.w[d - 2] = j.single ? 1.0 : diagonal_weight(kind, d);   // a single pass: weight 1
+    gemm_dispatch(kind, S, ta, tbm, g, st);
 }
 
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,

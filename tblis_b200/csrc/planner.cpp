@@ -402,6 +402,16 @@ void append_key(std::string& key, const ivec& v)
 }
 }
 
+// s when t[i] == i*s for every i < n, else -1
+static i64 affine_step(const i64* t, i64 n)
+{
+    if (n == 0) return 0;
+    const i64 s = n > 1 ? t[1] : 0;
+    for (i64 i = 0; i < n; i++)
+        if (t[i] != i*s) return -1;
+    return s;
+}
+
 std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 BK,
                                         cudaStream_t stream)
 {
@@ -448,6 +458,8 @@ std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 B
     fill_block_scatter(v.lenL, v.cL, 1, 0, v.l, c_l, bs.data(), false);
 
     auto t = std::make_shared<GemmTables>();
+    t->a_m_step = affine_step(a_m, v.m); t->a_k_step = affine_step(a_k, v.k);
+    t->b_n_step = affine_step(b_n, v.n); t->b_k_step = affine_step(b_k, v.k);
     t->bytes = n_total*sizeof(i64);
     TB_CUDA(cudaMalloc(&t->dev, t->bytes));
     TB_CUDA(cudaMemcpyAsync(t->dev, host.data(), t->bytes, cudaMemcpyHostToDevice, stream));

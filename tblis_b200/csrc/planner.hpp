@@ -67,6 +67,8 @@ struct GemmTables
 {
     i64* dev = nullptr;      // one allocation holding every vector below
     i64 *a_m, *c_m, *a_k, *b_k, *b_n, *c_n, *a_l, *b_l, *c_l, *a_kbs, *b_kbs;
+    // s where the table is i*s for every i (a single stride), else -1
+    i64 a_m_step = -1, a_k_step = -1, b_n_step = -1, b_k_step = -1;
     size_t bytes = 0;
     ~GemmTables();
 };
