@@ -9,18 +9,22 @@
 //     in [-127, 127] by round-to-nearest in base 254 (d_1 = rint(127 x'),
 //     then d_(p+1) = rint(254 r_p)), about 8 bits per slice, so
 //     x' = (sum_p d_p 254^(1-p) + r_S 254^(1-S))/127 with |r_S| <= 1/2.
-//     Digits are written as INT8 planes [l][p][row][k] (k contiguous, row
-//     pitch rounded to 64) straight from the strided tensor through the
-//     GEMM view's scatter vectors;
-//  3. one fused tcgen05 kernel per 128x64 output tile: for every k block,
-//     TMA brings the S planes of A and B into shared memory and one thread
+//     Digits are written straight from the strided tensor (through the
+//     GEMM view's scatter vectors) as tiled INT8 planes: for each row tile
+//     (128 rows of A, 64 of B) and k step (32 bytes), the S slice tiles lie
+//     back to back in one block, each in the tensor core's canonical K-major
+//     layout, so that a stage is one bulk copy per operand;
+//  3. one fused tcgen05 kernel per 128x64 output tile: for every k step,
+//     the bulk-copy engine brings the S slice tiles of A and B into shared
+//     memory and one thread
 //     issues tcgen05.mma.kind::i8 for the slice pairs (p, q) with
 //     p + q <= S + 1, accumulating pairs of equal p + q ("diagonal" d) in
 //     their own INT32 accumulator in tensor memory (slice p of A meets
-//     B slices 1..S+1-p in one wide MMA, the B planes and the diagonals
+//     B slices 1..S+1-p in one wide MMA, the B tiles and the diagonals
 //     being adjacent in shared and tensor memory). The sums are exact while
-//     (pairs on a diagonal) * K * 127^2 < 2^31, so K is split over launches
-//     beyond that; the epilogue sums the diagonals in FP64 with weights
+//     (pairs on a diagonal) * K * 127^2 < 2^31, so beyond that the kernel
+//     flushes the accumulators into C after each such run of k steps and
+//     restarts them; the epilogue sums the diagonals in FP64 with weights
 //     254^(2-d)/127^2, applies 2^(e_m + f_n), alpha and beta, and scatters
 //     into C through C's scatter vectors.
 //
@@ -31,8 +35,8 @@
 //
 // The same kernel runs two more plane formats: BF16 planes holding base-128
 // digits in [-64, 64] (tcgen05.mma.kind::f16, FP32 accumulators, exact while
-// a diagonal's sum stays below 2^24, so K is split over launches of at most
-// 2^24/(S*64^2) each), and a single low-precision pass (S = 1) whose plane
+// a diagonal's sum stays below 2^24, so the runs between flushes are at most
+// 2^24/(S*64^2) long), and a single low-precision pass (S = 1) whose plane
 // holds x' itself rounded to BF16 or TF32 (kind::f16 / kind::tf32, FP32
 // accumulation over the whole K) for callers who accept that error.
 #include "ozaki.hpp"
@@ -40,7 +44,6 @@
 
 #include <cuda.h>
 #include <cuda_bf16.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -123,13 +126,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int x, int y, int z)
+// one contiguous global -> shared copy by the bulk-copy engine (16-byte
+// aligned addresses, a multiple of 16 bytes), completing on the mbarrier
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%3, %4, %5}], [%2];"
-                 :: "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
-                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols)
@@ -185,16 +187,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int (&r)[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// shared-memory matrix descriptor: K-major tile of 32-byte rows with the
-// 32-byte swizzle TMA writes (8-row atoms of 256 bytes, SBO = 256 B)
-__device__ __forceinline__ uint64_t sdesc_sw32(const void* p)
+// Slice tiles in shared memory (and, block by block, in the planes in global
+// memory) use the tensor core's canonical K-major layout without swizzle:
+// core matrices of 8 rows x 16 bytes (128 contiguous bytes), the two 16-byte
+// halves of a row's 32 k bytes 128 bytes apart, successive 8-row groups 256
+// bytes apart. Byte (row, kb) of a tile:
+__host__ __device__ constexpr int tile_byte(int row, int kb)
+{
+    return (row >> 3)*256 + (kb >> 4)*128 + (row & 7)*16 + (kb & 15);
+}
+
+// shared-memory matrix descriptor of such a tile: leading byte offset (the
+// k direction) 128, stride byte offset (the row direction) 256, no swizzle
+__device__ __forceinline__ uint64_t sdesc_kmajor(const void* p)
 {
     const uint64_t addr = smem_u32(p);
     return ((addr >> 4) & 0x3FFFull)          // start address
-         | (1ull << 16)                        // leading byte offset (unused when swizzled)
-         | ((uint64_t)(256 >> 4) << 32)        // stride byte offset: 8 rows x 32 B
-         | (1ull << 46)                        // descriptor version (sm100)
-         | (6ull << 61);                       // SWIZZLE_32B
+         | ((uint64_t)(128 >> 4) << 16)        // leading byte offset: next 16 k bytes
+         | ((uint64_t)(256 >> 4) << 32)        // stride byte offset: next 8 rows
+         | (1ull << 46);                       // descriptor version (sm100); layout 0: no swizzle
 }
 
 // instruction descriptor, K-major A and B, M = 128, N = n (a multiple of 16
@@ -217,8 +228,10 @@ struct OzGemmArgs
     double* C;
     const i64 *c_m, *c_n, *c_l;
     const int *eA, *eB;          // [l][m], [l][n] exponents
+    const unsigned char *pA, *pB; // tiled planes: blocks [l][row tile][k step] of S slice tiles
     i64 M, N, K, L;
-    int k_begin, k_count;        // k range of this launch, in elements (multiples of the k step)
+    i64 tiles_m, tiles_n;        // row tiles of the A and B planes
+    int k_steps;                 // k steps of the planes (K rounded up)
     int kt_flush;                // k steps whose digit sums stay exact; the accumulators are
                                  // flushed into C after each such run of steps
     double alpha, beta;
@@ -235,11 +248,9 @@ struct TmemCols
 
 template <int S, int STAGES, int KIND>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                  const OzGemmArgs p)
+ozaki_gemm_kernel(const OzGemmArgs p)
 {
     constexpr int STAGE_BYTES = S*(A_TILE + B_TILE);
-    constexpr int KE = OZ_BK/elem_bytes(KIND);       // k elements per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned base for the swizzled tiles
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -259,7 +270,7 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     const i64 tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
     const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*OZ_BN);
     const int l = blockIdx.y;
-    const int kt_count = (p.k_count + KE - 1)/KE;
+    const int kt_count = p.k_steps;
     const int kt_flush = p.kt_flush > 0 ? p.kt_flush : kt_count;
     const int nchunks = (kt_count + kt_flush - 1)/kt_flush;
 
@@ -301,13 +312,10 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 if (kt >= STAGES && !mbar_wait(&empty[s], ((kt/STAGES) & 1) ^ 1, abort_flag)) break;
                 unsigned char* st = smem + s*STAGE_BYTES;
                 mbar_expect_tx(&full[s], STAGE_BYTES);
-                const int kx = (p.k_begin + kt*KE)*elem_bytes(KIND);     // byte coordinate
-                #pragma unroll
-                for (int q = 0; q < S; q++)
-                    tma_load_3d(st + q*A_TILE, &tmA, &full[s], kx, m0, l*S + q);
-                #pragma unroll
-                for (int q = 0; q < S; q++)
-                    tma_load_3d(st + S*A_TILE + q*B_TILE, &tmB, &full[s], kx, n0, l*S + q);
+                // the S slice tiles of A, then those of B, each one contiguous block
+                bulk_load(st, p.pA + (((i64)l*p.tiles_m + tm)*p.k_steps + kt)*(S*A_TILE), S*A_TILE, &full[s]);
+                bulk_load(st + S*A_TILE, p.pB + (((i64)l*p.tiles_n + tn)*p.k_steps + kt)*(S*B_TILE),
+                          S*B_TILE, &full[s]);
             }
             // drain: the copies of the last stages must have landed before exit
             const int last = min(kt_count, STAGES);
@@ -346,12 +354,12 @@ ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 #pragma unroll
                 for (int pa = 1; pa <= S; pa++)
                 {
-                    const uint64_t ad = sdesc_sw32(st + (pa - 1)*A_TILE);
+                    const uint64_t ad = sdesc_kmajor(st + (pa - 1)*A_TILE);
                     #pragma unroll
                     for (int n0c = 0; n0c < (S + 1 - pa)*OZ_BN; n0c += 256)
                     {
                         const int nc = min(256, (S + 1 - pa)*OZ_BN - n0c);
-                        const uint64_t bd = sdesc_sw32(st + S*A_TILE + n0c*OZ_BK);
+                        const uint64_t bd = sdesc_kmajor(st + S*A_TILE + n0c*OZ_BK);
                         const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*OZ_BN + n0c);
                         // the pa = 1 row spans every diagonal: it starts the sums
                         mma_op<KIND>(acc_addr, ad, bd, idesc_mma(KIND, nc),
@@ -634,20 +642,32 @@ __device__ __forceinline__ void sl_cp_async8(double* smem, const double* gmem, b
                  :: "r"(saddr), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
 }
 
+// geometry of tiled planes: blocks [l][row tile][k step], each holding the S
+// slice tiles (tile_rows x 32 bytes, tile_byte order) back to back
+struct PlaneGeom
+{
+    int tile_rows;
+    i64 tiles, k_steps;
+    int S;
+};
+
 constexpr int SL_LD = SL_T + 1;            // padded smem row (doubles)
 constexpr int SL_BLOCKS_PER_SM = 3;
 constexpr size_t SL_SMEM = 2*SL_T*SL_LD*sizeof(double);
 
-// writes the S planes of 64x64 tiles, out[(l*S + p)][r][k] (pitch kp
-// elements): digit planes, or (SINGLE, S = 1) x' rounded to the plane type.
+// writes the S tiled planes (PlaneGeom) of 64x64 tiles of the operand:
+// digit planes, or (SINGLE, S = 1) x' rounded to the plane type. Rows and k
+// beyond the operand, up to whole tiles and k steps, get zeros.
 // Persistent blocks walk the tiles; the gather of the next tile (cp.async,
 // zero-filled outside the operand) runs while the current one is converted.
 template <int S, int KIND, bool SINGLE>
 __global__ void __launch_bounds__(256, SL_BLOCKS_PER_SM)
-oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tiles_r, unsigned tiles_k)
+oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, unsigned tiles_r, unsigned tiles_k)
 {
     using T = typename PlaneElem<KIND>::T;
-    T* out = static_cast<T*>(out_);
+    constexpr int KE = OZ_BK/(int)sizeof(T);         // elements per k step
+    unsigned char* outb = static_cast<unsigned char*>(out_);
+    const i64 tile_bytes = (i64)pg.tile_rows*OZ_BK;
     extern __shared__ double sl_smem[];    // two [SL_T][SL_LD] buffers
     const unsigned per_l = tiles_r*tiles_k, ntiles = per_l*(unsigned)o.L;   // below 2^31 (host check)
     const int t = threadIdx.x;
@@ -702,7 +722,7 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tile
 
     // 4 threads per row of a tile, 16 consecutive k each
     const int rl = t >> 2, seg = (t & 3)*16;
-    const i64 plane = o.R*kp;              // elements between two planes
+    const i64 k_lim = pg.k_steps*KE;
     unsigned tile = blockIdx.x;
     At at{0, 0, 0};
     if (tile < ntiles) { at = where(tile); load(at, sl_smem); }
@@ -717,11 +737,18 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tile
         __syncthreads();
 
         const i64 r = at.r0 + rl, kk = at.k0 + seg;
-        if (r < o.R && kk < kp)
+        if (kk < k_lim)
         {
-            const int e = e_rows[(i64)at.l*o.R + r];
+            // rows past the operand hold zeros: any exponent serves
+            const int e = r < o.R ? e_rows[(i64)at.l*o.R + r] : 0;
             const double* src = cur + rl*SL_LD + seg;
-            T* dst = out + ((i64)at.l*S*o.R + r)*kp + kk;
+            const i64 rt = r/pg.tile_rows;
+            const int rin = (int)(r - rt*pg.tile_rows);
+            // slice tile 0 of the block of row tile rt holding element k
+            auto block = [&](i64 k) {
+                return outb + (((i64)at.l*pg.tiles + rt)*pg.k_steps + k/KE)*S*tile_bytes +
+                       tile_byte(rin, (int)(k % KE)*(int)sizeof(T));
+            };
             if constexpr (KIND == OZ_I8 && !SINGLE)
             {
                 // 2^-e*127 is exact: x*(2^-e*127) rounds once, as x'*127 does
@@ -740,9 +767,11 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tile
                         w[q][g] = __byte_perm(__byte_perm(lo[0][q], lo[1][q], 0x0040),
                                               __byte_perm(lo[2][q], lo[3][q], 0x0040), 0x5410);
                 }
+                // the 16 k bytes are one 16-byte row of a core matrix
+                unsigned char* dst = block(kk);
                 #pragma unroll
                 for (int q = 0; q < S; q++)
-                    *reinterpret_cast<uint4*>(dst + q*plane) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+                    *reinterpret_cast<uint4*>(dst + q*tile_bytes) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
             }
             else
             {
@@ -762,14 +791,17 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tile
                         for (int q = 0; q < S; q++) dg[q][j] = digit_elem<KIND>(d[q]);
                     }
                 }
-                constexpr int VEC = 16*sizeof(T)/16;     // 16-byte stores per row segment
+                // 16-byte pieces of 16/sizeof(T) elements, each one core-matrix row
+                constexpr int PER = 16/(int)sizeof(T);
                 #pragma unroll
-                for (int q = 0; q < S; q++)
+                for (int v = 0; v < 16/PER; v++)
                 {
-                    uint4* dq = reinterpret_cast<uint4*>(dst + q*plane);
-                    const uint4* sv = reinterpret_cast<const uint4*>(&dg[q][0]);
+                    const i64 k = kk + v*PER;
+                    if (k >= k_lim) break;
+                    unsigned char* dst = block(k);
                     #pragma unroll
-                    for (int v = 0; v < VEC; v++) dq[v] = sv[v];
+                    for (int q = 0; q < S; q++)
+                        *reinterpret_cast<uint4*>(dst + q*tile_bytes) = *reinterpret_cast<const uint4*>(&dg[q][v*PER]);
                 }
             }
         }
@@ -780,9 +812,11 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, i64 kp, unsigned tile
 }
 
 template <int S, int KIND, bool SINGLE>
-void launch_slice(const OzOperand& o, const int* e, void* out, i64 kp, cudaStream_t st)
+void launch_slice(const OzOperand& o, const int* e, void* out, const PlaneGeom& pg, cudaStream_t st)
 {
-    const i64 tiles_r = (o.R + SL_T - 1)/SL_T, tiles_k = (o.K + SL_T - 1)/SL_T;
+    // every row of the row tiles, every k of the k steps
+    const i64 tiles_r = pg.tiles*pg.tile_rows/SL_T;
+    const i64 tiles_k = (pg.k_steps*(OZ_BK/elem_bytes(KIND)) + SL_T - 1)/SL_T;
     const i64 ntiles = tiles_r*tiles_k*o.L;
     if (ntiles == 0) return;
     TB_CHECK(ntiles < ((i64)1 << 31), TB_ERR_SIZE, "Ozaki operand above 2^31 tiles of 64x64");
@@ -790,38 +824,38 @@ void launch_slice(const OzOperand& o, const int* e, void* out, i64 kp, cudaStrea
     TB_CUDA(cudaFuncSetAttribute(oz_slice<S, KIND, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SL_SMEM));
     TimedLaunch t("oz_slice", st);
-    oz_slice<S, KIND, SINGLE><<<(unsigned)grid, 256, SL_SMEM, st>>>(o, e, out, kp, (unsigned)tiles_r,
+    oz_slice<S, KIND, SINGLE><<<(unsigned)grid, 256, SL_SMEM, st>>>(o, e, out, pg, (unsigned)tiles_r,
                                                                      (unsigned)tiles_k);
     check_launch("oz_slice");
 }
 
 template <int KIND>
-void slice_dispatch_kind(int S, const OzOperand& o, const int* e, void* out, i64 kp, cudaStream_t st)
+void slice_dispatch_kind(int S, const OzOperand& o, const int* e, void* out, const PlaneGeom& pg, cudaStream_t st)
 {
     switch (S)
     {
-        case 1: launch_slice<1, KIND, false>(o, e, out, kp, st); break;
-        case 2: launch_slice<2, KIND, false>(o, e, out, kp, st); break;
-        case 3: launch_slice<3, KIND, false>(o, e, out, kp, st); break;
-        case 4: launch_slice<4, KIND, false>(o, e, out, kp, st); break;
-        case 5: launch_slice<5, KIND, false>(o, e, out, kp, st); break;
-        case 6: launch_slice<6, KIND, false>(o, e, out, kp, st); break;
-        case 7: launch_slice<7, KIND, false>(o, e, out, kp, st); break;
-        default: launch_slice<8, KIND, false>(o, e, out, kp, st); break;
+        case 1: launch_slice<1, KIND, false>(o, e, out, pg, st); break;
+        case 2: launch_slice<2, KIND, false>(o, e, out, pg, st); break;
+        case 3: launch_slice<3, KIND, false>(o, e, out, pg, st); break;
+        case 4: launch_slice<4, KIND, false>(o, e, out, pg, st); break;
+        case 5: launch_slice<5, KIND, false>(o, e, out, pg, st); break;
+        case 6: launch_slice<6, KIND, false>(o, e, out, pg, st); break;
+        case 7: launch_slice<7, KIND, false>(o, e, out, pg, st); break;
+        default: launch_slice<8, KIND, false>(o, e, out, pg, st); break;
     }
 }
 
-void slice_dispatch(int kind, bool single, int S, const OzOperand& o, const int* e, void* out, i64 kp,
-                    cudaStream_t st)
+void slice_dispatch(int kind, bool single, int S, const OzOperand& o, const int* e, void* out,
+                    const PlaneGeom& pg, cudaStream_t st)
 {
     if (single)
     {
-        if (kind == OZ_BF16) launch_slice<1, OZ_BF16, true>(o, e, out, kp, st);
-        else launch_slice<1, OZ_TF32, true>(o, e, out, kp, st);
+        if (kind == OZ_BF16) launch_slice<1, OZ_BF16, true>(o, e, out, pg, st);
+        else launch_slice<1, OZ_TF32, true>(o, e, out, pg, st);
         return;
     }
-    if (kind == OZ_I8) slice_dispatch_kind<OZ_I8>(S, o, e, out, kp, st);
-    else slice_dispatch_kind<OZ_BF16>(S, o, e, out, kp, st);
+    if (kind == OZ_I8) slice_dispatch_kind<OZ_I8>(S, o, e, out, pg, st);
+    else slice_dispatch_kind<OZ_BF16>(S, o, e, out, pg, st);
 }
 
 void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
@@ -854,38 +888,6 @@ void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
 // host side
 // ---------------------------------------------------------------------------------
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
-{
-    static std::mutex mtx;
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    std::lock_guard<std::mutex> lk(mtx);
-    if (!fn)
-    {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        TB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-        TB_CHECK(q == cudaDriverEntryPointSuccess && p, TB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-// 3-D map over the slice planes [L*S][R][kp] as bytes (K and kp in
-// elements of esz bytes), box 32 bytes x rows x 1
-CUtensorMap make_map(const void* base, i64 K, i64 R, i64 planes, i64 kp, int esz, int box_rows)
-{
-    CUtensorMap m;
-    cuuint64_t dims[3] = {(cuuint64_t)(K*esz), (cuuint64_t)R, (cuuint64_t)planes};
-    cuuint64_t strides[2] = {(cuuint64_t)(kp*esz), (cuuint64_t)(kp*esz*R)};
-    cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides,
-                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    TB_CHECK(r == CUDA_SUCCESS, TB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    return m;
-}
-
 template <int S>
 constexpr int stages_for()
 {
@@ -900,7 +902,7 @@ size_t gemm_smem_bytes()
 }
 
 template <int S, int KIND>
-void launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb_, const OzGemmArgs& a, cudaStream_t st)
+void launch_gemm(const OzGemmArgs& a, cudaStream_t st)
 {
     constexpr int STG = stages_for<S>();
     auto kern = ozaki_gemm_kernel<S, STG, KIND>;
@@ -908,33 +910,32 @@ void launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb_, const OzGemmArgs
     TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     const i64 tiles = ((a.M + OZ_BM - 1)/OZ_BM)*((a.N + OZ_BN - 1)/OZ_BN);
     dim3 grid((unsigned)tiles, (unsigned)a.L, 1);
-    kern<<<grid, OZ_THREADS, bytes, st>>>(ta, tb_, a);
+    kern<<<grid, OZ_THREADS, bytes, st>>>(a);
     check_launch("ozaki_gemm_kernel");
 }
 
 template <int KIND>
-void gemm_dispatch_kind(int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a, cudaStream_t st)
+void gemm_dispatch_kind(int S, const OzGemmArgs& a, cudaStream_t st)
 {
     switch (S)
     {
-        case 1: launch_gemm<1, KIND>(ta, tbm, a, st); break;
-        case 2: launch_gemm<2, KIND>(ta, tbm, a, st); break;
-        case 3: launch_gemm<3, KIND>(ta, tbm, a, st); break;
-        case 4: launch_gemm<4, KIND>(ta, tbm, a, st); break;
-        case 5: launch_gemm<5, KIND>(ta, tbm, a, st); break;
-        case 6: launch_gemm<6, KIND>(ta, tbm, a, st); break;
-        case 7: launch_gemm<7, KIND>(ta, tbm, a, st); break;
-        default: launch_gemm<8, KIND>(ta, tbm, a, st); break;
+        case 1: launch_gemm<1, KIND>(a, st); break;
+        case 2: launch_gemm<2, KIND>(a, st); break;
+        case 3: launch_gemm<3, KIND>(a, st); break;
+        case 4: launch_gemm<4, KIND>(a, st); break;
+        case 5: launch_gemm<5, KIND>(a, st); break;
+        case 6: launch_gemm<6, KIND>(a, st); break;
+        case 7: launch_gemm<7, KIND>(a, st); break;
+        default: launch_gemm<8, KIND>(a, st); break;
     }
 }
 
-void gemm_dispatch(int kind, int S, const CUtensorMap& ta, const CUtensorMap& tbm, const OzGemmArgs& a,
-                   cudaStream_t st)
+void gemm_dispatch(int kind, int S, const OzGemmArgs& a, cudaStream_t st)
 {
     TimedLaunch t("ozaki_gemm_kernel", st);
-    if (kind == OZ_I8) gemm_dispatch_kind<OZ_I8>(S, ta, tbm, a, st);
-    else if (kind == OZ_BF16) gemm_dispatch_kind<OZ_BF16>(S, ta, tbm, a, st);
-    else launch_gemm<1, OZ_TF32>(ta, tbm, a, st);
+    if (kind == OZ_I8) gemm_dispatch_kind<OZ_I8>(S, a, st);
+    else if (kind == OZ_BF16) gemm_dispatch_kind<OZ_BF16>(S, a, st);
+    else launch_gemm<1, OZ_TF32>(a, st);
 }
 
 // a-priori normwise error estimate for S slices (rounding of both operands
@@ -1072,13 +1073,11 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
                     j.tab->b_n_step, j.tab->b_k_step};
     const int esz = elem_bytes(kind);
     const i64 ke = OZ_BK/esz;              // k elements per MMA step
-    const i64 kp = (v.k + 63)/64*64;       // row pitch (elements): TMA strides and 16-byte stores
-    dbuf pa((size_t)v.l*S*v.m*kp*esz, st), pb((size_t)v.l*S*v.n*kp*esz, st);
-    slice_dispatch(kind, j.single, S, oa, j.eA.as<int>(), pa.ptr, kp, st);
-    slice_dispatch(kind, j.single, S, ob, j.eB.as<int>(), pb.ptr, kp, st);
-
-    const CUtensorMap ta = make_map(pa.ptr, v.k, v.m, v.l*S, kp, esz, OZ_BM);
-    const CUtensorMap tbm = make_map(pb.ptr, v.k, v.n, v.l*S, kp, esz, OZ_BN);
+    const PlaneGeom ga = {OZ_BM, (v.m + OZ_BM - 1)/OZ_BM, (v.k + ke - 1)/ke, S};
+    const PlaneGeom gb = {OZ_BN, (v.n + OZ_BN - 1)/OZ_BN, ga.k_steps, S};
+    dbuf pa((size_t)(v.l*ga.tiles*ga.k_steps*S*A_TILE), st), pb((size_t)(v.l*gb.tiles*gb.k_steps*S*B_TILE), st);
+    slice_dispatch(kind, j.single, S, oa, j.eA.as<int>(), pa.ptr, ga, st);
+    slice_dispatch(kind, j.single, S, ob, j.eB.as<int>(), pb.ptr, gb, st);
 
     // exact accumulation of the digit products, (#pairs on a diagonal) *
     // (k run) * max|digit|^2 below 2^31 (INT32, digits up to 127) or 2^24
@@ -1094,15 +1093,16 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
     g.C = j.C;
     g.c_m = j.tab->c_m; g.c_n = j.tab->c_n; g.c_l = j.tab->c_l;
     g.eA = j.eA.as<int>(); g.eB = j.eB.as<int>();
+    g.pA = pa.as<unsigned char>(); g.pB = pb.as<unsigned char>();
     g.M = v.m; g.N = v.n; g.K = v.k; g.L = v.l;
-    g.k_begin = 0;
-    g.k_count = (int)v.k;
+    g.tiles_m = ga.tiles; g.tiles_n = gb.tiles;
+    g.k_steps = (int)ga.k_steps;
     g.kt_flush = (int)(krun/ke);
     g.alpha = j.alpha;
     g.beta = j.beta;
     for (int d = 2; d < OZ_SMAX + 2; d++)
         g.w[d - 2] = j.single ? 1.0 : diagonal_weight(kind, d);   // a single pass: weight 1
-    gemm_dispatch(kind, S, ta, tbm, g, st);
+    gemm_dispatch(kind, S, g, st);
 }
 
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
