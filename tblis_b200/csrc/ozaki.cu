@@ -59,7 +59,7 @@ constexpr int OZ_BM = 128;           // tile rows (TMEM lanes)
 constexpr int OZ_BN = 64;            // tile columns per diagonal accumulator
 constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step of any kind)
 constexpr int OZ_SMAX = 8;           // 8 diagonals x 64 columns = all 512 TMEM columns
-constexpr int OZ_THREADS = 192;      // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int OZ_THREADS = 192;      // warp 0 bulk copies, warp 1 MMA, warps 2-5 epilogue
 constexpr int A_TILE = OZ_BM*OZ_BK;  // bytes of one A slice tile
 constexpr int B_TILE = OZ_BN*OZ_BK;  // bytes of one B slice tile
 constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded waits: 2 s
@@ -303,7 +303,7 @@ ozaki_gemm_kernel(const OzGemmArgs p)
 
     if (warp == 0)
     {
-        // ---- TMA producer -------------------------------------------------------
+        // ---- bulk-copy producer -------------------------------------------------
         if (lane == 0)
         {
             for (int kt = 0; kt < kt_count && !*abort_flag; kt++)

@@ -100,13 +100,16 @@ def test_batches_overlap_on_device(cuda):
     import torch
     import tblis_b200 as tb
     srv = tb.Server(slots=4)
-    n = 6144
+    # the small requests (and their references) are built before the long
+    # one is submitted, so that they arrive while it still runs
+    small = _requests(torch, cuda, range(9500, 9508), max_len=6)
+    n = 8192
     a = torch.rand((n, n), dtype=torch.float64, device=cuda)
     b = torch.rand((n, n), dtype=torch.float64, device=cuda)
     c = torch.zeros((n, n), dtype=torch.float64, device=cuda)
-    big = srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij")      # ~20 ms on the GPU
+    torch.cuda.synchronize()
+    big = srv.submit(1.0, a, "ik", b, "kj", 0.0, c, "ij")      # ~40 ms on the GPU
     time.sleep(0.003)
-    small = _requests(torch, cuda, range(9500, 9508), max_len=6)
     ids = [srv.submit(*r["args"]) for r in small]
     lat_small = [srv.wait(i) for i in ids]
     lat_big = srv.wait(big)
