@@ -87,15 +87,31 @@ def _lab(s):
     return s.encode() if isinstance(s, str) else s
 
 
+_TYPE_OF = {np.dtype(np.float32): 0, np.dtype(np.float64): 1,
+            np.dtype(np.complex64): 2, np.dtype(np.complex128): 3}
+_DTYPE_OF = {v: k for k, v in _TYPE_OF.items()}
+
+
+def _set_scalar(sc, value, type_):
+    """Write value into a tblis_scalar's 16-byte union as the given type."""
+    sc.type = type_
+    raw = np.zeros(2, dtype=np.float64)
+    raw.view(_DTYPE_OF[type_])[0] = value
+    sc.data[0], sc.data[1] = raw[0], raw[1]
+
+
+def _scalar_value(sc):
+    raw = np.array([sc.data[0], sc.data[1]], dtype=np.float64)
+    v = raw.view(_DTYPE_OF[sc.type])[0]
+    return complex(v) if sc.type >= 2 else float(v)
+
+
 def _tensor(a, alpha=1.0, keep=None, conj=False):
     L, S = _lens_strides(a)
     t = Tensor()
-    cplx = a.dtype == np.complex128
-    t.type = 3 if cplx else 1
+    t.type = _TYPE_OF[a.dtype]
     t.conj = 1 if conj else 0
-    t.scalar.data[0] = complex(alpha).real
-    t.scalar.data[1] = complex(alpha).imag if cplx else 0.0
-    t.scalar.type = t.type
+    _set_scalar(t.scalar, alpha, t.type)
     t.data = a.ctypes.data
     t.ndim = a.ndim
     t.len = ctypes.cast(L, _P(_sz))
@@ -229,34 +245,51 @@ def ref_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, threads=None, conj_A=Fal
                         ctypes.byref(tC), _lab(idx_C))
 
 
-def ref_add(alpha, A, idx_A, beta, B, idx_B, threads=None):
+def ref_add(alpha, A, idx_A, beta, B, idx_B, threads=None, conj_A=False, conj_B=False):
     keep = []
     r = ref()
     if threads:
         r.tblis_set_num_threads(int(threads))
-    tA = _tensor(A, alpha, keep)
-    tB = _tensor(B, beta, keep)
+    tA = _tensor(A, alpha, keep, conj_A)
+    tB = _tensor(B, beta, keep, conj_B)
     r.tblis_tensor_add(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B))
 
 
-def ref_dot(A, idx_A, B, idx_B):
+def ref_dot(A, idx_A, B, idx_B, conj_A=False, conj_B=False):
+    """The reference's tblis_tensor_dot (a float, or a complex for complex arrays)."""
     keep = []
-    tA = _tensor(A, 1.0, keep)
-    tB = _tensor(B, 1.0, keep)
+    tA = _tensor(A, 1.0, keep, conj_A)
+    tB = _tensor(B, 1.0, keep, conj_B)
     s = Scalar()
-    s.type = 1
+    s.type = tA.type
     ref().tblis_tensor_dot(None, None, ctypes.byref(tA), _lab(idx_A), ctypes.byref(tB), _lab(idx_B), ctypes.byref(s))
-    return s.data[0]
+    return _scalar_value(s)
 
 
-def ref_reduce(op, A, idx_A, alpha=1.0):
+def ref_reduce(op, A, idx_A, alpha=1.0, conj=False):
     keep = []
-    tA = _tensor(A, alpha, keep)
+    tA = _tensor(A, alpha, keep, conj)
     s = Scalar()
-    s.type = 1
+    s.type = tA.type
     i = _sz(-1)
     ref().tblis_tensor_reduce(None, None, op, ctypes.byref(tA), _lab(idx_A), ctypes.byref(s), ctypes.byref(i))
-    return s.data[0], i.value
+    return _scalar_value(s), i.value
+
+
+def ref_unary(kind, A, idx_A, alpha=1.0, value=0.0, conj=False):
+    """The reference's tblis_tensor_scale (kind 1: A = alpha*op(A)), set
+    (0: A = value) and shift (2: A = value + alpha*op(A)), in place."""
+    keep = []
+    tA = _tensor(A, alpha, keep, conj)
+    v = Scalar()
+    _set_scalar(v, value, tA.type)
+    r = ref()
+    if kind == 0:
+        r.tblis_tensor_set(None, None, ctypes.byref(v), ctypes.byref(tA), _lab(idx_A))
+    elif kind == 1:
+        r.tblis_tensor_scale(None, None, ctypes.byref(tA), _lab(idx_A))
+    else:
+        r.tblis_tensor_shift(None, None, ctypes.byref(v), ctypes.byref(tA), _lab(idx_A))
 
 
 def ref_fill_block_scatter(lens, strides, BS, off, size, pack_3d):

@@ -122,13 +122,15 @@ def _dtype_code(x):
         return TYPE_FLOAT, 4
     if name.endswith("complex128"):
         return TYPE_DCOMPLEX, 16
+    if name.endswith("complex64"):
+        return TYPE_SCOMPLEX, 8
     raise TypeError("tblis_b200: unsupported dtype %s" % name)
 
 
 class _View:
     """A tblis_tensor describing a torch tensor or numpy array (no copy)."""
 
-    def __init__(self, x, scalar=1.0):
+    def __init__(self, x, scalar=1.0, conj=False):
         self.obj = x
         code, esize = _dtype_code(x)
         if hasattr(x, "data_ptr"):          # torch
@@ -144,15 +146,8 @@ class _View:
         self.stride = (ctypes.c_ssize_t * max(n, 1))(*strides)
         t = tblis_tensor()
         t.type = code
-        t.conj = 0
-        t.scalar.type = code
-        if code == TYPE_DOUBLE:
-            t.scalar.data[0] = float(scalar)
-        elif code == TYPE_DCOMPLEX:
-            t.scalar.data[0] = complex(scalar).real
-            t.scalar.data[1] = complex(scalar).imag
-        else:
-            ctypes.cast(ctypes.byref(t.scalar), _P(ctypes.c_float))[0] = float(scalar)
+        t.conj = 1 if conj else 0
+        t.scalar = _make_scalar(scalar, code)
         t.data = ptr
         t.ndim = n
         t.len = ctypes.cast(self.len, _P(ctypes.c_ssize_t))
@@ -170,18 +165,20 @@ def get_config(name):
     return p
 
 
-def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, cfg=None):
-    """C[idx_C] = alpha*A[idx_A]*B[idx_B] + beta*C[idx_C] (src/iface/3t/mult.h:28-38)."""
-    a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, cfg=None, conj_A=False, conj_B=False):
+    """C[idx_C] = alpha*A[idx_A]*B[idx_B] + beta*C[idx_C] (src/iface/3t/mult.h:28-38);
+    conj_A / conj_B conjugate complex operands."""
+    a, b, c = _View(A, alpha, conj_A), _View(B, 1.0, conj_B), _View(C, beta)
     lib.tblis_tensor_mult(None, cfg, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref, _labels(idx_C))
     _check()
 
 
-def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, tolerance=0.0, cfg=None):
+def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, tolerance=0.0, cfg=None,
+            conj_A=False, conj_B=False):
     """mult with an explicit method and a report dict. Methods: 1 = FP64 DMMA,
     2 = Ozaki INT8 slices, 3 = Ozaki BF16 slices (slice count from the
     tolerance unless given), 4 = one TF32 pass, 5 = one BF16 pass."""
-    a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+    a, b, c = _View(A, alpha, conj_A), _View(B, 1.0, conj_B), _View(C, beta)
     o = tblis_b200_opts(method, slices, tolerance)
     r = tblis_b200_report()
     lib.tblis_b200_tensor_mult_ex(cfg, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref,
@@ -190,25 +187,26 @@ def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, toler
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
 
 
-def add(alpha, A, idx_A, beta, B, idx_B):
-    """B[idx_B] = alpha*A[idx_A] + beta*B[idx_B] (src/iface/1t/add.h:27-35)."""
-    a, b = _View(A, alpha), _View(B, beta)
+def add(alpha, A, idx_A, beta, B, idx_B, conj_A=False, conj_B=False):
+    """B[idx_B] = alpha*op(A[idx_A]) + beta*op(B[idx_B]) (src/iface/1t/add.h:27-35);
+    op conjugates a complex operand whose flag is set."""
+    a, b = _View(A, alpha, conj_A), _View(B, beta, conj_B)
     lib.tblis_tensor_add(None, None, a.ref, _labels(idx_A), b.ref, _labels(idx_B))
     _check()
 
 
-def dot(A, idx_A, B, idx_B):
-    """sum over all labels of A*B (src/iface/1t/dot.h)."""
-    a, b = _View(A), _View(B)
+def dot(A, idx_A, B, idx_B, conj_A=False, conj_B=False):
+    """sum over all labels of op(A)*op(B) (src/iface/1t/dot.h)."""
+    a, b = _View(A, 1.0, conj_A), _View(B, 1.0, conj_B)
     r = tblis_scalar()
     lib.tblis_tensor_dot(None, None, a.ref, _labels(idx_A), b.ref, _labels(idx_B), ctypes.byref(r))
     _check()
     return _scalar_value(r, a.t.type)
 
 
-def reduce(op, A, idx_A):
+def reduce(op, A, idx_A, conj=False):
     """(value, offset) of a reduction (src/iface/1t/reduce.h:47-53)."""
-    a = _View(A)
+    a = _View(A, 1.0, conj)
     r = tblis_scalar()
     r.type = a.t.type
     idx = ctypes.c_ssize_t(-1)
@@ -217,9 +215,9 @@ def reduce(op, A, idx_A):
     return _scalar_value(r, a.t.type), idx.value
 
 
-def scale(alpha, A, idx_A):
-    """A = alpha*A (src/iface/1t/scale.h)."""
-    a = _View(A, alpha)
+def scale(alpha, A, idx_A, conj=False):
+    """A = alpha*op(A) (src/iface/1t/scale.h)."""
+    a = _View(A, alpha, conj)
     lib.tblis_tensor_scale(None, None, a.ref, _labels(idx_A))
     _check()
 
@@ -232,9 +230,9 @@ def set(alpha, A, idx_A):  # noqa: A001 -- mirrors tblis::set
     _check()
 
 
-def shift(alpha, beta, A, idx_A):
-    """A = alpha + beta*A (src/iface/1t/shift.h)."""
-    a = _View(A, beta)
+def shift(alpha, beta, A, idx_A, conj=False):
+    """A = alpha + beta*op(A) (src/iface/1t/shift.h)."""
+    a = _View(A, beta, conj)
     s = _make_scalar(alpha, a.t.type)
     lib.tblis_tensor_shift(None, None, ctypes.byref(s), a.ref, _labels(idx_A))
     _check()
@@ -243,17 +241,29 @@ def shift(alpha, beta, A, idx_A):
 def _make_scalar(v, code):
     s = tblis_scalar()
     s.type = code
+    f = ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))
     if code == TYPE_DOUBLE:
         s.data[0] = float(v)
+    elif code == TYPE_DCOMPLEX:
+        s.data[0] = complex(v).real
+        s.data[1] = complex(v).imag
+    elif code == TYPE_SCOMPLEX:
+        f[0] = complex(v).real
+        f[1] = complex(v).imag
     else:
-        ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))[0] = float(v)
+        f[0] = float(v)
     return s
 
 
 def _scalar_value(s, code):
+    f = ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))
     if code == TYPE_DOUBLE:
         return s.data[0]
-    return ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))[0]
+    if code == TYPE_DCOMPLEX:
+        return complex(s.data[0], s.data[1])
+    if code == TYPE_SCOMPLEX:
+        return complex(f[0], f[1])
+    return f[0]
 
 
 def kernel_count():

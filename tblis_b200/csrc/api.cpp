@@ -129,7 +129,11 @@ struct Staged
         nelem = hi - lo + 1;
         buf = dbuf((size_t)nelem*es, s);
         char* hbase = static_cast<char*>(host) + lo*(i64)es;
-        if (copy_in)
+        // an extent with gaps is copied in even for an output: copy_out
+        // writes the whole extent back, and the gaps must come back unchanged
+        i64 count = 1;
+        for (unsigned d = 0; d < t->ndim; d++) count *= t->len[d];
+        if (copy_in || count != nelem)
             TB_CUDA(cudaMemcpyAsync(buf.ptr, hbase, (size_t)nelem*es, cudaMemcpyHostToDevice, s));
         dptr = buf.as<char>() - lo*(i64)es;
     }
@@ -152,12 +156,6 @@ static size_t type_size(int type)
         case TYPE_DCOMPLEX: return 16;
     }
     throw error(TB_ERR_TYPE, "unknown tensor type");
-}
-
-static void require_real(int type, const char* what)
-{
-    if (type != TYPE_FLOAT && type != TYPE_DOUBLE)
-        throw error(TB_ERR_TYPE, std::string(what) + ": complex types are not supported on the GPU path");
 }
 
 static void fill_strided(Strided& s, const ivec& len, const ivec& stride)
@@ -185,9 +183,37 @@ static Strided one_tensor_dims(const tblis_tensor* A, const label_type* idx)
 template <typename T> static T scalar_of(const tblis_scalar& s);
 template <> double scalar_of<double>(const tblis_scalar& s) { return s.data.d; }
 template <> float scalar_of<float>(const tblis_scalar& s) { return s.data.s; }
+template <> cplx<float> scalar_of<cplx<float>>(const tblis_scalar& s) { return {s.data.c[0], s.data.c[1]}; }
+template <> cplx<double> scalar_of<cplx<double>>(const tblis_scalar& s) { return {s.data.z[0], s.data.z[1]}; }
 template <typename T> static void set_scalar(tblis_scalar& s, T v);
 template <> void set_scalar<double>(tblis_scalar& s, double v) { s.data.d = v; s.type = TYPE_DOUBLE; }
 template <> void set_scalar<float>(tblis_scalar& s, float v) { s.data.s = v; s.type = TYPE_FLOAT; }
+template <> void set_scalar<cplx<float>>(tblis_scalar& s, cplx<float> v)
+{
+    s.data.c[0] = v.re; s.data.c[1] = v.im; s.type = TYPE_SCOMPLEX;
+}
+template <> void set_scalar<cplx<double>>(tblis_scalar& s, cplx<double> v)
+{
+    s.data.z[0] = v.re; s.data.z[1] = v.im; s.type = TYPE_DCOMPLEX;
+}
+
+// dispatch on the element type of a level-1 call
+template <typename F>
+static void with_type(int type, F&& f)
+{
+    switch (type)
+    {
+        case TYPE_FLOAT: f(float()); break;
+        case TYPE_DOUBLE: f(double()); break;
+        case TYPE_SCOMPLEX: f(cplx<float>(0.0f)); break;
+        case TYPE_DCOMPLEX: f(cplx<double>(0.0)); break;
+        default: throw error(TB_ERR_TYPE, "unknown tensor type");
+    }
+}
+
+// |x| of a scalar (std::abs)
+template <typename T> static T abs_scalar(T x) { return x < T(0) ? -x : x; }
+template <typename R> static cplx<R> abs_scalar(cplx<R> x) { return cplx<R>(std::hypot(x.re, x.im)); }
 
 static void finish_host_call(std::vector<Staged*> outs, bool any_staged, cudaStream_t s)
 {
@@ -206,6 +232,8 @@ static void do_unary(int op, const tblis_scalar* val, tblis_tensor* A, const lab
     Staged sa;
     const T alpha = scalar_of<T>(A->scalar);
     const bool needs_in = !(op == 0 || (op != 0 && alpha == T(0)));
+    // a conjugated complex tensor is rewritten even with a unit scalar
+    const bool cj = is_cplx<T>::value && A->conj;
     sa.init(A, sizeof(T), needs_in, st);
     T* d = static_cast<T*>(sa.dptr);
     if (op == 0)                                   // set (src/iface/1t/set.cxx:39-46)
@@ -213,14 +241,14 @@ static void do_unary(int op, const tblis_scalar* val, tblis_tensor* A, const lab
     else if (op == 1)                              // scale (src/iface/1t/scale.cxx:39-56)
     {
         if (alpha == T(0)) l1_set<T>(d, s, T(0), st);
-        else if (alpha != T(1)) l1_scale<T>(d, s, alpha, st);
+        else if (alpha != T(1) || cj) l1_scale<T>(d, s, alpha, st, cj);
     }
     else                                           // shift (src/iface/1t/shift.cxx:39-70)
     {
         const T sh = scalar_of<T>(*val);
         if (alpha == T(0)) l1_set<T>(d, s, T(0), st);
-        else if (sh == T(0)) { if (alpha != T(1)) l1_scale<T>(d, s, alpha, st); }
-        else l1_shift<T>(d, s, sh, alpha, st);
+        else if (sh == T(0)) { if (alpha != T(1) || cj) l1_scale<T>(d, s, alpha, st, cj); }
+        else l1_shift<T>(d, s, sh, alpha, st, cj);
     }
     finish_host_call({&sa}, sa.staged, st);
     set_scalar<T>(A->scalar, T(1));
@@ -264,18 +292,19 @@ static void do_add(const tblis_tensor* A, const label_type* idx_A_, tblis_tensor
     fold(len_bo, ibo, {&s_bo});
 
     const T alpha = scalar_of<T>(A->scalar), beta = scalar_of<T>(B->scalar);
+    const bool cja = is_cplx<T>::value && A->conj, cjb = is_cplx<T>::value && B->conj;
     Staged sta, stb;
     stb.init(B, sizeof(T), beta != T(0), st);
     if (alpha == T(0))
     {
-        // src/iface/1t/add.cxx:76-90: set or scale B
+        // src/iface/1t/add.cxx:76-90: set or scale B (conjugated B: rewritten)
         Strided s;
         ivec l = len_bo, str = s_bo;
         l.insert(l.end(), len_ab.begin(), len_ab.end());
         str.insert(str.end(), sb_ab.begin(), sb_ab.end());
         fill_strided(s, l, str);
         if (beta == T(0)) l1_set<T>(static_cast<T*>(stb.dptr), s, T(0), st);
-        else if (beta != T(1)) l1_scale<T>(static_cast<T*>(stb.dptr), s, beta, st);
+        else if (beta != T(1) || cjb) l1_scale<T>(static_cast<T*>(stb.dptr), s, beta, st, cjb);
     }
     else
     {
@@ -295,10 +324,11 @@ static void do_add(const tblis_tensor* A, const label_type* idx_A_, tblis_tensor
             Strided sb;
             fill_strided(sb, len_bo, s_bo);
             if (beta == T(0)) l1_set<T>(static_cast<T*>(stb.dptr), sb, T(0), st);
-            else l1_scale<T>(static_cast<T*>(stb.dptr), sb, beta, st);
+            else l1_scale<T>(static_cast<T*>(stb.dptr), sb, beta, st, cjb);
         }
         else
-            l1_add<T>(static_cast<const T*>(sta.dptr), static_cast<T*>(stb.dptr), ab, ao, bo, alpha, beta, st);
+            l1_add<T>(static_cast<const T*>(sta.dptr), static_cast<T*>(stb.dptr), ab, ao, bo, alpha, beta, st,
+                      cja, cjb);
     }
     finish_host_call({&stb}, sta.staged || stb.staged, st);
     set_scalar<T>(B->scalar, T(1));
@@ -345,7 +375,8 @@ static void do_dot(const tblis_tensor* A, const label_type* idx_A_, const tblis_
     sta.init(A, sizeof(T), true, st);
     stb.init(B, sizeof(T), true, st);
     dbuf out(sizeof(T), st);
-    l1_dot<T>(static_cast<const T*>(sta.dptr), static_cast<const T*>(stb.dptr), s, out.as<T>(), st);
+    l1_dot<T>(static_cast<const T*>(sta.dptr), static_cast<const T*>(stb.dptr), s, out.as<T>(), st,
+              is_cplx<T>::value && A->conj, is_cplx<T>::value && B->conj);
     T v;
     TB_CUDA(cudaMemcpyAsync(&v, out.ptr, sizeof(T), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
@@ -360,7 +391,8 @@ static void do_reduce(int op, const tblis_tensor* A, const label_type* idx_A, tb
     cudaStream_t st = current_stream();
     Strided s = one_tensor_dims(A, idx_A);
     const T alpha = scalar_of<T>(A->scalar);
-    // src/iface/1t/reduce.cxx:39-43: a negative scalar swaps MIN and MAX
+    // src/iface/1t/reduce.cxx:39-43: a negative scalar swaps MIN and MAX (a
+    // complex scalar: a negative real part)
     if (alpha < T(0))
     {
         if (op == REDUCE_MIN) op = REDUCE_MAX;
@@ -368,17 +400,18 @@ static void do_reduce(int op, const tblis_tensor* A, const label_type* idx_A, tb
     }
     Staged sa;
     sa.init(A, sizeof(T), true, st);
-    dbuf out(sizeof(T) + sizeof(i64), st);
+    dbuf out(16 + sizeof(i64), st);
     T* dv = out.as<T>();
-    i64* di = reinterpret_cast<i64*>(out.as<char>() + 8);
+    i64* di = reinterpret_cast<i64*>(out.as<char>() + 16);
     l1_reduce<T>(op, static_cast<const T*>(sa.dptr), s, dv, di, st);
     T v; i64 id;
     TB_CUDA(cudaMemcpyAsync(&v, dv, sizeof(T), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaMemcpyAsync(&id, di, sizeof(i64), cudaMemcpyDeviceToHost, st));
     TB_CUDA(cudaStreamSynchronize(st));
-    // src/iface/1t/reduce.cxx:57-65
+    // src/iface/1t/reduce.cxx:52-65: conjugate, then apply the scalar
+    if (is_cplx<T>::value && A->conj) v = cj(v, true);
     if (op == REDUCE_SUM) v *= alpha;
-    else if (op == REDUCE_SUM_ABS || op == REDUCE_NORM_2) v *= (alpha < T(0) ? -alpha : alpha);
+    else if (op == REDUCE_SUM_ABS || op == REDUCE_NORM_2) v *= abs_scalar(alpha);
     set_scalar<T>(*result, v);
     if (idx) *idx = id;
 }
@@ -418,9 +451,7 @@ void tblis_tensor_add(const tblis_comm*, const tblis_config*,
     {
         TB_CHECK(A && B, TB_ERR_ARG, "null tensor");
         TB_CHECK(A->type == B->type, TB_ERR_TYPE, "add: operand types differ");
-        require_real(A->type, "add");
-        if (A->type == TYPE_DOUBLE) do_add<double>(A, idx_A, B, idx_B);
-        else do_add<float>(A, idx_A, B, idx_B);
+        with_type(A->type, [&](auto t) { do_add<decltype(t)>(A, idx_A, B, idx_B); });
     });
 }
 
@@ -433,9 +464,7 @@ void tblis_tensor_dot(const tblis_comm*, const tblis_config*,
     {
         TB_CHECK(A && B && result, TB_ERR_ARG, "null argument");
         TB_CHECK(A->type == B->type, TB_ERR_TYPE, "dot: operand types differ");
-        require_real(A->type, "dot");
-        if (A->type == TYPE_DOUBLE) do_dot<double>(A, idx_A, B, idx_B, result);
-        else do_dot<float>(A, idx_A, B, idx_B, result);
+        with_type(A->type, [&](auto t) { do_dot<decltype(t)>(A, idx_A, B, idx_B, result); });
     });
 }
 
@@ -446,9 +475,7 @@ void tblis_tensor_reduce(const tblis_comm*, const tblis_config*, reduce_t op,
     guarded([&]
     {
         TB_CHECK(A && result, TB_ERR_ARG, "null argument");
-        require_real(A->type, "reduce");
-        if (A->type == TYPE_DOUBLE) do_reduce<double>((int)op, A, idx_A, result, idx);
-        else do_reduce<float>((int)op, A, idx_A, result, idx);
+        with_type(A->type, [&](auto t) { do_reduce<decltype(t)>((int)op, A, idx_A, result, idx); });
     });
 }
 
@@ -457,9 +484,7 @@ void tblis_tensor_scale(const tblis_comm*, const tblis_config*, tblis_tensor* A,
     guarded([&]
     {
         TB_CHECK(A, TB_ERR_ARG, "null tensor");
-        require_real(A->type, "scale");
-        if (A->type == TYPE_DOUBLE) do_unary<double>(1, nullptr, A, idx_A);
-        else do_unary<float>(1, nullptr, A, idx_A);
+        with_type(A->type, [&](auto t) { do_unary<decltype(t)>(1, nullptr, A, idx_A); });
     });
 }
 
@@ -469,9 +494,8 @@ void tblis_tensor_set(const tblis_comm*, const tblis_config*, const tblis_scalar
     guarded([&]
     {
         TB_CHECK(A && alpha, TB_ERR_ARG, "null argument");
-        require_real(A->type, "set");
-        if (A->type == TYPE_DOUBLE) do_unary<double>(0, alpha, A, idx_A);
-        else do_unary<float>(0, alpha, A, idx_A);
+        TB_CHECK(alpha->type == A->type, TB_ERR_TYPE, "set: scalar and tensor types differ");
+        with_type(A->type, [&](auto t) { do_unary<decltype(t)>(0, alpha, A, idx_A); });
     });
 }
 
@@ -481,9 +505,8 @@ void tblis_tensor_shift(const tblis_comm*, const tblis_config*, const tblis_scal
     guarded([&]
     {
         TB_CHECK(A && alpha, TB_ERR_ARG, "null argument");
-        require_real(A->type, "shift");
-        if (A->type == TYPE_DOUBLE) do_unary<double>(2, alpha, A, idx_A);
-        else do_unary<float>(2, alpha, A, idx_A);
+        TB_CHECK(alpha->type == A->type, TB_ERR_TYPE, "shift: scalar and tensor types differ");
+        with_type(A->type, [&](auto t) { do_unary<decltype(t)>(2, alpha, A, idx_A); });
     });
 }
 

@@ -9,8 +9,11 @@
 // accesses where the inner dim is unit-stride and 16-byte aligned, and
 // shared-memory tiles for transposes (the inner dims of A and B differ).
 // Reductions are two-pass and deterministic (fixed grid, fixed combine
-// order, no atomics).
+// order, no atomics). The element type is float, double or their complex
+// counterparts (cplx.hpp); conj flags apply to complex operands as the
+// reference's microkernels apply them (src/kernels/1v/{add,scale,shift,dot}.hpp).
 #include "level1.hpp"
+#include "cplx.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -25,6 +28,14 @@ namespace
 constexpr int SEG = 1024;          // inner elements per segment
 constexpr int L1_THREADS = 256;
 constexpr int RED_BLOCKS = 148*4;  // fixed grid of the reductions
+
+template <typename T>
+__device__ __forceinline__ T shfl_down(T v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
+template <typename R>
+__device__ __forceinline__ cplx<R> shfl_down(cplx<R> v, int o)
+{
+    return {__shfl_down_sync(0xffffffffu, v.re, o), __shfl_down_sync(0xffffffffu, v.im, o)};
+}
 
 int l1_grid(i64 work_items, int per_block)
 {
@@ -60,8 +71,9 @@ __device__ __forceinline__ void row_offset2(const Strided2& s, i64 r, i64& oa, i
 // ---- set / scale / shift ------------------------------------------------------
 
 // op: 0 = set(value), 1 = scale(alpha), 2 = shift: shift + alpha*A
+// (A conjugated first when conj)
 template <typename T, int OP>
-__global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v0, T v1)
+__global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v0, T v1, bool conj)
 {
     const i64 n0 = s.ndim ? s.len[0] : 1;
     const i64 st0 = s.ndim ? s.stride[0] : 0;
@@ -81,9 +93,32 @@ __global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v
         {
             T* p = base + i*st0;
             if (OP == 0) *p = v0;
-            else if (OP == 1) *p = v0*(*p);
-            else *p = v0 + v1*(*p);
+            else if (OP == 1) *p = v0*cj(*p, conj);
+            else *p = v0 + v1*cj(*p, conj);
         }
+    }
+}
+
+// ---- element-type conversion at equal offsets -------------------------------------
+
+template <typename S, typename D>
+__global__ void __launch_bounds__(L1_THREADS) k_convert(const S* __restrict__ src, D* __restrict__ dst, const Strided s)
+{
+    const i64 n0 = s.ndim ? s.len[0] : 1;
+    const i64 st0 = s.ndim ? s.stride[0] : 0;
+    i64 rows = 1;
+    for (int d = 1; d < s.ndim; d++) rows *= s.len[d];
+    const i64 nchunk = (n0 + SEG - 1)/SEG;
+    const i64 nseg = rows*nchunk;
+    const int lane = threadIdx.x & 31;
+    const i64 warp0 = (blockIdx.x*(i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
+    for (i64 sg = warp0; sg < nseg; sg += nwarps)
+    {
+        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 ro = row_offset(s.len, s.stride, s.ndim, r);
+        const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        for (i64 i = i0 + lane; i < i1; i += 32) dst[ro + i*st0] = (D)src[ro + i*st0];
     }
 }
 
@@ -92,7 +127,7 @@ __global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v
 template <typename T, bool BETA0>
 __global__ void __launch_bounds__(L1_THREADS)
 k_add_general(const T* __restrict__ A, T* __restrict__ B, const Strided2 ab, const Strided ao,
-              const Strided bo, T alpha, T beta)
+              const Strided bo, T alpha, T beta, bool conj_a, bool conj_b)
 {
     const i64 n0 = ab.len[0];
     i64 rows = 1;
@@ -115,13 +150,13 @@ k_add_general(const T* __restrict__ A, T* __restrict__ B, const Strided2 ab, con
             for (int d = 0; d < ao.ndim; d++) { i64 q = x/ao.len[d]; o += (x - q*ao.len[d])*ao.stride[d]; x = q; }
             sum += A[oa + o];
         }
-        const T v = alpha*sum;
+        const T v = alpha*cj(sum, conj_a);
         for (i64 t = 0; t < nbo; t++)
         {
             i64 x = t, o = 0;
             for (int d = 0; d < bo.ndim; d++) { i64 q = x/bo.len[d]; o += (x - q*bo.len[d])*bo.stride[d]; x = q; }
             T* p = B + ob + o;
-            *p = BETA0 ? v : v + beta*(*p);
+            *p = BETA0 ? v : v + beta*cj(*p, conj_b);
         }
     }
 }
@@ -130,7 +165,8 @@ k_add_general(const T* __restrict__ A, T* __restrict__ B, const Strided2 ab, con
 // 16-byte vectors when both inner strides are 1 and the rows are aligned
 template <typename T, bool BETA0>
 __global__ void __launch_bounds__(L1_THREADS)
-k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha, T beta)
+k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha, T beta, bool conj_a,
+           bool conj_b)
 {
     const i64 n0 = s.len[0];
     i64 rows = 1;
@@ -165,33 +201,37 @@ k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha
                 T* ys = reinterpret_cast<T*>(&y);
                 if (!BETA0) y = bv[v];
                 #pragma unroll
-                for (int q = 0; q < VW; q++) ys[q] = BETA0 ? alpha*xs[q] : alpha*xs[q] + beta*ys[q];
+                for (int q = 0; q < VW; q++)
+                    ys[q] = BETA0 ? alpha*cj(xs[q], conj_a) : alpha*cj(xs[q], conj_a) + beta*cj(ys[q], conj_b);
                 bv[v] = y;
             }
             for (i64 i = i0 + nv*VW + lane; i < i1; i += 32)
-                b[i] = BETA0 ? alpha*a[i] : alpha*a[i] + beta*b[i];
+                b[i] = BETA0 ? alpha*cj(a[i], conj_a) : alpha*cj(a[i], conj_a) + beta*cj(b[i], conj_b);
         }
         else
         {
             for (i64 i = i0 + lane; i < i1; i += 32)
             {
-                const T x = a[i*s.sa[0]];
+                const T x = cj(a[i*s.sa[0]], conj_a);
                 T* p = b + i*s.sb[0];
-                *p = BETA0 ? alpha*x : alpha*x + beta*(*p);
+                *p = BETA0 ? alpha*x : alpha*x + beta*cj(*p, conj_b);
             }
         }
     }
 }
 
 // transpose: dim p is A's unit dim, dim q is B's unit dim, the rest are outer.
-// 64x64 tile through shared memory; reads coalesced along p, writes along q.
-constexpr int TT = 64;
+// Square tile through shared memory (64 wide, 32 for 16-byte elements so the
+// tile stays below 48 KB); reads coalesced along p, writes along q.
+template <typename T>
+constexpr int tile_of() { return sizeof(T) >= 16 ? 32 : 64; }
 
 template <typename T, bool BETA0>
 __global__ void __launch_bounds__(L1_THREADS)
 k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p, int q,
-            i64 tiles_p, i64 tiles_q, i64 outer, T alpha, T beta)
+            i64 tiles_p, i64 tiles_q, i64 outer, T alpha, T beta, bool conj_a, bool conj_b)
 {
+    constexpr int TT = tile_of<T>();
     __shared__ T tile[TT][TT + 1];
     const i64 np = s.len[p], nq = s.len[q];
     const i64 ntiles = tiles_p*tiles_q*outer;
@@ -218,7 +258,7 @@ k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p,
         {
             const int ql = ty + 8*j;
             #pragma unroll
-            for (int h = 0; h < 2; h++)
+            for (int h = 0; h < TT/32; h++)
             {
                 const int pl = tx + 32*h;
                 const i64 pi = p0 + pl, qi = q0 + ql;
@@ -232,15 +272,15 @@ k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p,
         {
             const int pl = ty + 8*j;
             #pragma unroll
-            for (int h = 0; h < 2; h++)
+            for (int h = 0; h < TT/32; h++)
             {
                 const int ql = tx + 32*h;
                 const i64 pi = p0 + pl, qi = q0 + ql;
                 if (pi < np && qi < nq)
                 {
                     T* dst = B + ob + pi*s.sb[p] + qi*s.sb[q];
-                    const T v = alpha*tile[ql][pl];
-                    *dst = BETA0 ? v : v + beta*(*dst);
+                    const T v = alpha*cj(tile[ql][pl], conj_a);
+                    *dst = BETA0 ? v : v + beta*cj(*dst, conj_b);
                 }
             }
         }
@@ -252,7 +292,8 @@ k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p,
 
 template <typename T>
 __global__ void __launch_bounds__(L1_THREADS)
-k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s, T* partial)
+k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s, T* partial, bool conj_a,
+              bool conj_b)
 {
     const i64 n0 = s.ndim ? s.len[0] : 1;
     i64 rows = 1;
@@ -270,9 +311,9 @@ k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s
         i64 oa, ob;
         row_offset2(s, r, oa, ob);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
-        for (i64 i = i0 + lane; i < i1; i += 32) acc += A[oa + i*sa0]*B[ob + i*sb0];
+        for (i64 i = i0 + lane; i < i1; i += 32) acc += cj(A[oa + i*sa0], conj_a)*cj(B[ob + i*sb0], conj_b);
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    for (int o = 16; o > 0; o >>= 1) acc += shfl_down(acc, o);
     __shared__ T ws[L1_THREADS/32];
     if (lane == 0) ws[wib] = acc;
     __syncthreads();
@@ -291,7 +332,7 @@ __global__ void k_sum_partials(const T* partial, int n, T* out)
     const int lane = threadIdx.x;
     T acc = T(0);
     for (int i = lane; i < n; i += 32) acc += partial[i];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    for (int o = 16; o > 0; o >>= 1) acc += shfl_down(acc, o);
     if (lane == 0) *out = acc;
 }
 
@@ -306,10 +347,12 @@ __device__ __forceinline__ bool better(int op, const Cand<T>& a, const Cand<T>& 
     // position in iteration order (the reference's sequential result)
     if (a.lin < 0) return false;
     if (b.lin < 0) return true;
-    bool gt = a.v > b.v, lt = a.v < b.v;
+    // complex values order by their real parts, as the reference's operators do
+    const auto ka = order_key(a.v), kb = order_key(b.v);
+    bool gt = ka > kb, lt = ka < kb;
     bool maxop = op == REDUCE_MAX || op == REDUCE_MAX_ABS;
     if (maxop ? gt : lt) return true;
-    if (a.v == b.v) return a.lin < b.lin;
+    if (ka == kb) return a.lin < b.lin;
     return false;
 }
 
@@ -318,8 +361,8 @@ __device__ __forceinline__ T red_val(int op, T x)
 {
     switch (op)
     {
-        case REDUCE_SUM_ABS: case REDUCE_MAX_ABS: case REDUCE_MIN_ABS: return x < T(0) ? -x : x;
-        case REDUCE_NORM_2: return x*x;
+        case REDUCE_SUM_ABS: case REDUCE_MAX_ABS: case REDUCE_MIN_ABS: return abs_elem(x);
+        case REDUCE_NORM_2: return norm2_elem(x);
         default: return x;
     }
 }
@@ -361,7 +404,7 @@ k_reduce_partial(int op, const T* __restrict__ A, const Strided s, T* pv, i64* p
     __shared__ i64 sl[L1_THREADS], so[L1_THREADS];
     if (is_sum)
     {
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        for (int o = 16; o > 0; o >>= 1) acc += shfl_down(acc, o);
         if (lane == 0) sv[wib] = acc;
         __syncthreads();
         if (threadIdx.x == 0)
@@ -398,7 +441,7 @@ __global__ void k_reduce_final(int op, const T* pv, const i64* plin, const i64* 
     {
         T t = T(0);
         for (int i = 0; i < n; i++) t += pv[i];
-        if (op == REDUCE_NORM_2) t = sqrt(t);
+        if (op == REDUCE_NORM_2) t = sqrt_elem(t);
         *out_v = t; *out_idx = -1;
         return;
     }
@@ -411,10 +454,12 @@ __global__ void k_reduce_final(int op, const T* pv, const i64* plin, const i64* 
     if (b.lin < 0)
     {
         // empty tensor: the reference's initial values
+        using R = typename real_of<T>::type;
+        const R big = sizeof(R) == 8 ? (R)DBL_MAX : (R)FLT_MAX;
         switch (op)
         {
-            case REDUCE_MAX: b.v = sizeof(T) == 8 ? (T)-DBL_MAX : (T)-FLT_MAX; break;
-            case REDUCE_MIN: case REDUCE_MIN_ABS: b.v = sizeof(T) == 8 ? (T)DBL_MAX : (T)FLT_MAX; break;
+            case REDUCE_MAX: b.v = T(-big); break;
+            case REDUCE_MIN: case REDUCE_MIN_ABS: b.v = T(big); break;
             default: b.v = T(0);
         }
     }
@@ -429,26 +474,47 @@ static i64 total_of(const Strided& s) { i64 t = 1; for (int d = 0; d < s.ndim; d
 static i64 total_of(const Strided2& s) { i64 t = 1; for (int d = 0; d < s.ndim; d++) t *= s.len[d]; return t; }
 
 template <typename T>
-static void unary_launch(int op, T* A, const Strided& s, T v0, T v1, cudaStream_t st)
+static void unary_launch(int op, T* A, const Strided& s, T v0, T v1, bool conj, cudaStream_t st)
 {
     i64 total = total_of(s);
     if (total == 0) return;
     i64 n0 = s.ndim ? s.len[0] : 1;
     i64 segs = (total/n0)*((n0 + SEG - 1)/SEG);
     int grid = l1_grid(segs, L1_THREADS/32);
-    if (op == 0) k_unary<T, 0><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
-    else if (op == 1) k_unary<T, 1><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
-    else k_unary<T, 2><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1);
+    if (op == 0) k_unary<T, 0><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1, conj);
+    else if (op == 1) k_unary<T, 1><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1, conj);
+    else k_unary<T, 2><<<grid, L1_THREADS, 0, st>>>(A, s, v0, v1, conj);
     check_launch("k_unary");
 }
 
-template <typename T> void l1_set(T* A, const Strided& s, T value, cudaStream_t st) { unary_launch<T>(0, A, s, value, T(0), st); }
-template <typename T> void l1_scale(T* A, const Strided& s, T alpha, cudaStream_t st) { unary_launch<T>(1, A, s, alpha, T(0), st); }
-template <typename T> void l1_shift(T* A, const Strided& s, T shift, T alpha, cudaStream_t st) { unary_launch<T>(2, A, s, shift, alpha, st); }
+template <typename T> void l1_set(T* A, const Strided& s, T value, cudaStream_t st) { unary_launch<T>(0, A, s, value, T(0), false, st); }
+template <typename T> void l1_scale(T* A, const Strided& s, T alpha, cudaStream_t st, bool conj)
+{
+    unary_launch<T>(1, A, s, alpha, T(0), conj, st);
+}
+template <typename T> void l1_shift(T* A, const Strided& s, T shift, T alpha, cudaStream_t st, bool conj)
+{
+    unary_launch<T>(2, A, s, shift, alpha, conj, st);
+}
+
+template <typename S, typename D>
+void l1_convert(const S* src, D* dst, const Strided& s, cudaStream_t st)
+{
+    i64 total = total_of(s);
+    if (total == 0) return;
+    i64 n0 = s.ndim ? s.len[0] : 1;
+    i64 segs = (total/n0)*((n0 + SEG - 1)/SEG);
+    int grid = l1_grid(segs, L1_THREADS/32);
+    k_convert<S, D><<<grid, L1_THREADS, 0, st>>>(src, dst, s);
+    check_launch("k_convert");
+}
+
+template void l1_convert<float, double>(const float*, double*, const Strided&, cudaStream_t);
+template void l1_convert<double, float>(const double*, float*, const Strided&, cudaStream_t);
 
 template <typename T>
 void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strided& bo,
-            T alpha, T beta, cudaStream_t st)
+            T alpha, T beta, cudaStream_t st, bool conj_a, bool conj_b)
 {
     i64 nab = total_of(ab);
     if (nab == 0 || total_of(bo) == 0) return;
@@ -472,18 +538,21 @@ void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strid
             i64 segs = (nab/n0)*((n0 + SEG - 1)/SEG);
             int grid = l1_grid(segs, L1_THREADS/32);
             TimedLaunch t("k_add_rows", st);
-            if (b0) k_add_rows<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
-            else k_add_rows<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta);
+            if (b0) k_add_rows<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta, conj_a, conj_b);
+            else k_add_rows<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, alpha, beta, conj_a, conj_b);
             check_launch("k_add_rows");
             return;
         }
+        constexpr int TT = tile_of<T>();
         i64 tp = (ab.len[pa] + TT - 1)/TT, tq = (ab.len[pb] + TT - 1)/TT;
         i64 outer = nab/(ab.len[pa]*ab.len[pb]);
         i64 ntiles = tp*tq*outer;
         int grid = (int)std::min<i64>(ntiles, 148*16);
         TimedLaunch t("k_transpose", st);
-        if (b0) k_transpose<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
-        else k_transpose<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta);
+        if (b0) k_transpose<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
+                                                                  conj_a, conj_b);
+        else k_transpose<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
+                                                                 conj_a, conj_b);
         check_launch("k_transpose");
         return;
     }
@@ -491,16 +560,16 @@ void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strid
     Strided2 s = ab;
     if (s.ndim == 0) { s.ndim = 1; s.len[0] = 1; s.sa[0] = 0; s.sb[0] = 0; }
     int grid = l1_grid(nab, L1_THREADS);
-    if (b0) k_add_general<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta);
-    else k_add_general<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta);
+    if (b0) k_add_general<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta, conj_a, conj_b);
+    else k_add_general<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, s, ao, bo, alpha, beta, conj_a, conj_b);
     check_launch("k_add_general");
 }
 
 template <typename T>
-void l1_dot(const T* A, const T* B, const Strided2& ab, T* d_result, cudaStream_t st)
+void l1_dot(const T* A, const T* B, const Strided2& ab, T* d_result, cudaStream_t st, bool conj_a, bool conj_b)
 {
     dbuf part(RED_BLOCKS*sizeof(T), st);
-    k_dot_partial<T><<<RED_BLOCKS, L1_THREADS, 0, st>>>(A, B, ab, part.as<T>());
+    k_dot_partial<T><<<RED_BLOCKS, L1_THREADS, 0, st>>>(A, B, ab, part.as<T>(), conj_a, conj_b);
     check_launch("k_dot_partial");
     k_sum_partials<T><<<1, 32, 0, st>>>(part.as<T>(), RED_BLOCKS, d_result);
     check_launch("k_sum_partials");
@@ -512,7 +581,7 @@ void l1_reduce(int op, const T* A, const Strided& s, T* d_value, i64* d_idx, cud
     TB_CHECK(op >= 0 && op <= 6, TB_ERR_ARG, "unknown reduce op");
     dbuf part(RED_BLOCKS*(sizeof(T) + 2*sizeof(i64)), st);
     T* pv = part.as<T>();
-    i64* pl = reinterpret_cast<i64*>(part.as<char>() + RED_BLOCKS*sizeof(T));
+    i64* pl = reinterpret_cast<i64*>(part.as<char>() + RED_BLOCKS*sizeof(T));   // 8-byte aligned
     i64* po = pl + RED_BLOCKS;
     k_reduce_partial<T><<<RED_BLOCKS, L1_THREADS, 0, st>>>(op, A, s, pv, pl, po);
     check_launch("k_reduce_partial");
@@ -522,13 +591,16 @@ void l1_reduce(int op, const T* A, const Strided& s, T* d_value, i64* d_idx, cud
 
 #define TB_L1_INST(T) \
     template void l1_set<T>(T*, const Strided&, T, cudaStream_t); \
-    template void l1_scale<T>(T*, const Strided&, T, cudaStream_t); \
-    template void l1_shift<T>(T*, const Strided&, T, T, cudaStream_t); \
-    template void l1_add<T>(const T*, T*, const Strided2&, const Strided&, const Strided&, T, T, cudaStream_t); \
-    template void l1_dot<T>(const T*, const T*, const Strided2&, T*, cudaStream_t); \
+    template void l1_scale<T>(T*, const Strided&, T, cudaStream_t, bool); \
+    template void l1_shift<T>(T*, const Strided&, T, T, cudaStream_t, bool); \
+    template void l1_add<T>(const T*, T*, const Strided2&, const Strided&, const Strided&, T, T, cudaStream_t, \
+                            bool, bool); \
+    template void l1_dot<T>(const T*, const T*, const Strided2&, T*, cudaStream_t, bool, bool); \
     template void l1_reduce<T>(int, const T*, const Strided&, T*, i64*, cudaStream_t);
 
 TB_L1_INST(float)
 TB_L1_INST(double)
+TB_L1_INST(cplx<float>)
+TB_L1_INST(cplx<double>)
 
 } // namespace tb

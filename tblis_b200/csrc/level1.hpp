@@ -3,6 +3,7 @@
 #pragma once
 
 #include "common.hpp"
+#include "cplx.hpp"
 
 namespace tb
 {
@@ -26,18 +27,27 @@ struct Strided2
     i64 sb[L1_MAX_DIM];
 };
 
+// T: float, double, cplx<float>, cplx<double>; conj flags act on complex
+// elements only (A <- alpha*conj(A) for scale, shift + alpha*conj(A) for shift)
 template <typename T> void l1_set(T* A, const Strided& s, T value, cudaStream_t st);
-template <typename T> void l1_scale(T* A, const Strided& s, T alpha, cudaStream_t st);
-template <typename T> void l1_shift(T* A, const Strided& s, T shift, T alpha, cudaStream_t st);
+template <typename T> void l1_scale(T* A, const Strided& s, T alpha, cudaStream_t st, bool conj = false);
+template <typename T> void l1_shift(T* A, const Strided& s, T shift, T alpha, cudaStream_t st, bool conj = false);
 
-// B[ab, bo] = alpha * sum_ao A[ab, ao] + beta * B[ab, bo]  (beta == 0: no read)
+// B[ab, bo] = alpha * op(sum_ao A[ab, ao]) + beta * op(B[ab, bo])  (beta == 0:
+// no read; op conjugates when the operand's flag is set)
 template <typename T>
 void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strided& bo,
-            T alpha, T beta, cudaStream_t st);
+            T alpha, T beta, cudaStream_t st, bool conj_a = false, bool conj_b = false);
 
-// sum_ab A*B into a device scalar (deterministic two-pass)
+// sum_ab op(A)*op(B) into a device scalar (deterministic two-pass)
 template <typename T>
-void l1_dot(const T* A, const T* B, const Strided2& ab, T* d_result, cudaStream_t st);
+void l1_dot(const T* A, const T* B, const Strided2& ab, T* d_result, cudaStream_t st, bool conj_a = false,
+            bool conj_b = false);
+
+// dst[o] = (D)src[o] for every offset o of the strided space (widening and
+// rounding copies between float and double storage of the same layout)
+template <typename S, typename D>
+void l1_convert(const S* src, D* dst, const Strided& s, cudaStream_t st);
 
 // reduction of A with op (reduce_t); writes value and offset to device memory
 template <typename T>

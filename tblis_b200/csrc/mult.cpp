@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 
 namespace tb
 {
@@ -36,11 +37,14 @@ struct StagedOp
     dbuf buf;
     void* host = nullptr;
     i64 lo = 0, n = 0;
+    size_t esz = sizeof(double);
     bool staged = false;
 };
 
-static void stage(StagedOp& o, const tblis_tensor* t, bool copy_in, cudaStream_t s)
+// t's strides count elements of esz bytes
+static void stage(StagedOp& o, const tblis_tensor* t, bool copy_in, cudaStream_t s, size_t esz = sizeof(double))
 {
+    o.esz = esz;
     if (!t->data) return;
     if (pointer_kind(t->data) == MEM_DEVICE) { o.dptr = t->data; return; }
     i64 lo, hi;
@@ -50,11 +54,15 @@ static void stage(StagedOp& o, const tblis_tensor* t, bool copy_in, cudaStream_t
     o.host = t->data;
     o.lo = lo;
     o.n = hi - lo + 1;
-    o.buf = dbuf((size_t)o.n*sizeof(double), s);
-    if (copy_in)
-        TB_CUDA(cudaMemcpyAsync(o.buf.ptr, static_cast<double*>(o.host) + lo, (size_t)o.n*sizeof(double),
+    o.buf = dbuf((size_t)o.n*esz, s);
+    // an extent with gaps is copied in even for an output: the copy back
+    // writes the whole extent, and the gaps must come back unchanged
+    i64 nelem = 1;
+    for (unsigned d = 0; d < t->ndim; d++) nelem *= t->len[d];
+    if (copy_in || nelem != o.n)
+        TB_CUDA(cudaMemcpyAsync(o.buf.ptr, static_cast<char*>(o.host) + lo*(i64)esz, (size_t)o.n*esz,
                                 cudaMemcpyHostToDevice, s));
-    o.dptr = o.buf.as<double>() - lo;
+    o.dptr = o.buf.as<char>() - lo*(i64)esz;
 }
 
 // A host-resident A is copied in slices on a copy stream while the slices
@@ -125,7 +133,7 @@ static cudaStream_t copy_stream()
 static void unstage(StagedOp& o, cudaStream_t s)
 {
     if (!o.staged) return;
-    TB_CUDA(cudaMemcpyAsync(static_cast<double*>(o.host) + o.lo, o.buf.ptr, (size_t)o.n*sizeof(double),
+    TB_CUDA(cudaMemcpyAsync(static_cast<char*>(o.host) + o.lo*(i64)o.esz, o.buf.ptr, (size_t)o.n*o.esz,
                             cudaMemcpyDeviceToHost, s));
 }
 
@@ -311,6 +319,98 @@ static void mult_complex(const tblis_config* cfg,
     }
 }
 
+// The float view of a float or scomplex tensor (a scomplex tensor is a float
+// tensor with strides x2 and an inner dim of 2), its dims merged where
+// contiguous, as the strided space of the conversions.
+struct RealView
+{
+    Strided s;
+    i64 lo = 0, hi = -1;                   // extent in float units
+    explicit RealView(const tblis_tensor* X)
+    {
+        const bool cx = X->type == TYPE_SCOMPLEX;
+        std::vector<std::pair<i64, i64>> d;  // (stride, len)
+        for (unsigned i = 0; i < X->ndim; i++)
+            if (X->len[i] != 1) d.push_back({(cx ? 2 : 1)*X->stride[i], X->len[i]});
+        if (cx) d.push_back({1, 2});
+        for (auto& x : d) if (x.second == 0) { s.ndim = 1; s.len[0] = 0; s.stride[0] = 1; return; }
+        std::sort(d.begin(), d.end(), [](const std::pair<i64, i64>& a, const std::pair<i64, i64>& b)
+                  { return std::llabs(a.first) < std::llabs(b.first); });
+        std::vector<std::pair<i64, i64>> m;
+        for (auto& x : d)
+        {
+            if (!m.empty() && x.first == m.back().first*m.back().second && x.first > 0) m.back().second *= x.second;
+            else m.push_back(x);
+        }
+        TB_CHECK(m.size() <= (size_t)L1_MAX_DIM, TB_ERR_SIZE, "too many dimensions");
+        s.ndim = (int)std::max<size_t>(m.size(), 1);
+        s.len[0] = 1; s.stride[0] = 0;
+        for (size_t i = 0; i < m.size(); i++) { s.stride[i] = m[i].first; s.len[i] = m[i].second; }
+        lo = 0; hi = 0;
+        for (auto& x : m)
+        {
+            if (x.first >= 0) hi += (x.second - 1)*x.first;
+            else lo += (x.second - 1)*x.first;
+        }
+    }
+    i64 count() const { return hi - lo + 1; }
+};
+
+// float and scomplex contractions: the operands are widened to double /
+// dcomplex on the device (same layout, equal offsets), the contraction runs on
+// the FP64 or configured kernels, and C is rounded back to float. The result
+// is at least as accurate as the reference's float arithmetic
+// (src/kernels/3m/gemm.hpp:30-67 in float / scomplex).
+static void mult_widened(const tblis_config* cfg,
+                         const tblis_tensor* A, const label_type* idx_A,
+                         const tblis_tensor* B, const label_type* idx_B,
+                         tblis_tensor* C, const label_type* idx_C,
+                         const tblis_b200_opts* opts, tblis_b200_report* report)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    const bool cx = A->type == TYPE_SCOMPLEX;
+    const bool read_c = cx ? (C->scalar.data.c[0] != 0.0f || C->scalar.data.c[1] != 0.0f)
+                           : C->scalar.data.s != 0.0f;
+    StagedOp sa, sb, sc;
+    stage(sc, C, read_c, st, cx ? 8 : 4);
+    stage(sa, A, true, st, cx ? 8 : 4);
+    stage(sb, B, true, st, cx ? 8 : 4);
+
+    const tblis_tensor* src[3] = {A, B, C};
+    StagedOp* sto[3] = {&sa, &sb, &sc};
+    tblis_tensor wide[3];
+    dbuf wbuf[3];
+    RealView* rv[3] = {nullptr, nullptr, nullptr};
+    std::vector<std::unique_ptr<RealView>> views;
+    for (int t = 0; t < 3; t++)
+    {
+        const tblis_tensor* X = src[t];
+        views.emplace_back(new RealView(X));
+        rv[t] = views.back().get();
+        wide[t] = *X;
+        wide[t].type = cx ? TYPE_DCOMPLEX : TYPE_DOUBLE;
+        wide[t].scalar.type = wide[t].type;
+        if (cx) { wide[t].scalar.data.z[0] = X->scalar.data.c[0]; wide[t].scalar.data.z[1] = X->scalar.data.c[1]; }
+        else wide[t].scalar.data.d = X->scalar.data.s;
+        if (!X->data || rv[t]->s.len[0] == 0) continue;
+        wbuf[t] = dbuf((size_t)rv[t]->count()*sizeof(double), st);
+        double* base = wbuf[t].as<double>() - rv[t]->lo;          // element 0 of the widened tensor
+        wide[t].data = base;
+        if (t < 2 || read_c)
+            l1_convert<float, double>(static_cast<const float*>(sto[t]->dptr), base, rv[t]->s, st);
+    }
+    mult_dispatch(cfg, &wide[0], idx_A, &wide[1], idx_B, &wide[2], idx_C, opts, report);
+    if (C->data && rv[2]->s.len[0] != 0)
+        l1_convert<double, float>(static_cast<const double*>(wide[2].data), static_cast<float*>(sc.dptr), rv[2]->s,
+                                  st);
+    unstage(sc, st);
+    if (sa.staged || sb.staged || sc.staged) TB_CUDA(cudaStreamSynchronize(st));
+    if (cx) { C->scalar.data.c[0] = 1.0f; C->scalar.data.c[1] = 0.0f; }
+    else C->scalar.data.s = 1.0f;
+    C->conj = 0;
+}
+
 void mult_dispatch(const tblis_config* cfg,
                    const tblis_tensor* A, const label_type* idx_A,
                    const tblis_tensor* B, const label_type* idx_B,
@@ -324,8 +424,12 @@ void mult_dispatch(const tblis_config* cfg,
         mult_complex(cfg, A, idx_A, B, idx_B, C, idx_C, opts, report);
         return;
     }
-    TB_CHECK(A->type == TYPE_DOUBLE, TB_ERR_TYPE,
-             "mult: double and dcomplex are supported on the GPU path");
+    if (A->type == TYPE_FLOAT || A->type == TYPE_SCOMPLEX)
+    {
+        mult_widened(cfg, A, idx_A, B, idx_B, C, idx_C, opts, report);
+        return;
+    }
+    TB_CHECK(A->type == TYPE_DOUBLE, TB_ERR_TYPE, "mult: unknown element type");
     ensure_device();
     cudaStream_t st = current_stream();
     const int kernels_before = (int)g_kernel_count.load();
