@@ -335,8 +335,8 @@ typedef struct tblis_b200_indexed_dpd_tensor
     const unsigned* idx_irrep;
     len_type nidx;
     const len_type* indices;
-    double* const* data;
-    const double* factor;
+    void* const* data;          /* per entry: its dense storage (elements of `type`) */
+    const void* factor;         /* per entry: its factor (an element of `type`), or NULL for 1 */
     const stride_type* offset;
     const stride_type* stride;
 } tblis_b200_indexed_dpd_tensor;

@@ -430,6 +430,57 @@ def _dpd_flat(nirrep, lens):
     return (_sz * (len(lens) * nirrep))(*[x for row in lens for x in row])
 
 
+def _value_buf(value, dtype):
+    """A 16-byte buffer holding value as one element of dtype."""
+    b = np.zeros(2, dtype=np.float64)
+    b.view(np.dtype(dtype))[0] = value
+    return b
+
+
+def ref_dpd_mult_typed(nirrep, alpha, irrep_A, lens_A, A, idx_A, irrep_B, lens_B, B, idx_B,
+                       beta, irrep_C, lens_C, C, idx_C):
+    """The reference's tblis::mult over dpd_varray_view for the element type of
+    the numpy storage (float32, float64, complex64, complex128); C in place."""
+    t = _TYPE_OF[C.dtype]
+    a, b = _value_buf(alpha, C.dtype), _value_buf(beta, C.dtype)
+    rc = shim().refshim_dpd_mult_t(
+        t, nirrep, ctypes.c_void_p(a.ctypes.data), irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A),
+        ctypes.c_void_p(A.ctypes.data), _lab(idx_A), irrep_B, len(lens_B), _dpd_flat(nirrep, lens_B),
+        ctypes.c_void_p(B.ctypes.data), _lab(idx_B), ctypes.c_void_p(b.ctypes.data), irrep_C, len(lens_C),
+        _dpd_flat(nirrep, lens_C), ctypes.c_void_p(C.ctypes.data), _lab(idx_C))
+    if rc:
+        raise ValueError("reference dpd mult failed")
+
+
+def ref_dpd_level1_typed(op, nirrep, irrep_A, lens_A, A, idx_A, irrep_B=0, lens_B=None, B=None, idx_B="",
+                         alpha=1.0, beta=0.0):
+    """The reference's DPD level-1 operation for A's element type. op: "add"
+    (B = alpha*A + beta*B), "dot", "scale" (A *= alpha), "set" (A = alpha),
+    "shift" (A = alpha + beta*A), or ("reduce", r). Returns the dot value, a
+    (value, idx) pair for a reduction, else None; A / B updated in place."""
+    codes = {"add": 0, "dot": 1, "scale": 2, "set": 3, "shift": 4}
+    code = 10 + op[1] if isinstance(op, tuple) else codes[op]
+    a, b = _value_buf(alpha, A.dtype), _value_buf(beta, A.dtype)
+    res = np.zeros(2, dtype=np.float64)
+    i = ctypes.c_long(-1)
+    lb = _dpd_flat(nirrep, lens_B) if lens_B is not None else None
+    rc = shim().refshim_dpd_level1_t(
+        _TYPE_OF[A.dtype], code, nirrep, ctypes.c_void_p(a.ctypes.data), ctypes.c_void_p(b.ctypes.data),
+        irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A), ctypes.c_void_p(A.ctypes.data), _lab(idx_A),
+        irrep_B, len(lens_B) if lens_B is not None else 0, lb,
+        ctypes.c_void_p(B.ctypes.data) if B is not None else None, _lab(idx_B),
+        ctypes.c_void_p(res.ctypes.data), ctypes.byref(i))
+    if rc:
+        raise ValueError("reference dpd level-1 failed")
+    v = res.view(A.dtype)[0]
+    v = complex(v) if np.dtype(A.dtype).kind == "c" else float(v)
+    if code == 1:
+        return v
+    if code >= 10:
+        return v, i.value
+    return None
+
+
 def ref_dpd_add(nirrep, alpha, irrep_A, lens_A, A, idx_A, beta, irrep_B, lens_B, B, idx_B):
     """The reference's tblis::add over dpd_varray_view (default layout storage)."""
     rc = shim().refshim_dpd_add(nirrep, ctypes.c_double(alpha), irrep_A, len(lens_A), _dpd_flat(nirrep, lens_A),

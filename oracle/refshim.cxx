@@ -32,6 +32,63 @@ struct bsm_access : block_scatter_matrix<double>
 {
     using block_scatter_matrix<double>::fill_block_scatter;
 };
+
+std::vector<std::vector<len_type>> lens_of(unsigned ndim, unsigned nirrep, const len_type* lens)
+{
+    std::vector<std::vector<len_type>> len(ndim, std::vector<len_type>(nirrep));
+    for (unsigned i = 0; i < ndim; i++)
+        for (unsigned j = 0; j < nirrep; j++) len[i][j] = lens[i*nirrep+j];
+    return len;
+}
+
+/*
+ * The reference's C++ DPD operations for any of its element types (float,
+ * double, scomplex, dcomplex: type_t codes 0-3); scalars and results are
+ * passed by pointer to a value of the element type.
+ */
+template <typename T>
+int dpd_mult_t(unsigned nirrep, const void* alpha, unsigned irrep_A, unsigned ndim_A, const len_type* lens_A,
+               const void* data_A, const char* idx_A, unsigned irrep_B, unsigned ndim_B, const len_type* lens_B,
+               const void* data_B, const char* idx_B, const void* beta, unsigned irrep_C, unsigned ndim_C,
+               const len_type* lens_C, void* data_C, const char* idx_C)
+{
+    MArray::dpd_varray_view<const T> A(irrep_A, nirrep, lens_of(ndim_A, nirrep, lens_A), (const T*)data_A);
+    MArray::dpd_varray_view<const T> B(irrep_B, nirrep, lens_of(ndim_B, nirrep, lens_B), (const T*)data_B);
+    MArray::dpd_varray_view<T> C(irrep_C, nirrep, lens_of(ndim_C, nirrep, lens_C), (T*)data_C);
+    tblis::mult<T>(*(const T*)alpha, A, idx_A, B, idx_B, *(const T*)beta, C, idx_C);
+    return 0;
+}
+
+template <typename T>
+int dpd_level1_t(int op, unsigned nirrep, const void* alpha, const void* beta,
+                 unsigned irrep_A, unsigned ndim_A, const len_type* lens_A, const void* data_A, const char* idx_A,
+                 unsigned irrep_B, unsigned ndim_B, const len_type* lens_B, void* data_B, const char* idx_B,
+                 void* result, long* idx)
+{
+    /* op: 0 add (B = alpha*A + beta*B), 1 dot (result), 2 scale (A *= alpha),
+     * 3 set (A = alpha), 4 shift (A = alpha + beta*A), 10 + r: reduce r */
+    MArray::dpd_varray_view<T> A(irrep_A, nirrep, lens_of(ndim_A, nirrep, lens_A), (T*)data_A);
+    if (op == 0)
+    {
+        MArray::dpd_varray_view<T> B(irrep_B, nirrep, lens_of(ndim_B, nirrep, lens_B), (T*)data_B);
+        tblis::add<T>(*(const T*)alpha, A, idx_A, *(const T*)beta, B, idx_B);
+    }
+    else if (op == 1)
+    {
+        MArray::dpd_varray_view<const T> B(irrep_B, nirrep, lens_of(ndim_B, nirrep, lens_B), (const T*)data_B);
+        *(T*)result = tblis::dot<T>(A, idx_A, B, idx_B);
+    }
+    else if (op == 2) tblis::scale<T>(*(const T*)alpha, A, idx_A);
+    else if (op == 3) tblis::set<T>(*(const T*)alpha, A, idx_A);
+    else if (op == 4) tblis::shift<T>(*(const T*)alpha, *(const T*)beta, A, idx_A);
+    else
+    {
+        auto r = tblis::reduce<T>((tblis::reduce_t)(op - 10), MArray::dpd_varray_view<const T>(A), idx_A);
+        *(T*)result = r.first;
+        *idx = r.second;
+    }
+    return 0;
+}
 }
 
 extern "C"
@@ -320,6 +377,44 @@ int refshim_indexed_dpd_mult(unsigned nirrep, double alpha,
     const len_type n = C.dense_size();
     for (long e = 0; e < nidx_C; e++) std::copy_n(C.data(e), n, data_C + e*n);
     return 0;
+}
+
+
+int refshim_dpd_mult_t(int type, unsigned nirrep, const void* alpha, unsigned irrep_A, unsigned ndim_A,
+                       const len_type* lens_A, const void* data_A, const char* idx_A, unsigned irrep_B,
+                       unsigned ndim_B, const len_type* lens_B, const void* data_B, const char* idx_B,
+                       const void* beta, unsigned irrep_C, unsigned ndim_C, const len_type* lens_C, void* data_C,
+                       const char* idx_C)
+{
+#define REFSHIM_ARGS nirrep, alpha, irrep_A, ndim_A, lens_A, data_A, idx_A, irrep_B, ndim_B, lens_B, data_B, \
+                     idx_B, beta, irrep_C, ndim_C, lens_C, data_C, idx_C
+    switch (type)
+    {
+        case 0: return dpd_mult_t<float>(REFSHIM_ARGS);
+        case 1: return dpd_mult_t<double>(REFSHIM_ARGS);
+        case 2: return dpd_mult_t<scomplex>(REFSHIM_ARGS);
+        case 3: return dpd_mult_t<dcomplex>(REFSHIM_ARGS);
+    }
+#undef REFSHIM_ARGS
+    return 1;
+}
+
+int refshim_dpd_level1_t(int type, int op, unsigned nirrep, const void* alpha, const void* beta,
+                         unsigned irrep_A, unsigned ndim_A, const len_type* lens_A, const void* data_A,
+                         const char* idx_A, unsigned irrep_B, unsigned ndim_B, const len_type* lens_B,
+                         void* data_B, const char* idx_B, void* result, long* idx)
+{
+#define REFSHIM_ARGS op, nirrep, alpha, beta, irrep_A, ndim_A, lens_A, data_A, idx_A, irrep_B, ndim_B, lens_B, \
+                     data_B, idx_B, result, idx
+    switch (type)
+    {
+        case 0: return dpd_level1_t<float>(REFSHIM_ARGS);
+        case 1: return dpd_level1_t<double>(REFSHIM_ARGS);
+        case 2: return dpd_level1_t<scomplex>(REFSHIM_ARGS);
+        case 3: return dpd_level1_t<dcomplex>(REFSHIM_ARGS);
+    }
+#undef REFSHIM_ARGS
+    return 1;
 }
 
 }

@@ -325,14 +325,15 @@ class DpdTensor:
         self.irrep, self.nirrep, self.layout = int(irrep), int(nirrep), int(layout)
         self.lens = [list(map(int, r)) for r in lens]
         self.data = data
+        # element type from the buffer (float32 / float64 / complex64 / complex128)
+        self.code = _dtype_code(data)[0] if data is not None else TYPE_DOUBLE
         self._len = (ctypes.c_ssize_t * (len(self.lens) * self.nirrep))(*[x for r in self.lens for x in r])
 
     def struct(self, scalar=1.0):
         t = tblis_b200_dpd_tensor()
-        t.type = TYPE_DOUBLE
+        t.type = self.code
         t.conj = 0
-        t.scalar.type = TYPE_DOUBLE
-        t.scalar.data[0] = float(scalar)
+        t.scalar = _make_scalar(scalar, self.code)
         if self.data is None:
             t.data = None
         elif hasattr(self.data, "data_ptr"):
@@ -414,10 +415,9 @@ def _dpd_table(T, scalar=1.0):
     keep = [(ctypes.c_ssize_t * (nd * n))(*[x for r in T.lens for x in r]), (ctypes.c_ssize_t * nt)(*off),
             (ctypes.c_ssize_t * max(1, len(st)))(*st)]
     b = tblis_b200_dpd_block_table()
-    b.type = TYPE_DOUBLE
+    b.type = T.code
     b.conj = 0
-    b.scalar.type = TYPE_DOUBLE
-    b.scalar.data[0] = float(scalar)
+    b.scalar = _make_scalar(scalar, T.code)
     b.data = T.data.data_ptr() if hasattr(T.data, "data_ptr") else T.data.ctypes.data
     b.ndim, b.nirrep, b.irrep = nd, n, T.irrep
     b.len = ctypes.cast(keep[0], _P(ctypes.c_ssize_t))
@@ -440,7 +440,7 @@ def dpd_dot(A, idx_A, B, idx_B):
     r = tblis_scalar()
     lib.tblis_b200_dpd_dot(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B), ctypes.byref(r))
     _check()
-    return r.data[0]
+    return _scalar_value(r, A.code)
 
 
 def dpd_reduce(op, A, idx_A):
@@ -450,7 +450,7 @@ def dpd_reduce(op, A, idx_A):
     i = ctypes.c_ssize_t(-1)
     lib.tblis_b200_dpd_reduce(int(op), ctypes.byref(a), _labels(idx_A), ctypes.byref(r), ctypes.byref(i))
     _check()
-    return r.data[0], i.value
+    return _scalar_value(r, A.code), i.value
 
 
 def dpd_scale(alpha, A, idx_A):
@@ -461,9 +461,7 @@ def dpd_scale(alpha, A, idx_A):
 
 def dpd_set(alpha, A, idx_A):
     a, ka = _dpd_table(A)
-    s = tblis_scalar()
-    s.type = TYPE_DOUBLE
-    s.data[0] = float(alpha)
+    s = _make_scalar(alpha, A.code)
     lib.tblis_b200_dpd_set(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
     _check()
 
@@ -471,9 +469,7 @@ def dpd_set(alpha, A, idx_A):
 def dpd_shift(alpha, beta, A, idx_A):
     """A = alpha + beta*A over the stored elements."""
     a, ka = _dpd_table(A, beta)
-    s = tblis_scalar()
-    s.type = TYPE_DOUBLE
-    s.data[0] = float(alpha)
+    s = _make_scalar(alpha, A.code)
     lib.tblis_b200_dpd_shift(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
     _check()
 
@@ -482,7 +478,7 @@ class tblis_b200_indexed_dpd_tensor(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("scalar", tblis_scalar), ("ndim", ctypes.c_uint),
                 ("dense_ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint), ("dense_irrep", ctypes.c_uint),
                 ("len", _P(ctypes.c_ssize_t)), ("idx_irrep", _P(ctypes.c_uint)), ("nidx", ctypes.c_ssize_t),
-                ("indices", _P(ctypes.c_ssize_t)), ("data", _P(ctypes.c_void_p)), ("factor", _P(ctypes.c_double)),
+                ("indices", _P(ctypes.c_ssize_t)), ("data", _P(ctypes.c_void_p)), ("factor", ctypes.c_void_p),
                 ("offset", _P(ctypes.c_ssize_t)), ("stride", _P(ctypes.c_ssize_t))]
 
 
@@ -515,9 +511,11 @@ class IndexedDpdTensor:
             self.dense_irrep ^= r
         self.indices = [list(map(int, t)) for t in indices] if self.idx_irreps else [[]]
         self.nidx = max(1, len(self.indices))
-        self.factors = [1.0] * self.nidx if factors is None else [float(f) for f in factors]
+        self.factors = [1.0] * self.nidx if factors is None else [complex(f) for f in factors]
         self.layout = int(layout)
         self.data = data
+        # element type from the buffer (float32 / float64 / complex64 / complex128)
+        self.code, self.esize = _dtype_code(data) if data is not None else (TYPE_DOUBLE, 8)
         dense = DpdTensor(self.dense_irrep, self.nirrep, self.lens[:self.dense_ndim], layout=self.layout)
         self._dense_size = dense.size()
         # block table of one entry: every irrep tuple of the dense dims, dim 0 fastest
@@ -550,19 +548,26 @@ class IndexedDpdTensor:
 
     def struct(self, scalar=1.0):
         t = tblis_b200_indexed_dpd_tensor()
-        t.type = TYPE_DOUBLE
-        t.scalar.type = TYPE_DOUBLE
-        t.scalar.data[0] = float(scalar)
+        t.type = self.code
+        t.scalar = _make_scalar(scalar, self.code)
         t.ndim, t.dense_ndim, t.nirrep, t.dense_irrep = self.ndim, self.dense_ndim, self.nirrep, self.dense_irrep
         t.len = ctypes.cast(self._len, _P(ctypes.c_ssize_t))
         t.idx_irrep = ctypes.cast(self._irr, _P(ctypes.c_uint))
         t.nidx = self.nidx
         t.indices = ctypes.cast(self._idx, _P(ctypes.c_ssize_t))
         base = self.data.data_ptr() if hasattr(self.data, "data_ptr") else self.data.ctypes.data
-        self._ptrs = (ctypes.c_void_p * self.nidx)(*[base + 8 * e * self._dense_size for e in range(self.nidx)])
+        self._ptrs = (ctypes.c_void_p * self.nidx)(*[base + self.esize * e * self._dense_size
+                                                     for e in range(self.nidx)])
         t.data = ctypes.cast(self._ptrs, _P(ctypes.c_void_p))
-        self._fac = (ctypes.c_double * self.nidx)(*self.factors)
-        t.factor = ctypes.cast(self._fac, _P(ctypes.c_double))
+        # the factors as elements of the tensor's type
+        if self.code == TYPE_DOUBLE:
+            self._fac = (ctypes.c_double * self.nidx)(*[f.real for f in self.factors])
+        elif self.code == TYPE_FLOAT:
+            self._fac = (ctypes.c_float * self.nidx)(*[f.real for f in self.factors])
+        else:
+            part = ctypes.c_double if self.code == TYPE_DCOMPLEX else ctypes.c_float
+            self._fac = (part * (2 * self.nidx))(*[x for f in self.factors for x in (f.real, f.imag)])
+        t.factor = ctypes.cast(self._fac, ctypes.c_void_p)
         t.offset = ctypes.cast(self._off, _P(ctypes.c_ssize_t))
         t.stride = ctypes.cast(self._str, _P(ctypes.c_ssize_t))
         return t
@@ -578,11 +583,6 @@ lib.tblis_b200_indexed_dpd_set.argtypes = [_P(tblis_scalar), _IT, ctypes.c_char_
 lib.tblis_b200_indexed_dpd_shift.argtypes = [_P(tblis_scalar), _IT, ctypes.c_char_p]
 
 
-def _dscalar(v):
-    s = tblis_scalar()
-    s.type = TYPE_DOUBLE
-    s.data[0] = float(v)
-    return s
 
 
 def indexed_dpd_add(alpha, A, idx_A, beta, B, idx_B):
@@ -598,7 +598,7 @@ def indexed_dpd_dot(A, idx_A, B, idx_B):
     lib.tblis_b200_indexed_dpd_dot(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B),
                                    ctypes.byref(r))
     _check()
-    return r.data[0]
+    return _scalar_value(r, A.code)
 
 
 def indexed_dpd_reduce(op, A, idx_A):
@@ -607,7 +607,7 @@ def indexed_dpd_reduce(op, A, idx_A):
     i = ctypes.c_ssize_t(-1)
     lib.tblis_b200_indexed_dpd_reduce(int(op), ctypes.byref(a), _labels(idx_A), ctypes.byref(r), ctypes.byref(i))
     _check()
-    return r.data[0], i.value
+    return _scalar_value(r, A.code), i.value
 
 
 def indexed_dpd_scale(alpha, A, idx_A):
@@ -618,14 +618,14 @@ def indexed_dpd_scale(alpha, A, idx_A):
 
 def indexed_dpd_set(alpha, A, idx_A):
     a = A.struct()
-    s = _dscalar(alpha)
+    s = _make_scalar(alpha, A.code)
     lib.tblis_b200_indexed_dpd_set(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
     _check()
 
 
 def indexed_dpd_shift(alpha, beta, A, idx_A):
     a = A.struct(beta)
-    s = _dscalar(alpha)
+    s = _make_scalar(alpha, A.code)
     lib.tblis_b200_indexed_dpd_shift(ctypes.byref(s), ctypes.byref(a), _labels(idx_A))
     _check()
 

@@ -21,7 +21,7 @@ namespace
 void to_layout(const tblis_b200_dpd_tensor* t, DpdLayout& lay)
 {
     TB_CHECK(t, TB_ERR_ARG, "null DPD tensor");
-    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "DPD: only double is supported");
+    elem_size(t->type);
     TB_CHECK(t->len, TB_ERR_ARG, "DPD: null lengths");
     std::vector<i64> lens(t->len, t->len + (size_t)t->ndim*t->nirrep);
     lay.init(t->irrep, t->nirrep, t->ndim, lens.data(), t->layout < 0 ? 5 : t->layout);
@@ -31,29 +31,29 @@ void to_layout(const tblis_b200_dpd_tensor* t, DpdLayout& lay)
 struct DpdStage
 {
     dbuf buf;
-    double* host = nullptr;
-    double* dev = nullptr;
-    i64 n = 0;
-    void init(void* data, i64 total, bool copy_in, cudaStream_t st)
+    char* host = nullptr;
+    char* dev = nullptr;
+    size_t bytes = 0;
+    void init(void* data, i64 total, size_t esz, bool copy_in, cudaStream_t st)
     {
-        n = total;
-        if (!data || total == 0) { dev = static_cast<double*>(data); return; }
-        if (pointer_kind(data) == MEM_DEVICE) { dev = static_cast<double*>(data); return; }
-        host = static_cast<double*>(data);
-        buf = dbuf((size_t)total*sizeof(double), st);
-        dev = buf.as<double>();
-        if (copy_in) TB_CUDA(cudaMemcpyAsync(dev, host, (size_t)total*sizeof(double), cudaMemcpyHostToDevice, st));
+        bytes = (size_t)total*esz;
+        dev = static_cast<char*>(data);
+        if (!data || total == 0 || pointer_kind(data) == MEM_DEVICE) return;
+        host = static_cast<char*>(data);
+        buf = dbuf(bytes, st);
+        dev = buf.as<char>();
+        if (copy_in) TB_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, st));
     }
     void out(cudaStream_t st)
     {
-        if (host) TB_CUDA(cudaMemcpyAsync(host, dev, (size_t)n*sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (host) TB_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st));
     }
 };
 
 void to_layout(const tblis_b200_dpd_block_table* t, DpdLayout& lay)
 {
     TB_CHECK(t, TB_ERR_ARG, "null DPD tensor");
-    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "DPD: only double is supported");
+    elem_size(t->type);
     TB_CHECK(t->len, TB_ERR_ARG, "DPD: null lengths");
     std::vector<i64> lens(t->len, t->len + (size_t)t->ndim*t->nirrep);
     lay.init_explicit(t->irrep, t->nirrep, t->ndim, lens.data(), t->offset, t->stride);
@@ -67,22 +67,56 @@ void run_dpd_mult(const Desc* A, const label_type* idx_A, const Desc* B, const l
     ensure_device();
     cudaStream_t st = current_stream();
     const int k0 = (int)g_kernel_count.load();
+    TB_CHECK(A && B && C, TB_ERR_ARG, "null DPD tensor");
+    TB_CHECK(A->type == B->type && A->type == C->type, TB_ERR_TYPE, "DPD mult: operand types differ");
+    const int type = C->type;
+    const size_t esz = elem_size(type);
     DpdTensor a, b, c;
     to_layout(A, a.lay);
     to_layout(B, b.lay);
     to_layout(C, c.lay);
-    const double alpha = A->scalar.data.d*B->scalar.data.d, beta = C->scalar.data.d;
+    const zd alpha = scalar_get(A->scalar)*scalar_get(B->scalar), beta = scalar_get(C->scalar);
     DpdStage sa, sb, sc;
-    sa.init(A->data, a.lay.total(), true, st);
-    sb.init(B->data, b.lay.total(), true, st);
-    sc.init(C->data, c.lay.total(), beta != 0.0, st);
-    a.data = sa.dev; b.data = sb.dev; c.data = sc.dev;
+    sa.init(A->data, a.lay.total(), esz, true, st);
+    sb.init(B->data, b.lay.total(), esz, true, st);
+    // a block table may leave gaps in the storage: those come back unchanged
+    sc.init(C->data, c.lay.total(), esz, beta != 0.0 || c.lay.is_explicit(), st);
     DpdMultReport r;
-    dpd_mult(a, idx_A, b, idx_B, c, idx_C, alpha, beta, st, &r);
+    if (type == TYPE_DOUBLE)
+    {
+        a.data = reinterpret_cast<double*>(sa.dev); b.data = reinterpret_cast<double*>(sb.dev);
+        c.data = reinterpret_cast<double*>(sc.dev);
+        dpd_mult(a, idx_A, b, idx_B, c, idx_C, alpha.real(), beta.real(), st, &r);
+    }
+    else if (type == TYPE_DCOMPLEX)
+        dpd_mult_z(a.lay, reinterpret_cast<const double*>(sa.dev), idx_A, b.lay, reinterpret_cast<const double*>(sb.dev),
+                   idx_B, c.lay, reinterpret_cast<double*>(sc.dev), idx_C, alpha, beta, st, &r);
+    else
+    {
+        // float / scomplex: contracted in double / dcomplex and rounded back
+        const bool cx = type == TYPE_SCOMPLEX;
+        dbuf wa = dpd_widen(sa.dev, a.lay.total(), cx, st), wb = dpd_widen(sb.dev, b.lay.total(), cx, st);
+        dbuf wc;
+        if (beta != 0.0) wc = dpd_widen(sc.dev, c.lay.total(), cx, st);
+        else
+        {
+            // beta == 0: C is not read; zeros stand in for it
+            wc = dbuf((size_t)std::max<i64>(c.lay.total()*(cx ? 2 : 1), 1)*sizeof(double), st);
+            TB_CUDA(cudaMemsetAsync(wc.ptr, 0, wc.bytes, st));
+        }
+        if (cx)
+            dpd_mult_z(a.lay, wa.as<double>(), idx_A, b.lay, wb.as<double>(), idx_B, c.lay, wc.as<double>(), idx_C,
+                       alpha, beta, st, &r);
+        else
+        {
+            a.data = wa.as<double>(); b.data = wb.as<double>(); c.data = wc.as<double>();
+            dpd_mult(a, idx_A, b, idx_B, c, idx_C, alpha.real(), beta.real(), st, &r);
+        }
+        dpd_narrow_blocks(c.lay, cx, wc.as<double>(), reinterpret_cast<float*>(sc.dev), st);
+    }
     sc.out(st);
     if (sa.host || sb.host || sc.host) TB_CUDA(cudaStreamSynchronize(st));
-    C->scalar.data.d = 1.0;
-    C->scalar.type = TYPE_DOUBLE;
+    scalar_put(C->scalar, type, 1.0);
     C->conj = 0;
     if (report)
     {

@@ -179,6 +179,26 @@ void DpdLayout::init_explicit(unsigned irrep_, unsigned nirrep_, unsigned ndim_,
 }
 
 // get_block (dpd_marray_base.hpp:171-228) for a full (unsliced) tensor
+DpdLayout scaled_layout(const DpdLayout& X, i64 scale, i64 shift)
+{
+    size_t nt = 1;
+    for (unsigned d = 0; d < X.ndim; d++) nt *= X.nirrep;
+    std::vector<i64> lens((size_t)X.ndim*X.nirrep), offs(nt, -1), strides(nt*X.ndim, 0);
+    for (unsigned d = 0; d < X.ndim; d++)
+        for (unsigned r = 0; r < X.nirrep; r++) lens[(size_t)d*X.nirrep + r] = X.len[d][r];
+    X.for_each_block([&](const std::vector<unsigned>& irr, const std::vector<i64>&, const std::vector<i64>& bs,
+                         i64 off)
+    {
+        size_t t = 0;
+        for (unsigned d = X.ndim; d-- > 0;) t = t*X.nirrep + irr[d];
+        offs[t] = off*scale + shift;
+        for (unsigned d = 0; d < X.ndim; d++) strides[t*X.ndim + d] = bs[d]*scale;
+    });
+    DpdLayout out;
+    out.init_explicit(X.irrep, X.nirrep, X.ndim, lens.data(), offs.data(), strides.data());
+    return out;
+}
+
 void DpdLayout::block(const unsigned* irreps, i64* blen, i64* bstride, i64& offset) const
 {
     if (is_explicit())
@@ -586,6 +606,48 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
         rep->flops = plan->flops;
         rep->variant = plan->variant;
     }
+}
+
+void dpd_mult_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
+                const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, zd beta,
+                cudaStream_t st, DpdMultReport* rep, bool reference_irrep_check)
+{
+    const std::string iC(idx_C, lc.ndim);
+    // beta first (set when zero: beta == 0 never reads C), on the complex layout
+    if (beta == 0.0) dpd_unary_dev_t(TYPE_DCOMPLEX, 1, 0.0, 1.0, lc, c, iC);
+    else if (beta != 1.0) dpd_unary_dev_t(TYPE_DCOMPLEX, 0, 0.0, beta, lc, c, iC);
+    if (rep) *rep = DpdMultReport();
+    if (alpha == 0.0) return;
+    DpdTensor ar, ai, br, bi, cr, ci;
+    ar.lay = scaled_layout(la, 2, 0); ai.lay = scaled_layout(la, 2, 1);
+    br.lay = scaled_layout(lb, 2, 0); bi.lay = scaled_layout(lb, 2, 1);
+    cr.lay = scaled_layout(lc, 2, 0); ci.lay = scaled_layout(lc, 2, 1);
+    ar.data = ai.data = const_cast<double*>(a);
+    br.data = bi.data = const_cast<double*>(b);
+    cr.data = ci.data = c;
+    const double alr = alpha.real(), ali = alpha.imag();
+    // (A part, B part, coefficient into Re C, coefficient into Im C)
+    struct Term { const DpdTensor* x; const DpdTensor* y; double cr, ci; };
+    const Term terms[4] = {
+        {&ar, &br, alr, ali},       // Ar Br
+        {&ai, &bi, -alr, -ali},     // Ai Bi
+        {&ar, &bi, -ali, alr},      // Ar Bi
+        {&ai, &br, -ali, alr},      // Ai Br
+    };
+    for (const Term& t : terms)
+        for (int part = 0; part < 2; part++)
+        {
+            const double coef = part == 0 ? t.cr : t.ci;
+            if (coef == 0.0) continue;
+            DpdMultReport r;
+            dpd_mult(*t.x, idx_A, *t.y, idx_B, part == 0 ? cr : ci, idx_C, coef, 1.0, st, &r, reference_irrep_check);
+            if (rep)
+            {
+                rep->flops += r.flops;
+                rep->groups += r.groups;
+                rep->variant = r.variant;
+            }
+        }
 }
 
 } // namespace tb

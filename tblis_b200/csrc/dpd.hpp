@@ -5,6 +5,9 @@
 
 #include "planner.hpp"
 
+#include <complex>
+#include <string>
+
 namespace tb
 {
 
@@ -80,15 +83,68 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
               DpdMultReport* rep, bool reference_irrep_check = true);
 
-// level-1 operations on device-resident DPD storage (dpd_level1.cpp):
-// B = alpha*A + beta*B (trace / replicate per block), sum A*B, a reduction
-// with the offset of its extreme element, and the unary updates (kind 0:
-// A *= scal, 1: A = alpha, 2: A = alpha + scal*A)
-void dpd_add_dev(double alpha, const DpdLayout& A, const double* a, const std::string& iA, double beta,
-                 const DpdLayout& B, double* b, const std::string& iB);
-double dpd_dot_dev(const DpdLayout& A, const double* a, const std::string& iA,
-                   const DpdLayout& B, const double* b, const std::string& iB);
-void dpd_reduce_dev(int op, const DpdLayout& A, const double* a, const std::string& iA, double& result, i64& idx);
-void dpd_unary_dev(int kind, double alpha, double scal, const DpdLayout& A, double* a, const std::string& iA);
+// Element types of the DPD operations: float, double, scomplex, dcomplex
+// (type_t); scalars of any type travel as complex<double>.
+using zd = std::complex<double>;
+size_t elem_size(int type);
+inline bool is_complex_type(int type) { return type == TYPE_SCOMPLEX || type == TYPE_DCOMPLEX; }
+zd scalar_get(const tblis_scalar& s);
+void scalar_put(tblis_scalar& s, int type, zd v);
+
+// float / scomplex DPD storage of `total` elements widened to double /
+// dcomplex at equal offsets (a new device buffer), and the stored blocks of
+// such a widened copy rounded back into the float storage (gaps untouched)
+dbuf dpd_widen(const void* src, i64 total, bool cx, cudaStream_t st);
+void dpd_narrow_blocks(const DpdLayout& X, bool cx, const double* src, float* dst, cudaStream_t st);
+
+// the same blocks with every offset and stride multiplied by `scale` and the
+// offsets shifted by `shift`: the real (shift 0) or imaginary (shift 1) part
+// of a complex DPD tensor, seen as doubles
+DpdLayout scaled_layout(const DpdLayout& X, i64 scale, i64 shift);
+
+// complex DPD contraction on dcomplex device storage (double pointers to the
+// storage base): C = beta*C, then the four real products of the parts, each
+// a real DPD contraction (src/internal/3t/dense/mult.cxx:653-720 as 4M)
+void dpd_mult_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
+                const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, zd beta,
+                cudaStream_t st, DpdMultReport* rep, bool reference_irrep_check = true);
+
+// level-1 operations on device-resident DPD storage of element type `type`
+// (dpd_level1.cpp): B = alpha*op(A) + beta*op(B) (trace / replicate per
+// block), sum op(A)*op(B), a reduction with the offset of its extreme
+// element, and the unary updates (kind 0: A = scal*op(A), 1: A = alpha,
+// 2: A = alpha + scal*op(A)); op conjugates a complex operand whose flag is set
+void dpd_add_dev_t(int type, zd alpha, const DpdLayout& A, const void* a, const std::string& iA, zd beta,
+                   const DpdLayout& B, void* b, const std::string& iB, bool conj_a = false, bool conj_b = false);
+zd dpd_dot_dev_t(int type, const DpdLayout& A, const void* a, const std::string& iA,
+                 const DpdLayout& B, const void* b, const std::string& iB, bool conj_a = false,
+                 bool conj_b = false);
+void dpd_reduce_dev_t(int type, int op, const DpdLayout& A, const void* a, const std::string& iA, zd& result,
+                      i64& idx);
+void dpd_unary_dev_t(int type, int kind, zd alpha, zd scal, const DpdLayout& A, void* a, const std::string& iA,
+                     bool conj = false);
+
+// the same on double storage
+inline void dpd_add_dev(double alpha, const DpdLayout& A, const double* a, const std::string& iA, double beta,
+                        const DpdLayout& B, double* b, const std::string& iB)
+{
+    dpd_add_dev_t(TYPE_DOUBLE, alpha, A, a, iA, beta, B, b, iB);
+}
+inline double dpd_dot_dev(const DpdLayout& A, const double* a, const std::string& iA,
+                          const DpdLayout& B, const double* b, const std::string& iB)
+{
+    return dpd_dot_dev_t(TYPE_DOUBLE, A, a, iA, B, b, iB).real();
+}
+inline void dpd_reduce_dev(int op, const DpdLayout& A, const double* a, const std::string& iA, double& result,
+                           i64& idx)
+{
+    zd r;
+    dpd_reduce_dev_t(TYPE_DOUBLE, op, A, a, iA, r, idx);
+    result = r.real();
+}
+inline void dpd_unary_dev(int kind, double alpha, double scal, const DpdLayout& A, double* a, const std::string& iA)
+{
+    dpd_unary_dev_t(TYPE_DOUBLE, kind, alpha, scal, A, a, iA);
+}
 
 } // namespace tb

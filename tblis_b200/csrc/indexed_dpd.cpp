@@ -18,7 +18,10 @@
 // with the selected slices folded into per-block offsets (an explicit block
 // table), so no dense copy of any tensor is made; every triple runs through
 // the grouped persistent FP64 kernel with the factor-weighted alpha and
-// beta = 1 on top of the initial scaling.
+// beta = 1 on top of the initial scaling. Element types: double; dcomplex as
+// four real contractions of the parts (dpd_mult_z); float and scomplex
+// widened to double / dcomplex for the contraction and rounded back; the
+// level-1 operations run on every type directly.
 #include "common.hpp"
 #include "dpd.hpp"
 #include "level1.hpp"
@@ -43,8 +46,10 @@ struct IdxTensor
     std::vector<unsigned> idx_irrep;            // [ndim - dense_ndim]
     i64 nidx = 0;
     std::vector<i64> indices;                   // [nidx][ndim - dense_ndim]
-    std::vector<double*> data;                  // per entry (device after staging)
-    std::vector<double> factor;
+    int type = TYPE_DOUBLE;
+    size_t esz = sizeof(double);
+    std::vector<char*> data;                    // per entry (device after staging)
+    std::vector<zd> factor;
     DpdLayout dense;                            // block table of one entry, relative to its data
     unsigned irrep() const
     {
@@ -59,7 +64,8 @@ struct IdxTensor
 void parse(const tblis_b200_indexed_dpd_tensor* t, IdxTensor& x)
 {
     TB_CHECK(t, TB_ERR_ARG, "null indexed DPD tensor");
-    TB_CHECK(t->type == TYPE_DOUBLE, TB_ERR_TYPE, "indexed DPD: only double is supported");
+    x.type = t->type;
+    x.esz = elem_size(t->type);
     TB_CHECK(t->dense_ndim >= 1 && t->dense_ndim <= t->ndim, TB_ERR_ARG, "indexed DPD: needs 1..ndim dense dimensions");
     TB_CHECK(t->nidx >= 1, TB_ERR_ARG, "indexed DPD: needs at least one index entry");
     TB_CHECK(t->len && t->data && t->offset && t->stride, TB_ERR_ARG, "indexed DPD: null array");
@@ -81,9 +87,17 @@ void parse(const tblis_b200_indexed_dpd_tensor* t, IdxTensor& x)
             TB_CHECK(v >= 0 && v < x.len[t->dense_ndim + d][x.idx_irrep[d]], TB_ERR_ARG,
                      "indexed DPD: index value out of range");
         }
-    x.data.assign(t->data, t->data + t->nidx);
-    x.factor.assign(t->factor ? t->factor : nullptr, t->factor ? t->factor + t->nidx : nullptr);
-    if (!t->factor) x.factor.assign(t->nidx, 1.0);
+    x.data.resize(t->nidx);
+    for (i64 e = 0; e < t->nidx; e++) x.data[e] = static_cast<char*>(t->data[e]);
+    x.factor.assign(t->nidx, 1.0);
+    if (t->factor)
+        for (i64 e = 0; e < t->nidx; e++)
+        {
+            tblis_scalar f;
+            f.type = t->type;
+            std::memcpy(&f.data, static_cast<const char*>(t->factor) + e*(i64)x.esz, x.esz);
+            x.factor[e] = scalar_get(f);
+        }
     std::vector<i64> dl((size_t)x.dense_ndim*x.nirrep);
     for (unsigned d = 0; d < x.dense_ndim; d++)
         for (unsigned r = 0; r < x.nirrep; r++) dl[(size_t)d*x.nirrep + r] = x.len[d][r];
@@ -94,26 +108,59 @@ void parse(const tblis_b200_indexed_dpd_tensor* t, IdxTensor& x)
 struct EntryStage
 {
     std::vector<dbuf> bufs;
-    std::vector<std::pair<double*, double*>> back;      // (host, device) to copy out
+    std::vector<std::pair<char*, char*>> back;          // (host, device) to copy out
+    size_t bytes = 0;
     void init(IdxTensor& x, bool copy_in, bool copy_out, cudaStream_t st)
     {
-        const i64 n = x.dense.total();
+        bytes = (size_t)x.dense.total()*x.esz;
         for (auto& p : x.data)
         {
-            if (!p || n == 0 || pointer_kind(p) == MEM_DEVICE) continue;
-            bufs.emplace_back((size_t)n*sizeof(double), st);
-            double* d = bufs.back().as<double>();
-            if (copy_in) TB_CUDA(cudaMemcpyAsync(d, p, (size_t)n*sizeof(double), cudaMemcpyHostToDevice, st));
+            if (!p || bytes == 0 || pointer_kind(p) == MEM_DEVICE) continue;
+            bufs.emplace_back(bytes, st);
+            char* d = bufs.back().as<char>();
+            if (copy_in) TB_CUDA(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, st));
             if (copy_out) back.push_back({p, d});
             p = d;
         }
     }
-    void out(i64 n, cudaStream_t st)
+    void out(cudaStream_t st)
     {
         for (auto& hd : back)
-            TB_CUDA(cudaMemcpyAsync(hd.first, hd.second, (size_t)n*sizeof(double), cudaMemcpyDeviceToHost, st));
+            TB_CUDA(cudaMemcpyAsync(hd.first, hd.second, bytes, cudaMemcpyDeviceToHost, st));
     }
     bool staged() const { return !bufs.empty(); }
+};
+
+// float / scomplex entries widened to double / dcomplex device copies for a
+// contraction; narrow() rounds the stored blocks back into the entries
+struct EntryWiden
+{
+    std::vector<dbuf> bufs;
+    std::vector<char*> orig;
+    bool cx = false;
+    void init(IdxTensor& x, bool read, cudaStream_t st)
+    {
+        cx = x.type == TYPE_SCOMPLEX;
+        orig = x.data;
+        const i64 n = x.dense.total();
+        for (auto& p : x.data)
+        {
+            if (read) bufs.push_back(dpd_widen(p, n, cx, st));
+            else
+            {
+                bufs.emplace_back((size_t)std::max<i64>(n*(cx ? 2 : 1), 1)*sizeof(double), st);
+                TB_CUDA(cudaMemsetAsync(bufs.back().ptr, 0, bufs.back().bytes, st));
+            }
+            p = bufs.back().as<char>();
+        }
+        x.type = cx ? TYPE_DCOMPLEX : TYPE_DOUBLE;
+        x.esz = elem_size(x.type);
+    }
+    void narrow(const IdxTensor& x, cudaStream_t st)
+    {
+        for (size_t e = 0; e < orig.size(); e++)
+            dpd_narrow_blocks(x.dense, cx, bufs[e].as<double>(), reinterpret_cast<float*>(orig[e]), st);
+    }
 };
 
 // one operand of a triple: which dense dims stay, which are sliced
@@ -174,7 +221,7 @@ bool slice_entry(const IdxTensor& x, i64 e, const Slicing& s, const std::vector<
     }
     out.lay = DpdLayout();
     out.lay.init_explicit(irrep, nirrep, nd, lens.data(), off.data(), str.data());
-    out.data = x.data[e];
+    out.data = reinterpret_cast<double*>(x.data[e]);     // storage of x.type elements
     return true;
 }
 
@@ -214,29 +261,38 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
             TB_CHECK(n >= 2, TB_ERR_ARG, "indexed DPD: a label appears in one tensor only");
         }
 
-    const double alpha = A_->scalar.data.d*B_->scalar.data.d, beta = C_->scalar.data.d;
+    TB_CHECK(A.type == B.type && A.type == C.type, TB_ERR_TYPE, "indexed DPD: operand types differ");
+    const int type = C.type;
+    const zd alpha = scalar_get(A_->scalar)*scalar_get(B_->scalar), beta = scalar_get(C_->scalar);
 
     EntryStage sa, sb, sc;
     sa.init(A, true, false, st);
     sb.init(B, true, false, st);
     sc.init(C, beta != 0.0, true, st);
+    // float / scomplex: contracted in double / dcomplex
+    EntryWiden wa, wb, wc;
+    const bool widened = type == TYPE_FLOAT || type == TYPE_SCOMPLEX;
+    if (widened)
+    {
+        wa.init(A, true, st);
+        wb.init(B, true, st);
+        wc.init(C, beta != 0.0, st);
+    }
+    const int wtype = C.type;
 
     // beta through the entries' factors (src/internal/3t/indexed_dpd/mult.cxx:1217-1224
     // with src/internal/1t/indexed_dpd/scale.cxx and set.cxx): beta == 1
     // leaves C, beta == 0 or a zero factor sets the entry to 0, otherwise
     // entry e is scaled by f_e*beta
     if (beta != 1.0)
+    {
+        const std::string dl = iC.substr(0, C.dense_ndim);
         for (i64 e = 0; e < C.nidx; e++)
-            C.dense.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
-                                       const std::vector<i64>& bs, i64 off)
-            {
-                TB_CHECK(C.dense_ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "indexed DPD: too many dimensions");
-                Strided s;
-                s.ndim = (int)C.dense_ndim;
-                for (unsigned d = 0; d < C.dense_ndim; d++) { s.len[d] = bl[d]; s.stride[d] = bs[d]; }
-                if (beta == 0.0 || C.factor[e] == 0.0) l1_set<double>(C.data[e] + off, s, 0.0, st);
-                else l1_scale<double>(C.data[e] + off, s, C.factor[e]*beta, st);
-            });
+        {
+            if (beta == 0.0 || C.factor[e] == 0.0) dpd_unary_dev_t(wtype, 1, 0.0, 1.0, C.dense, C.data[e], dl);
+            else dpd_unary_dev_t(wtype, 0, 0.0, C.factor[e]*beta, C.dense, C.data[e], dl);
+        }
+    }
 
     // labels shared by all three tensors must not be dense in all of them
     // (batch labels are not supported, as in the DPD contraction)
@@ -356,10 +412,14 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
                     if (!slice_entry(A, ea, S[0], vA, dumA, a) || !slice_entry(B, eb, S[1], vB, dumB, b) ||
                         !slice_entry(C, ec, S[2], vC, dumC, c))
                         continue;
-                    const double w = alpha*A.factor[ea]*B.factor[eb]*C.factor[ec];
+                    const zd w = alpha*A.factor[ea]*B.factor[eb]*C.factor[ec];
                     if (w == 0.0) continue;
                     DpdMultReport r;
-                    dpd_mult(a, lA.c_str(), b, lB.c_str(), c, lC.c_str(), w, 1.0, st, &r, false);
+                    if (wtype == TYPE_DOUBLE)
+                        dpd_mult(a, lA.c_str(), b, lB.c_str(), c, lC.c_str(), w.real(), 1.0, st, &r, false);
+                    else
+                        dpd_mult_z(a.lay, a.data, lA.c_str(), b.lay, b.data, lB.c_str(), c.lay, c.data, lC.c_str(),
+                                   w, 1.0, st, &r, false);
                     launches += r.groups > 0;
                     flops += r.flops;
                 }
@@ -367,10 +427,10 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
         }
     }
 
-    sc.out(C.dense.total(), st);
-    if (sa.staged() || sb.staged() || sc.staged()) TB_CUDA(cudaStreamSynchronize(st));
-    C_->scalar.data.d = 1.0;
-    C_->scalar.type = TYPE_DOUBLE;
+    if (widened) wc.narrow(C, st);
+    sc.out(st);
+    if (sa.staged() || sb.staged() || sc.staged() || widened) TB_CUDA(cudaStreamSynchronize(st));
+    scalar_put(C_->scalar, type, 1.0);
     if (report)
     {
         memset(report, 0, sizeof(*report));
@@ -386,13 +446,13 @@ namespace
 
 // scales every entry's blocks by f_e*beta (set when beta == 0 or f_e == 0),
 // as src/internal/1t/indexed_dpd/scale.cxx and set.cxx do
-void scale_entries(const IdxTensor& X, double beta, const std::string& labels)
+void scale_entries(const IdxTensor& X, zd beta, const std::string& labels)
 {
     const std::string dl = labels.substr(0, X.dense_ndim);
     for (i64 e = 0; e < X.nidx; e++)
     {
-        if (beta == 0.0 || X.factor[e] == 0.0) dpd_unary_dev(1, 0.0, 1.0, X.dense, X.data[e], dl);
-        else dpd_unary_dev(0, 0.0, X.factor[e]*beta, X.dense, X.data[e], dl);
+        if (beta == 0.0 || X.factor[e] == 0.0) dpd_unary_dev_t(X.type, 1, 0.0, 1.0, X.dense, X.data[e], dl);
+        else dpd_unary_dev_t(X.type, 0, 0.0, X.factor[e]*beta, X.dense, X.data[e], dl);
     }
 }
 
@@ -489,7 +549,8 @@ void indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A_, const label_type* 
     std::string Aonly, Bonly;
     for (char c : iA) if (iB.find(c) == std::string::npos) Aonly.push_back(c);
     for (char c : iB) if (iA.find(c) == std::string::npos) Bonly.push_back(c);
-    const double alpha = A_->scalar.data.d, beta = B_->scalar.data.d;
+    TB_CHECK(A.type == B.type, TB_ERR_TYPE, "indexed DPD add: operand types differ");
+    const zd alpha = scalar_get(A_->scalar), beta = scalar_get(B_->scalar);
     EntryStage sa, sb;
     sa.init(A, true, false, st);
     sb.init(B, beta != 0.0, true, st);
@@ -500,8 +561,8 @@ void indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A_, const label_type* 
         for (i64 e = 0; e < B.nidx; e++)
         {
             const std::string dl = iB.substr(0, B.dense_ndim);
-            if (beta == 0.0 || B.factor[e] == 0.0) dpd_unary_dev(1, 0.0, 1.0, B.dense, B.data[e], dl);
-            else dpd_unary_dev(0, 0.0, B.factor[e]*beta, B.dense, B.data[e], dl);
+            if (beta == 0.0 || B.factor[e] == 0.0) dpd_unary_dev_t(B.type, 1, 0.0, 1.0, B.dense, B.data[e], dl);
+            else dpd_unary_dev_t(B.type, 0, 0.0, B.factor[e]*beta, B.dense, B.data[e], dl);
         }
     }
     else
@@ -511,19 +572,18 @@ void indexed_dpd_add(const tblis_b200_indexed_dpd_tensor* A_, const label_type* 
             for_each_pair(A, iA, B, iB, [&](i64 ea, i64 eb, const DpdTensor& a, const std::string& la,
                                             const DpdTensor& b, const std::string& lb)
             {
-                const double w = alpha*A.factor[ea]*B.factor[eb];
+                const zd w = alpha*A.factor[ea]*B.factor[eb];
                 if (w == 0.0) return;
-                dpd_add_dev(w, a.lay, a.data, la, 1.0, b.lay, b.data, lb);
+                dpd_add_dev_t(A.type, w, a.lay, a.data, la, 1.0, b.lay, b.data, lb);
             });
     }
-    sb.out(B.dense.total(), st);
+    sb.out(st);
     if (sa.staged() || sb.staged()) TB_CUDA(cudaStreamSynchronize(st));
-    B_->scalar.data.d = 1.0;
-    B_->scalar.type = TYPE_DOUBLE;
+    scalar_put(B_->scalar, B.type, 1.0);
 }
 
-double indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
-                       const tblis_b200_indexed_dpd_tensor* B_, const label_type* idx_B)
+zd indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
+                   const tblis_b200_indexed_dpd_tensor* B_, const label_type* idx_B)
 {
     ensure_device();
     cudaStream_t st = current_stream();
@@ -532,96 +592,103 @@ double indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A_, const label_type
     TB_CHECK(A.nirrep == B.nirrep && A.ndim == B.ndim, TB_ERR_ARG, "indexed DPD dot: shapes differ");
     const std::string iA(idx_A, A.ndim), iB(idx_B, B.ndim);
     for (char c : iA) TB_CHECK(iB.find(c) != std::string::npos, TB_ERR_ARG, "indexed DPD dot: labels must match");
+    TB_CHECK(A.type == B.type, TB_ERR_TYPE, "indexed DPD dot: operand types differ");
     EntryStage sa, sb;
     sa.init(A, true, false, st);
     sb.init(B, true, false, st);
-    double sum = 0.0;
+    zd sum = 0.0;
     if (indexed_irreps_agree(A, iA, B, iB))
         for_each_pair(A, iA, B, iB, [&](i64 ea, i64 eb, const DpdTensor& a, const std::string& la,
                                         const DpdTensor& b, const std::string& lb)
         {
-            const double w = A.factor[ea]*B.factor[eb];
+            const zd w = A.factor[ea]*B.factor[eb];
             if (w == 0.0) return;
-            sum += w*dpd_dot_dev(a.lay, a.data, la, b.lay, b.data, lb);
+            sum += w*dpd_dot_dev_t(A.type, a.lay, a.data, la, b.lay, b.data, lb);
         });
     if (sa.staged() || sb.staged()) TB_CUDA(cudaStreamSynchronize(st));
-    return A_->scalar.data.d*B_->scalar.data.d*sum;
+    return scalar_get(A_->scalar)*scalar_get(B_->scalar)*sum;
 }
 
 // src/internal/1t/indexed_dpd/reduce.cxx: each entry's reduction scaled by
 // its factor, combined in entry order; idx counts from entry 0's data
 void indexed_dpd_reduce(int op, const tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A,
-                        double& result, i64& idx)
+                        zd& result, i64& idx)
 {
     ensure_device();
     cudaStream_t st = current_stream();
     IdxTensor A;
     parse(A_, A);
-    const std::vector<double*> orig = A.data;
+    const std::vector<char*> orig = A.data;
     EntryStage sa;
     sa.init(A, true, false, st);
     const std::string dl(idx_A, A.dense_ndim);
+    // complex values compare by their real parts, as the reference's operators do
     using lim = std::numeric_limits<double>;
-    double acc = op == REDUCE_MAX ? lim::lowest() : (op == REDUCE_MIN || op == REDUCE_MIN_ABS) ? lim::max() : 0.0;
+    const double big = A.type == TYPE_FLOAT || A.type == TYPE_SCOMPLEX ? (double)std::numeric_limits<float>::max()
+                                                                       : lim::max();
+    zd acc = op == REDUCE_MAX ? zd(-big) : (op == REDUCE_MIN || op == REDUCE_MIN_ABS) ? zd(big) : zd(0.0);
     i64 at = -1;
     for (i64 e = 0; e < A.nidx; e++)
     {
-        double v;
+        zd v;
         i64 bi;
-        dpd_reduce_dev(op == REDUCE_NORM_2 ? REDUCE_NORM_2 : op, A.dense, A.data[e], dl, v, bi);
-        const double f = A.factor[e], fv = f*v;
-        const i64 gi = bi + (i64)(orig[e] - orig[0]);
+        dpd_reduce_dev_t(A.type, op, A.dense, A.data[e], dl, v, bi);
+        const zd fv = A.factor[e]*v;
+        const i64 gi = bi + (i64)((orig[e] - orig[0])/(i64)A.esz);
         switch (op)
         {
             case REDUCE_SUM: case REDUCE_SUM_ABS: acc += fv; break;
-            case REDUCE_NORM_2: acc += fv*fv; break;
-            case REDUCE_MAX: if (fv > acc) { acc = fv; at = gi; } break;
-            case REDUCE_MAX_ABS: if (std::fabs(fv) > acc) { acc = std::fabs(fv); at = gi; } break;
-            case REDUCE_MIN: if (fv < acc) { acc = fv; at = gi; } break;
-            case REDUCE_MIN_ABS: if (std::fabs(fv) < acc) { acc = std::fabs(fv); at = gi; } break;
+            case REDUCE_NORM_2: acc += std::norm(fv); break;
+            case REDUCE_MAX: if (fv.real() > acc.real()) { acc = fv; at = gi; } break;
+            case REDUCE_MAX_ABS: if (std::abs(fv) > acc.real()) { acc = std::abs(fv); at = gi; } break;
+            case REDUCE_MIN: if (fv.real() < acc.real()) { acc = fv; at = gi; } break;
+            case REDUCE_MIN_ABS: if (std::abs(fv) < acc.real()) { acc = std::abs(fv); at = gi; } break;
             default: throw error(TB_ERR_ARG, "indexed DPD reduce: unknown operation");
         }
     }
     if (sa.staged()) TB_CUDA(cudaStreamSynchronize(st));
-    if (op == REDUCE_NORM_2) acc = std::sqrt(acc);
+    if (op == REDUCE_NORM_2) acc = std::sqrt(acc.real());
     result = acc;
     idx = at;
 }
 
 // kind 0: scale by A.scalar, 1: set to alpha, 2: shift (alpha + A.scalar*A),
 // each entry through its factor (src/internal/1t/indexed_dpd/{scale,set,shift}.cxx)
-void indexed_dpd_unary(int kind, double alpha, tblis_b200_indexed_dpd_tensor* A_, const label_type* idx_A)
+void indexed_dpd_unary(int kind, const tblis_scalar* alpha_, tblis_b200_indexed_dpd_tensor* A_,
+                       const label_type* idx_A)
 {
     ensure_device();
     cudaStream_t st = current_stream();
     IdxTensor A;
     parse(A_, A);
+    if (alpha_) TB_CHECK(alpha_->type == A.type, TB_ERR_TYPE, "indexed DPD set/shift: scalar and tensor types differ");
+    const zd alpha = alpha_ ? scalar_get(*alpha_) : zd(0.0);
     EntryStage sa;
     sa.init(A, kind != 1, true, st);
     const std::string dl(idx_A, A.dense_ndim);
-    const double scal = A_->scalar.data.d;
+    const zd scal = scalar_get(A_->scalar);
+    const int ty = A.type;
     for (i64 e = 0; e < A.nidx; e++)
     {
-        const double f = A.factor[e];
+        const zd f = A.factor[e];
         if (kind == 0)
         {
-            if (scal == 0.0 || f == 0.0) dpd_unary_dev(1, 0.0, 1.0, A.dense, A.data[e], dl);
-            else dpd_unary_dev(0, 0.0, f*scal, A.dense, A.data[e], dl);
+            if (scal == 0.0 || f == 0.0) dpd_unary_dev_t(ty, 1, 0.0, 1.0, A.dense, A.data[e], dl);
+            else dpd_unary_dev_t(ty, 0, 0.0, f*scal, A.dense, A.data[e], dl);
         }
         else if (kind == 1)
-            dpd_unary_dev(1, f*alpha, 1.0, A.dense, A.data[e], dl);
+            dpd_unary_dev_t(ty, 1, f*alpha, 1.0, A.dense, A.data[e], dl);
         else if (f == 0.0)
         {
-            if (scal == 0.0) dpd_unary_dev(1, 0.0, 1.0, A.dense, A.data[e], dl);
-            else if (scal != 1.0) dpd_unary_dev(0, 0.0, scal, A.dense, A.data[e], dl);
+            if (scal == 0.0) dpd_unary_dev_t(ty, 1, 0.0, 1.0, A.dense, A.data[e], dl);
+            else if (scal != 1.0) dpd_unary_dev_t(ty, 0, 0.0, scal, A.dense, A.data[e], dl);
         }
         else
-            dpd_unary_dev(2, f*alpha, scal, A.dense, A.data[e], dl);
+            dpd_unary_dev_t(ty, 2, f*alpha, scal, A.dense, A.data[e], dl);
     }
-    sa.out(A.dense.total(), st);
+    sa.out(st);
     if (sa.staged()) TB_CUDA(cudaStreamSynchronize(st));
-    A_->scalar.data.d = 1.0;
-    A_->scalar.type = TYPE_DOUBLE;
+    scalar_put(A_->scalar, ty, 1.0);
 }
 
 } // namespace tb
@@ -640,9 +707,8 @@ int tblis_b200_indexed_dpd_dot(const tblis_b200_indexed_dpd_tensor* A, const lab
 {
     return tb::guarded([&]
     {
-        TB_CHECK(result, tb::TB_ERR_ARG, "null result");
-        result->type = TYPE_DOUBLE;
-        result->data.d = tb::indexed_dpd_dot(A, idx_A, B, idx_B);
+        TB_CHECK(result && A, tb::TB_ERR_ARG, "null argument");
+        tb::scalar_put(*result, A->type, tb::indexed_dpd_dot(A, idx_A, B, idx_B));
     });
 }
 
@@ -651,19 +717,18 @@ int tblis_b200_indexed_dpd_reduce(reduce_t op, const tblis_b200_indexed_dpd_tens
 {
     return tb::guarded([&]
     {
-        TB_CHECK(result && idx, tb::TB_ERR_ARG, "null result");
-        double r = 0;
+        TB_CHECK(result && idx && A, tb::TB_ERR_ARG, "null argument");
+        tb::zd r = 0.0;
         tb::i64 i = -1;
         tb::indexed_dpd_reduce((int)op, A, idx_A, r, i);
-        result->type = TYPE_DOUBLE;
-        result->data.d = r;
+        tb::scalar_put(*result, A->type, r);
         *idx = i;
     });
 }
 
 int tblis_b200_indexed_dpd_scale(tblis_b200_indexed_dpd_tensor* A, const label_type* idx_A)
 {
-    return tb::guarded([&] { tb::indexed_dpd_unary(0, 0.0, A, idx_A); });
+    return tb::guarded([&] { tb::indexed_dpd_unary(0, nullptr, A, idx_A); });
 }
 
 int tblis_b200_indexed_dpd_set(const tblis_scalar* alpha, tblis_b200_indexed_dpd_tensor* A,
@@ -672,7 +737,7 @@ int tblis_b200_indexed_dpd_set(const tblis_scalar* alpha, tblis_b200_indexed_dpd
     return tb::guarded([&]
     {
         TB_CHECK(alpha, tb::TB_ERR_ARG, "null alpha");
-        tb::indexed_dpd_unary(1, alpha->data.d, A, idx_A);
+        tb::indexed_dpd_unary(1, alpha, A, idx_A);
     });
 }
 
@@ -682,7 +747,7 @@ int tblis_b200_indexed_dpd_shift(const tblis_scalar* alpha, tblis_b200_indexed_d
     return tb::guarded([&]
     {
         TB_CHECK(alpha, tb::TB_ERR_ARG, "null alpha");
-        tb::indexed_dpd_unary(2, alpha->data.d, A, idx_A);
+        tb::indexed_dpd_unary(2, alpha, A, idx_A);
     });
 }
 

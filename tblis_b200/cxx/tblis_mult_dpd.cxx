@@ -25,6 +25,7 @@
 #include "../../include/tblis_b200.h"
 
 #include <complex>
+#include <cstring>
 #include <vector>
 
 namespace tci { class communicator; }
@@ -55,11 +56,20 @@ template <> type_t type_of<double>() { return TYPE_DOUBLE; }
 template <> type_t type_of<std::complex<float>>() { return TYPE_SCOMPLEX; }
 template <> type_t type_of<std::complex<double>>() { return TYPE_DCOMPLEX; }
 
+// a value of T into / out of tblis_scalar's union (float, double,
+// complex<float> and complex<double> share its leading bytes)
 template <typename T> void set_scalar(tblis_scalar& s, T v)
 {
     s.type = type_of<T>();
-    s.data.d = 0;
-    if (s.type == TYPE_DOUBLE) s.data.d = *reinterpret_cast<const double*>(&v);
+    std::memset(&s.data, 0, sizeof(s.data));
+    std::memcpy(&s.data, &v, sizeof(T));
+}
+
+template <typename T> T get_scalar(const tblis_scalar& s)
+{
+    T v;
+    std::memcpy(&v, &s.data, sizeof(T));
+    return v;
 }
 
 // lengths and the per-block geometry of one DPD view
@@ -113,8 +123,8 @@ struct IdxTable
 {
     std::vector<len_type> len, indices;
     std::vector<unsigned> idx_irrep;
-    std::vector<double*> data;
-    std::vector<double> factor;
+    std::vector<void*> data;
+    std::vector<unsigned char> factor;        // the entries' factors, elements of the view's type
     Table dense;
     tblis_b200_indexed_dpd_tensor t;
 
@@ -131,9 +141,10 @@ struct IdxTable
         for (len_type e = 0; e < n; e++)
         {
             for (unsigned d = 0; d < ni; d++) indices.push_back(ni ? V.indices(e)[d] : 0);
-            data.push_back(reinterpret_cast<double*>(const_cast<U*>(V.data(e))));
+            data.push_back(const_cast<U*>(V.data(e)));
             const U f = V.factor(e);
-            factor.push_back(type_of<U>() == TYPE_DOUBLE ? *reinterpret_cast<const double*>(&f) : 0.0);
+            const unsigned char* fb = reinterpret_cast<const unsigned char*>(&f);
+            factor.insert(factor.end(), fb, fb + sizeof(U));
         }
         t.type = type_of<U>();
         set_scalar(t.scalar, scalar);
@@ -202,11 +213,6 @@ typedef enum
     REDUCE_MIN_ = 4, REDUCE_MIN_ABS_ = 5, REDUCE_NORM_2_ = 6
 } reduce_t;
 
-namespace
-{
-template <typename T> T from_double(double v) { return T(v); }
-}
-
 // level-1 operations over DPD views (src/iface/1t/{add,dot,reduce,scale,set,
 // shift}.cxx, instantiated there for the same four types)
 template <typename T>
@@ -231,7 +237,7 @@ void dot(const tci::communicator& comm,
     {
         Table a(A, T(1)), b(B, T(1));
         tblis_scalar r;
-        if (tblis_b200_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = from_double<T>(r.data.d);
+        if (tblis_b200_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = get_scalar<T>(r);
     }
     wait_all(comm);
 }
@@ -247,7 +253,7 @@ void reduce(const tci::communicator& comm, reduce_t op,
         len_type i = -1;
         if (tblis_b200_dpd_reduce((::reduce_t)op, &a.t, idx_A, &r, &i) == 0)
         {
-            result = from_double<T>(r.data.d);
+            result = get_scalar<T>(r);
             idx = i;
         }
     }
@@ -329,7 +335,7 @@ void dot(const tci::communicator& comm,
     {
         IdxTable a(A, T(1)), b(B, T(1));
         tblis_scalar r;
-        if (tblis_b200_indexed_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = from_double<T>(r.data.d);
+        if (tblis_b200_indexed_dpd_dot(&a.t, idx_A, &b.t, idx_B, &r) == 0) result = get_scalar<T>(r);
     }
     wait_all(comm);
 }
@@ -345,7 +351,7 @@ void reduce(const tci::communicator& comm, reduce_t op,
         len_type i = -1;
         if (tblis_b200_indexed_dpd_reduce((::reduce_t)op, &a.t, idx_A, &r, &i) == 0)
         {
-            result = from_double<T>(r.data.d);
+            result = get_scalar<T>(r);
             idx = i;
         }
     }

@@ -45,7 +45,7 @@ def dense_geometry(T, nirrep):
 
 
 def block_view(flat, off, shape, strides):
-    return as_strided(flat[off:], shape=shape, strides=[8 * s for s in strides])
+    return as_strided(flat[off:], shape=shape, strides=[flat.itemsize * s for s in strides])
 
 
 def make(rng, nirrep, irrep, lens, idx_irreps, indices, factors=None):
@@ -63,7 +63,7 @@ def full(T, nirrep):
     nd = len(T["lens"]) - len(T["idx_irreps"])
     ext = [sum(r) for r in T["lens"]]
     off = [np.concatenate([[0], np.cumsum(r)[:-1]]).astype(int) for r in T["lens"]]
-    F = np.zeros(ext)
+    F = np.zeros(ext, dtype=np.result_type(T["data"].dtype, np.float64))
     size, geo = dense_geometry(T, nirrep)
     entries = T["indices"] if T["idx_irreps"] else [[]]
     for e, ix in enumerate(entries):
@@ -77,7 +77,7 @@ def full(T, nirrep):
 
 def restated_mult(nirrep, alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     """C's storage after the contraction, in the FULL form."""
-    out = C["data"].copy()
+    out = C["data"].astype(np.result_type(C["data"].dtype, np.float64))
     size, geo = dense_geometry(C, nirrep)
     entries = C["indices"] if C["idx_irreps"] else [[]]
     # beta goes through the entries' factors (src/internal/1t/indexed_dpd/
