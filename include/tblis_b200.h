@@ -442,6 +442,29 @@ int tblis_b200_server_poll(tblis_b200_server* srv, int64_t id, double* latency_m
 int tblis_b200_server_wait(tblis_b200_server* srv, int64_t id, double* latency_ms);
 int tblis_b200_server_get_stats(tblis_b200_server* srv, tblis_b200_server_stats* out);
 
+/* Multi-GPU sharding (no counterpart in TBLIS, whose parallelism is TCI
+ * threads on one node): a contraction split across `nranks` processes, one per
+ * GPU, with no collective on the data path. C is partitioned along its longest
+ * label that appears in exactly one of A and B; rank `rank` owns the range
+ * [len*rank/nranks, len*(rank+1)/nranks) of that label and contracts the
+ * matching slice of A (or B) into its slab of C. The slabs are disjoint and
+ * cover C. Without such a label rank 0 computes everything.
+ *
+ * tblis_b200_shard_plan: host-only (needs no device): the cut label (0 when
+ * none) and this rank's [begin, end).
+ * tblis_b200_tensor_mult_shard: C's slab = alpha*A*B + beta*C's slab for
+ * this rank, through the same path as tblis_tensor_mult; the rest of C is
+ * untouched. Both return 0 or an error code. */
+int tblis_b200_shard_plan(const tblis_tensor* A, const label_type* idx_A,
+                          const tblis_tensor* B, const label_type* idx_B,
+                          const tblis_tensor* C, const label_type* idx_C,
+                          int nranks, int rank, char* label, len_type* begin, len_type* end);
+int tblis_b200_tensor_mult_shard(const tblis_config* cfg,
+                                 const tblis_tensor* A, const label_type* idx_A,
+                                 const tblis_tensor* B, const label_type* idx_B,
+                                       tblis_tensor* C, const label_type* idx_C,
+                                 int nranks, int rank, tblis_b200_report* report);
+
 /* No counterpart in the reference. tblis_tensor_mult for callers that cannot
  * let a library allocate device memory (their device memory is owned by
  * another allocator, or they must avoid cudaMalloc/cudaFree because those can

@@ -238,6 +238,72 @@ def shift(alpha, beta, A, idx_A, conj=False):
     _check()
 
 
+lib.tblis_b200_shard_plan.restype = ctypes.c_int
+lib.tblis_b200_tensor_mult_shard.restype = ctypes.c_int
+
+
+def shard_plan(A, idx_A, B, idx_B, C, idx_C, nranks, rank):
+    """(label, begin, end) of rank's slab of C when the contraction is split
+    over nranks processes (label '' when there is nothing to cut: rank 0 then
+    owns all of C). Host-only: needs no GPU."""
+    a, b, c = _View(A), _View(B), _View(C)
+    lab = ctypes.c_char()
+    beg, end = ctypes.c_ssize_t(), ctypes.c_ssize_t()
+    lib.tblis_b200_shard_plan(a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref, _labels(idx_C),
+                              int(nranks), int(rank), ctypes.byref(lab), ctypes.byref(beg), ctypes.byref(end))
+    _check()
+    label = lab.value.decode() if lab.value != b"\x00" else ""
+    return label, beg.value, end.value
+
+
+def _rank_world(rank, nranks, group):
+    if rank is None or nranks is None:
+        import torch.distributed as dist
+        return dist.get_rank(group), dist.get_world_size(group)
+    return rank, nranks
+
+
+def mult_shard(alpha, A, idx_A, B, idx_B, beta, C, idx_C, rank=None, nranks=None, gather=False, group=None,
+               cfg=None):
+    """This rank's slab of C = alpha*A*B + beta*C (tblis_b200_tensor_mult_shard);
+    rank / nranks default to the torch.distributed group's. gather=True then
+    hands every slab to every rank (gather_shards), so each holds all of C."""
+    rank, nranks = _rank_world(rank, nranks, group)
+    a, b, c = _View(A, alpha), _View(B), _View(C, beta)
+    r = tblis_b200_report()
+    lib.tblis_b200_tensor_mult_shard(cfg, a.ref, _labels(idx_A), b.ref, _labels(idx_B), c.ref, _labels(idx_C),
+                                     int(nranks), int(rank), ctypes.byref(r))
+    _check()
+    if gather:
+        gather_shards(A, idx_A, B, idx_B, C, idx_C, rank, nranks, group)
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
+def _slab(C, idx_C, label, begin, end):
+    """The view of torch tensor C restricted to label in [begin, end)."""
+    dims = [d for d, c in enumerate(idx_C) if c == label]
+    if len(dims) != 1:
+        raise ValueError("gather_shards: the cut label must appear once in C")
+    return C.narrow(dims[0], begin, end - begin)
+
+
+def gather_shards(A, idx_A, B, idx_B, C, idx_C, rank=None, nranks=None, group=None):
+    """Every rank broadcasts its slab of C (torch tensor, same shape on every
+    rank) in rank order; afterwards all ranks hold the whole C. Over NCCL on
+    GPUs, gloo on CPU tensors."""
+    import torch.distributed as dist
+    rank, nranks = _rank_world(rank, nranks, group)
+    for r in range(nranks):
+        label, b, e = shard_plan(A, idx_A, B, idx_B, C, idx_C, nranks, r)
+        view = C if not label else _slab(C, idx_C, label, b, e)
+        if view.numel() == 0:
+            continue
+        buf = view.contiguous() if r == rank else view.new_empty(view.shape).contiguous()
+        dist.broadcast(buf, src=dist.get_global_rank(group, r) if group is not None else r, group=group)
+        if r != rank:
+            view.copy_(buf)
+
+
 def _make_scalar(v, code):
     s = tblis_scalar()
     s.type = code
