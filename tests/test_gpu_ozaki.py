@@ -207,3 +207,24 @@ def test_named_configs_select_methods(cuda):
         assert rep["method"] == method
         err = (torch.linalg.norm(c - a @ b) / torch.linalg.norm(a @ b)).item()
         assert err <= (1e-12 if method <= 3 else 2e-2)
+
+
+def test_medium_exponent_spread_matches_fp64(cuda):
+    """A medium-size contraction (m = 9216, n = 2304, k = 6144: 72 x 36 output
+    tiles, 340 MB of A planes, one exactness run) with exponent spread in A:
+    the Ozaki result at tolerance 1e-12 matches the FP64 path."""
+    import torch
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(21)
+    A = torch.empty((6144, 9216), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    B = torch.empty((2304, 6144), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    exps = torch.randint(-20, 21, A.shape, device=cuda, generator=g, dtype=torch.int32)
+    A = torch.ldexp(A, exps)
+    C = torch.empty((2304, 9216), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    ref = C.clone()
+    tb.mult_ex(1.0, A, "ik", B, "kj", 0.5, ref, "ij", method=1)
+    rep = tb.mult_ex(1.0, A, "ik", B, "kj", 0.5, C, "ij", method=2, tolerance=1e-12)
+    torch.cuda.synchronize()
+    err = (torch.linalg.vector_norm(C - ref) / torch.linalg.vector_norm(ref)).item()
+    assert rep["slices"] >= 1 and err <= 1e-12
