@@ -56,12 +56,18 @@ namespace
 {
 
 constexpr int OZ_BM = 128;           // tile rows (TMEM lanes)
-constexpr int OZ_BN = 64;            // tile columns per diagonal accumulator
+// tile columns per diagonal accumulator: the S diagonals of BN columns fill
+// up to the 512 TMEM columns (wider tiles reuse each A slice tile over more
+// B columns, fewer shared-memory bytes per MAC). BF16 digit planes (S >= 2)
+// flush every 2^24/(S*64^2) k and keep 64 columns: measured faster there.
+constexpr int bn_of(int S, int kind)
+{
+    return kind == OZ_BF16 && S >= 2 ? 64 : S <= 4 ? 128 : S == 5 ? 96 : S == 6 ? 80 : 64;
+}
 constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step of any kind)
 constexpr int OZ_SMAX = 8;           // 8 diagonals x 64 columns = all 512 TMEM columns
 constexpr int OZ_THREADS = 192;      // warp 0 bulk copies, warp 1 MMA, warps 2-5 epilogue
 constexpr int A_TILE = OZ_BM*OZ_BK;  // bytes of one A slice tile
-constexpr int B_TILE = OZ_BN*OZ_BK;  // bytes of one B slice tile
 constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded waits: 2 s
 
 __device__ int g_oz_error = 0;       // set by a kernel whose bounded wait gave up
@@ -238,11 +244,11 @@ struct OzGemmArgs
     double w[OZ_SMAX];           // weight of diagonal d = p + q at w[d - 2]
 };
 
-// TMEM columns for S diagonal accumulators of OZ_BN columns (a power of two >= 32)
-template <int S>
+// TMEM columns for S diagonal accumulators of bn_of(S, KIND) columns (a power of two >= 32)
+template <int S, int KIND>
 struct TmemCols
 {
-    static constexpr uint32_t need = (uint32_t)(S*OZ_BN);
+    static constexpr uint32_t need = (uint32_t)(S*bn_of(S, KIND));
     static constexpr uint32_t value = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 };
 
@@ -250,6 +256,8 @@ template <int S, int STAGES, int KIND>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 ozaki_gemm_kernel(const OzGemmArgs p)
 {
+    constexpr int BN = bn_of(S, KIND);
+    constexpr int B_TILE = BN*OZ_BK;                 // bytes of one B slice tile
     constexpr int STAGE_BYTES = S*(A_TILE + B_TILE);
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned base for the swizzled tiles
@@ -263,12 +271,12 @@ ozaki_gemm_kernel(const OzGemmArgs p)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     i64* sCm = reinterpret_cast<i64*>(tmem_slot + 4);
     i64* sCn = sCm + OZ_BM;
-    double* sScaleN = reinterpret_cast<double*>(sCn + OZ_BN);
+    double* sScaleN = reinterpret_cast<double*>(sCn + BN);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const i64 tiles_n = (p.N + OZ_BN - 1)/OZ_BN;
+    const i64 tiles_n = (p.N + BN - 1)/BN;
     const i64 tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
-    const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*OZ_BN);
+    const int m0 = (int)(tm*OZ_BM), n0 = (int)(tn*BN);
     const int l = blockIdx.y;
     const int kt_count = p.k_steps;
     const int kt_flush = p.kt_flush > 0 ? p.kt_flush : kt_count;
@@ -284,13 +292,13 @@ ozaki_gemm_kernel(const OzGemmArgs p)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    if (warp == 1) tmem_alloc(tmem_slot, TmemCols<S>::value);
+    if (warp == 1) tmem_alloc(tmem_slot, TmemCols<S, KIND>::value);
     for (int i = threadIdx.x; i < OZ_BM; i += OZ_THREADS)
     {
         const i64 m = m0 + i;
         sCm[i] = m < p.M ? p.c_m[m] : -1;
     }
-    for (int i = threadIdx.x; i < OZ_BN; i += OZ_THREADS)
+    for (int i = threadIdx.x; i < BN; i += OZ_THREADS)
     {
         const i64 n = n0 + i;
         sCn[i] = n < p.N ? p.c_n[n] : -1;
@@ -356,11 +364,11 @@ ozaki_gemm_kernel(const OzGemmArgs p)
                 {
                     const uint64_t ad = sdesc_kmajor(st + (pa - 1)*A_TILE);
                     #pragma unroll
-                    for (int n0c = 0; n0c < (S + 1 - pa)*OZ_BN; n0c += 256)
+                    for (int n0c = 0; n0c < (S + 1 - pa)*BN; n0c += 256)
                     {
-                        const int nc = min(256, (S + 1 - pa)*OZ_BN - n0c);
+                        const int nc = min(256, (S + 1 - pa)*BN - n0c);
                         const uint64_t bd = sdesc_kmajor(st + S*A_TILE + n0c*OZ_BK);
-                        const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*OZ_BN + n0c);
+                        const uint32_t acc_addr = tmem_base + (uint32_t)((pa - 1)*BN + n0c);
                         // the pa = 1 row spans every diagonal: it starts the sums
                         mma_op<KIND>(acc_addr, ad, bd, idesc_mma(KIND, nc),
                                      (kt % kt_flush == 0 && pa == 1) ? 0u : 1u);
@@ -390,7 +398,7 @@ ozaki_gemm_kernel(const OzGemmArgs p)
             const double rscale = (rc >= 0 && ok) ? p.alpha*ldexp(1.0, p.eA[(i64)l*p.M + m]) : 0.0;
             const double beta = chunk == 0 ? p.beta : 1.0;
             #pragma unroll 1
-            for (int c = 0; c < OZ_BN/16; c++)
+            for (int c = 0; c < BN/16; c++)
             {
                 double v[16];
                 #pragma unroll
@@ -400,7 +408,7 @@ ozaki_gemm_kernel(const OzGemmArgs p)
                 for (int d = S + 1; d >= 2; d--)
                 {
                     int r[16];
-                    tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*OZ_BN + c*16), r);
+                    tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)((d - 2)*BN + c*16), r);
                     const double w = p.w[d - 2];
                     #pragma unroll
                     for (int j = 0; j < 16; j++)
@@ -435,7 +443,7 @@ ozaki_gemm_kernel(const OzGemmArgs p)
     if (warp == 1)
     {
         tc_fence_after();
-        tmem_dealloc(tmem_base, TmemCols<S>::value);
+        tmem_dealloc(tmem_base, TmemCols<S, KIND>::value);
     }
 }
 
@@ -723,6 +731,7 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
     // 4 threads per row of a tile, 16 consecutive k each
     const int rl = t >> 2, seg = (t & 3)*16;
     const i64 k_lim = pg.k_steps*KE;
+    const i64 r_lim = pg.tiles*pg.tile_rows;         // rows of the planes (whole row tiles)
     unsigned tile = blockIdx.x;
     At at{0, 0, 0};
     if (tile < ntiles) { at = where(tile); load(at, sl_smem); }
@@ -737,7 +746,7 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
         __syncthreads();
 
         const i64 r = at.r0 + rl, kk = at.k0 + seg;
-        if (kk < k_lim)
+        if (kk < k_lim && r < r_lim)
         {
             // rows past the operand hold zeros: any exponent serves
             const int e = r < o.R ? e_rows[(i64)at.l*o.R + r] : 0;
@@ -814,8 +823,9 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
 template <int S, int KIND, bool SINGLE>
 void launch_slice(const OzOperand& o, const int* e, void* out, const PlaneGeom& pg, cudaStream_t st)
 {
-    // every row of the row tiles, every k of the k steps
-    const i64 tiles_r = pg.tiles*pg.tile_rows/SL_T;
+    // every row of the row tiles (64-row slicing tiles may pass the last
+    // one: the kernel stops at it), every k of the k steps
+    const i64 tiles_r = (pg.tiles*pg.tile_rows + SL_T - 1)/SL_T;
     const i64 tiles_k = (pg.k_steps*(OZ_BK/elem_bytes(KIND)) + SL_T - 1)/SL_T;
     const i64 ntiles = tiles_r*tiles_k*o.L;
     if (ntiles == 0) return;
@@ -888,27 +898,28 @@ void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
 // host side
 // ---------------------------------------------------------------------------------
 
-template <int S>
+template <int S, int KIND>
 constexpr int stages_for()
 {
-    return std::min(6, (200*1024)/(S*(A_TILE + B_TILE)));
+    return std::min(6, (200*1024)/(S*(A_TILE + bn_of(S, KIND)*OZ_BK)));
 }
 
-template <int S>
+template <int S, int KIND>
 size_t gemm_smem_bytes()
 {
-    return (size_t)stages_for<S>()*S*(A_TILE + B_TILE) + 1024 /* alignment */ +
-           (2*stages_for<S>() + 3)*8 + 16 + (OZ_BM + OZ_BN)*8 + OZ_BN*8;
+    constexpr int BN = bn_of(S, KIND);
+    return (size_t)stages_for<S, KIND>()*S*(A_TILE + BN*OZ_BK) + 1024 /* alignment */ +
+           (2*stages_for<S, KIND>() + 3)*8 + 16 + (OZ_BM + BN)*8 + BN*8;
 }
 
 template <int S, int KIND>
 void launch_gemm(const OzGemmArgs& a, cudaStream_t st)
 {
-    constexpr int STG = stages_for<S>();
+    constexpr int STG = stages_for<S, KIND>();
     auto kern = ozaki_gemm_kernel<S, STG, KIND>;
-    const size_t bytes = gemm_smem_bytes<S>();
+    const size_t bytes = gemm_smem_bytes<S, KIND>();
     TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    const i64 tiles = ((a.M + OZ_BM - 1)/OZ_BM)*((a.N + OZ_BN - 1)/OZ_BN);
+    const i64 tiles = ((a.M + OZ_BM - 1)/OZ_BM)*((a.N + bn_of(S, KIND) - 1)/bn_of(S, KIND));
     dim3 grid((unsigned)tiles, (unsigned)a.L, 1);
     kern<<<grid, OZ_THREADS, bytes, st>>>(a);
     check_launch("ozaki_gemm_kernel");
@@ -1074,8 +1085,9 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
     const int esz = elem_bytes(kind);
     const i64 ke = OZ_BK/esz;              // k elements per MMA step
     const PlaneGeom ga = {OZ_BM, (v.m + OZ_BM - 1)/OZ_BM, (v.k + ke - 1)/ke, S};
-    const PlaneGeom gb = {OZ_BN, (v.n + OZ_BN - 1)/OZ_BN, ga.k_steps, S};
-    dbuf pa((size_t)(v.l*ga.tiles*ga.k_steps*S*A_TILE), st), pb((size_t)(v.l*gb.tiles*gb.k_steps*S*B_TILE), st);
+    const int bn = bn_of(S, kind);
+    const PlaneGeom gb = {bn, (v.n + bn - 1)/bn, ga.k_steps, S};
+    dbuf pa((size_t)(v.l*ga.tiles*ga.k_steps*S*A_TILE), st), pb((size_t)(v.l*gb.tiles*gb.k_steps*S*bn*OZ_BK), st);
     slice_dispatch(kind, j.single, S, oa, j.eA.as<int>(), pa.ptr, ga, st);
     slice_dispatch(kind, j.single, S, ob, j.eB.as<int>(), pb.ptr, gb, st);
 
