@@ -505,7 +505,8 @@ def e2e_ladder(torch, tb, method, steps, rank=0):
     return {"value": FLOPS_LADDER / dt / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "normwise_rel_err_vs_fp64": err,
             "note": "host pinned buffers through tblis_tensor_mult; H2D of A,B and D2H of C inside each call "
-                    "(the library copies A in slices overlapped with the contraction of the slices already copied)"}
+                    "(the library copies A in slabs of rows of C overlapped with the contraction of the slabs "
+                    "already copied, and each slab of C back as soon as it is final)"}
 
 
 OCC = [12, 4, 8, 6, 10, 3, 7, 5]

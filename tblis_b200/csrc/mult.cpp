@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <mutex>
 
 namespace tb
 {
@@ -120,12 +121,102 @@ static bool plan_slices(const tblis_tensor* A, const label_type* idx_A, const tb
     return sl.range.size() >= 2;
 }
 
+// Row slabs of a host-resident A and C: a label of A and C (not B) whose
+// lower-stride dims tile [0, stride) densely and whose higher-stride dims
+// continue it as one regular pitch, in both tensors. A slab (a range of the
+// label) is then a pitched block of `rows` rows of width range*stride in A
+// and in C, so each slab contracts the whole K into its final part of C: its
+// copy back can run while the next slab of A comes in.
+struct Slabs
+{
+    int dim_A = -1, dim_C = -1;
+    i64 s_A = 0, s_C = 0;                      // the label's strides
+    i64 pitch_A = 0, pitch_C = 0;              // elements between rows
+    i64 rows_A = 0, rows_C = 0;
+    std::vector<std::pair<i64, i64>> range;    // [q0, q1) of the label
+};
+
+// dims below q tile [0, stride_q); dims above continue q as one pitch
+static bool pitched(const tblis_tensor* X, int q, i64& pitch, i64& rows)
+{
+    const i64 sq = X->stride[q], lq = X->len[q];
+    i64 inner = 1, span = 0;
+    std::vector<std::pair<i64, i64>> outer;
+    for (unsigned d = 0; d < X->ndim; d++)
+    {
+        if ((int)d == q || X->len[d] == 1) continue;
+        if (X->stride[d] <= 0) return false;
+        if (X->stride[d] < sq) { inner *= X->len[d]; span += (X->len[d] - 1)*X->stride[d]; }
+        else outer.push_back({X->stride[d], X->len[d]});
+    }
+    if (inner != sq || span + 1 != sq) return false;
+    std::sort(outer.begin(), outer.end());
+    i64 expect = lq*sq;
+    rows = 1;
+    for (auto& o : outer)
+    {
+        if (o.first != expect) return false;
+        expect *= o.second;
+        rows *= o.second;
+    }
+    pitch = lq*sq;
+    return true;
+}
+
+static bool plan_slabs(const tblis_tensor* A, const label_type* idx_A, const tblis_tensor* B,
+                       const label_type* idx_B, const tblis_tensor* C, const label_type* idx_C, Slabs& sl)
+{
+    constexpr i64 kSliceBytes = (i64)384 << 20;
+    constexpr i64 kMinRowBytes = 4096;         // narrower rows copy slowly
+    i64 lo, hi;
+    tensor_extent(A->ndim, A->len, A->stride, lo, hi);
+    const i64 bytes = (hi - lo + 1)*8;
+    if (bytes < 2*kSliceBytes) return false;
+    i64 best_s = 0;
+    for (unsigned qa = 0; qa < A->ndim; qa++)
+    {
+        const label_type c = idx_A[qa];
+        if (A->len[qa] < 2) continue;
+        int nA = 0, nB = 0, nC = 0, qc = -1;
+        for (unsigned d = 0; d < A->ndim; d++) nA += idx_A[d] == c;
+        for (unsigned d = 0; d < B->ndim; d++) nB += idx_B[d] == c;
+        for (unsigned d = 0; d < C->ndim; d++) if (idx_C[d] == c) { nC++; qc = (int)d; }
+        if (nA != 1 || nB != 0 || nC != 1) continue;
+        i64 pa, ra, pc, rc;
+        if (!pitched(A, (int)qa, pa, ra) || !pitched(C, qc, pc, rc)) continue;
+        const i64 L = A->len[qa];
+        const i64 n = std::min<i64>({16, L, std::max<i64>(2, bytes/kSliceBytes)});
+        const i64 per = (L + n - 1)/n;
+        if (per*std::min(A->stride[qa], C->stride[qc])*8 < kMinRowBytes) continue;
+        if (A->stride[qa] <= best_s) continue;
+        best_s = A->stride[qa];
+        sl.dim_A = (int)qa; sl.dim_C = qc;
+        sl.s_A = A->stride[qa]; sl.s_C = C->stride[qc];
+        sl.pitch_A = pa; sl.pitch_C = pc; sl.rows_A = ra; sl.rows_C = rc;
+        sl.range.clear();
+        for (i64 q0 = 0; q0 < L; q0 += per) sl.range.push_back({q0, std::min(L, q0 + per)});
+    }
+    return sl.range.size() >= 2;
+}
+
 static cudaStream_t copy_stream()
 {
     static cudaStream_t s[64] = {};
     int dev = 0;
     TB_CUDA(cudaGetDevice(&dev));
     TB_CHECK(dev < 64, TB_ERR_ARG, "device index");
+    if (!s[dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
+    return s[dev];
+}
+
+static cudaStream_t copy_back_stream()
+{
+    static std::mutex mtx;
+    static cudaStream_t s[64] = {};
+    int dev = 0;
+    TB_CUDA(cudaGetDevice(&dev));
+    TB_CHECK(dev < 64, TB_ERR_ARG, "device index");
+    std::lock_guard<std::mutex> lk(mtx);
     if (!s[dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
     return s[dev];
 }
@@ -463,6 +554,7 @@ void mult_dispatch(const tblis_config* cfg,
     const bool trivial = alpha == 0.0 || v.k == 0;
     StagedOp sa, sb, sc;
     stage(sc, C, beta != 0.0, st);
+    bool sc_back_done = false;      // C copied back slab by slab already
 
     if (v.m*v.n*v.l != 0)
     {
@@ -488,12 +580,78 @@ void mult_dispatch(const tblis_config* cfg,
             TB_CHECK(method >= 1 && method <= 5, TB_ERR_ARG, "unknown contraction method");
             stage(sb, B, true, st);
             Slices sl;
-            const bool sliced = A->data && pointer_kind(A->data) == MEM_HOST &&
-                                plan_slices(A, idx_A, B, idx_B, C, idx_C, sl);
-            stage(sa, A, !sliced, st);
+            Slabs sb2;
+            const bool host_a = A->data && pointer_kind(A->data) == MEM_HOST;
+            const bool slabbed = host_a && plan_slabs(A, idx_A, B, idx_B, C, idx_C, sb2);
+            const bool sliced = host_a && !slabbed && plan_slices(A, idx_A, B, idx_B, C, idx_C, sl);
+            stage(sa, A, !sliced && !slabbed, st);
             int used = 0;
             double est = 0;
-            if (sliced)
+            if (slabbed)
+            {
+                // A's slabs in on the copy stream, each slab's contraction on
+                // st after its copy, and C's slab back on a second copy
+                // stream as soon as it is final
+                cudaStream_t cs = copy_stream(), bs = copy_back_stream();
+                cudaEvent_t ready;
+                TB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+                TB_CUDA(cudaEventRecord(ready, st));
+                TB_CUDA(cudaStreamWaitEvent(cs, ready, 0));
+                const size_t nsl = sb2.range.size();
+                std::vector<cudaEvent_t> in(nsl), done(nsl);
+                for (size_t c = 0; c < nsl; c++)
+                {
+                    const i64 q0 = sb2.range[c].first, nq = sb2.range[c].second - q0;
+                    TB_CUDA(cudaMemcpy2DAsync(static_cast<double*>(sa.dptr) + q0*sb2.s_A, (size_t)sb2.pitch_A*8,
+                                              static_cast<const double*>(A->data) + q0*sb2.s_A,
+                                              (size_t)sb2.pitch_A*8, (size_t)(nq*sb2.s_A*8), (size_t)sb2.rows_A,
+                                              cudaMemcpyHostToDevice, cs));
+                    TB_CUDA(cudaEventCreateWithFlags(&in[c], cudaEventDisableTiming));
+                    TB_CUDA(cudaEventRecord(in[c], cs));
+                }
+                std::vector<len_type> lenA(A->len, A->len + A->ndim), lenC(C->len, C->len + C->ndim);
+                for (size_t c = 0; c < nsl; c++)
+                {
+                    TB_CUDA(cudaStreamWaitEvent(st, in[c], 0));
+                    const i64 q0 = sb2.range[c].first, nq = sb2.range[c].second - q0;
+                    tblis_tensor a = *A, b = *B, cc = *C;
+                    lenA[sb2.dim_A] = nq;
+                    lenC[sb2.dim_C] = nq;
+                    a.len = lenA.data();
+                    a.data = static_cast<double*>(sa.dptr) + q0*sb2.s_A;
+                    b.data = sb.dptr;
+                    cc.len = lenC.data();
+                    cc.data = static_cast<double*>(sc.dptr) + q0*sb2.s_C;
+                    const GemmView vs = gemm_view(mult_groups(&a, idx_A, &b, idx_B, &cc, idx_C));
+                    int u = 0;
+                    double e = 0;
+                    contract_device(vs, static_cast<const double*>(a.data), static_cast<const double*>(b.data),
+                                    static_cast<double*>(cc.data), alpha, beta, method, tol, slices, st, u, e);
+                    used = std::max(used, u);
+                    est = std::max(est, e);
+                    if (sc.staged)
+                    {
+                        TB_CUDA(cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming));
+                        TB_CUDA(cudaEventRecord(done[c], st));
+                        TB_CUDA(cudaStreamWaitEvent(bs, done[c], 0));
+                        TB_CUDA(cudaMemcpy2DAsync(static_cast<double*>(C->data) + q0*sb2.s_C, (size_t)sb2.pitch_C*8,
+                                                  static_cast<const double*>(sc.dptr) + q0*sb2.s_C,
+                                                  (size_t)sb2.pitch_C*8, (size_t)(nq*sb2.s_C*8),
+                                                  (size_t)sb2.rows_C, cudaMemcpyDeviceToHost, bs));
+                        TB_CUDA(cudaEventDestroy(done[c]));
+                    }
+                }
+                for (auto e : in) cudaEventDestroy(e);
+                cudaEventDestroy(ready);
+                if (sc.staged)
+                {
+                    // C went back slab by slab: the copy-back stream finishes it
+                    TB_CUDA(cudaStreamSynchronize(bs));
+                    sc.staged = false;
+                    sc_back_done = true;
+                }
+            }
+            else if (sliced)
             {
                 // copies on the copy stream (once the buffer exists), each
                 // slice's contraction on st after its copy
@@ -560,7 +718,7 @@ void mult_dispatch(const tblis_config* cfg,
     }
 
     unstage(sc, st);
-    if (sa.staged || sb.staged || sc.staged) TB_CUDA(cudaStreamSynchronize(st));
+    if (sa.staged || sb.staged || sc.staged || sc_back_done) TB_CUDA(cudaStreamSynchronize(st));
 
     C->scalar.data.d = 1.0;
     C->scalar.type = TYPE_DOUBLE;

@@ -219,10 +219,11 @@ def test_bad_labels_raise(cuda):
 
 @pytest.mark.parametrize("method,tol", [(1, 1e-13), (2, 1e-12)])
 def test_large_host_operand_pipelined(cuda, method, tol):
-    """A host-resident A of 800 MB is copied in row chunks overlapped with the
-    contraction of the chunks already on the device; the result matches the
-    device-resident call (FP64) or meets the tolerance (Ozaki). A second
-    layout whose row chunks overlap in memory takes the one-copy path."""
+    """A host-resident A of 800 MB is copied in slabs overlapped with the
+    contraction of the slabs already on the device, and C's slabs go back as
+    they finish; the result matches the device-resident call (FP64) or meets
+    the tolerance (Ozaki). Two layouts: slabs of one contiguous block each
+    (a outermost) and slabs of 10^4 pitched rows (e, f outermost)."""
     import torch
     import tblis_b200 as tb
     v, o = 100, 8
@@ -244,3 +245,27 @@ def test_large_host_operand_pipelined(cuda, method, tol):
         assert err <= tol, (lab, err, rep)
     del dA, dB, dC
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("method, tol", [(1, 1e-14), (2, 1e-12)])
+def test_large_host_operand_k_slices(cuda, method, tol):
+    """A host-resident A (1000 x 100000, 800 MB, a fastest) whose C label
+    would give slab rows of 4000 bytes: it is copied in slices of the
+    contracted label instead, each slice accumulating into C."""
+    import torch
+    import tblis_b200 as tb
+    m, k, n = 1000, 100000, 24
+    g = torch.Generator(device=cuda)
+    g.manual_seed(8)
+    dA = torch.empty((k, m), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    dB = torch.empty((k, n), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g)
+    dC = torch.empty((n, m), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    want = dC.clone()
+    tb.mult_ex(1.0, dA, "ak", dB, "kb", 0.5, want, "ab", method=1)
+    torch.cuda.synchronize()
+    want = want.cpu()
+    hA = dA.t().cpu().pin_memory().t()
+    C = dC.t().cpu().t()
+    rep = tb.mult_ex(1.0, hA, "ak", dB.cpu(), "kb", 0.5, C, "ab", method=method, tolerance=tol)
+    err = (torch.linalg.norm(C - want) / torch.linalg.norm(want)).item()
+    assert err <= tol, (err, rep)
