@@ -43,7 +43,7 @@ def parse(argv=None):
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
     p.add_argument("--o", type=int, default=48, help="occupied extent (profiling runs use a smaller case)")
     p.add_argument("--v", type=int, default=160, help="virtual extent")
-    p.add_argument("--case", default=None, choices=["ring", "transpose"],
+    p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce"],
                    help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
     a = p.parse_args(argv)
     global O, V, FLOPS_LADDER, WORKLOAD
@@ -721,13 +721,25 @@ def single_case(torch, tb, dev, stream, args):
         def fn():
             tb.mult_ex(1.0, A, "aeim", B, "mbej", 1.0, C, "aibj", method=1)
         work, unit = 2.0 * v ** 3 * o ** 3 / 1e9, "GFLOP/s"
-    else:
+    elif args.case == "transpose":
         C = cm([v, v, o, o])
         D = torch.zeros((v, v, o, o), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
 
         def fn():
             tb.add(1.0, C, "abij", 0.0, D, "ijab")
         work, unit = 2 * C.numel() * 8 / 1e9, "GB/s"
+    elif args.case == "dot":
+        C, E = cm([v, v, o, o]), cm([v, v, o, o])
+
+        def fn():
+            tb.dot(C, "abij", E, "abij")
+        work, unit = 2 * C.numel() * 8 / 1e9, "GB/s"
+    else:
+        C = cm([v, v, o, o])
+
+        def fn():
+            tb.reduce(tb.REDUCE_NORM_2, C, "abij")
+        work, unit = C.numel() * 8 / 1e9, "GB/s"
     for _ in range(args.warmup):
         fn()
     total, _ = time_steps(torch, fn, args.steps, stream)
@@ -788,7 +800,26 @@ def extra_workloads(torch, tb, dev, stream, peaks):
     out["transpose_gbs"] = gbs
     if peaks.get("hbm_gbs"):
         out["transpose_frac_of_measured_hbm"] = gbs / peaks["hbm_gbs"]
-    del C, Cs, D, flush
+    del D
+    # dot of two 2.15 GB tensors (bytes = both reads) and a NORM_2 reduction
+    # of one (its read), L2 flushed before each timed call
+    E = cm([v, v, o, o])
+
+    def bw(fn, nbytes):
+        for _ in range(3):
+            fn()
+        pers = []
+        for _ in range(5):
+            flush.fill_(1)
+            _, p = time_steps(torch, fn, 1, stream)
+            pers.append(p[0])
+        return nbytes / (statistics.median(pers) * 1e-3) / 1e9
+    out["dot_gbs"] = bw(lambda: tb.dot(Cs, "abij", E, "abij"), 2 * Cs.numel() * 8)
+    out["reduce_norm2_gbs"] = bw(lambda: tb.reduce(tb.REDUCE_NORM_2, Cs, "abij"), Cs.numel() * 8)
+    if peaks.get("hbm_gbs"):
+        out["dot_frac_of_measured_hbm"] = out["dot_gbs"] / peaks["hbm_gbs"]
+        out["reduce_frac_of_measured_hbm"] = out["reduce_norm2_gbs"] / peaks["hbm_gbs"]
+    del C, Cs, E, flush
     torch.cuda.empty_cache()
     return out
 
