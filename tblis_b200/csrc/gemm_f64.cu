@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <type_traits>
 
 namespace tb
 {
@@ -42,6 +43,27 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
     int src_size = valid ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
                  :: "r"(saddr), "l"(gmem), "r"(src_size));
+}
+
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem)
+{
+    unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" :: "r"(saddr), "l"(gmem));
+}
+
+// two adjacent tile elements (smem 16-byte aligned): one 16-byte copy when both
+// are valid and adjacent, 16-byte aligned, in global memory; else two 8-byte
+// copies (zero-filled where not valid)
+__device__ __forceinline__ void cp_pair(double* smem, const double* X, i64 off0, bool ok0, i64 off1, bool ok1,
+                                        const double* dummy)
+{
+    if (ok0 && ok1 && off1 == off0 + 1 && (((uintptr_t)(X + off0)) & 15) == 0)
+    {
+        cp_async16(smem, X + off0);
+        return;
+    }
+    cp_async8(smem, ok0 ? X + off0 : dummy, ok0);
+    cp_async8(smem + 1, ok1 ? X + off1 : dummy, ok1);
 }
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
@@ -116,7 +138,10 @@ __host__ __device__ constexpr int tile_smem_doubles(int STAGES)
 }
 
 // one BM x BN output tile: gathered cp.async mainloop + DMMA + scatter epilogue
-template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE>
+// PA / PB: gather A / B in pairs of adjacent elements (16-byte copies where
+// the pair is adjacent and aligned in global memory), for operands whose
+// contiguous GEMM dimension mostly is; else one 8-byte copy per element
+template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, bool PA = false, bool PB = false>
 __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* sAm, i64* sBn, i64* sCm, i64* sCn)
 {
     constexpr int NT = (BM/WM)*(BN/WN)*32;
@@ -177,27 +202,93 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
 
         const i64 kt_count = (k_end - k_begin + BK - 1)/BK;
 
-        // Per-thread gather geometry, fixed for the whole tile: in the
-        // rows-contiguous layout (mode 0) a thread always copies the same row
-        // at k = k0 + j*KSTEP; in the k-contiguous layout (mode 1) the same k
-        // of rows r0 + j*RSTEP. Row offsets are read from shared memory once
-        // per tile, k offsets once per stage (stride arithmetic when the
-        // 16-block of k is regular).
-        constexpr int AJ = BK*BM/NT, BJ = BK*BN/NT;
-        static_assert(NT % BM == 0 && NT % BN == 0 && NT % BK == 0, "gather geometry");
-        i64 a_ro[AMODE == 0 ? 1 : AJ], b_ro[BMODE == 0 ? 1 : BJ];
-        if (AMODE == 0) a_ro[0] = sAm[tid % BM];
-        else
+        // Per-thread gather geometry, fixed for the whole tile. In the
+        // rows-contiguous layout (mode 0) a thread copies the same row (or
+        // pair of rows) at k = k0 + j*KSTEP; in the k-contiguous layout (mode
+        // 1) the same k (or pair of k, even and odd) of rows r0 + j*RSTEP.
+        // Row offsets are read from shared memory once per tile, k offsets
+        // once per stage (stride arithmetic when the 16-block of k is regular).
+        auto gather = [&](auto pairs, auto mode, auto rows, const i64* sX, const double* X, double* Xs,
+                          const i64* scat, const KInfo& ki, i64 k0, int kvalid, const i64* ro)
         {
-            #pragma unroll
-            for (int j = 0; j < (AMODE == 0 ? 1 : AJ); j++) a_ro[j] = sAm[tid/BK + j*(NT/BK)];
-        }
-        if (BMODE == 0) b_ro[0] = sBn[tid % BN];
-        else
+            constexpr bool PR = decltype(pairs)::value;
+            constexpr int MD = decltype(mode)::value, R = decltype(rows)::value;
+            constexpr int W = PR ? 2 : 1;                 // elements per copy slot
+            constexpr int J = BK*R/(W*NT);
+            using TX = Tile<R, MD>;
+            if (MD == 0)
+            {
+                const int r = W*(tid % (R/W)), kl0 = tid/(R/W);
+                constexpr int KS = NT/(R/W);
+                #pragma unroll
+                for (int j = 0; j < J; j++)
+                {
+                    const int kl = kl0 + j*KS;
+                    const bool kok = kl < kvalid;
+                    const i64 ko = kok ? koff(scat, ki, k0, kl) : 0;
+                    if (PR)
+                        cp_pair(Xs + TX::idx(r, kl), X, ro[0] + ko, kok && ro[0] >= 0, ro[1] + ko, kok && ro[1] >= 0,
+                                X);
+                    else
+                    {
+                        const bool ok = kok && ro[0] >= 0;
+                        cp_async8(Xs + TX::idx(r, kl), ok ? X + ro[0] + ko : X, ok);
+                    }
+                }
+            }
+            else
+            {
+                const int kl = W*(tid % (BK/W)), r0 = tid/(BK/W);
+                constexpr int RS = NT/(BK/W);
+                const bool k0ok = kl < kvalid, k1ok = PR && kl + 1 < kvalid;
+                const i64 ko0 = k0ok ? koff(scat, ki, k0, kl) : 0;
+                const i64 ko1 = k1ok ? koff(scat, ki, k0, kl + 1) : 0;
+                #pragma unroll
+                for (int j = 0; j < J; j++)
+                {
+                    const i64 o = ro[j];
+                    if (PR)
+                        cp_pair(Xs + TX::idx(r0 + j*RS, kl), X, o + ko0, k0ok && o >= 0, o + ko1, k1ok && o >= 0, X);
+                    else
+                    {
+                        const bool ok = k0ok && o >= 0;
+                        cp_async8(Xs + TX::idx(r0 + j*RS, kl), ok ? X + o + ko0 : X, ok);
+                    }
+                }
+            }
+        };
+        // the row offsets a thread copies, per the scheme above
+        auto rows_of = [&](auto pairs, auto mode, auto rows, const i64* sX, i64* ro)
         {
-            #pragma unroll
-            for (int j = 0; j < (BMODE == 0 ? 1 : BJ); j++) b_ro[j] = sBn[tid/BK + j*(NT/BK)];
-        }
+            constexpr bool PR = decltype(pairs)::value;
+            constexpr int MD = decltype(mode)::value, R = decltype(rows)::value;
+            constexpr int W = PR ? 2 : 1;
+            constexpr int J = BK*R/(W*NT);
+            if (MD == 0)
+            {
+                const int r = W*(tid % (R/W));
+                ro[0] = sX[r];
+                if (PR) ro[1] = sX[r + 1];
+            }
+            else
+            {
+                #pragma unroll
+                for (int j = 0; j < J; j++) ro[j] = sX[tid/(BK/W) + j*(NT/(BK/W))];
+            }
+        };
+        using PAc = std::integral_constant<bool, PA>;
+        using PBc = std::integral_constant<bool, PB>;
+        using AMc = std::integral_constant<int, AMODE>;
+        using BMc = std::integral_constant<int, BMODE>;
+        using BMr = std::integral_constant<int, BM>;
+        using BNr = std::integral_constant<int, BN>;
+        static_assert(NT % (BM/2) == 0 && NT % (BN/2) == 0 && NT % BM == 0 && NT % BN == 0 && NT % BK == 0 &&
+                      BK*BM % (2*NT) == 0 && BK*BN % (2*NT) == 0, "gather geometry");
+        constexpr int ANR = AMODE == 0 ? 2 : BK*BM/((PA ? 2 : 1)*NT);
+        constexpr int BNR = BMODE == 0 ? 2 : BK*BN/((PB ? 2 : 1)*NT);
+        i64 a_ro[ANR], b_ro[BNR];
+        rows_of(PAc(), AMc(), BMr(), sAm, a_ro);
+        rows_of(PBc(), BMc(), BNr(), sBn, b_ro);
 
         auto load_tile = [&](int stage, i64 kt, const KInfo& ka, const KInfo& kb)
         {
@@ -205,62 +296,8 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
             double* Bs = As + TA::SIZE;
             const i64 k0 = k_begin + kt*BK;
             const int kvalid = (int)min((i64)BK, k_end - k0);
-            if (AMODE == 0)
-            {
-                const int ml = tid % BM, kl0 = tid / BM;
-                constexpr int KS = NT/BM;
-                const i64 ro = a_ro[0];
-                #pragma unroll
-                for (int j = 0; j < AJ; j++)
-                {
-                    const int kl = kl0 + j*KS;
-                    const bool ok = ro >= 0 && kl < kvalid;
-                    const i64 ko = ok ? koff(a_k, ka, k0, kl) : 0;
-                    cp_async8(As + TA::idx(ml, kl), ok ? A + ro + ko : p.A, ok);
-                }
-            }
-            else
-            {
-                const int kl = tid % BK, ml0 = tid / BK;
-                constexpr int RS = NT/BK;
-                const bool kok = kl < kvalid;
-                const i64 ko = kok ? koff(a_k, ka, k0, kl) : 0;
-                #pragma unroll
-                for (int j = 0; j < AJ; j++)
-                {
-                    const i64 ro = a_ro[AMODE == 0 ? 0 : j];
-                    const bool ok = kok && ro >= 0;
-                    cp_async8(As + TA::idx(ml0 + j*RS, kl), ok ? A + ro + ko : p.A, ok);
-                }
-            }
-            if (BMODE == 0)
-            {
-                const int nl = tid % BN, kl0 = tid / BN;
-                constexpr int KS = NT/BN;
-                const i64 co = b_ro[0];
-                #pragma unroll
-                for (int j = 0; j < BJ; j++)
-                {
-                    const int kl = kl0 + j*KS;
-                    const bool ok = co >= 0 && kl < kvalid;
-                    const i64 ko = ok ? koff(b_k, kb, k0, kl) : 0;
-                    cp_async8(Bs + TB::idx(nl, kl), ok ? B + co + ko : p.B, ok);
-                }
-            }
-            else
-            {
-                const int kl = tid % BK, nl0 = tid / BK;
-                constexpr int RS = NT/BK;
-                const bool kok = kl < kvalid;
-                const i64 ko = kok ? koff(b_k, kb, k0, kl) : 0;
-                #pragma unroll
-                for (int j = 0; j < BJ; j++)
-                {
-                    const i64 co = b_ro[BMODE == 0 ? 0 : j];
-                    const bool ok = kok && co >= 0;
-                    cp_async8(Bs + TB::idx(nl0 + j*RS, kl), ok ? B + co + ko : p.B, ok);
-                }
-            }
+            gather(PAc(), AMc(), BMr(), sAm, A, As, a_k, ka, k0, kvalid, a_ro);
+            gather(PBc(), BMc(), BNr(), sBn, B, Bs, b_k, kb, k0, kvalid, b_ro);
         };
 
         #pragma unroll
@@ -355,7 +392,7 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
     __syncthreads();
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, int MINB>
+template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, bool PA, bool PB, int MINB>
 __global__ void __launch_bounds__((BM/WM)*(BN/WN)*32, MINB)
 gemm_f64_kernel(const GemmF64Args p)
 {
@@ -393,7 +430,7 @@ gemm_f64_kernel(const GemmF64Args p)
     t.W = p.splits > 1 ? p.partial + ((i64)split*p.L + l)*p.M*p.N : nullptr;
     t.nseg = 0;
     t.segs = nullptr;
-    tile_body<BM, BN, WM, WN, STAGES, AMODE, BMODE>(t, smem, sAm, sBn, sCm, sCn);
+    tile_body<BM, BN, WM, WN, STAGES, AMODE, BMODE, PA, PB>(t, smem, sAm, sBn, sCm, sCn);
 }
 
 // Persistent grouped kernel: every CTA walks the global tile list (all
@@ -485,7 +522,9 @@ struct Variant
     void (*grouped)(const GroupDesc*, const i64*, int, i64, unsigned long long*, cudaStream_t);
 };
 
-template <int BM_, int BN_, int WM, int WN, int STAGES, int MINB>
+// PAIRS: the dense launch may gather in pairs (the default tile shape only,
+// to bound the number of kernel instances)
+template <int BM_, int BN_, int WM, int WN, int STAGES, int MINB, bool PAIRS = false>
 struct Config
 {
     static constexpr int NT = (BM_/WM)*(BN_/WN)*32;
@@ -495,10 +534,10 @@ struct Config
         size_t b = bmd == 0 ? BK*(BN_ + PAD) : BN_*(BK + PAD);
         return (size_t)STAGES*(a + b)*sizeof(double) + (2*BM_ + 2*BN_)*sizeof(i64);
     }
-    template <int AM, int BMd>
+    template <int AM, int BMd, bool PA, bool PB>
     static void go(const GemmF64Args& a, dim3 grid, cudaStream_t s)
     {
-        auto kern = gemm_f64_kernel<BM_, BN_, WM, WN, STAGES, AM, BMd, MINB>;
+        auto kern = gemm_f64_kernel<BM_, BN_, WM, WN, STAGES, AM, BMd, PA, PB, MINB>;
         const size_t bytes = smem_bytes(AM, BMd);
         TB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         TimedLaunch t("gemm_f64_kernel", s);
@@ -521,15 +560,27 @@ struct Config
         kern<<<(unsigned)grid, NT, bytes, s>>>(g, tb, ngroups, total, ctr);
         check_launch("gemm_f64_grouped_kernel");
     }
-    static void launch(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
+    template <bool PA, bool PB>
+    static void go_modes(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
     {
         switch (am*2 + bmd)
         {
-            case 0: go<0,0>(a, grid, s); break;
-            case 1: go<0,1>(a, grid, s); break;
-            case 2: go<1,0>(a, grid, s); break;
-            default: go<1,1>(a, grid, s); break;
+            case 0: go<0, 0, PA, PB>(a, grid, s); break;
+            case 1: go<0, 1, PA, PB>(a, grid, s); break;
+            case 2: go<1, 0, PA, PB>(a, grid, s); break;
+            default: go<1, 1, PA, PB>(a, grid, s); break;
         }
+    }
+    static void launch(const GemmF64Args& a, dim3 grid, cudaStream_t s, int am, int bmd)
+    {
+        const int pr = PAIRS ? (a.pair_a ? 2 : 0) + (a.pair_b ? 1 : 0) : 0;
+        if constexpr (PAIRS)
+        {
+            if (pr == 3) { go_modes<true, true>(a, grid, s, am, bmd); return; }
+            if (pr == 2) { go_modes<true, false>(a, grid, s, am, bmd); return; }
+            if (pr == 1) { go_modes<false, true>(a, grid, s, am, bmd); return; }
+        }
+        go_modes<false, false>(a, grid, s, am, bmd);
     }
 };
 
@@ -538,7 +589,7 @@ const Variant kVariants[] = {
     {128, 128, Config<128, 128, 64, 32, 4, 1>::launch, Config<128, 128, 64, 32, 4, 1>::grouped},  // 1
     {64, 128, Config<64, 128, 32, 64, 3, 2>::launch, Config<64, 128, 32, 64, 3, 2>::grouped},     // 2
     {128, 64, Config<128, 64, 64, 32, 3, 2>::launch, Config<128, 64, 64, 32, 3, 2>::grouped},     // 3
-    {64, 64, Config<64, 64, 32, 32, 3, 3>::launch, Config<64, 64, 32, 32, 3, 3>::grouped},        // 4
+    {64, 64, Config<64, 64, 32, 32, 3, 3, true>::launch, Config<64, 64, 32, 32, 3, 3, true>::grouped},  // 4
 };
 constexpr int kNumVariants = sizeof(kVariants)/sizeof(kVariants[0]);
 

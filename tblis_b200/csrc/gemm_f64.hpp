@@ -22,6 +22,7 @@ struct GemmF64Args
     i64 k_per_split;         // set by the launcher
     double* partial;         // split-K workspace (splits*L*M*N doubles)
     int variant;             // tile configuration, 0 = automatic
+    int pair_a, pair_b;      // gather the operand's contiguous dimension in pairs (16-byte copies)
 };
 
 // one K segment of a grouped GEMM: the rows of A / columns of B it reads

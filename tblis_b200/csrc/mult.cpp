@@ -247,6 +247,10 @@ static void contract_device(const GemmView& v, const double* A, const double* B,
     GemmF64Args a = {};
     a.A = A; a.B = B; a.C = C;
     a.a_m = tab->a_m; a.a_k = tab->a_k; a.b_k = tab->b_k; a.b_n = tab->b_n;
+    // pairs of 16-byte copies where the layout gives them (the kernel checks
+    // every pair; this only picks the gather code)
+    a.pair_a = tab->a_pairs[v.amode] && ((uintptr_t)A & 15) == 0;
+    a.pair_b = tab->b_pairs[v.bmode] && ((uintptr_t)B & 15) == 0;
     a.c_m = tab->c_m; a.c_n = tab->c_n; a.a_l = tab->a_l; a.b_l = tab->b_l; a.c_l = tab->c_l;
     a.a_kbs = tab->a_kbs; a.b_kbs = tab->b_kbs;
     a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;

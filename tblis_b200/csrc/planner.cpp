@@ -412,6 +412,17 @@ static i64 affine_step(const i64* t, i64 n)
     return s;
 }
 
+// fraction of index pairs (2i, 2i+1) adjacent in memory with an even first
+// offset, and fraction of even offsets
+static void pair_stats(const i64* t, i64 n, double& adj, double& even)
+{
+    i64 a = 0, e = 0;
+    for (i64 i = 0; i + 1 < n; i += 2) a += t[i + 1] == t[i] + 1 && (t[i] & 1) == 0;
+    for (i64 i = 0; i < n; i++) e += (t[i] & 1) == 0;
+    adj = n > 1 ? (double)a/(double)(n/2) : 0.0;
+    even = n > 0 ? (double)e/(double)n : 0.0;
+}
+
 std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 BK,
                                         cudaStream_t stream)
 {
@@ -460,6 +471,18 @@ std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 B
     auto t = std::make_shared<GemmTables>();
     t->a_m_step = affine_step(a_m, v.m); t->a_k_step = affine_step(a_k, v.k);
     t->b_n_step = affine_step(b_n, v.n); t->b_k_step = affine_step(b_k, v.k);
+    {
+        double am_adj, am_even, ak_adj, ak_even, bn_adj, bn_even, bk_adj, bk_even, l_adj, l_even_a, l_even_b;
+        pair_stats(a_m, v.m, am_adj, am_even); pair_stats(a_k, v.k, ak_adj, ak_even);
+        pair_stats(b_n, v.n, bn_adj, bn_even); pair_stats(b_k, v.k, bk_adj, bk_even);
+        pair_stats(a_l, v.l, l_adj, l_even_a); pair_stats(b_l, v.l, l_adj, l_even_b);
+        const double q = 0.9;
+        const bool la = l_even_a == 1.0, lb = l_even_b == 1.0;
+        t->a_pairs[0] = la && am_adj >= q && ak_even >= q;
+        t->a_pairs[1] = la && ak_adj >= q && am_even >= q;
+        t->b_pairs[0] = lb && bn_adj >= q && bk_even >= q;
+        t->b_pairs[1] = lb && bk_adj >= q && bn_even >= q;
+    }
     t->bytes = n_total*sizeof(i64);
     TB_CUDA(cudaMalloc(&t->dev, t->bytes));
     TB_CUDA(cudaMemcpyAsync(t->dev, host.data(), t->bytes, cudaMemcpyHostToDevice, stream));

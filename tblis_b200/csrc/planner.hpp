@@ -69,6 +69,11 @@ struct GemmTables
     i64 *a_m, *c_m, *a_k, *b_k, *b_n, *c_n, *a_l, *b_l, *c_l, *a_kbs, *b_kbs;
     // s where the table is i*s for every i (a single stride), else -1
     i64 a_m_step = -1, a_k_step = -1, b_n_step = -1, b_k_step = -1;
+    // per gather mode (0: rows contiguous, 1: k contiguous): whether nearly
+    // all pairs of adjacent elements of the contiguous dimension are adjacent
+    // and 16-byte aligned in memory (offsets even), so that the FP64 kernel
+    // gathers A / B in pairs
+    bool a_pairs[2] = {false, false}, b_pairs[2] = {false, false};
     size_t bytes = 0;
     ~GemmTables();
 };
