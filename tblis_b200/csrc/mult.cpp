@@ -199,27 +199,22 @@ static bool plan_slabs(const tblis_tensor* A, const label_type* idx_A, const tbl
     return sl.range.size() >= 2;
 }
 
-static cudaStream_t copy_stream()
-{
-    static cudaStream_t s[64] = {};
-    int dev = 0;
-    TB_CUDA(cudaGetDevice(&dev));
-    TB_CHECK(dev < 64, TB_ERR_ARG, "device index");
-    if (!s[dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
-    return s[dev];
-}
-
-static cudaStream_t copy_back_stream()
+// per-device non-blocking streams for the host copies of the pipelined
+// paths: 0 host-to-device, 1 device-to-host (created on first use)
+static cudaStream_t aux_stream(int which)
 {
     static std::mutex mtx;
-    static cudaStream_t s[64] = {};
+    static cudaStream_t s[2][64] = {};
     int dev = 0;
     TB_CUDA(cudaGetDevice(&dev));
     TB_CHECK(dev < 64, TB_ERR_ARG, "device index");
     std::lock_guard<std::mutex> lk(mtx);
-    if (!s[dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking));
-    return s[dev];
+    if (!s[which][dev]) TB_CUDA(cudaStreamCreateWithFlags(&s[which][dev], cudaStreamNonBlocking));
+    return s[which][dev];
 }
+
+static cudaStream_t copy_stream() { return aux_stream(0); }
+static cudaStream_t copy_back_stream() { return aux_stream(1); }
 
 static void unstage(StagedOp& o, cudaStream_t s)
 {
