@@ -392,9 +392,18 @@ static std::string dpd_key(const DpdTensor& A, const char* ia, const DpdTensor& 
     return k;
 }
 
-void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
-              DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
-              DpdMultReport* rep, bool reference_irrep_check)
+namespace
+{
+
+// the label groups of a DPD contraction and whether its irreps rule it out
+struct DpdLabels
+{
+    std::string ABC, AB, AC, BC;
+    bool mismatch = false;
+};
+
+DpdLabels dpd_labels(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                     const DpdTensor& C, const char* idx_C, bool reference_irrep_check)
 {
     const unsigned nirrep = A.lay.nirrep;
     TB_CHECK(B.lay.nirrep == nirrep && C.lay.nirrep == nirrep, TB_ERR_ARG, "DPD: nirrep differs");
@@ -437,31 +446,21 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
     const unsigned irrA = A.lay.irrep, irrB = B.lay.irrep, irrC = C.lay.irrep;
     const bool mismatch = reference_irrep_check ? (irrA ^ (unsigned)(irrB != irrC)) != 0
                                                 : (irrA ^ irrB) != irrC;
-    const i64 ctotal = C.lay.total();
-    if (alpha == 0.0 || (ABC.empty() && mismatch))
-    {
-        if (beta == 1.0 || ctotal == 0) return;
-        if (C.lay.is_explicit())
-        {
-            // a view's blocks need not fill [0, extent): scale block by block
-            C.lay.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
-                                     const std::vector<i64>& bs, i64 off)
-            {
-                TB_CHECK(C.lay.ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "DPD: too many dimensions");
-                Strided s;
-                s.ndim = (int)C.lay.ndim;
-                for (unsigned d = 0; d < C.lay.ndim; d++) { s.len[d] = bl[d]; s.stride[d] = bs[d]; }
-                if (beta == 0.0) l1_set<double>(C.data + off, s, 0.0, st);
-                else l1_scale<double>(C.data + off, s, beta, st);
-            });
-            return;
-        }
-        Strided s; s.ndim = 1; s.len[0] = ctotal; s.stride[0] = 1;
-        if (beta == 0.0) l1_set<double>(C.data, s, 0.0, st);
-        else l1_scale<double>(C.data, s, beta, st);
-        return;
-    }
-    TB_CHECK(ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
+    DpdLabels r;
+    r.ABC = ABC; r.AB = AB; r.AC = AC; r.BC = BC;
+    r.mismatch = mismatch;
+    return r;
+}
+
+// the cached grouped plan of a DPD contraction without batch labels
+std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                                      const DpdTensor& C, const char* idx_C, const DpdLabels& lab, cudaStream_t st)
+{
+    const unsigned nirrep = A.lay.nirrep;
+    const std::string iA(idx_A, A.lay.ndim), iB(idx_B, B.lay.ndim), iC(idx_C, C.lay.ndim);
+    auto pos = [](const std::string& s, char c) { return (unsigned)s.find(c); };
+    const unsigned irrA = A.lay.irrep, irrB = B.lay.irrep;
+    std::string AB = lab.AB, AC = lab.AC, BC = lab.BC;
 
     // label order inside each group: stride order of the dense-equivalent
     // layout (src/internal/3t/dpd/mult.cxx:256-270), C then A (AC), C then B
@@ -594,6 +593,42 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
         p->finalize(st);
         plan = grouped_plan_cache().insert(key, p);
     }
+    return plan;
+}
+
+} // namespace
+
+void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+              DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
+              DpdMultReport* rep, bool reference_irrep_check)
+{
+    const DpdLabels lab = dpd_labels(A, idx_A, B, idx_B, C, idx_C, reference_irrep_check);
+    const i64 ctotal = C.lay.total();
+    if (alpha == 0.0 || (lab.ABC.empty() && lab.mismatch))
+    {
+        if (beta == 1.0 || ctotal == 0) return;
+        if (C.lay.is_explicit())
+        {
+            // a view's blocks need not fill [0, extent): scale block by block
+            C.lay.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
+                                     const std::vector<i64>& bs, i64 off)
+            {
+                TB_CHECK(C.lay.ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "DPD: too many dimensions");
+                Strided s;
+                s.ndim = (int)C.lay.ndim;
+                for (unsigned d = 0; d < C.lay.ndim; d++) { s.len[d] = bl[d]; s.stride[d] = bs[d]; }
+                if (beta == 0.0) l1_set<double>(C.data + off, s, 0.0, st);
+                else l1_scale<double>(C.data + off, s, beta, st);
+            });
+            return;
+        }
+        Strided s; s.ndim = 1; s.len[0] = ctotal; s.stride[0] = 1;
+        if (beta == 0.0) l1_set<double>(C.data, s, 0.0, st);
+        else l1_scale<double>(C.data, s, beta, st);
+        return;
+    }
+    TB_CHECK(lab.ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
+    const std::shared_ptr<GroupedPlan> plan = dpd_plan(A, idx_A, B, idx_B, C, idx_C, lab, st);
 
     const double* ptrs[3] = {A.data, B.data, C.data};
     // C patches without contracted blocks: beta scaling (rare; irreps with K_h == 0)
@@ -608,6 +643,123 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
     }
 }
 
+int dpd_mult_terms(const std::vector<DpdTerm>& terms, cudaStream_t st, DpdMultReport* rep,
+                   bool reference_irrep_check)
+{
+    if (rep) *rep = DpdMultReport();
+    std::vector<std::shared_ptr<GroupedPlan>> plans(terms.size());
+    std::vector<int> wave(terms.size(), -1);
+    std::map<i64, int> seen;
+    int nwave = 0;
+    for (size_t t = 0; t < terms.size(); t++)
+    {
+        const DpdTerm& x = terms[t];
+        const DpdLabels lab = dpd_labels(*x.a, x.ia, *x.b, x.ib, *x.c, x.ic, reference_irrep_check);
+        if (x.alpha == 0.0 || (lab.ABC.empty() && lab.mismatch)) continue;
+        TB_CHECK(lab.ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
+        plans[t] = dpd_plan(*x.a, x.ia, *x.b, x.ib, *x.c, x.ic, lab, st);
+        // beta = 1: C patches without contracted blocks stay as they are
+        if (plans[t]->groups.empty()) continue;
+        wave[t] = seen[x.c_key]++;
+        nwave = std::max(nwave, wave[t] + 1);
+        if (rep)
+        {
+            rep->groups += (int)plans[t]->groups.size();
+            rep->flops += plans[t]->flops;
+        }
+    }
+    for (int w = 0; w < nwave; w++)
+    {
+        std::vector<size_t> mem;
+        for (size_t t = 0; t < terms.size(); t++)
+            if (wave[t] == w) mem.push_back(t);
+        std::vector<const double*> ptrs;
+        std::vector<double> alphas, betas(mem.size(), 1.0);
+        for (size_t t : mem)
+        {
+            ptrs.push_back(terms[t].a->data);
+            ptrs.push_back(terms[t].b->data);
+            ptrs.push_back(terms[t].c->data);
+            alphas.push_back(terms[t].alpha);
+        }
+        std::shared_ptr<GroupedPlan> plan;
+        if (mem.size() == 1) plan = plans[mem[0]];
+        else
+        {
+            // the merged plan is keyed by its members' plans, which it keeps
+            // alive, so a key never names a freed and reused plan
+            std::string key = "dpd-terms:";
+            for (size_t t : mem)
+            {
+                const GroupedPlan* q = plans[t].get();
+                key.append(reinterpret_cast<const char*>(&q), sizeof(q));
+            }
+            plan = grouped_plan_cache().find(key);
+            if (!plan)
+            {
+                auto p = std::make_shared<GroupedPlan>();
+                for (size_t i = 0; i < mem.size(); i++)
+                {
+                    const std::shared_ptr<GroupedPlan>& q = plans[mem[i]];
+                    p->parts.push_back(q);
+                    for (const GroupTables& g : q->groups)
+                    {
+                        GroupTables h = g;
+                        h.a_slot = 3*(int)i + g.a_slot;
+                        h.b_slot = 3*(int)i + g.b_slot;
+                        h.c_slot = 3*(int)i + g.c_slot;
+                        h.sidx = (int)i;
+                        p->groups.push_back(std::move(h));
+                    }
+                    p->flops += q->flops;
+                }
+                p->nslots = 3*(int)mem.size();
+                p->finalize(st);
+                plan = grouped_plan_cache().insert(key, p);
+            }
+        }
+        grouped_run(*plan, ptrs.data(), alphas.data(), betas.data(), st);
+        if (rep) rep->variant = plan->variant;
+    }
+    return nwave;
+}
+
+void dpd_terms_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
+                 const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, i64 c_key,
+                 std::deque<DpdTensor>& store, std::vector<DpdTerm>& terms)
+{
+    if (alpha == 0.0) return;
+    auto part = [&](const DpdLayout& l, const double* x, i64 shift)
+    {
+        store.emplace_back();
+        store.back().lay = scaled_layout(l, 2, shift);
+        store.back().data = const_cast<double*>(x);
+        return &store.back();
+    };
+    const DpdTensor *ar = part(la, a, 0), *ai = part(la, a, 1), *br = part(lb, b, 0), *bi = part(lb, b, 1);
+    const DpdTensor *cr = part(lc, c, 0), *ci = part(lc, c, 1);
+    const double alr = alpha.real(), ali = alpha.imag();
+    // (A part, B part, coefficient into Re C, coefficient into Im C)
+    struct Term { const DpdTensor* x; const DpdTensor* y; double cr, ci; };
+    const Term four[4] = {
+        {ar, br, alr, ali},         // Ar Br
+        {ai, bi, -alr, -ali},       // Ai Bi
+        {ar, bi, -ali, alr},        // Ar Bi
+        {ai, br, -ali, alr},        // Ai Br
+    };
+    for (const Term& t : four)
+        for (int p = 0; p < 2; p++)
+        {
+            DpdTerm d;
+            d.a = t.x; d.ia = idx_A;
+            d.b = t.y; d.ib = idx_B;
+            d.c = p == 0 ? cr : ci; d.ic = idx_C;
+            d.alpha = p == 0 ? t.cr : t.ci;
+            d.c_key = 2*c_key + p;
+            if (d.alpha != 0.0) terms.push_back(d);
+        }
+}
+
 void dpd_mult_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
                 const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, zd beta,
                 cudaStream_t st, DpdMultReport* rep, bool reference_irrep_check)
@@ -618,36 +770,12 @@ void dpd_mult_z(const DpdLayout& la, const double* a, const char* idx_A, const D
     else if (beta != 1.0) dpd_unary_dev_t(TYPE_DCOMPLEX, 0, 0.0, beta, lc, c, iC);
     if (rep) *rep = DpdMultReport();
     if (alpha == 0.0) return;
-    DpdTensor ar, ai, br, bi, cr, ci;
-    ar.lay = scaled_layout(la, 2, 0); ai.lay = scaled_layout(la, 2, 1);
-    br.lay = scaled_layout(lb, 2, 0); bi.lay = scaled_layout(lb, 2, 1);
-    cr.lay = scaled_layout(lc, 2, 0); ci.lay = scaled_layout(lc, 2, 1);
-    ar.data = ai.data = const_cast<double*>(a);
-    br.data = bi.data = const_cast<double*>(b);
-    cr.data = ci.data = c;
-    const double alr = alpha.real(), ali = alpha.imag();
-    // (A part, B part, coefficient into Re C, coefficient into Im C)
-    struct Term { const DpdTensor* x; const DpdTensor* y; double cr, ci; };
-    const Term terms[4] = {
-        {&ar, &br, alr, ali},       // Ar Br
-        {&ai, &bi, -alr, -ali},     // Ai Bi
-        {&ar, &bi, -ali, alr},      // Ar Bi
-        {&ai, &br, -ali, alr},      // Ai Br
-    };
-    for (const Term& t : terms)
-        for (int part = 0; part < 2; part++)
-        {
-            const double coef = part == 0 ? t.cr : t.ci;
-            if (coef == 0.0) continue;
-            DpdMultReport r;
-            dpd_mult(*t.x, idx_A, *t.y, idx_B, part == 0 ? cr : ci, idx_C, coef, 1.0, st, &r, reference_irrep_check);
-            if (rep)
-            {
-                rep->flops += r.flops;
-                rep->groups += r.groups;
-                rep->variant = r.variant;
-            }
-        }
+    // the real and imaginary parts of C are disjoint, so each pair of terms
+    // that write them shares a launch
+    std::deque<DpdTensor> store;
+    std::vector<DpdTerm> terms;
+    dpd_terms_z(la, a, idx_A, lb, b, idx_B, lc, c, idx_C, alpha, 0, store, terms);
+    dpd_mult_terms(terms, st, rep, reference_irrep_check);
 }
 
 } // namespace tb

@@ -6,6 +6,7 @@
 #include "planner.hpp"
 
 #include <complex>
+#include <deque>
 #include <string>
 
 namespace tb
@@ -83,6 +84,27 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
               DpdMultReport* rep, bool reference_irrep_check = true);
 
+// One real term C += alpha*A*B (beta = 1) of a sequence of DPD contractions.
+// Terms whose C storage may overlap carry the same c_key.
+struct DpdTerm
+{
+    const DpdTensor* a = nullptr;
+    const char* ia = nullptr;
+    const DpdTensor* b = nullptr;
+    const char* ib = nullptr;
+    const DpdTensor* c = nullptr;
+    const char* ic = nullptr;
+    double alpha = 1.0;
+    i64 c_key = 0;
+};
+
+// Runs the terms with the result of running them one after another: the k-th
+// contributing term on each c_key goes into the k-th grouped launch, so terms
+// on distinct C storage share a launch and terms on the same storage keep
+// their order. rep (if given) sums groups and flops; returns the launches.
+int dpd_mult_terms(const std::vector<DpdTerm>& terms, cudaStream_t st, DpdMultReport* rep,
+                   bool reference_irrep_check = true);
+
 // Element types of the DPD operations: float, double, scomplex, dcomplex
 // (type_t); scalars of any type travel as complex<double>.
 using zd = std::complex<double>;
@@ -108,6 +130,14 @@ DpdLayout scaled_layout(const DpdLayout& X, i64 scale, i64 shift);
 void dpd_mult_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
                 const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, zd beta,
                 cudaStream_t st, DpdMultReport* rep, bool reference_irrep_check = true);
+
+// the real terms of the complex contraction C += alpha*A*B on dcomplex
+// storage (4M, beta = 1), appended to `terms` with the real and imaginary
+// parts of C under the keys 2*c_key and 2*c_key + 1; `store` holds the part
+// tensors the terms point to
+void dpd_terms_z(const DpdLayout& la, const double* a, const char* idx_A, const DpdLayout& lb, const double* b,
+                 const char* idx_B, const DpdLayout& lc, double* c, const char* idx_C, zd alpha, i64 c_key,
+                 std::deque<DpdTensor>& store, std::vector<DpdTerm>& terms);
 
 // level-1 operations on device-resident DPD storage of element type `type`
 // (dpd_level1.cpp): B = alpha*op(A) + beta*op(B) (trace / replicate per

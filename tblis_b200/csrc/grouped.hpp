@@ -56,6 +56,7 @@ struct GroupedPlan
     cudaEvent_t last_use = nullptr;
     i64 c_lo = 0, c_hi = -1;                  // extent of C offsets (for the tuner's scratch)
     std::string histogram;
+    std::vector<std::shared_ptr<GroupedPlan>> parts;   // plans whose groups this one merges (kept alive)
 
     void finalize(cudaStream_t st);
     ~GroupedPlan();

@@ -18,8 +18,11 @@
 // with the selected slices folded into per-block offsets (an explicit block
 // table), so no dense copy of any tensor is made; every triple runs through
 // the grouped persistent FP64 kernel with the factor-weighted alpha and
-// beta = 1 on top of the initial scaling. Element types: double; dcomplex as
-// four real contractions of the parts (dpd_mult_z); float and scomplex
+// beta = 1 on top of the initial scaling. Triples on distinct entries of C
+// share one grouped launch: the k-th triple of every entry of C runs in the
+// k-th launch, so each entry accumulates its triples in the sequential order.
+// Element types: double; dcomplex as four real contractions of the parts
+// (dpd_terms_z); float and scomplex
 // widened to double / dcomplex for the contraction and rounded back; the
 // level-1 operations run on every type directly.
 #include "common.hpp"
@@ -370,6 +373,19 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
             v = T[t]->index(e, slot);
             return true;
         };
+        // terms on distinct entries of C share launches unless entries overlap
+        bool c_overlap = false;
+        {
+            std::vector<std::pair<const char*, const char*>> span;
+            const i64 bytes = C.dense.total()*(i64)C.esz;
+            for (i64 e = 0; e < C.nidx; e++)
+                if (bytes > 0) span.push_back({C.data[e], C.data[e] + bytes});
+            std::sort(span.begin(), span.end());
+            for (size_t i = 1; i < span.size(); i++)
+                if (span[i].first < span[i - 1].second) c_overlap = true;
+        }
+        std::deque<DpdTensor> store;
+        std::vector<DpdTerm> terms;
         // entries of A and B keyed by the values of the fixed labels they index
         for (i64 ec = 0; ec < C.nidx; ec++)
         {
@@ -414,17 +430,31 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
                         continue;
                     const zd w = alpha*A.factor[ea]*B.factor[eb]*C.factor[ec];
                     if (w == 0.0) continue;
-                    DpdMultReport r;
+                    const i64 key = c_overlap ? 0 : ec;
                     if (wtype == TYPE_DOUBLE)
-                        dpd_mult(a, lA.c_str(), b, lB.c_str(), c, lC.c_str(), w.real(), 1.0, st, &r, false);
+                    {
+                        store.push_back(std::move(a)); const DpdTensor* pa = &store.back();
+                        store.push_back(std::move(b)); const DpdTensor* pb = &store.back();
+                        store.push_back(std::move(c)); const DpdTensor* pc = &store.back();
+                        DpdTerm t;
+                        t.a = pa; t.ia = lA.c_str();
+                        t.b = pb; t.ib = lB.c_str();
+                        t.c = pc; t.ic = lC.c_str();
+                        t.alpha = w.real();
+                        t.c_key = key;
+                        terms.push_back(t);
+                    }
                     else
-                        dpd_mult_z(a.lay, a.data, lA.c_str(), b.lay, b.data, lB.c_str(), c.lay, c.data, lC.c_str(),
-                                   w, 1.0, st, &r, false);
-                    launches += r.groups > 0;
-                    flops += r.flops;
+                        dpd_terms_z(a.lay, a.data, lA.c_str(), b.lay, b.data, lB.c_str(), c.lay, c.data, lC.c_str(),
+                                    w, key, store, terms);
                 }
             }
         }
+        // every term with beta = 1 on top of the initial scaling; the k-th
+        // term on each entry of C goes into the k-th grouped launch
+        DpdMultReport r;
+        launches = dpd_mult_terms(terms, st, &r, false);
+        flops = r.flops;
     }
 
     if (widened) wc.narrow(C, st);
@@ -436,7 +466,7 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
         memset(report, 0, sizeof(*report));
         report->method = 1;
         report->flops = flops;
-        report->m = launches;            // triples that ran a grouped launch
+        report->m = launches;            // grouped launches of the contraction terms
         report->kernels = (int)(g_kernel_count.load() - k0);
     }
 }

@@ -290,8 +290,13 @@ k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p,
 
 // ---- dot / reduce -----------------------------------------------------------------
 
+// Loads a lane keeps in flight per inner step of the reductions. The segment
+// loops issue U loads before the first add, in the order of the plain loop,
+// so the sums are the same bit for bit.
+template <typename T> constexpr int red_unroll(int operands) { return sizeof(T) >= 16 ? 4/operands : 8/operands; }
+
 template <typename T>
-__global__ void __launch_bounds__(L1_THREADS)
+__global__ void __launch_bounds__(L1_THREADS, RED_BLOCKS/148)
 k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s, T* partial, bool conj_a,
               bool conj_b)
 {
@@ -311,7 +316,17 @@ k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s
         i64 oa, ob;
         row_offset2(s, r, oa, ob);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
-        for (i64 i = i0 + lane; i < i1; i += 32) acc += cj(A[oa + i*sa0], conj_a)*cj(B[ob + i*sb0], conj_b);
+        constexpr int U = red_unroll<T>(2);
+        i64 i = i0 + lane;
+        for (; i + 32*(U - 1) < i1; i += 32*U)
+        {
+            T x[U], y[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) { x[u] = A[oa + (i + 32*u)*sa0]; y[u] = B[ob + (i + 32*u)*sb0]; }
+#pragma unroll
+            for (int u = 0; u < U; u++) acc += cj(x[u], conj_a)*cj(y[u], conj_b);
+        }
+        for (; i < i1; i += 32) acc += cj(A[oa + i*sa0], conj_a)*cj(B[ob + i*sb0], conj_b);
     }
     for (int o = 16; o > 0; o >>= 1) acc += shfl_down(acc, o);
     __shared__ T ws[L1_THREADS/32];
@@ -368,7 +383,7 @@ __device__ __forceinline__ T red_val(int op, T x)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(L1_THREADS)
+__global__ void __launch_bounds__(L1_THREADS, RED_BLOCKS/148)
 k_reduce_partial(int op, const T* __restrict__ A, const Strided s, T* pv, i64* plin, i64* poff)
 {
     const i64 n0 = s.ndim ? s.len[0] : 1;
@@ -388,6 +403,21 @@ k_reduce_partial(int op, const T* __restrict__ A, const Strided s, T* pv, i64* p
         const i64 r = sg / nchunk, c = sg - r*nchunk;
         const i64 ro = row_offset(s.len, s.stride, s.ndim, r);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
+        if (is_sum)
+        {
+            constexpr int U = red_unroll<T>(1);
+            i64 i = i0 + lane;
+            for (; i + 32*(U - 1) < i1; i += 32*U)
+            {
+                T x[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) x[u] = A[ro + (i + 32*u)*st0];
+#pragma unroll
+                for (int u = 0; u < U; u++) acc += red_val(op, x[u]);
+            }
+            for (; i < i1; i += 32) acc += red_val(op, A[ro + i*st0]);
+            continue;
+        }
         for (i64 i = i0 + lane; i < i1; i += 32)
         {
             const i64 off = ro + i*st0;

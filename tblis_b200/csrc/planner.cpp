@@ -386,7 +386,13 @@ struct TableCache
     std::list<std::string> lru;
     std::unordered_map<std::string, std::pair<std::shared_ptr<GemmTables>,
                                               std::list<std::string>::iterator>> map;
-    size_t capacity = 128;
+    size_t capacity = 512;
+    // evicted tables: kernels queued before their last holder let go of them
+    // may still read them, so they are freed in batches after a device
+    // synchronisation, never one synchronisation per eviction (which would
+    // stall every other stream's caller, e.g. a server's other slots)
+    std::vector<std::shared_ptr<GemmTables>> retired;
+    size_t retired_bytes = 0;
 };
 
 TableCache& table_cache()
@@ -496,15 +502,41 @@ std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 B
     t->c_l = d + (c_l - host.data());
     t->a_kbs = d + (a_kbs - host.data()); t->b_kbs = d + (b_kbs - host.data());
 
-    std::lock_guard<std::mutex> lk(cache.mtx);
-    cache.lru.push_front(key);
-    cache.map[key] = {t, cache.lru.begin()};
-    while (cache.map.size() > cache.capacity)
+    std::vector<std::shared_ptr<GemmTables>> drop;
     {
-        // tables may still be read by queued kernels: drain the device first
+        std::lock_guard<std::mutex> lk(cache.mtx);
+        cache.lru.push_front(key);
+        cache.map[key] = {t, cache.lru.begin()};
+        while (cache.map.size() > cache.capacity)
+        {
+            auto it = cache.map.find(cache.lru.back());
+            cache.retired_bytes += it->second.first->bytes;
+            cache.retired.push_back(std::move(it->second.first));
+            cache.map.erase(it);
+            cache.lru.pop_back();
+        }
+        if (cache.retired.size() >= 256 || cache.retired_bytes >= ((size_t)64 << 20))
+        {
+            // tables no caller holds any more: nobody can fetch them again, and
+            // every kernel that reads them was queued before the synchronisation
+            // below
+            std::vector<std::shared_ptr<GemmTables>> keep;
+            for (auto& r : cache.retired)
+            {
+                if (r.use_count() == 1)
+                {
+                    cache.retired_bytes -= r->bytes;
+                    drop.push_back(std::move(r));
+                }
+                else keep.push_back(std::move(r));
+            }
+            cache.retired.swap(keep);
+        }
+    }
+    if (!drop.empty())
+    {
         cudaDeviceSynchronize();
-        cache.map.erase(cache.lru.back());
-        cache.lru.pop_back();
+        drop.clear();
     }
     return t;
 }

@@ -60,6 +60,7 @@ struct Slot
     cudaEvent_t stats = nullptr;     // Ozaki statistics of the current batch done
     char* hbuf = nullptr;            // pinned staging
     size_t hcap = 0;
+    std::vector<char*> old_hbufs;    // outgrown staging, freed with the server (freeing syncs the device)
     char* dbuf_ = nullptr;           // device copy
     size_t dcap = 0;
     std::vector<int64_t> reqs;
@@ -129,7 +130,9 @@ struct Server
         {
             if (s.stream) cudaStreamSynchronize(s.stream);
             if (s.hbuf) cudaFreeHost(s.hbuf);
-            if (s.dbuf_) cudaFree(s.dbuf_);
+            for (char* h : s.old_hbufs) cudaFreeHost(h);
+            if (s.dbuf_) cudaFreeAsync(s.dbuf_, s.stream);
+            if (s.stream) cudaStreamSynchronize(s.stream);
             if (s.done) cudaEventDestroy(s.done);
             if (s.counter) cudaFree(s.counter);
             if (s.stats) cudaEventDestroy(s.stats);
@@ -249,17 +252,23 @@ struct Server
         const size_t desc_bytes = align_up(ngroups*sizeof(GroupDesc));
         const size_t tb_bytes = align_up((ngroups + 1)*sizeof(i64));
         const size_t need = tab_bytes + desc_bytes + tb_bytes;
+        // growth without a device-wide synchronisation, which would wait for
+        // the batches running on the other slots: the outgrown pinned buffer
+        // is kept until the server closes, the device buffer is freed and
+        // reallocated in this slot's stream order
         if (need > s.hcap)
         {
-            if (s.hbuf) cudaFreeHost(s.hbuf);
+            if (s.hbuf) s.old_hbufs.push_back(s.hbuf);
+            s.hbuf = nullptr;
             s.hcap = std::max(need, 2*s.hcap);
             TB_CUDA(cudaMallocHost(&s.hbuf, s.hcap));
         }
         if (need > s.dcap)
         {
-            if (s.dbuf_) cudaFree(s.dbuf_);
+            if (s.dbuf_) TB_CUDA(cudaFreeAsync(s.dbuf_, st));
+            s.dbuf_ = nullptr;
             s.dcap = std::max(need, 2*s.dcap);
-            TB_CUDA(cudaMalloc(&s.dbuf_, s.dcap));
+            TB_CUDA(cudaMallocAsync(&s.dbuf_, s.dcap, st));
         }
         i64* htab = reinterpret_cast<i64*>(s.hbuf);
         GroupDesc* hdesc = reinterpret_cast<GroupDesc*>(s.hbuf + tab_bytes);
