@@ -14,6 +14,7 @@
 // reference's microkernels apply them (src/kernels/1v/{add,scale,shift,dot}.hpp).
 #include "level1.hpp"
 #include "cplx.hpp"
+#include "mult.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -41,6 +42,20 @@ int l1_grid(i64 work_items, int per_block)
 {
     i64 b = (work_items + per_block - 1)/per_block;
     return (int)std::max<i64>(1, std::min<i64>(b, 148*32));
+}
+
+// one full wave of a grid-stride kernel: every SM holds as many blocks as
+// fit, and no partial last wave leaves SMs idle at the end
+template <typename K>
+int resident_grid(K kernel, i64 work_items, int threads)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+    {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return (int)std::max<i64>(1, std::min<i64>(work_items, (i64)per_sm*device_sm_count()));
 }
 
 __device__ __forceinline__ i64 row_offset(const i64* len, const i64* stride, int ndim, i64 r)
@@ -222,65 +237,115 @@ k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha
 
 // transpose: dim p is A's unit dim, dim q is B's unit dim, the rest are outer.
 // Square tile through shared memory (64 wide, 32 for 16-byte elements so the
-// tile stays below 48 KB); reads coalesced along p, writes along q.
+// tile stays below 48 KB); reads coalesced along p, writes along q. VW = 2
+// moves pairs of elements (16 bytes for 8-byte types) on both sides when the
+// host has checked that both unit strides are 1, both extents and every other
+// stride are even and both bases are aligned to a pair, so every pair is
+// contiguous and aligned.
 template <typename T>
 constexpr int tile_of() { return sizeof(T) >= 16 ? 32 : 64; }
 
-template <typename T, bool BETA0>
-__global__ void __launch_bounds__(L1_THREADS)
+template <int BYTES> struct RawVec;
+template <> struct RawVec<8> { typedef uint2 type; };
+template <> struct RawVec<16> { typedef uint4 type; };
+
+template <typename T, bool BETA0, int VW>
+__global__ void __launch_bounds__(L1_THREADS, 3)
 k_transpose(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, int p, int q,
             i64 tiles_p, i64 tiles_q, i64 outer, T alpha, T beta, bool conj_a, bool conj_b)
 {
     constexpr int TT = tile_of<T>();
+    typedef typename RawVec<(VW == 1 || sizeof(T)*VW < 8) ? 8 : sizeof(T)*VW>::type Raw;
+    static_assert(VW == 1 || sizeof(Raw) == sizeof(T)*VW, "pair width");
     __shared__ T tile[TT][TT + 1];
     const i64 np = s.len[p], nq = s.len[q];
-    const i64 ntiles = tiles_p*tiles_q*outer;
+    // tile indices in 32 bits (the host checks the tile count), so each tile
+    // costs a few 32-bit divisions instead of 64-bit ones
+    const unsigned ntiles = (unsigned)(tiles_p*tiles_q*outer);
+    const unsigned tpn = (unsigned)tiles_p, tpq = (unsigned)(tiles_p*tiles_q);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
-    for (i64 t = blockIdx.x; t < ntiles; t += gridDim.x)
+    for (unsigned t = blockIdx.x; t < ntiles; t += gridDim.x)
     {
-        i64 o = t / (tiles_p*tiles_q);
-        i64 pq = t - o*tiles_p*tiles_q;
-        i64 tq = pq / tiles_p, tp = pq - tq*tiles_p;
+        unsigned o = t / tpq;
+        const unsigned pq = t - o*tpq;
+        const unsigned tq = pq / tpn, tp = pq - tq*tpn;
         // outer offsets: decompose o over dims other than p and q
         i64 oa = 0, ob = 0;
         for (int d = 0; d < s.ndim; d++)
         {
             if (d == p || d == q) continue;
-            i64 qq = o / s.len[d];
-            i64 i = o - qq*s.len[d];
-            oa += i*s.sa[d]; ob += i*s.sb[d];
+            const unsigned ld = (unsigned)s.len[d];
+            const unsigned qq = o / ld;
+            const unsigned i = o - qq*ld;
+            oa += (i64)i*s.sa[d]; ob += (i64)i*s.sb[d];
             o = qq;
         }
-        const i64 p0 = tp*TT, q0 = tq*TT;
-        // load: lanes along p (A contiguous)
+        const i64 p0 = (i64)tp*TT, q0 = (i64)tq*TT;
+        // load: lanes along p (A contiguous), VW consecutive p per lane. All
+        // of a thread's loads are issued into registers before the first
+        // shared-memory store, so they are in flight together.
+        constexpr int NJ = TT/8, NH = TT/(32*VW);
+        typedef typename std::conditional<VW == 1, T, Raw>::type Item;
+        Item in[NJ][NH];
         #pragma unroll
-        for (int j = 0; j < TT/8; j++)
+        for (int j = 0; j < NJ; j++)
+        {
+            #pragma unroll
+            for (int h = 0; h < NH; h++)
+            {
+                const i64 pi = p0 + (tx + 32*h)*VW, qi = q0 + ty + 8*j;
+                if (pi < np && qi < nq)
+                    in[j][h] = *reinterpret_cast<const Item*>(A + oa + pi*s.sa[p] + qi*s.sa[q]);
+            }
+        }
+        #pragma unroll
+        for (int j = 0; j < NJ; j++)
         {
             const int ql = ty + 8*j;
             #pragma unroll
-            for (int h = 0; h < TT/32; h++)
+            for (int h = 0; h < NH; h++)
             {
-                const int pl = tx + 32*h;
-                const i64 pi = p0 + pl, qi = q0 + ql;
-                if (pi < np && qi < nq) tile[ql][pl] = A[oa + pi*s.sa[p] + qi*s.sa[q]];
+                const int pl = (tx + 32*h)*VW;
+                if (p0 + pl < np && q0 + ql < nq)
+                {
+                    const T* e = reinterpret_cast<const T*>(&in[j][h]);
+                    #pragma unroll
+                    for (int u = 0; u < VW; u++) tile[ql][pl + u] = e[u];
+                }
             }
         }
         __syncthreads();
-        // store: lanes along q (B contiguous)
+        // store: lanes along q (B contiguous), VW consecutive q per lane
         #pragma unroll
         for (int j = 0; j < TT/8; j++)
         {
             const int pl = ty + 8*j;
             #pragma unroll
-            for (int h = 0; h < TT/32; h++)
+            for (int h = 0; h < TT/(32*VW); h++)
             {
-                const int ql = tx + 32*h;
+                const int ql = (tx + 32*h)*VW;
                 const i64 pi = p0 + pl, qi = q0 + ql;
                 if (pi < np && qi < nq)
                 {
                     T* dst = B + ob + pi*s.sb[p] + qi*s.sb[q];
-                    const T v = alpha*cj(tile[ql][pl], conj_a);
-                    *dst = BETA0 ? v : v + beta*cj(*dst, conj_b);
+                    if (VW == 1)
+                    {
+                        const T v = alpha*cj(tile[ql][pl], conj_a);
+                        *dst = BETA0 ? v : v + beta*cj(*dst, conj_b);
+                    }
+                    else
+                    {
+                        Raw r;
+                        if (!BETA0) r = *reinterpret_cast<const Raw*>(dst);
+                        T* e = reinterpret_cast<T*>(&r);
+                        #pragma unroll
+                        for (int u = 0; u < VW; u++)
+                        {
+                            const T v = alpha*cj(tile[ql + u][pl], conj_a);
+                            e[u] = BETA0 ? v : v + beta*cj(e[u], conj_b);
+                        }
+                        *reinterpret_cast<Raw*>(dst) = r;
+                    }
                 }
             }
         }
@@ -577,12 +642,36 @@ void l1_add(const T* A, T* B, const Strided2& ab, const Strided& ao, const Strid
         i64 tp = (ab.len[pa] + TT - 1)/TT, tq = (ab.len[pb] + TT - 1)/TT;
         i64 outer = nab/(ab.len[pa]*ab.len[pb]);
         i64 ntiles = tp*tq*outer;
-        int grid = (int)std::min<i64>(ntiles, 148*16);
+        TB_CHECK(ntiles < ((i64)1 << 32), TB_ERR_SIZE, "transpose: too many tiles");
+        // pairs: every pair (2i, 2i+1) along p in A and along q in B is
+        // contiguous and aligned to twice the element size
+        bool pairs = sizeof(T) <= 8 && ab.sa[pa] == 1 && ab.sb[pb] == 1 && ab.len[pa] % 2 == 0 &&
+                     ab.len[pb] % 2 == 0 && ((uintptr_t)A % (2*sizeof(T))) == 0 &&
+                     ((uintptr_t)B % (2*sizeof(T))) == 0;
+        for (int d = 0; d < ab.ndim && pairs; d++)
+        {
+            if (d != pa && ab.sa[d] % 2 != 0) pairs = false;
+            if (d != pb && ab.sb[d] % 2 != 0) pairs = false;
+        }
         TimedLaunch t("k_transpose", st);
-        if (b0) k_transpose<T, true><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
-                                                                  conj_a, conj_b);
-        else k_transpose<T, false><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
-                                                                 conj_a, conj_b);
+        if constexpr (sizeof(T) <= 8)
+        {
+            if (pairs)
+            {
+                const int grid = resident_grid(k_transpose<T, true, 2>, ntiles, L1_THREADS);
+                if (b0) k_transpose<T, true, 2><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer,
+                                                                             alpha, beta, conj_a, conj_b);
+                else k_transpose<T, false, 2><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer,
+                                                                            alpha, beta, conj_a, conj_b);
+                check_launch("k_transpose");
+                return;
+            }
+        }
+        const int grid = resident_grid(k_transpose<T, true, 1>, ntiles, L1_THREADS);
+        if (b0) k_transpose<T, true, 1><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
+                                                                     conj_a, conj_b);
+        else k_transpose<T, false, 1><<<grid, L1_THREADS, 0, st>>>(A, B, ab, pa, pb, tp, tq, outer, alpha, beta,
+                                                                    conj_a, conj_b);
         check_launch("k_transpose");
         return;
     }

@@ -78,7 +78,7 @@ def test_mismatched_indexed_irreps_only_scale(cuda):
 @pytest.mark.parametrize("dtype", ["float64", "complex128"])
 def test_triples_share_launches(cuda, dtype):
     """C[abij] (j indexed, 3 entries) = A[abem] (m indexed, 3 entries) *
-    B[emij] (m and j indexed, 9 entries): 9 consistent triples, 3 on each
+    B[eimj] (m and j indexed, 9 entries): 9 consistent triples, 3 on each
     entry of C, run in 3 grouped launches (the k-th triple of every entry of
     C in the k-th launch) with the reference's result. dcomplex: the 4 real
     products of each triple into each part of C (complex alpha) make 12
@@ -94,14 +94,14 @@ def test_triples_share_launches(cuda, dtype):
     if dtype == "float64":
         alpha = 0.75
         want = copy.deepcopy(C)
-        oracle.ref_indexed_dpd_mult(n, alpha, A, "abem", B, "emij", 0.5, want, "abij", impl=0)
+        oracle.ref_indexed_dpd_mult(n, alpha, A, "abem", B, "eimj", 0.5, want, "abij", impl=0)
         want = want["data"]
     else:
         alpha = 0.75 - 0.25j
         for T in (A, B, C):
             T["data"] = T["data"] + 1j * rng.uniform(-1, 1, T["data"].shape)
-        want = restated_mult(n, alpha, A, "abem", B, "emij", 0.5, C, "abij")
-    got, rep = _gpu(torch, cuda, n, alpha, A, "abem", B, "emij", 0.5, C, "abij")
+        want = restated_mult(n, alpha, A, "abem", B, "eimj", 0.5, C, "abij")
+    got, rep = _gpu(torch, cuda, n, alpha, A, "abem", B, "eimj", 0.5, C, "abij")
     assert np.linalg.norm(got - want) <= 1e-13 * max(1.0, np.linalg.norm(want))
     assert rep["m"] == (3 if dtype == "float64" else 12)
 

@@ -136,3 +136,39 @@ def test_unary_matches_oracle(cuda, kind):
                                           strides=[s * 8 for s in A[2]])
     mask[idx.ravel()] = False
     assert np.array_equal(base_after[mask], A[0][mask])
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64", "complex64", "complex128"])
+@pytest.mark.parametrize("shape", [(130, 70, 4), (64, 96, 6), (66, 34, 3), (65, 64, 2), (64, 65, 2)])
+@pytest.mark.parametrize("beta", [0.0, 0.5])
+def test_transpose_pairs_and_singles(cuda, dtype, shape, beta):
+    """B[cba] = alpha*A[abc] + beta*B[cba] through the shared-memory transpose.
+    Even unit extents with even strides take the paired form (two elements per
+    access, 16 bytes for 8-byte types); an odd extent on either side, a
+    16-byte element type or an offset base take single elements. Both agree
+    with torch to rounding (a misplaced element would be an O(1) error)."""
+    import torch
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(sum(shape))
+    dt = getattr(torch, dtype)
+    real = torch.float32 if dtype in ("float32", "complex64") else torch.float64
+
+    def rnd(*s):
+        x = torch.empty(s, dtype=real, device=cuda).uniform_(-1, 1, generator=g)
+        if dt.is_complex:
+            x = torch.complex(x, torch.empty(s, dtype=real, device=cuda).uniform_(-1, 1, generator=g))
+        return x
+    a, b, c = shape
+    A = rnd(c, b, a).permute(2, 1, 0)              # a fastest
+    Bbuf = rnd(a * b * c + 1)                      # one extra element: offset (unaligned) view too
+    for off in (0, 1):
+        B = Bbuf[off:off + a * b * c].view(a, b, c)   # c fastest: B[cba] column-major
+        before = B.clone()
+        alpha = 0.75
+        tb.add(alpha, A, "abc", beta, B, "abc")
+        want = alpha * A + beta * before if beta != 0 else alpha * A
+        torch.cuda.synchronize()
+        tol = 1e-6 if real == torch.float32 else 1e-15
+        err = (torch.linalg.vector_norm(B - want) / torch.linalg.vector_norm(want)).item()
+        assert err <= tol, (dtype, shape, beta, off, err)
