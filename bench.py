@@ -43,7 +43,7 @@ def parse(argv=None):
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
     p.add_argument("--o", type=int, default=48, help="occupied extent (profiling runs use a smaller case)")
     p.add_argument("--v", type=int, default=160, help="virtual extent")
-    p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce"],
+    p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce", "dpd"],
                    help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
     a = p.parse_args(argv)
     global O, V, FLOPS_LADDER, WORKLOAD
@@ -707,7 +707,9 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
 
 def single_case(torch, tb, dev, stream, args):
     """One secondary kernel alone at extents o, v (for profiling captures):
-    ring C[aibj] += A[aeim]*B[mbej] (FP64 DMMA) or transpose D[ijab] = C[abij]."""
+    ring C[aibj] += A[aeim]*B[mbej] (FP64 DMMA), transpose D[ijab] = C[abij],
+    dot, NORM_2 reduce, or (dpd, fixed extents) the D2h DPD ladder of the
+    secondary workloads in one grouped launch."""
     o, v = args.o, args.v
     g = torch.Generator(device=dev)
     g.manual_seed(7)
@@ -715,7 +717,22 @@ def single_case(torch, tb, dev, stream, args):
     def cm(shape):
         return torch.empty(list(reversed(shape)), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g) \
             .permute(*reversed(range(len(shape))))
-    if args.case == "ring":
+    if args.case == "dpd":
+        # per-irrep extents scaled by o/48 and v/160 (the defaults give the
+        # secondary workload's D2h ladder itself)
+        vir = [max(1, round(x * v / 160)) for x in VIR]
+        occ = [max(1, round(x * o / 48)) for x in OCC]
+        A = tb.DpdTensor(0, 8, [vir, vir, vir, vir])
+        B = tb.DpdTensor(0, 8, [vir, vir, occ, occ])
+        C = tb.DpdTensor(0, 8, [vir, vir, occ, occ])
+        A.data = torch.empty(A.size(), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        B.data = torch.empty(B.size(), dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
+        C.data = torch.zeros(C.size(), dtype=torch.float64, device=dev)
+
+        def fn():
+            return tb.dpd_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij")
+        work, unit = fn()["flops"] / 1e9, "GFLOP/s"
+    elif args.case == "ring":
         A, B, C = cm([v, v, o, o]), cm([o, v, v, o]), cm([v, o, v, o])
 
         def fn():
