@@ -728,8 +728,11 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
 
-    // 4 threads per row of a tile, 16 consecutive k each
-    const int rl = t >> 2, seg = (t & 3)*16;
+    // 4 threads per row of a tile, 16 consecutive k each; a warp takes 32
+    // consecutive rows of one 16-k segment, so its shared-memory reads
+    // spread over the banks (the padded rows shift by two banks each) and
+    // its plane stores still fill whole 128-byte lines
+    const int rl = t & (SL_T - 1), seg = (t >> 6)*16;
     const i64 k_lim = pg.k_steps*KE;
     const i64 r_lim = pg.tiles*pg.tile_rows;         // rows of the planes (whole row tiles)
     unsigned tile = blockIdx.x;
