@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(L1_THREADS) k_unary(T* A, const Strided s, T v
     const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
     for (i64 sg = warp0; sg < nseg; sg += nwarps)
     {
-        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 r = rows == 1 ? 0 : sg / nchunk, c = sg - r*nchunk;   // one row: no division
         T* base = A + row_offset(s.len, s.stride, s.ndim, r);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
         for (i64 i = i0 + lane; i < i1; i += 32)
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(L1_THREADS) k_convert(const S* __restrict__ sr
     const i64 nwarps = ((i64)gridDim.x*blockDim.x) >> 5;
     for (i64 sg = warp0; sg < nseg; sg += nwarps)
     {
-        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 r = rows == 1 ? 0 : sg / nchunk, c = sg - r*nchunk;   // one row: no division
         const i64 ro = row_offset(s.len, s.stride, s.ndim, r);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
         for (i64 i = i0 + lane; i < i1; i += 32) dst[ro + i*st0] = (D)src[ro + i*st0];
@@ -195,7 +195,7 @@ k_add_rows(const T* __restrict__ A, T* __restrict__ B, const Strided2 s, T alpha
     constexpr int VW = 16/sizeof(T);
     for (i64 sg = warp0; sg < nseg; sg += nwarps)
     {
-        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 r = rows == 1 ? 0 : sg / nchunk, c = sg - r*nchunk;   // one row: no division
         i64 oa, ob;
         row_offset2(s, r, oa, ob);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
@@ -377,7 +377,7 @@ k_dot_partial(const T* __restrict__ A, const T* __restrict__ B, const Strided2 s
     T acc = T(0);
     for (i64 sg = warp0; sg < nseg; sg += nwarps)
     {
-        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 r = rows == 1 ? 0 : sg / nchunk, c = sg - r*nchunk;   // one row: no division
         i64 oa, ob;
         row_offset2(s, r, oa, ob);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
@@ -465,7 +465,7 @@ k_reduce_partial(int op, const T* __restrict__ A, const Strided s, T* pv, i64* p
     Cand<T> best = {T(0), -1, -1};
     for (i64 sg = warp0; sg < nseg; sg += nwarps)
     {
-        const i64 r = sg / nchunk, c = sg - r*nchunk;
+        const i64 r = rows == 1 ? 0 : sg / nchunk, c = sg - r*nchunk;   // one row: no division
         const i64 ro = row_offset(s.len, s.stride, s.ndim, r);
         const i64 i0 = c*SEG, i1 = min(n0, i0 + SEG);
         if (is_sum)
