@@ -29,6 +29,8 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
+#include <memory>
 
 namespace tb
 {
@@ -53,6 +55,28 @@ struct Request
     std::string msg;
 };
 
+// The GEMM view of one request shape (lengths, strides and labels of A, B
+// and C) and, for the FP64 kernel, its scatter vectors in device memory:
+// built once per shape and reused by every later request of that shape.
+struct ShapeEntry
+{
+    GemmView v;
+    bool has_tables = false;
+    std::vector<i64> host;           // a_l, b_l, c_l (descriptor offsets), kept on the host
+    i64 *dev = nullptr;              // a_m, c_m, b_n, c_n, a_k, b_k, a_kbs, b_kbs, a_l, b_l, c_l
+    cudaStream_t owner = nullptr;    // stream the device block was allocated on
+    const i64 *a_m = nullptr, *c_m = nullptr, *b_n = nullptr, *c_n = nullptr;
+    const i64 *a_k = nullptr, *b_k = nullptr, *a_kbs = nullptr, *b_kbs = nullptr;
+    const i64 *a_l = nullptr, *b_l = nullptr, *c_l = nullptr;      // into host
+    const i64* dev_l[3] = {nullptr, nullptr, nullptr};              // a_l, b_l, c_l on the device
+    ~ShapeEntry()
+    {
+        // the last holder is a finished batch or the server's teardown: no
+        // queued kernel reads the block any more
+        if (dev) cudaFreeAsync(dev, owner);
+    }
+};
+
 struct Slot
 {
     cudaStream_t stream = nullptr;
@@ -64,6 +88,7 @@ struct Slot
     char* dbuf_ = nullptr;           // device copy
     size_t dcap = 0;
     std::vector<int64_t> reqs;
+    std::vector<std::shared_ptr<ShapeEntry>> shapes;   // held until the batch completes
     bool busy = false;
     i64 footprint = 0;
     unsigned long long* counter = nullptr;   // dynamic tile queue of the grouped launch
@@ -97,6 +122,9 @@ struct Server
     i64 budget = 0, in_use = 0;
     int device = 0;
     int max_batch = 256;
+    // request shapes seen so far (scheduler thread only)
+    std::unordered_map<std::string, std::shared_ptr<ShapeEntry>> shape_cache;
+    static constexpr size_t kShapeCap = 1024;
     // statistics
     int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_requests = 0, n_ozaki = 0;
     int max_running = 0;
@@ -126,6 +154,11 @@ struct Server
         }
         cv.notify_all();
         if (worker.joinable()) worker.join();
+        for (auto& s : slots)
+            if (s.stream) cudaStreamSynchronize(s.stream);
+        // shapes free their device blocks in their streams' order
+        for (auto& s : slots) s.shapes.clear();
+        shape_cache.clear();
         for (auto& s : slots)
         {
             if (s.stream) cudaStreamSynchronize(s.stream);
@@ -206,6 +239,78 @@ struct Server
     // large enough to fill the GPU run as their own dense launch (with split-K
     // where it pays), the rest are folded into one grouped launch whose tiles
     // are handed out longest-K first
+    // the view of a request's shape, from the cache or built now
+    std::shared_ptr<ShapeEntry> shape_of(const Request& r)
+    {
+        std::string key;
+        for (int t = 0; t < 3; t++)
+        {
+            key.append(reinterpret_cast<const char*>(r.len[t].data()), r.len[t].size()*sizeof(len_type));
+            key.append(reinterpret_cast<const char*>(r.stride[t].data()), r.stride[t].size()*sizeof(stride_type));
+            key += r.idx[t];
+            key.push_back('|');
+        }
+        auto it = shape_cache.find(key);
+        if (it != shape_cache.end()) return it->second;
+        auto e = std::make_shared<ShapeEntry>();
+        e->v = gemm_view(mult_groups(&r.A, r.idx[0].c_str(), &r.B, r.idx[1].c_str(), &r.C, r.idx[2].c_str()));
+        // entries still used by running batches stay alive through the slots
+        if (shape_cache.size() >= kShapeCap) shape_cache.clear();
+        shape_cache.emplace(std::move(key), e);
+        return e;
+    }
+
+    // the shape's scatter vectors on the device (built once per shape)
+    static void tables_of(ShapeEntry& e, i64 BK, cudaStream_t st)
+    {
+        if (e.has_tables) return;
+        const GemmView& v = e.v;
+        const i64 nkb = (v.k + BK - 1)/BK;
+        const i64 n = 2*v.m + 2*v.n + 2*v.k + 2*nkb + 3*v.l;
+        std::vector<i64> h((size_t)std::max<i64>(n, 1)), bs((size_t)std::max({v.m, v.n, v.k, v.l, (i64)1}) + 1);
+        i64* q = h.data();
+        i64 *a_m = q; q += v.m;  i64 *c_m = q; q += v.m;
+        i64 *b_n = q; q += v.n;  i64 *c_n = q; q += v.n;
+        i64 *a_k = q; q += v.k;  i64 *b_k = q; q += v.k;
+        i64 *a_kbs = q; q += nkb; i64 *b_kbs = q; q += nkb;
+        i64 *a_l = q; q += v.l;  i64 *b_l = q; q += v.l;  i64 *c_l = q;
+        fill_block_scatter(v.lenM, v.aM, 1, 0, v.m, a_m, bs.data(), v.pack_m_3d);
+        fill_block_scatter(v.lenM, v.cM, 1, 0, v.m, c_m, bs.data(), v.pack_m_3d);
+        fill_block_scatter(v.lenN, v.bN, 1, 0, v.n, b_n, bs.data(), v.pack_n_3d);
+        fill_block_scatter(v.lenN, v.cN, 1, 0, v.n, c_n, bs.data(), v.pack_n_3d);
+        fill_block_scatter(v.lenK, v.aK, 1, 0, v.k, a_k, bs.data(), v.pack_k_3d);
+        fill_block_scatter(v.lenK, v.bK, 1, 0, v.k, b_k, bs.data(), v.pack_k_3d);
+        // per k block of BK: its common stride, or 0 when the offsets are not affine
+        auto kbs = [&](const i64* k, i64* out)
+        {
+            for (i64 b = 0; b < nkb; b++)
+            {
+                const i64 i0 = b*BK, bl = std::min(v.k - i0, BK);
+                i64 sv = bl > 1 ? k[i0 + 1] - k[i0] : 1;
+                for (i64 j = i0 + 1; j + 1 < i0 + bl; j++) if (k[j + 1] - k[j] != sv) sv = 0;
+                out[b] = sv;
+            }
+        };
+        kbs(a_k, a_kbs);
+        kbs(b_k, b_kbs);
+        fill_block_scatter(v.lenL, v.aL, 1, 0, v.l, a_l, bs.data(), false);
+        fill_block_scatter(v.lenL, v.bL, 1, 0, v.l, b_l, bs.data(), false);
+        fill_block_scatter(v.lenL, v.cL, 1, 0, v.l, c_l, bs.data(), false);
+        // the slot's stream is idle here (its previous batch is complete): the
+        // copy from pageable memory has the source staged when it returns
+        TB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&e.dev), (size_t)h.size()*sizeof(i64), st));
+        e.owner = st;
+        TB_CUDA(cudaMemcpyAsync(e.dev, h.data(), h.size()*sizeof(i64), cudaMemcpyHostToDevice, st));
+        const i64* d = e.dev;
+        auto at = [&](const i64* hp) { return d + (hp - h.data()); };
+        e.a_m = at(a_m); e.c_m = at(c_m); e.b_n = at(b_n); e.c_n = at(c_n);
+        e.a_k = at(a_k); e.b_k = at(b_k); e.a_kbs = at(a_kbs); e.b_kbs = at(b_kbs);
+        e.dev_l[0] = at(a_l); e.dev_l[1] = at(b_l); e.dev_l[2] = at(c_l);
+        e.host.assign(a_l, a_l + 3*v.l);
+        e.a_l = e.host.data(); e.b_l = e.host.data() + v.l; e.c_l = e.host.data() + 2*v.l;
+        e.has_tables = true;
+    }
+
     void launch(Slot& s, std::vector<Request*>& batch)
     {
         cudaStream_t st = s.stream;
@@ -213,11 +318,11 @@ struct Server
         {
             Request* r;
             GemmView v;
+            std::shared_ptr<ShapeEntry> e;
             bool trivial, dense, ozaki;
             double alpha, beta;
         };
         std::vector<Prep> prep;
-        size_t table_elems = 0;
         size_t ngroups = 0;
         const i64 BK = gemm_f64_tile_k();
         int bm, bn;
@@ -226,8 +331,8 @@ struct Server
         {
             try
             {
-                GemmView v = gemm_view(mult_groups(&r->A, r->idx[0].c_str(), &r->B, r->idx[1].c_str(),
-                                                   &r->C, r->idx[2].c_str()));
+                std::shared_ptr<ShapeEntry> e = shape_of(*r);
+                const GemmView& v = e->v;
                 const double alpha = r->A.scalar.data.d*r->B.scalar.data.d, beta = r->C.scalar.data.d;
                 const bool trivial = alpha == 0.0 || v.k == 0 || v.m*v.n*v.l == 0;
                 const bool ozaki = !trivial && use_ozaki(v, r->tol);
@@ -235,10 +340,11 @@ struct Server
                                    ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn)*v.l >= kDenseTiles;
                 if (!trivial && !ozaki)
                 {
-                    table_elems += 2*v.m + 2*v.n + 2*v.k + 2*((v.k + BK - 1)/BK) + 3*v.l + 8;
+                    tables_of(*e, BK, st);
                     if (!dense) ngroups += v.l;
                 }
-                prep.push_back({r, v, trivial, dense, ozaki, alpha, beta});
+                s.shapes.push_back(e);
+                prep.push_back({r, v, e, trivial, dense, ozaki, alpha, beta});
             }
             catch (const error& e)
             {
@@ -248,10 +354,11 @@ struct Server
         // longest K first in the grouped launch
         std::stable_sort(prep.begin(), prep.end(), [](const Prep& a, const Prep& b) { return a.v.k > b.v.k; });
 
-        const size_t tab_bytes = align_up(table_elems*sizeof(i64));
+        // only the descriptors and the tile prefix travel per batch: the
+        // scatter vectors of every shape are already on the device
         const size_t desc_bytes = align_up(ngroups*sizeof(GroupDesc));
         const size_t tb_bytes = align_up((ngroups + 1)*sizeof(i64));
-        const size_t need = tab_bytes + desc_bytes + tb_bytes;
+        const size_t need = desc_bytes + tb_bytes;
         // growth without a device-wide synchronisation, which would wait for
         // the batches running on the other slots: the outgrown pinned buffer
         // is kept until the server closes, the device buffer is freed and
@@ -270,16 +377,13 @@ struct Server
             s.dcap = std::max(need, 2*s.dcap);
             TB_CUDA(cudaMallocAsync(&s.dbuf_, s.dcap, st));
         }
-        i64* htab = reinterpret_cast<i64*>(s.hbuf);
-        GroupDesc* hdesc = reinterpret_cast<GroupDesc*>(s.hbuf + tab_bytes);
-        i64* htb = reinterpret_cast<i64*>(s.hbuf + tab_bytes + desc_bytes);
-        const i64* dtab = reinterpret_cast<const i64*>(s.dbuf_);
-        GroupDesc* ddesc = reinterpret_cast<GroupDesc*>(s.dbuf_ + tab_bytes);
-        const i64* dtb = reinterpret_cast<const i64*>(s.dbuf_ + tab_bytes + desc_bytes);
+        GroupDesc* hdesc = reinterpret_cast<GroupDesc*>(s.hbuf);
+        i64* htb = reinterpret_cast<i64*>(s.hbuf + desc_bytes);
+        GroupDesc* ddesc = reinterpret_cast<GroupDesc*>(s.dbuf_);
+        const i64* dtb = reinterpret_cast<const i64*>(s.dbuf_ + desc_bytes);
 
-        size_t pos = 0, g = 0;
+        size_t g = 0;
         i64 tiles = 0;
-        std::vector<i64> bs;
         std::vector<GemmF64Args> dense;
         for (Prep& p : prep)
         {
@@ -300,54 +404,16 @@ struct Server
                 else l1_scale<double>(static_cast<double*>(p.r->C.data), sc, p.beta, st);
                 continue;
             }
-            bs.resize(std::max({v.m, v.n, v.k, v.l}) + 1);
-            auto put = [&](const ivec& lens, const ivec& strides, i64 n, bool p3) -> const i64*
-            {
-                i64* h = htab + pos;
-                fill_block_scatter(lens, strides, 1, 0, n, h, bs.data(), p3);
-                const i64* d = dtab + pos;
-                pos += n;
-                return d;
-            };
-            const i64* a_m = put(v.lenM, v.aM, v.m, v.pack_m_3d);
-            const i64* c_m = put(v.lenM, v.cM, v.m, v.pack_m_3d);
-            const i64* b_n = put(v.lenN, v.bN, v.n, v.pack_n_3d);
-            const i64* c_n = put(v.lenN, v.cN, v.n, v.pack_n_3d);
-            i64* ha_k = htab + pos;
-            const i64* a_k = put(v.lenK, v.aK, v.k, v.pack_k_3d);
-            i64* hb_k = htab + pos;
-            const i64* b_k = put(v.lenK, v.bK, v.k, v.pack_k_3d);
-            const i64 nkb = (v.k + BK - 1)/BK;
-            auto kbs = [&](const i64* k) -> const i64*
-            {
-                i64* h = htab + pos;
-                for (i64 b = 0; b < nkb; b++)
-                {
-                    const i64 i0 = b*BK, bl = std::min(v.k - i0, BK);
-                    i64 sv = bl > 1 ? k[i0 + 1] - k[i0] : 1;
-                    for (i64 j = i0 + 1; j + 1 < i0 + bl; j++) if (k[j + 1] - k[j] != sv) sv = 0;
-                    h[b] = sv;
-                }
-                const i64* d = dtab + pos;
-                pos += nkb;
-                return d;
-            };
-            const i64* a_kbs = kbs(ha_k);
-            const i64* b_kbs = kbs(hb_k);
-            i64* hal = htab + pos;
-            const i64* a_l = put(v.lenL, v.aL, v.l, false);
-            i64* hbl = htab + pos;
-            const i64* b_l = put(v.lenL, v.bL, v.l, false);
-            i64* hcl = htab + pos;
-            const i64* c_l = put(v.lenL, v.cL, v.l, false);
+            const ShapeEntry& e = *p.e;
             if (p.dense)
             {
                 GemmF64Args a = {};
                 a.A = static_cast<const double*>(p.r->A.data);
                 a.B = static_cast<const double*>(p.r->B.data);
                 a.C = static_cast<double*>(p.r->C.data);
-                a.a_m = a_m; a.a_k = a_k; a.b_k = b_k; a.b_n = b_n; a.c_m = c_m; a.c_n = c_n;
-                a.a_l = a_l; a.b_l = b_l; a.c_l = c_l; a.a_kbs = a_kbs; a.b_kbs = b_kbs;
+                a.a_m = e.a_m; a.a_k = e.a_k; a.b_k = e.b_k; a.b_n = e.b_n; a.c_m = e.c_m; a.c_n = e.c_n;
+                a.a_l = e.dev_l[0]; a.b_l = e.dev_l[1]; a.c_l = e.dev_l[2];
+                a.a_kbs = e.a_kbs; a.b_kbs = e.b_kbs;
                 a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;
                 a.alpha = p.alpha; a.beta = p.beta;
                 a.amode = v.amode; a.bmode = v.bmode;
@@ -358,11 +424,11 @@ struct Server
             for (i64 l = 0; l < v.l; l++)
             {
                 GroupDesc& d = hdesc[g];
-                d.A = static_cast<const double*>(p.r->A.data) + hal[l];
-                d.B = static_cast<const double*>(p.r->B.data) + hbl[l];
-                d.C = static_cast<double*>(p.r->C.data) + hcl[l];
-                d.a_m = a_m; d.a_k = a_k; d.b_k = b_k; d.b_n = b_n; d.c_m = c_m; d.c_n = c_n;
-                d.a_kbs = a_kbs; d.b_kbs = b_kbs;
+                d.A = static_cast<const double*>(p.r->A.data) + e.a_l[l];
+                d.B = static_cast<const double*>(p.r->B.data) + e.b_l[l];
+                d.C = static_cast<double*>(p.r->C.data) + e.c_l[l];
+                d.a_m = e.a_m; d.a_k = e.a_k; d.b_k = e.b_k; d.b_n = e.b_n; d.c_m = e.c_m; d.c_n = e.c_n;
+                d.a_kbs = e.a_kbs; d.b_kbs = e.b_kbs;
                 d.M = v.m; d.N = v.n; d.K = v.k;
                 d.alpha = p.alpha; d.beta = p.beta;
                 d.amode = v.amode; d.bmode = v.bmode;
@@ -387,8 +453,11 @@ struct Server
             jobs.push_back(std::move(j));
         }
         if (!jobs.empty()) TB_CUDA(cudaEventRecord(s.stats, st));
-        if (pos > 0 || g > 0)
+        if (g > 0)
+        {
+            htb[g] = tiles;
             TB_CUDA(cudaMemcpyAsync(s.dbuf_, s.hbuf, need, cudaMemcpyHostToDevice, st));
+        }
         if (g > 0)
             gemm_f64_grouped_launch(ddesc, dtb, (int)g, tiles, kVariant, st, s.counter);
         for (GemmF64Args& a : dense)
@@ -439,6 +508,7 @@ struct Server
                         else if (r.state == 3) { r.t_done = now; n_failed++; }
                     }
                     s.reqs.clear();
+                    s.shapes.clear();
                     s.busy = false;
                     in_use -= s.footprint;
                     s.footprint = 0;
