@@ -183,3 +183,35 @@ def test_tolerant_requests_use_int8_slices(cuda):
         assert normwise_rel(got, r["ref"]) <= TOL
     assert srv.stats()["ozaki"] == 3
     srv.close()
+
+
+def test_repeated_shapes_across_batches(cuda):
+    """Requests that share a shape (lengths, strides, labels) reuse the
+    server's cached view and device scatter vectors: four shapes, each
+    submitted in three waves with fresh operands and scalars, every result
+    against torch."""
+    import torch
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(12)
+    shapes = [((9, 7, 5), "ac", "cb", "ab"), ((33, 17, 40), "ca", "bc", "ba"),
+              ((64, 80, 96), "ac", "cb", "ab"), ((5, 130, 3), "ac", "bc", "ba")]
+    srv = tb.Server(hbm_budget_bytes=8 << 30, slots=4)
+    try:
+        for wave in range(3):
+            work = []
+            for (m, n, k), ia, ib, ic in shapes * 4:
+                dims = {"a": m, "b": n, "c": k}
+                mk = lambda lab: torch.empty([dims[x] for x in lab], dtype=torch.float64,
+                                             device=cuda).uniform_(-1, 1, generator=g)
+                A, B, C = mk(ia), mk(ib), mk(ic)
+                alpha, beta = 0.5 + wave, (0.0, 1.0, -0.5)[wave]
+                want = alpha * torch.einsum("%s,%s->%s" % (ia, ib, ic), A, B) + (beta * C if beta else 0.0)
+                rid = srv.submit(alpha, A, ia, B, ib, beta, C, ic, 1e-14)
+                work.append((rid, C, want))
+            for rid, C, want in work:
+                srv.wait(rid)
+                err = (torch.linalg.vector_norm(C - want) / torch.linalg.vector_norm(want)).item()
+                assert err <= 1e-14, (wave, err)
+    finally:
+        srv.close()
