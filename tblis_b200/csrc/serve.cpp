@@ -4,12 +4,16 @@
 // by tblis_b200_server_submit from any host thread. One scheduler thread
 // admits queued requests in arrival order while their operand footprint fits
 // the HBM budget, folds every admitted request into one grouped launch of the
-// FP64 DMMA kernel (scatter vectors, descriptors and tile prefix table packed
-// into one pinned buffer and copied with a single transfer), and launches it
-// on the next free slot -- each slot owns a stream, so up to `slots` batches
-// run on the GPU at once and requests that arrive while others run are
-// admitted as soon as a slot and budget free up. Completion is detected with
-// events; each request records its latency (submit to completion).
+// FP64 DMMA kernel and launches it on the next free slot. Each request shape
+// (lengths, strides and labels of A, B and C) gets its GEMM view and device
+// scatter vectors once; a batch then packs only its descriptors and tile
+// prefix table into one pinned buffer, copied with a single transfer. Large
+// requests whose tolerance allows it run as Ozaki jobs beside the grouped
+// launch, and large FP64 ones as their own launch. Each slot owns a stream,
+// so up to `slots` batches run on the GPU at once, and requests that arrive
+// while others run are admitted as soon as a slot and budget free up.
+// Completion is detected with events; each request records its latency
+// (submit to completion).
 //
 // Each request's result does not depend on the batch it lands in: every
 // output tile is computed by one CTA with a fixed k order and a fixed tile
