@@ -141,7 +141,9 @@ class ClockSampler:
         vis = os.environ.get("CUDA_VISIBLE_DEVICES")
         ids = [x.strip() for x in vis.split(",")] if vis else []
         self.gpu = ids[local_index] if local_index < len(ids) else str(local_index)
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+        # one file per rank: several ranks on one node must not share it
+        name = "clocks_bench.csv" if local_index == 0 else "clocks_bench_rank%d.csv" % local_index
+        self.path = os.path.join(ROOT, "gpurun_out", name)
 
     def start(self):
         try:
