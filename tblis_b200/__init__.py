@@ -150,8 +150,8 @@ class _View:
         t.scalar = _make_scalar(scalar, code)
         t.data = ptr
         t.ndim = n
-        t.len = ctypes.cast(self.len, _P(ctypes.c_ssize_t))
-        t.stride = ctypes.cast(self.stride, _P(ctypes.c_ssize_t))
+        t.len = self.len          # ctypes converts the arrays to the pointer fields
+        t.stride = self.stride
         self.t = t
 
     @property
@@ -307,17 +307,18 @@ def gather_shards(A, idx_A, B, idx_B, C, idx_C, rank=None, nranks=None, group=No
 def _make_scalar(v, code):
     s = tblis_scalar()
     s.type = code
-    f = ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))
     if code == TYPE_DOUBLE:
         s.data[0] = float(v)
     elif code == TYPE_DCOMPLEX:
         s.data[0] = complex(v).real
         s.data[1] = complex(v).imag
-    elif code == TYPE_SCOMPLEX:
-        f[0] = complex(v).real
-        f[1] = complex(v).imag
     else:
-        f[0] = float(v)
+        f = ctypes.cast(ctypes.byref(s), _P(ctypes.c_float))
+        if code == TYPE_SCOMPLEX:
+            f[0] = complex(v).real
+            f[1] = complex(v).imag
+        else:
+            f[0] = float(v)
     return s
 
 
