@@ -4,16 +4,22 @@
 Headline workload (one "step" = one contraction through tblis_tensor_mult):
 the ladder term C[abij] = A[abef] * B[efij] with o=48, v=160 (m=25600,
 n=2304, k=25600; 3.02 TFLOP), FP64 inputs uniform(-1,1) * 2^k with k a
-uniform integer in [-20, 20] per element, computed by the fastest method
-whose normwise relative error against the FP64 path is at most 1e-12.
+uniform integer in [-20, 20] per element, generated once on the host from
+fixed seeds (the same bits in every arm), computed by the fastest method whose
+normwise relative error is at most 1e-12.
 
-Prints one JSON line (rank 0). Extra keys: the plain FP64 (DMMA) rate on the
-same workload, the ring contraction and the transpose bandwidth case, the
-roofline of the dominant kernel, the CPU baseline (the TBLIS reference built
-from its own sources, timed on a bounded slice on this host) and the
-end-to-end rate through the C ABI with pinned host buffers.
+Prints one JSON line (rank 0). Extra keys: the accuracy of the GPU results
+against the reference's own FP64 output on the same inputs, the plain FP64
+(DMMA) rate on the same workload, the roofline of the dominant kernel, the
+CPU baseline (the TBLIS reference built from its own sources, timed on the
+whole ladder on this host), the end-to-end rate through tblis_tensor_mult with
+pinned host buffers, and the secondary workloads (DPD, batch, serving, ring,
+transpose, dot/reduce), each with its own check against the reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's tblis_tensor_mult on the host cores on
+the same inputs, one whole ladder contraction per step.
 """
 import argparse
 import ctypes
@@ -30,6 +36,7 @@ sys.path.insert(0, ROOT)
 O, V = 48, 160
 FLOPS_LADDER = 2.0 * V * V * V * V * O * O
 WORKLOAD = "ladder C[abij]=A[abef]*B[efij] o=48 v=160 fp64 exponent spread 2^[-20,20]"
+METRIC = "contraction GFLOP/s at <=1e-12 normwise rel err"
 
 
 def parse(argv=None):
@@ -63,42 +70,122 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------------------
-# CPU reference leg (oracle/_ref: the TBLIS reference compiled from its own sources)
+# Inputs: one host-side seeded recipe for every arm (GPU, end to end, CPU reference)
 # ---------------------------------------------------------------------------------------
 
-def cpu_reference_sample(threads=None, reps=2):
-    """Times the reference's tblis_tensor_mult on a bounded slice of the ladder
-    workload: a restricted to the first 16 of 160 (m = 2560 of 25600 rows),
-    i.e. 1/10 of the contraction, same exponent-spread inputs. Returns
-    (GFLOP/s, cores, sample text)."""
+SEED_A, SEED_B = 1001, 1002
+GEN_CHUNK = 1 << 24
+INPUTS = ("host-generated FP64, numpy PCG64 stream per 16M-element chunk seeded (tensor seed, chunk) with "
+          "A=1001, B=1002: uniform(-1,1) * 2^k, k uniform integer in [-20,20]; every arm uses the same bits")
+
+
+def fill_spread(flat, seed):
+    """Fills a flat float64 array (a tensor's storage in memory order) with
+    uniform(-1,1) * 2^k, k a uniform integer in [-20, 20]; chunk c draws from
+    numpy's PCG64 seeded with (seed, c), so the result does not depend on how
+    many threads fill it."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(c):
+        s = c * GEN_CHUNK
+        e = min(flat.size, s + GEN_CHUNK)
+        rng = np.random.default_rng([seed, c])
+        u = rng.uniform(-1.0, 1.0, e - s)
+        k = rng.integers(-20, 21, e - s, dtype=np.int32)
+        np.ldexp(u, k, out=flat[s:e])
+    n = (flat.size + GEN_CHUNK - 1) // GEN_CHUNK
+    with ThreadPoolExecutor(max_workers=max(1, min(16, len(os.sched_getaffinity(0))))) as ex:
+        list(ex.map(one, range(n)))
+
+
+def ladder_inputs(pinned=False):
+    """A[abef] (V^4) and B[efij] (V^2 O^2), column-major in label order, as
+    numpy arrays (backed by pinned torch host memory when `pinned`), plus a
+    zeroed column-major C[abij]; the returned torch tensors keep the pinned
+    storage alive."""
+    import numpy as np
+    keep = []
+
+    def empty(shape):
+        n = 1
+        for x in shape:
+            n *= x
+        if pinned:
+            import torch
+            t = torch.empty(n, dtype=torch.float64).pin_memory()
+            keep.append(t)
+            flat = t.numpy()
+        else:
+            flat = np.empty(n, dtype=np.float64)
+        return flat, flat.reshape(shape, order="F")
+    fa, A = empty((V, V, V, V))
+    fb, B = empty((V, V, O, O))
+    fc, C = empty((V, V, O, O))
+    fill_spread(fa, SEED_A)
+    fill_spread(fb, SEED_B)
+    fc[:] = 0.0
+    return A, B, C, keep
+
+
+def host_cpu():
+    """(threads usable by this process, physical cores among them, CPU model)."""
+    cpus = sorted(os.sched_getaffinity(0))
+    model, phys, cur = None, set(), {}
+    try:
+        for line in open("/proc/cpuinfo"):
+            if ":" not in line:
+                if cur.get("processor") is not None and int(cur["processor"]) in cpus:
+                    phys.add((cur.get("physical id"), cur.get("core id")))
+                cur = {}
+                continue
+            k, v = [x.strip() for x in line.split(":", 1)]
+            cur[k] = v
+            if k == "model name" and model is None:
+                model = v
+        if cur.get("processor") is not None and int(cur["processor"]) in cpus:
+            phys.add((cur.get("physical id"), cur.get("core id")))
+    except OSError:
+        pass
+    return len(cpus), (len(phys) or len(cpus)), model
+
+
+def normwise(got, want):
+    """||got - want||_F / ||want||_F over numpy arrays."""
+    import numpy as np
+    return float(np.linalg.norm((got - want).ravel(order="K")) / np.linalg.norm(want.ravel(order="K")))
+
+
+# ---------------------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the TBLIS reference compiled from its own sources)
+# ---------------------------------------------------------------------------------------
+
+def cpu_reference_ladder(A, B, reps=2):
+    """Times the reference's tblis_tensor_mult on the whole ladder (the same
+    inputs as the GPU arm), best of `reps`, with every usable host thread.
+    Returns (GFLOP/s, threads, physical cores, model, sample text, C)."""
     import numpy as np
     import oracle
     if not oracle.have_ref():
         return None
-    cores = threads or os.cpu_count() or 1
-    rng = np.random.default_rng(0)
-    asub = 16
-
-    def spread(shape):
-        x = np.asfortranarray(rng.uniform(-1, 1, shape))
-        x *= np.ldexp(1.0, rng.integers(-20, 21, shape, dtype=np.int32))
-        return x
-    A = spread((asub, V, V, V))
-    B = spread((V, V, O, O))
-    C = np.asfortranarray(np.zeros((asub, V, O, O)))
-    flops = 2.0 * asub * V ** 3 * O * O
+    threads, phys, model = host_cpu()
+    C = np.zeros((V, V, O, O), order="F")
     best = None
     for _ in range(reps):
         t0 = time.perf_counter()
-        oracle.ref_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij", threads=cores)
+        oracle.ref_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij", threads=threads)
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
-    return flops / best / 1e9, cores, ("ladder slice a<16 of 160 (m=2560 of 25600, %.0f GFLOP), best of %d, "
-                                       "tblis_tensor_mult of the reference built from its own sources, %d threads"
-                                       % (flops / 1e9, reps, cores))
+    sample = ("the whole ladder (%.0f GFLOP, same inputs as the GPU arm), best of %d, tblis_tensor_mult of "
+              "the reference built from its own sources, %d threads on %d physical cores (%s)"
+              % (FLOPS_LADDER / 1e9, reps, threads, phys, model))
+    return FLOPS_LADDER / best / 1e9, threads, phys, model, sample, C
 
 
 def run_reference(args):
+    """The reference arm: the reference's own tblis_tensor_mult on the host
+    cores, one whole ladder contraction per step on the same seeded inputs
+    as the GPU arm, exactly W warm-up and K timed steps (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -106,25 +193,40 @@ def run_reference(args):
     if not oracle.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources at build time)"}))
         return
-    cores = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_reference_sample(cores, reps=1)
-    vals = []
-    t0 = time.perf_counter()
-    for _ in range(max(1, min(args.steps, 3))):
-        v, _, sample = cpu_reference_sample(cores, reps=1)
-        vals.append(v)
-    wall = time.perf_counter() - t0
-    value = statistics.median(vals)
+    threads, phys, model = host_cpu()
+    A, B, C, _ = ladder_inputs()
+
+    def step():
+        oracle.ref_mult(1.0, A, "abef", B, "efij", 0.0, C, "abij", threads=threads)
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    wall = sum(times)
+    value = FLOPS_LADDER * len(times) / wall / 1e9
+    sample = ("the whole ladder (%.0f GFLOP) per step, tblis_tensor_mult of the reference built from its own "
+              "sources, %d threads on %d physical cores (%s)" % (FLOPS_LADDER / 1e9, threads, phys, model))
     print(json.dumps({
-        "impl": "reference", "metric": "contraction GFLOP/s at <=1e-12 normwise rel err",
-        "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": len(vals), "warmup": args.warmup,
-        "ms_per_step": 1e3 * wall / len(vals), "higher_is_better": True, "scaling": "weak",
+        "impl": "reference", "metric": METRIC,
+        "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
-        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": "reference", "sample": sample},
+        "config": headline_config(),
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads, "physical_cores": phys,
+                         "cpu_model": model, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def headline_config():
+    """The headline workload, identical in every arm."""
+    return {"workload": WORKLOAD, "m": V * V, "n": O * O, "k": V * V, "inputs": INPUTS,
+            "tolerance": "normwise relative error <= 1e-12 against the reference's FP64 result",
+            "l2": "inputs larger than L2 (A is %.2f GB)" % (V ** 4 * 8 / 1e9),
+            "parallelism": "replicas (one ladder contraction per GPU per step)"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -143,7 +245,10 @@ class ClockSampler:
         self.gpu = ids[local_index] if local_index < len(ids) else str(local_index)
         # one file per rank: several ranks on one node must not share it
         name = "clocks_bench.csv" if local_index == 0 else "clocks_bench_rank%d.csv" % local_index
-        self.path = os.path.join(ROOT, "gpurun_out", name)
+        # TBLIS_B200_CLOCKS_DIR names where the samples go (default: the
+        # system's temporary directory)
+        import tempfile
+        self.path = os.path.join(os.environ.get("TBLIS_B200_CLOCKS_DIR") or tempfile.gettempdir(), name)
 
     def start(self):
         try:
@@ -181,23 +286,6 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
-
-
-def spread_tensor(torch, shape, seed, dev):
-    """uniform(-1,1) * 2^k, k uniform integer in [-20, 20], column-major in
-    label order, generated in chunks on the device."""
-    g = torch.Generator(device=dev)
-    g.manual_seed(seed)
-    rev = list(reversed(shape))
-    t = torch.empty(rev, dtype=torch.float64, device=dev)
-    flat = t.view(-1)
-    chunk = 1 << 26
-    for s in range(0, flat.numel(), chunk):
-        e = min(flat.numel(), s + chunk)
-        u = torch.empty(e - s, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
-        k = torch.randint(-20, 21, (e - s,), device=dev, generator=g, dtype=torch.int32)
-        flat[s:e] = torch.ldexp(u, k)
-    return t.permute(*reversed(range(len(shape))))
 
 
 def time_steps(torch, fn, steps, stream):
@@ -296,31 +384,32 @@ def main():
         return
 
     # --- headline workload: ladder with exponent spread --------------------------------
-    A = spread_tensor(torch, [V, V, V, V], 1001 + rank, dev)
-    B = spread_tensor(torch, [V, V, O, O], 1002 + rank, dev)
+    # the same host-generated bits on every rank and in every arm
+    hA, hB, hC, keep = ladder_inputs(pinned=True)
+    A = keep[0].to(dev).view(V, V, V, V).permute(3, 2, 1, 0)
+    B = keep[1].to(dev).view(O, O, V, V).permute(3, 2, 1, 0)
     C = torch.zeros((O, O, V, V), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
 
-    # method selection: Ozaki INT8 when it is built and meets 1e-12 on this input,
-    # else the plain FP64 DMMA path (its error is the FP64 rounding itself)
-    method, method_name, err = 1, "fp64_dmma", 0.0
-    Cref = torch.zeros_like(C)
-    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cref, "abij", method=1)
+    # method selection: Ozaki INT8 with the slice count the library picks for
+    # 1e-12, kept when it meets 1e-12 against the FP64 path on this input, else
+    # the plain FP64 DMMA path (its error is the FP64 rounding itself)
+    method, method_name, cfg_name = 1, "fp64_dmma", "b200_fp64"
+    Cfp = torch.zeros_like(C)
+    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cfp, "abij", method=1)
     try:
         rep = tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=2, tolerance=1e-12)
         torch.cuda.synchronize()
-        err = (torch.linalg.vector_norm(C - Cref) / torch.linalg.vector_norm(Cref)).item()
+        err = (torch.linalg.vector_norm(C - Cfp) / torch.linalg.vector_norm(Cfp)).item()
         if err <= 1e-12:
-            method, method_name = 2, "ozaki_int8_%d_slices" % rep["slices"]
+            method, method_name, cfg_name = 2, "ozaki_int8_%d_slices" % rep["slices"], "b200_ozaki_i8"
     except tb.TblisError:
         pass
-    del Cref
-    torch.cuda.empty_cache()
 
     def step():
         tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
 
     def step_fp64():
-        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=1)
+        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cfp, "abij", method=1)
 
     for _ in range(args.warmup):
         step()
@@ -344,28 +433,25 @@ def main():
     ms_per_step = total_ms / args.steps
     value = job_value(world, args.steps, total_ms)
 
-    # end to end through the C ABI with pinned host buffers (copies inside the
-    # timed region), on every rank, max over ranks; del the device copies first
+    # end to end through tblis_tensor_mult(NULL, tblis_get_config(cfg_name), ...)
+    # with the pinned host buffers (copies inside the timed region), on every
+    # rank, max over ranks
     e2e = None
     if not args.no_e2e:
-        del A, B, C
-        torch.cuda.empty_cache()
         if dist:
             dist.barrier()
-        e2e = e2e_ladder(torch, tb, method, max(2, min(args.steps, 3)), rank)
+        e2e = e2e_ladder(torch, tb, cfg_name, max(2, min(args.steps, 3)), hA, hB, hC)
         e2e_ms = max_over_ranks(dist, torch, e2e["ms_per_step"], dev)
         e2e["ms_per_step"] = e2e_ms
         e2e["value"] = job_value(world, 1, e2e_ms)
 
     result = {
-        "metric": "contraction GFLOP/s at <=1e-12 normwise rel err",
+        "metric": METRIC,
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "method": method_name, "m": V * V, "n": O * O, "k": V * V,
-                   "normwise_rel_err_vs_fp64": err,
-                   "l2": "inputs larger than L2 (A is %.2f GB)" % (V ** 4 * 8 / 1e9),
-                   "parallelism": "replicas x%d (one contraction per GPU)" % world},
+        "config": headline_config(),
+        "method": method_name,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -373,10 +459,6 @@ def main():
         result["e2e"] = e2e
 
     if rank == 0:
-        if e2e:
-            A = spread_tensor(torch, [V, V, V, V], 1001, dev)
-            B = spread_tensor(torch, [V, V, O, O], 1002, dev)
-            C = torch.zeros((O, O, V, V), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
         peaks = load_peaks()
         extra = {}
         # plain FP64 rate on the same workload and the roofline of its kernel
@@ -419,22 +501,45 @@ def main():
                                   "share_of_step": k_total_ms / total_ms,
                                   "fp64_equivalent_tflops_kernel": FLOPS_LADDER * units_per_launch /
                                                                    (launch_ms * 1e-3) / 1e12}
+
+        # accuracy: every GPU result against the reference's own FP64 output
+        # on the same inputs (N=1: the CPU leg computes it); with several
+        # ranks, against the library's FP64 path
+        acc = {}
+        Cref_dev = None
+        if world == 1 and not args.no_cpu:
+            cb = cpu_reference_ladder(hA, hB)
+            if cb:
+                v, threads, phys, model, sample, Cref = cb
+                result["cpu_baseline"] = {"value": v, "unit": "GFLOP/s", "cores": threads, "physical_cores": phys,
+                                          "cpu_model": model, "kind": "reference", "sample": sample}
+                acc["against"] = "the reference's tblis_tensor_mult (FP64, CPU) on the same inputs"
+                acc["normwise_rel_err_vs_reference"] = normwise(
+                    C.permute(3, 2, 1, 0).cpu().numpy().transpose(3, 2, 1, 0), Cref)
+                acc["fp64_path_normwise_rel_err_vs_reference"] = normwise(
+                    Cfp.permute(3, 2, 1, 0).cpu().numpy().transpose(3, 2, 1, 0), Cref)
+                if e2e:
+                    e2e["normwise_rel_err_vs_reference"] = normwise(hC, Cref)
+                Cref_dev = torch.from_numpy(Cref.transpose(3, 2, 1, 0).copy()).to(dev).permute(3, 2, 1, 0)
+                del Cref
+        if Cref_dev is None:
+            acc["against"] = "the library's plain FP64 path on the same inputs"
+            acc["normwise_rel_err_vs_fp64_path"] = (torch.linalg.vector_norm(C - Cfp) /
+                                                    torch.linalg.vector_norm(Cfp)).item()
+        err = acc.get("normwise_rel_err_vs_reference", acc.get("normwise_rel_err_vs_fp64_path"))
+        acc["meets_1e-12"] = bool(err is not None and err <= 1e-12)
+        result["accuracy"] = acc
+
         if not args.no_extra and world == 1:
-            extra["precision_variants"] = precision_variants(torch, tb, A, B, C, stream)
-        del A, B, C
+            extra["precision_variants"] = precision_variants(torch, tb, A, B, C, stream,
+                                                             Cref_dev if Cref_dev is not None else Cfp)
+        del A, B, C, Cfp, Cref_dev
         torch.cuda.empty_cache()
 
         # the secondary workloads are single-GPU; with several ranks the others
         # would wait at the closing barrier for minutes
         if not args.no_extra and world == 1:
-            extra.update(extra_workloads(torch, tb, dev, stream, peaks))
-
-        if world == 1 and not args.no_cpu:
-            cb = cpu_reference_sample()
-            if cb:
-                v, cores, sample = cb
-                result["cpu_baseline"] = {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "reference",
-                                          "sample": sample}
+            extra.update(extra_workloads(torch, tb, dev, stream, peaks, check=not args.no_cpu))
         result["extra"] = extra
         print(json.dumps(result))
     if dist:
@@ -442,14 +547,12 @@ def main():
         dist.destroy_process_group()
 
 
-def precision_variants(torch, tb, A, B, C, stream):
+def precision_variants(torch, tb, A, B, C, stream, Cref):
     """The ladder under every arithmetic the library offers: plain FP64 DMMA,
     Ozaki INT8 and BF16 slices with 3..8 slices, one TF32 and one BF16 pass.
-    Error = normwise relative difference to the FP64 DMMA result (which the
-    GPU tests pin to the FP64 oracle within 1e-13); rate = FP64-equivalent
-    GFLOP/s of the whole call (statistics, slicing and GEMM), mean of 2."""
-    Cref = torch.zeros_like(C)
-    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cref, "abij", method=1)
+    Error = normwise relative difference to Cref (the reference's own FP64
+    result on the same inputs at N=1); rate = FP64-equivalent GFLOP/s of the
+    whole call (statistics, slicing and GEMM), mean of 2."""
     nref = torch.linalg.vector_norm(Cref).item()
     runs = [("fp64_dmma", 1, 0)]
     runs += [("ozaki_int8", 2, s) for s in range(3, 9)]
@@ -465,7 +568,6 @@ def precision_variants(torch, tb, A, B, C, stream):
         total, _ = time_steps(torch, call, 2, stream)
         out.append({"variant": name, "slices": slices, "normwise_rel_err": err,
                     "gflops_fp64_equiv": FLOPS_LADDER * 2 / (total * 1e-3) / 1e9})
-    del Cref
     return out
 
 
@@ -485,42 +587,38 @@ def job_value(world, steps, total_ms):
     return world * FLOPS_LADDER * steps / (total_ms * 1e-3) / 1e9
 
 
-def e2e_ladder(torch, tb, method, steps, rank=0):
-    A = spread_tensor(torch, [V, V, V, V], 1001 + rank, torch.device("cuda")).cpu().pin_memory()
-    B = spread_tensor(torch, [V, V, O, O], 1002 + rank, torch.device("cuda")).cpu().pin_memory()
-    C = torch.zeros((O, O, V, V), dtype=torch.float64).pin_memory().permute(3, 2, 1, 0)
-    h2d = (A.numel() + B.numel()) * 8
-    d2h = C.numel() * 8
-    tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
+def e2e_ladder(torch, tb, cfg_name, steps, hA, hB, hC):
+    """The same contraction through tblis_tensor_mult(NULL,
+    tblis_get_config(cfg_name), ...) on pinned host buffers: the H2D copies of
+    A and B and the D2H copy of C happen inside every call."""
+    cfg = tb.get_config(cfg_name)
+    h2d = (hA.size + hB.size) * 8
+    d2h = hC.size * 8
+    tb.mult(1.0, hA, "abef", hB, "efij", 0.0, hC, "abij", cfg=cfg)
     t0 = time.perf_counter()
     for _ in range(steps):
-        tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, C, "abij", method=method, tolerance=1e-12)
+        tb.mult(1.0, hA, "abef", hB, "efij", 0.0, hC, "abij", cfg=cfg)
     dt = (time.perf_counter() - t0) / steps
-    # the host result against the plain FP64 path on the device (outside the timed region)
-    dev = torch.device("cuda")
-    dA, dB = A.to(dev), B.to(dev)
-    Cref = torch.zeros((O, O, V, V), dtype=torch.float64, device=dev).permute(3, 2, 1, 0)
-    tb.mult_ex(1.0, dA, "abef", dB, "efij", 0.0, Cref, "abij", method=1)
-    err = (torch.linalg.vector_norm(C.to(dev) - Cref) / torch.linalg.vector_norm(Cref)).item()
-    del dA, dB, Cref
-    torch.cuda.empty_cache()
     return {"value": FLOPS_LADDER / dt / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "normwise_rel_err_vs_fp64": err,
-            "note": "host pinned buffers through tblis_tensor_mult; H2D of A,B and D2H of C inside each call "
-                    "(the library copies A in slabs of rows of C overlapped with the contraction of the slabs "
-                    "already copied, and each slab of C back as soon as it is final)"}
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3,
+            "call": "tblis_tensor_mult(NULL, tblis_get_config(\"%s\"), ...)" % cfg_name,
+            "note": "host pinned buffers; H2D of A,B and D2H of C inside each call (the library copies A in "
+                    "slabs of rows of C overlapped with the contraction of the slabs already copied, and each "
+                    "slab of C back as soon as it is final)"}
 
 
 OCC = [12, 4, 8, 6, 10, 3, 7, 5]
 VIR = [60, 22, 40, 30, 52, 14, 36, 26]
 
 
-def dpd_workload(torch, tb, dev, stream):
+def dpd_workload(torch, tb, dev, stream, check=True):
     """DPD ladder C[abij] = A[abef]*B[efij] under D2h (8 irreps, XOR, total
     irrep 0), occ [12,4,8,6,10,3,7,5], vir [60,22,40,30,52,14,36,26], default
     MArray layout; one grouped launch per call (graph-replayed). Returns the
     DPD rate and the dense-equivalent rate: dense FP64 GEMMs of the same
-    per-irrep M x N x K on the same kernel."""
+    per-irrep M x N x K on the same kernel; with `check`, the normwise error of
+    C against the reference's own DPD contraction on the same inputs."""
+    import numpy as np
     out = {}
     g = torch.Generator(device=dev)
     g.manual_seed(41)
@@ -556,16 +654,32 @@ def dpd_workload(torch, tb, dev, stream):
         del a, b, c
     out["dpd_dense_equiv_gflops"] = tot_f / (tot_ms * 1e-3) / 1e9
     out["dpd_frac_of_dense_equiv"] = out["dpd_gflops"] / out["dpd_dense_equiv_gflops"]
+    if check:
+        # the grouped launch's C against the reference's own DPD tblis::mult
+        # (src/internal/3t/dpd/mult.cxx:1067-1267) on the host, same inputs
+        import oracle
+        if oracle.have_ref():
+            threads, _, _ = host_cpu()
+            oracle.ref().tblis_set_num_threads(threads)
+            hA, hB = A.data.cpu().numpy(), B.data.cpu().numpy()
+            want = np.zeros(C.size())
+            t0 = time.perf_counter()
+            oracle.ref_dpd_mult(8, 1.0, 0, [VIR] * 4, hA, "abef", 0, [VIR, VIR, OCC, OCC], hB, "efij",
+                                0.0, 0, [VIR, VIR, OCC, OCC], want, "abij")
+            out["dpd_reference_s"] = time.perf_counter() - t0
+            out["dpd_normwise_rel_err_vs_reference"] = normwise(C.data.cpu().numpy(), want)
+            del hA, hB, want
     del A, B, C
     torch.cuda.empty_cache()
     return out
 
 
-def batch_workload(torch, tb, dev, stream, count=10000, serial_sample=500):
+def batch_workload(torch, tb, dev, stream, count=10000, serial_sample=500, check=True, check_sample=400):
     """A batch of `count` independent 4-index contractions (2 labels per group,
     extents uniform 4..32, random index order of every operand) in one grouped
     launch, against the same contractions issued one call at a time (timed on
-    the first `serial_sample` and scaled)."""
+    the first `serial_sample` and scaled); with `check`, a seeded sample of
+    `check_sample` members against the reference on the host."""
     import random
     rnd = random.Random(0)
     g = torch.Generator(device=dev)
@@ -605,9 +719,24 @@ def batch_workload(torch, tb, dev, stream, count=10000, serial_sample=500):
         tb.mult(*it)
     torch.cuda.synchronize()
     serial_s = (time.perf_counter() - t0) * count / len(sample)
-    return {"batch_count": count, "batch_gflop": flops / 1e9, "batch_gflops": flops / batch_s / 1e9,
-            "batch_ms": batch_s * 1e3, "batch_call_ms_incl_host": device_ms, "serial_gflops_est": flops / serial_s / 1e9,
-            "batch_speedup_vs_serial": serial_s / batch_s}
+    out = {"batch_count": count, "batch_gflop": flops / 1e9, "batch_gflops": flops / batch_s / 1e9,
+           "batch_wall_ms": batch_s * 1e3, "batch_event_ms": device_ms, "serial_gflops_est": flops / serial_s / 1e9,
+           "batch_speedup_vs_serial": serial_s / batch_s}
+    if check:
+        # a seeded sample of members (their C holds the batch's last result:
+        # beta is 0) against the reference's tblis_tensor_mult on the host
+        import numpy as np
+        import oracle
+        if oracle.have_ref():
+            errs = []
+            for j in random.Random(1).sample(range(count), check_sample):
+                al, a, ia, b, ib, be, c, ic = items[j]
+                want = np.zeros(c.shape, order="F")
+                oracle.ref_mult(al, a.cpu().numpy(), ia, b.cpu().numpy(), ib, 0.0, want, ic, threads=1)
+                errs.append(normwise(c.cpu().numpy(), want))
+            out["batch_checked_members"] = len(errs)
+            out["batch_max_normwise_rel_err_vs_reference"] = max(errs)
+    return out
 
 
 def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
@@ -766,7 +895,7 @@ def single_case(torch, tb, dev, stream, args):
             "ms_per_step": total / args.steps}
 
 
-def extra_workloads(torch, tb, dev, stream, peaks):
+def extra_workloads(torch, tb, dev, stream, peaks, check=True):
     out = {}
     for rate, n in ((2000, 2000), (50, 150), (1e9, 2000)):
         try:
@@ -774,11 +903,11 @@ def extra_workloads(torch, tb, dev, stream, peaks):
         except Exception as e:
             out["serve_%d_error" % rate] = str(e)[:200]
     try:
-        out.update(dpd_workload(torch, tb, dev, stream))
+        out.update(dpd_workload(torch, tb, dev, stream, check))
     except Exception as e:     # keep the headline line even if a secondary workload fails
         out["dpd_error"] = str(e)[:200]
     try:
-        out.update(batch_workload(torch, tb, dev, stream))
+        out.update(batch_workload(torch, tb, dev, stream, check=check))
     except Exception as e:
         out["batch_error"] = str(e)[:200]
     torch.cuda.empty_cache()

@@ -471,12 +471,17 @@ int tblis_b200_tensor_mult_shard(const tblis_config* cfg,
  * synchronise the device): the same FP64 DMMA kernel, with its scatter vectors
  * and split-K partial tiles in one fixed file-scope device array of
  * TBLIS_B200_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
- * until exit. Tensors must be in device memory; a contraction whose scatter
- * vectors exceed the array is rejected (TB_ERR_SIZE = 5), and split-K is
- * reduced until its partials fit. Calls share the array: calls that overlap on
- * the GPU race and must be serialised. The first call on a device looks up the
- * array's address; make it before any stream capture. Returns 0 or an error
- * code (also recorded as the last error). */
+ * until exit. Where tblis_tensor_mult would run the FP64 path, it gives the
+ * same result, with these differences: only double tensors (TB_ERR_TYPE = 2
+ * otherwise), device memory only (host data is TB_ERR_ARG = 1: staging it
+ * would allocate), no Ozaki or other method from a config. alpha == 0 or an
+ * empty contracted extent sets or scales C by beta, as tblis_tensor_mult does.
+ * A contraction whose scatter vectors exceed the array is rejected
+ * (TB_ERR_SIZE = 5), and split-K is reduced until its partials fit. Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised. The first call on a device looks up the array's address; make
+ * it before any stream capture. A failed call leaves C and its scalar as they
+ * were. Returns 0 or an error code (also recorded as the last error). */
 #define TBLIS_B200_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int tblis_b200_tensor_mult_noalloc(const tblis_tensor* A, const label_type* idx_A,
                                    const tblis_tensor* B, const label_type* idx_B,

@@ -16,6 +16,8 @@
 //  * tensors must already be in device (or managed) memory: host data would
 //    need a staging buffer, which is an allocation, so host pointers are
 //    rejected with TB_ERR_ARG;
+//  * alpha == 0 or an empty contracted extent sets C (beta == 0) or scales it
+//    by beta, as tblis_tensor_mult does; that path needs no scratch at all;
 //  * scatter vectors plus split-K partials must fit in
 //    TBLIS_B200_NOALLOC_SCRATCH_BYTES; when the partials do not fit the
 //    split-K factor is reduced (down to no split), and a contraction whose
@@ -24,6 +26,8 @@
 //    in it has to start at zero (each call overwrites every word it reads),
 //    but calls whose work overlaps on the GPU -- concurrent streams, or
 //    several host threads -- race on it and must be serialised by the caller;
+//  * a call that fails leaves C and its scalar untouched, as
+//    tblis_tensor_mult does;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (the array's name is only a host-side stand-in in
 //    host code); make that first call before any stream capture.
@@ -31,6 +35,7 @@
 #include "planner.hpp"
 #include "gemm_f64.hpp"
 #include "mult.hpp"
+#include "level1.hpp"
 
 #include <algorithm>
 #include <mutex>
@@ -93,11 +98,26 @@ void run_noalloc(const tblis_tensor* A, const label_type* idx_A,
                      "noalloc mult: tensors must be in device memory (host data would need a staging allocation)");
     }
 
-    if (v.m*v.n*v.l != 0)
+    if (v.m*v.n*v.l != 0 && (alpha == 0.0 || v.k == 0))
     {
-        TB_CHECK(alpha != 0.0 && v.k != 0, TB_ERR_ARG,
-                 "noalloc mult: alpha == 0 or an empty contracted extent (use tblis_tensor_scale on C)");
-
+        // no product: C = beta*C over all its dims, or C = 0 without reading
+        // it (src/iface/3t/mult.cxx:133-148)
+        if (beta != 1.0)
+        {
+            Strided s;
+            ivec len, str;
+            for (size_t i = 0; i < v.lenM.size(); i++) { len.push_back(v.lenM[i]); str.push_back(v.cM[i]); }
+            for (size_t i = 0; i < v.lenN.size(); i++) { len.push_back(v.lenN[i]); str.push_back(v.cN[i]); }
+            for (size_t i = 0; i < v.lenL.size(); i++) { len.push_back(v.lenL[i]); str.push_back(v.cL[i]); }
+            TB_CHECK(len.size() <= (size_t)L1_MAX_DIM, TB_ERR_SIZE, "too many dimensions");
+            s.ndim = (int)len.size();
+            for (size_t i = 0; i < len.size(); i++) { s.len[i] = len[i]; s.stride[i] = str[i]; }
+            if (beta == 0.0) l1_set<double>(static_cast<double*>(C->data), s, 0.0, st);
+            else l1_scale<double>(static_cast<double*>(C->data), s, beta, st);
+        }
+    }
+    else if (v.m*v.n*v.l != 0)
+    {
         const i64 BM = gemm_f64_tile_m(), BN = gemm_f64_tile_n(), BK = gemm_f64_tile_k();
         const i64 nkb = (v.k + BK - 1)/BK;
         const size_t n_tab = 2*v.m + 2*v.k + 2*v.n + 3*v.l + 2*nkb;
@@ -142,6 +162,12 @@ void run_noalloc(const tblis_tensor* A, const label_type* idx_A,
         a.M = v.m; a.N = v.n; a.K = v.k; a.L = v.l;
         a.alpha = alpha; a.beta = beta;
         a.amode = v.amode; a.bmode = v.bmode;
+        // 16-byte pair gathers where the layout gives them, decided as for
+        // tblis_tensor_mult (the kernel still checks every pair)
+        bool a_pairs[2], b_pairs[2];
+        gemm_pair_modes(v, a_m, a_k, b_n, b_k, a_l, b_l, a_pairs, b_pairs);
+        a.pair_a = a_pairs[v.amode] && ((uintptr_t)a.A & 15) == 0;
+        a.pair_b = b_pairs[v.bmode] && ((uintptr_t)a.B & 15) == 0;
 
         // split-K partials go after the tables; shrink the split until they fit
         int splits = gemm_f64_choose_splits(v.m, v.n, v.k, v.l, device_sm_count());

@@ -11,10 +11,11 @@
 //     x' = (sum_p d_p 254^(1-p) + r_S 254^(1-S))/127 with |r_S| <= 1/2.
 //     Digits are written straight from the strided tensor (through the
 //     GEMM view's scatter vectors) as tiled INT8 planes: for each row tile
-//     (128 rows of A, 64 of B) and k step (32 bytes), the S slice tiles lie
+//     (128 rows of A, BN rows of B) and k step (32 bytes), the S slice tiles lie
 //     back to back in one block, each in the tensor core's canonical K-major
 //     layout, so that a stage is one bulk copy per operand;
-//  3. one fused tcgen05 kernel per 128x64 output tile: for every k step,
+//  3. one fused tcgen05 kernel per 128xBN output tile (BN = 128 for S <= 4,
+//     96 for S = 5, 80 for S = 6, 64 for S = 7-8 and for BF16 digits): for every k step,
 //     the bulk-copy engine brings the S slice tiles of A and B into shared
 //     memory and one thread
 //     issues tcgen05.mma.kind::i8 for the slice pairs (p, q) with

@@ -429,6 +429,21 @@ static void pair_stats(const i64* t, i64 n, double& adj, double& even)
     even = n > 0 ? (double)e/(double)n : 0.0;
 }
 
+void gemm_pair_modes(const GemmView& v, const i64* a_m, const i64* a_k, const i64* b_n, const i64* b_k,
+                     const i64* a_l, const i64* b_l, bool a_pairs[2], bool b_pairs[2])
+{
+    double am_adj, am_even, ak_adj, ak_even, bn_adj, bn_even, bk_adj, bk_even, l_adj, l_even_a, l_even_b;
+    pair_stats(a_m, v.m, am_adj, am_even); pair_stats(a_k, v.k, ak_adj, ak_even);
+    pair_stats(b_n, v.n, bn_adj, bn_even); pair_stats(b_k, v.k, bk_adj, bk_even);
+    pair_stats(a_l, v.l, l_adj, l_even_a); pair_stats(b_l, v.l, l_adj, l_even_b);
+    const double q = 0.9;
+    const bool la = l_even_a == 1.0, lb = l_even_b == 1.0;
+    a_pairs[0] = la && am_adj >= q && ak_even >= q;
+    a_pairs[1] = la && ak_adj >= q && am_even >= q;
+    b_pairs[0] = lb && bn_adj >= q && bk_even >= q;
+    b_pairs[1] = lb && bk_adj >= q && bn_even >= q;
+}
+
 std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 BK,
                                         cudaStream_t stream)
 {
@@ -477,18 +492,7 @@ std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 B
     auto t = std::make_shared<GemmTables>();
     t->a_m_step = affine_step(a_m, v.m); t->a_k_step = affine_step(a_k, v.k);
     t->b_n_step = affine_step(b_n, v.n); t->b_k_step = affine_step(b_k, v.k);
-    {
-        double am_adj, am_even, ak_adj, ak_even, bn_adj, bn_even, bk_adj, bk_even, l_adj, l_even_a, l_even_b;
-        pair_stats(a_m, v.m, am_adj, am_even); pair_stats(a_k, v.k, ak_adj, ak_even);
-        pair_stats(b_n, v.n, bn_adj, bn_even); pair_stats(b_k, v.k, bk_adj, bk_even);
-        pair_stats(a_l, v.l, l_adj, l_even_a); pair_stats(b_l, v.l, l_adj, l_even_b);
-        const double q = 0.9;
-        const bool la = l_even_a == 1.0, lb = l_even_b == 1.0;
-        t->a_pairs[0] = la && am_adj >= q && ak_even >= q;
-        t->a_pairs[1] = la && ak_adj >= q && am_even >= q;
-        t->b_pairs[0] = lb && bn_adj >= q && bk_even >= q;
-        t->b_pairs[1] = lb && bk_adj >= q && bn_even >= q;
-    }
+    gemm_pair_modes(v, a_m, a_k, b_n, b_k, a_l, b_l, t->a_pairs, t->b_pairs);
     t->bytes = n_total*sizeof(i64);
     TB_CUDA(cudaMalloc(&t->dev, t->bytes));
     TB_CUDA(cudaMemcpyAsync(t->dev, host.data(), t->bytes, cudaMemcpyHostToDevice, stream));

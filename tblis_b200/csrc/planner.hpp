@@ -78,6 +78,11 @@ struct GemmTables
     ~GemmTables();
 };
 
+// Decides, from a view's host scatter vectors, whether the FP64 kernel may
+// gather A and B in 16-byte pairs in each gather mode (GemmTables::a_pairs).
+void gemm_pair_modes(const GemmView& v, const i64* a_m, const i64* a_k, const i64* b_n, const i64* b_k,
+                     const i64* a_l, const i64* b_l, bool a_pairs[2], bool b_pairs[2]);
+
 // Builds (or fetches from the plan cache) the device tables for a view.
 std::shared_ptr<GemmTables> gemm_tables(const GemmView& v, i64 BM, i64 BN, i64 BK,
                                         cudaStream_t stream);

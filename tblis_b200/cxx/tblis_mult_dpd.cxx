@@ -13,8 +13,10 @@
 //
 // Each view is described to the C ABI by the geometry of its stored blocks as
 // the view itself reports it (operator()(irreps), dpd_varray_base.hpp:482-508),
-// so permuted views work as well as the six storage layouts. Only double
-// computes on the GPU; the other types record TB_ERR_TYPE as the last error.
+// so permuted views work as well as the six storage layouts. Every
+// instantiated type computes on the GPU: double directly, dcomplex as four
+// real contractions, float and scomplex widened to double on the device and
+// rounded back.
 //
 // Threading follows TCI's contract (src/util/thread.h:333-352): every thread
 // of the communicator enters; the master thread issues the GPU work and the

@@ -3,7 +3,7 @@
 `strides` and `offsets` tables, and the tensor they describe: irrep 1,
 2 irreps, lengths {{3,1},{2,2},{1,2},{3,4}}) into dpd_layout_golden.json.
 
-    python tests/golden/make_dpd_golden.py /root/reference
+    python tests/golden/make_dpd_golden.py <tblis source tree>   (default: $TBLIS_REFERENCE)
 """
 import json
 import os
@@ -64,4 +64,4 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TBLIS_REFERENCE", "/root/reference"))
