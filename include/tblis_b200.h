@@ -149,10 +149,11 @@ unsigned tblis_get_num_threads(void);
 void tblis_set_num_threads(unsigned num_threads);
 
 /* src/util/configs.h:11: returns a GPU configuration by name, or NULL.
- * Names: "b200_fp64" (default; FP64 DMMA), "b200_ozaki_i8" and
- * "b200_ozaki_bf16" (Ozaki INT8 / BF16 slices on tcgen05, slice count chosen
- * from the tolerance), "b200_tf32" and "b200_bf16" (one low-precision pass
- * with FP32 accumulation). */
+ * Names: "b200_fp64" (default; FP64 DMMA), "b200_ozaki_i8" (Ozaki INT8 on
+ * tcgen05: slices or moduli, whichever needs less INT8 work for the
+ * tolerance), "b200_ozaki_bf16" (Ozaki BF16 slices), "b200_ozaki_crt" (Ozaki
+ * INT8 over pairwise-coprime moduli only, scheme II), "b200_tf32" and
+ * "b200_bf16" (one low-precision pass with FP32 accumulation). */
 const tblis_config* tblis_get_config(const char* name);
 
 /* ---- extensions (no counterpart in the reference) ------------------------ */
@@ -178,17 +179,20 @@ double tblis_b200_config_get_tolerance(const tblis_config* cfg);
 /* Per-call options and report of the extended contraction entry point. */
 typedef struct tblis_b200_opts
 {
-    int method;          /* 0 = from cfg, 1 = FP64 DMMA, 2 = Ozaki INT8 slices,
-                            3 = Ozaki BF16 slices, 4 = one TF32 pass, 5 = one
-                            BF16 pass (FP32 accumulation; no tolerance) */
-    int slices;          /* Ozaki slice count; 0 = choose from tolerance */
+    int method;          /* 0 = from cfg, 1 = FP64 DMMA, 2 = Ozaki INT8 (slices
+                            or moduli, whichever needs less INT8 work for the
+                            tolerance), 3 = Ozaki BF16 slices, 4 = one TF32
+                            pass, 5 = one BF16 pass (FP32 accumulation; no
+                            tolerance), 6 = Ozaki INT8 over moduli (scheme II) */
+    int slices;          /* Ozaki slice count (method 2: forces slices) or
+                            moduli count (method 6, 2..16); 0 = from tolerance */
     double tolerance;    /* normwise relative target; 0 = from cfg */
 } tblis_b200_opts;
 
 typedef struct tblis_b200_report
 {
-    int method;          /* method that ran */
-    int slices;          /* slice count used (0 for FP64) */
+    int method;          /* method that ran (6 when method 2 chose moduli) */
+    int slices;          /* slice count, or moduli count for method 6 (0 for FP64) */
     double est_error;    /* a-priori normwise error estimate */
     double flops;        /* algorithmic FLOPs, 2*m*n*k*l */
     int64_t m, n, k, l;  /* GEMM view of the contraction */

@@ -176,8 +176,11 @@ def mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C, cfg=None, conj_A=False, conj
 def mult_ex(alpha, A, idx_A, B, idx_B, beta, C, idx_C, method=0, slices=0, tolerance=0.0, cfg=None,
             conj_A=False, conj_B=False):
     """mult with an explicit method and a report dict. Methods: 1 = FP64 DMMA,
-    2 = Ozaki INT8 slices, 3 = Ozaki BF16 slices (slice count from the
-    tolerance unless given), 4 = one TF32 pass, 5 = one BF16 pass."""
+    2 = Ozaki INT8 (slices or moduli, whichever needs less INT8 work; a given
+    slice count forces slices), 3 = Ozaki BF16 slices (slice count from the
+    tolerance unless given), 4 = one TF32 pass, 5 = one BF16 pass, 6 = Ozaki
+    INT8 over moduli (scheme II; `slices` counts the moduli). The report's
+    method is 6 when method 2 chose moduli."""
     a, b, c = _View(A, alpha, conj_A), _View(B, 1.0, conj_B), _View(C, beta)
     o = tblis_b200_opts(method, slices, tolerance)
     r = tblis_b200_report()

@@ -49,6 +49,7 @@ tblis_config_s g_cfgs[] = {
     {"b200_ozaki_bf16", 3, 1e-12},
     {"b200_tf32", 4, 1e-12},
     {"b200_bf16", 5, 1e-12},
+    {"b200_ozaki_crt", 6, 1e-12},
 };
 }
 

@@ -226,15 +226,21 @@ static void unstage(StagedOp& o, cudaStream_t s)
 // one contraction on device data (a GEMM view of device-resident operands)
 static void contract_device(const GemmView& v, const double* A, const double* B, double* C, double alpha,
                             double beta, int method, double tol, int slices, cudaStream_t st,
-                            int& used_slices, double& est_error)
+                            int& used_slices, double& est_error, int* used_method = nullptr)
 {
+    if (used_method) *used_method = method;
     if (method >= 2)
     {
-        // 2: Ozaki INT8 slices, 3: Ozaki BF16 slices, 4: one TF32 pass, 5: one BF16 pass
-        const int kind = method == 2 ? OZ_I8 : method == 4 ? OZ_TF32 : OZ_BF16;
-        OzakiResult r = ozaki_mult(v, A, B, C, alpha, beta, tol, slices, st, kind, method >= 4);
+        // 2: Ozaki INT8 (slices or moduli, whichever needs less work for tol),
+        // 3: Ozaki BF16 slices, 4: one TF32 pass, 5: one BF16 pass, 6: Ozaki
+        // INT8 over moduli (scheme II)
+        const int kind = method == 2 || method == 6 ? OZ_I8 : method == 4 ? OZ_TF32 : OZ_BF16;
+        const int scheme = method == 6 ? 2 : method == 2 && slices > 0 ? 1 : 0;
+        OzakiResult r = ozaki_mult(v, A, B, C, alpha, beta, tol, slices, st, kind, method == 4 || method == 5,
+                                   scheme);
         used_slices = r.slices;
         est_error = r.est_error;
+        if (used_method && kind == OZ_I8) *used_method = r.scheme == 2 ? 6 : 2;
         return;
     }
     const i64 BMt = gemm_f64_tile_m(), BNt = gemm_f64_tile_n(), BKt = gemm_f64_tile_k();
@@ -576,7 +582,7 @@ void mult_dispatch(const tblis_config* cfg,
         }
         else
         {
-            TB_CHECK(method >= 1 && method <= 5, TB_ERR_ARG, "unknown contraction method");
+            TB_CHECK(method >= 1 && method <= 6, TB_ERR_ARG, "unknown contraction method");
             stage(sb, B, true, st);
             Slices sl;
             Slabs sb2;
@@ -584,7 +590,7 @@ void mult_dispatch(const tblis_config* cfg,
             const bool slabbed = host_a && plan_slabs(A, idx_A, B, idx_B, C, idx_C, sb2);
             const bool sliced = host_a && !slabbed && plan_slices(A, idx_A, B, idx_B, C, idx_C, sl);
             stage(sa, A, !sliced && !slabbed, st);
-            int used = 0;
+            int used = 0, ran = method;
             double est = 0;
             if (slabbed)
             {
@@ -625,7 +631,8 @@ void mult_dispatch(const tblis_config* cfg,
                     int u = 0;
                     double e = 0;
                     contract_device(vs, static_cast<const double*>(a.data), static_cast<const double*>(b.data),
-                                    static_cast<double*>(cc.data), alpha, beta, method, tol, slices, st, u, e);
+                                    static_cast<double*>(cc.data), alpha, beta, method, tol, slices, st, u, e,
+                                    &ran);
                     used = std::max(used, u);
                     est = std::max(est, e);
                     if (sc.staged)
@@ -700,7 +707,7 @@ void mult_dispatch(const tblis_config* cfg,
                     double e = 0;
                     contract_device(vs, static_cast<const double*>(a.data), static_cast<const double*>(b.data),
                                     static_cast<double*>(cc.data), alpha, over_k && c > 0 ? 1.0 : beta, method,
-                                    tol_slice, slices, st, u, e);
+                                    tol_slice, slices, st, u, e, &ran);
                     used = std::max(used, u);
                     est = over_k ? est + e : std::max(est, e);
                 }
@@ -710,9 +717,10 @@ void mult_dispatch(const tblis_config* cfg,
             else
             {
                 contract_device(v, static_cast<const double*>(sa.dptr), static_cast<const double*>(sb.dptr),
-                                static_cast<double*>(sc.dptr), alpha, beta, method, tol, slices, st, used, est);
+                                static_cast<double*>(sc.dptr), alpha, beta, method, tol, slices, st, used, est,
+                                &ran);
             }
-            if (report) { report->slices = used; report->est_error = est; }
+            if (report) { report->slices = used; report->est_error = est; report->method = ran; }
         }
     }
 

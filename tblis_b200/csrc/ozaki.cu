@@ -44,10 +44,12 @@
 #include "mult.hpp"
 
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 
 namespace tb
@@ -611,6 +613,44 @@ __device__ __forceinline__ double pow2i(int n)
     return (n >= -1022 && n <= 1023) ? __longlong_as_double((long long)(n + 1023) << 52) : ldexp(1.0, n);
 }
 
+// ---- Ozaki scheme II (residues modulo pairwise-coprime moduli) ------------------
+//
+// a = rint(x*2^s) with |a| <= 2^50 is an exact integer; its residues modulo
+// the moduli m_q are INT8 planes, one INT8 GEMM per modulus gives
+// sum_k a*b exactly modulo m_q (INT32 accumulation, reduced mod m_q), and
+// the Chinese remainder theorem over M = prod m_q recovers the integer
+// product exactly while |sum_k a*b| < M/2 (the row and column scalings are
+// chosen so). The only rounding is that of a and b to integers.
+constexpr int CRT_MAX = 16;
+// 256 and the largest odd numbers below it that are coprime to all before
+__host__ __device__ constexpr int crt_modulus(int q)
+{
+    constexpr int m[CRT_MAX] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193};
+    return m[q];
+}
+
+struct CrtConsts
+{
+    int nm;                                  // moduli in use (the first nm)
+    float m[CRT_MAX], inv[CRT_MAX];          // m_q and fl(1/m_q)
+    float c16[CRT_MAX];                      // 2^16 mod m_q, in [0, m_q)
+    float g[CRT_MAX][CRT_MAX];               // g[q][j] = (m_0 ... m_(j-1)) mod m_q (centred)
+    float ginv[CRT_MAX];                     // (m_0 ... m_(q-1))^-1 mod m_q (centred)
+    double md[CRT_MAX];                      // m_q
+    double invd[CRT_MAX];                    // fl64(1/m_q)
+};
+
+constexpr float F_BIAS = 8388608.0f;         // 2^23: (0x4B000000 | u) as float is 2^23 + u
+constexpr float F_SHIFT = 12582912.0f;       // 1.5*2^23: rounds to an integer when added
+
+// r = t - m*rint(t/m), exact for |t| < 2^22 (the quotient may be off by one
+// at a tie of the rounded reciprocal, so |r| <= m/2 + 1/4)
+__device__ __forceinline__ float crt_reduce(float t, float m, float inv)
+{
+    const float q = __fsub_rn(__fmaf_rn(t, inv, F_SHIFT), F_SHIFT);
+    return __fmaf_rn(-q, m, t);
+}
+
 constexpr int SL_T = 64;     // 64 rows x 64 k per block
 
 // x' rounded to the nearest TF32 value (10 fraction bits), as FP32 bits
@@ -669,9 +709,10 @@ constexpr size_t SL_SMEM = 2*SL_T*SL_LD*sizeof(double);
 // beyond the operand, up to whole tiles and k steps, get zeros.
 // Persistent blocks walk the tiles; the gather of the next tile (cp.async,
 // zero-filled outside the operand) runs while the current one is converted.
-template <int S, int KIND, bool SINGLE>
+template <int S, int KIND, bool SINGLE, bool CRT = false>
 __global__ void __launch_bounds__(256, SL_BLOCKS_PER_SM)
-oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, unsigned tiles_r, unsigned tiles_k)
+oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, unsigned tiles_r, unsigned tiles_k,
+         const CrtConsts cc)
 {
     using T = typename PlaneElem<KIND>::T;
     constexpr int KE = OZ_BK/(int)sizeof(T);         // elements per k step
@@ -762,7 +803,51 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
                 return outb + (((i64)at.l*pg.tiles + rt)*pg.k_steps + k/KE)*S*tile_bytes +
                        tile_byte(rin, (int)(k % KE)*(int)sizeof(T));
             };
-            if constexpr (KIND == OZ_I8 && !SINGLE)
+            if constexpr (CRT)
+            {
+                // e_rows holds the row's shift s. y = 1.5*2^52 + a with
+                // a = rint(x*2^s) (one rounding, |a| <= 2^50); the low byte of
+                // y is a mod 256; for odd m, y - m*rint(a/m) = 1.5*2^52 + r
+                // exactly, |r| <= (m-1)/2, and its low word is r. Three FP64
+                // operations per modulus; 16 k bytes per plane row.
+                constexpr double SH = 6755399441055744.0;
+                const int sh1 = e >> 1, sh2 = e - sh1;
+                const double sc1 = pow2i(sh1), sc2 = pow2i(sh2);
+                double y[16], av[16];
+                #pragma unroll
+                for (int u = 0; u < 16; u++)
+                {
+                    y[u] = __fma_rn(__dmul_rn(src[u], sc1), sc2, SH);
+                    av[u] = __dsub_rn(y[u], SH);
+                }
+                const i64 plane_stride = tile_bytes;
+                unsigned char* dst = block(kk);
+                #pragma unroll
+                for (int q = 0; q < S; q++)
+                {
+                    uint32_t w[4];
+                    #pragma unroll
+                    for (int g = 0; g < 4; g++)
+                    {
+                        uint32_t b[4];
+                        #pragma unroll
+                        for (int u = 0; u < 4; u++)
+                        {
+                            const int i = g*4 + u;
+                            if (q == 0) b[u] = (uint32_t)__double2loint(y[i]);
+                            else
+                            {
+                                const double qm = __dsub_rn(__fma_rn(av[i], cc.invd[q], SH), SH);
+                                b[u] = (uint32_t)__double2loint(__fma_rn(-qm, cc.md[q], y[i]));
+                            }
+                        }
+                        // byte 0 of each word, four to a word
+                        w[g] = __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
+                    }
+                    *reinterpret_cast<uint4*>(dst + q*plane_stride) = make_uint4(w[0], w[1], w[2], w[3]);
+                }
+            }
+            else if constexpr (KIND == OZ_I8 && !SINGLE)
             {
                 // 2^-e*127 is exact: x*(2^-e*127) rounds once, as x'*127 does
                 const double sc = pow2i(-e)*first_digit_scale<KIND>();
@@ -824,8 +909,9 @@ oz_slice(const OzOperand o, const int* e_rows, void* out_, const PlaneGeom pg, u
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
-template <int S, int KIND, bool SINGLE>
-void launch_slice(const OzOperand& o, const int* e, void* out, const PlaneGeom& pg, cudaStream_t st)
+template <int S, int KIND, bool SINGLE, bool CRT = false>
+void launch_slice(const OzOperand& o, const int* e, void* out, const PlaneGeom& pg, cudaStream_t st,
+                  const CrtConsts* cc = nullptr)
 {
     // every row of the row tiles (64-row slicing tiles may pass the last
     // one: the kernel stops at it), every k of the k steps
@@ -835,11 +921,12 @@ void launch_slice(const OzOperand& o, const int* e, void* out, const PlaneGeom& 
     if (ntiles == 0) return;
     TB_CHECK(ntiles < ((i64)1 << 31), TB_ERR_SIZE, "Ozaki operand above 2^31 tiles of 64x64");
     const i64 grid = std::min<i64>(ntiles, (i64)device_sm_count()*SL_BLOCKS_PER_SM);
-    TB_CUDA(cudaFuncSetAttribute(oz_slice<S, KIND, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TB_CUDA(cudaFuncSetAttribute(oz_slice<S, KIND, SINGLE, CRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SL_SMEM));
+    CrtConsts none = {};
     TimedLaunch t("oz_slice", st);
-    oz_slice<S, KIND, SINGLE><<<(unsigned)grid, 256, SL_SMEM, st>>>(o, e, out, pg, (unsigned)tiles_r,
-                                                                     (unsigned)tiles_k);
+    oz_slice<S, KIND, SINGLE, CRT><<<(unsigned)grid, 256, SL_SMEM, st>>>(o, e, out, pg, (unsigned)tiles_r,
+                                                                          (unsigned)tiles_k, cc ? *cc : none);
     check_launch("oz_slice");
 }
 
@@ -870,6 +957,420 @@ void slice_dispatch(int kind, bool single, int S, const OzOperand& o, const int*
     }
     if (kind == OZ_I8) slice_dispatch_kind<OZ_I8>(S, o, e, out, pg, st);
     else slice_dispatch_kind<OZ_BF16>(S, o, e, out, pg, st);
+}
+
+// ---- Ozaki scheme II: INT8 GEMM per modulus and the CRT combination -------------
+
+constexpr int CRT_BN = 256;                    // output columns per tile (B plane row tile)
+constexpr int CRT_OUT_TILE = OZ_BM*CRT_BN;     // residue bytes of one output tile and modulus
+constexpr int CRT_KT_RUN = 4096;               // k steps whose INT32 sums stay exact: 4096*32*128^2 = 2^31
+
+struct CrtGemmArgs
+{
+    CUtensorMap tmA, tmB;          // the planes as 4-D maps (one modulus's tiles of four blocks per copy)
+    const unsigned char *pA, *pB;  // residue planes: blocks [l][row tile][k step] of nm tiles
+    unsigned char* R;              // residues [l][tile][modulus][128][256], each in [0, m_q)
+    i64 tiles_m, tiles_n;          // 128-row tiles of A (even), 256-column tiles of the output
+    int k_steps;                   // k steps of the planes
+    int kt0, kt1;                  // k steps of this launch (one exact run)
+    int nm, L;
+    float m[CRT_MAX], inv[CRT_MAX], c16[CRT_MAX];
+};
+
+// ---- the modulus GEMMs on CTA pairs (tcgen05 cta_group::2), persistent -------
+//
+// A cluster of two CTAs on one SM pair computes 256 x 256 output tiles: CTA
+// r holds rows 128r..128r+127 of A and columns 128r..128r+127 of B in its
+// shared memory, and each MMA of 256 x 256 x 32 issued by CTA 0 reads both
+// halves of B, so each SM reads half of B per MAC. A stage holds four k
+// steps (four MMAs per barrier round). Both CTAs copy their tiles with
+// cta_group::2 tensor copies (no multicast) that complete on CTA 0's
+// barrier, which expects the bytes of both; CTA 0's commits arrive on both
+// CTAs' barriers (tcgen05.commit multicast). The pair walks its share of
+// the (modulus, 256 x 256 tile) work items with two accumulators in tensor
+// memory, so the epilogue of one item (each CTA reading its accumulator
+// rows) overlaps the MMAs of the next; the epilogue warps of both CTAs
+// release an accumulator on CTA 0's barrier.
+
+constexpr int CRT_KSUB = 4;                    // k steps per stage
+constexpr int CRT2_STAGES = 6;                 // 32 KB per stage: 192 KB, one CTA per SM
+constexpr int CRT2_TILE = OZ_BM*OZ_BK;         // one 128-row x 32-byte tile (A, or a CTA's half of B)
+constexpr int CRT2_STAGE_BYTES = 2*CRT_KSUB*CRT2_TILE;
+constexpr uint32_t CRT2_TMEM_COLS = 512;       // two 128 x 256 INT32 accumulators
+
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// arrives on a barrier of another CTA of the cluster (a shared::cluster address)
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" :: "r"(cluster_addr) : "memory");
+}
+
+// modulus q's tiles of four consecutive plane blocks from block w (one
+// stage) into this CTA's shared memory, completing on CTA 0's barrier (a
+// shared::cluster address)
+__device__ __forceinline__ void tma_load_pair(void* dst, const CUtensorMap* map, int q, int w, uint32_t bar_cluster)
+{
+    asm volatile("cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %3, %4, %5}], [%2];"
+                 :: "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(bar_cluster), "r"(0), "r"(q), "r"(w) : "memory");
+}
+
+// arrives on the barrier at this offset in both CTAs of the pair once the
+// MMAs issued so far are complete
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 :: "r"(smem_u32(bar)), "h"((unsigned short)3) : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(slot)), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                 :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+constexpr size_t crt_gemm2_smem()
+{
+    return (size_t)CRT2_STAGES*CRT2_STAGE_BYTES + 1024 + (2*CRT2_STAGES + 4)*8 + 16;
+}
+
+// work item w of n_items: modulus-major, then the batch index, then 256-row
+// tiles, then 256-column tiles (consecutive pairs share A rows, and one
+// modulus's B planes stay in L2 while its items run)
+struct CrtItem { int q, l; i64 tm2, tn; };
+__device__ __forceinline__ CrtItem crt_item(i64 w, int L, i64 tiles_m2, i64 tiles_n)
+{
+    const i64 per_q = (i64)L*tiles_m2*tiles_n;
+    CrtItem it;
+    it.q = (int)(w / per_q);
+    i64 r = w - it.q*per_q;
+    it.l = (int)(r / (tiles_m2*tiles_n));
+    r -= (i64)it.l*tiles_m2*tiles_n;
+    it.tm2 = r / tiles_n;
+    it.tn = r - it.tm2*tiles_n;
+    return it;
+}
+
+// grid.x = 2 x (number of pairs), one CTA per SM; the planes have 128-row
+// tiles of A and B in blocks [l][row tile][k step] of nm tiles (k steps a
+// multiple of four); residues go out as column-major 128 x 256 tiles
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
+oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
+{
+    constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(CRT_BN >> 3) << 17) |
+                               ((uint32_t)(256 >> 4) << 24);      // s8 x s8 -> s32, M = 256, N = 256
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + CRT2_STAGES*CRT2_STAGE_BYTES);
+    uint64_t* empty = full + CRT2_STAGES;
+    uint64_t* tfull = empty + CRT2_STAGES;       // [2] accumulator ready
+    uint64_t* tempty = tfull + 2;                // [2] accumulator drained (CTA 0's count 8)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const i64 pair0 = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const i64 tiles_m2 = p.tiles_m >> 1;
+    const i64 n_items = (i64)p.nm*p.L*tiles_m2*p.tiles_n;
+    const int kt0 = p.kt0, kt_count = p.kt1 - p.kt0;    // a multiple of CRT_KSUB
+    const int nstage = kt_count/CRT_KSUB;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < CRT2_STAGES; s++)
+        {
+            mbar_init(&full[s], 1);       // CTA 0's: its producer's arrival plus both CTAs' bytes
+            mbar_init(&empty[s], 1);      // CTA 0's MMA commit, multicast to both
+        }
+        for (int b = 0; b < 2; b++)
+        {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 8);     // the four epilogue warps of each CTA
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc_pair(tmem_slot, CRT2_TMEM_COLS);
+    tc_fence_before();
+    // both CTAs' barriers and tensor memory exist before any remote arrive or MMA
+    cluster_sync_all();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            const uint32_t full0 = mapa_shared(smem_u32(full), 0);
+            int g = 0;                    // stage counter over all items
+            for (i64 w = pair0; w < n_items && !*abort_flag; w += npairs)
+            {
+                const CrtItem it = crt_item(w, p.L, tiles_m2, p.tiles_n);
+                const i64 tm = 2*it.tm2 + rank, tb = 2*it.tn + rank;
+                // plane blocks of this CTA's A and B tiles at k step kt0
+                const i64 a_blk = ((i64)it.l*p.tiles_m + tm)*p.k_steps + kt0;
+                const i64 b_blk = ((i64)it.l*2*p.tiles_n + tb)*p.k_steps + kt0;
+                for (int i = 0; i < nstage; i++, g++)
+                {
+                    const int s = g % CRT2_STAGES;
+                    if (g >= CRT2_STAGES && !mbar_wait(&empty[s], ((g/CRT2_STAGES) & 1) ^ 1, abort_flag)) break;
+                    unsigned char* st = smem + s*CRT2_STAGE_BYTES;
+                    if (rank == 0) mbar_expect_tx(&full[s], 2*CRT2_STAGE_BYTES);
+                    tma_load_pair(st, &p.tmA, it.q, (int)(a_blk + i*CRT_KSUB), full0 + 8u*(uint32_t)s);
+                    tma_load_pair(st + CRT_KSUB*CRT2_TILE, &p.tmB, it.q, (int)(b_blk + i*CRT_KSUB),
+                                  full0 + 8u*(uint32_t)s);
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0 && rank == 0)
+        {
+            int g = 0, j = 0;
+            for (i64 w = pair0; w < n_items && !*abort_flag; w += npairs, j++)
+            {
+                const int b = j & 1;
+                // the epilogues of both CTAs have drained this accumulator
+                if (j >= 2 && !mbar_wait(&tempty[b], ((j >> 1) & 1) ^ 1, abort_flag)) break;
+                tc_fence_after();
+                const uint32_t acc_addr = tmem_base + (uint32_t)(b*CRT_BN);
+                bool ok = true;
+                for (int i = 0; i < nstage; i++, g++)
+                {
+                    const int s = g % CRT2_STAGES;
+                    if (!mbar_wait(&full[s], (g/CRT2_STAGES) & 1, abort_flag)) { ok = false; break; }
+                    tc_fence_after();
+                    const unsigned char* st = smem + s*CRT2_STAGE_BYTES;
+                    #pragma unroll
+                    for (int u = 0; u < CRT_KSUB; u++)
+                        mma_i8_pair(acc_addr, sdesc_kmajor(st + u*CRT2_TILE),
+                                    sdesc_kmajor(st + (CRT_KSUB + u)*CRT2_TILE), IDESC, (i > 0 || u > 0) ? 1u : 0u);
+                    mma_commit_pair(&empty[s]);
+                }
+                if (!ok) break;
+                mma_commit_pair(&tfull[b]);
+            }
+        }
+    }
+    else
+    {
+        // warps 2..5: TMEM lane quarter warp % 4, one output row per thread
+        const int quarter = warp & 3;
+        const int row = quarter*32 + lane;
+        const uint32_t tempty0 = mapa_shared(smem_u32(tempty), 0);
+        int j = 0;
+        for (i64 w = pair0; w < n_items; w += npairs, j++)
+        {
+            const int b = j & 1;
+            if (!mbar_wait(&tfull[b], (j >> 1) & 1, abort_flag)) break;
+            tc_fence_after();
+            const CrtItem it = crt_item(w, p.L, tiles_m2, p.tiles_n);
+            const i64 tm = 2*it.tm2 + rank;
+            const int q = it.q;
+            const int mq = (int)p.m[q];
+            const float mf = p.m[q], inv = p.inv[q], c16 = p.c16[q];
+            // residue tiles are column-major (byte (col, row) at col*128 + row)
+            unsigned char* out = p.R + ((((i64)it.l*p.tiles_m + tm)*p.tiles_n + it.tn)*p.nm + q)*(i64)CRT_OUT_TILE + row;
+            #pragma unroll 1
+            for (int c = 0; c < CRT_BN/16; c++)
+            {
+                int r[16];
+                tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)(b*CRT_BN + c*16), r);
+                #pragma unroll
+                for (int jj = 0; jj < 16; jj++)
+                {
+                    uint32_t v;
+                    if (mq == 256) v = (uint32_t)r[jj] & 0xFFu;
+                    else
+                    {
+                        // r = hi*2^16 + lo: hi*(2^16 mod m) + lo is below 2^23 in magnitude, exact in FP32
+                        const float fh = __fsub_rn(__int_as_float(0x4B400000 + (r[jj] >> 16)), F_SHIFT);
+                        const float fl = __fsub_rn(__int_as_float(0x4B000000 | (r[jj] & 0xFFFF)), F_BIAS);
+                        float x = crt_reduce(__fmaf_rn(fh, c16, fl), mf, inv);
+                        if (x < 0.0f) x += mf;
+                        v = (uint32_t)__float_as_int(__fadd_rn(x, F_SHIFT));
+                    }
+                    out[(c*16 + jj)*OZ_BM] = (unsigned char)v;
+                }
+            }
+            // this warp's reads of the accumulator are done: release it on CTA 0
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(tempty0 + 8u*(uint32_t)b);
+        }
+    }
+
+    tc_fence_before();
+    // neither CTA leaves while the pair's MMAs, arrivals or copies may touch it
+    cluster_sync_all();
+    if (warp == 1)
+    {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem_base, CRT2_TMEM_COLS);
+    }
+}
+
+// per-row shift s = P - e with 2^e above the row's norm (times 1 + 2^-20,
+// which covers the rounding of its sum of squares), so that rint(x*2^s)
+// has a norm of at most 2^P (+ sqrt(K)/2 from the rounding); 0 for a zero row
+__global__ void oz_crt_shifts(const double* ss, i64 n, int P, int* s_out)
+{
+    const i64 i = blockIdx.x*(i64)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = sqrt(ss[i]);
+    int s = 0;
+    if (v > 0.0 && v <= 1.7e308)
+    {
+        int e = 0;
+        frexp(v*(1.0 + 0x1p-20), &e);
+        s = P - e;
+    }
+    s_out[i] = s;
+}
+
+struct CrtCombineArgs
+{
+    const unsigned char* R;        // residues of the chunks, chunk_bytes apart
+    int chunks;
+    i64 chunk_bytes;
+    double* C;
+    const i64 *c_m, *c_n, *c_l;
+    const int *sA, *sB;            // shifts [l][m], [l][n]
+    i64 M, N, tiles_m, tiles_n;
+    double alpha, beta;
+    CrtConsts cc;
+};
+
+// One block of 256 threads per (output tile, batch index, quarter of the
+// tile's columns): lane t of a warp takes rows 4t..4t+3 and warp w the
+// columns w, w+8, ... of the quarter; for each element
+// it sums the chunk residues, recovers the balanced mixed-radix digits v_q of
+// the integer product (Garner's algorithm, exact in FP32), evaluates
+// sum v_q m_0...m_(q-1) by Horner in FP64, scales by 2^-(sA+sB) and applies
+// alpha and beta through C's scatter vectors (beta == 0: C is not read).
+template <int NM>
+__global__ void __launch_bounds__(256)
+oz_crt_combine(const CrtCombineArgs p)
+{
+    constexpr int RW = 4;                      // rows per thread (one 32-bit load per modulus)
+    const i64 tile = blockIdx.x;
+    const int l = blockIdx.y;
+    const i64 tm = tile / p.tiles_n, tn = tile % p.tiles_n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const i64 m0 = tm*OZ_BM + lane*RW;
+    if (m0 >= p.M) return;
+    double* C = p.C + p.c_l[l];
+    i64 cm[RW];
+    double rsc[RW];                            // 2^-sA of each row (0 past the operand)
+    bool fast = true;
+    int sa[RW];
+    #pragma unroll
+    for (int r = 0; r < RW; r++)
+    {
+        const bool in = m0 + r < p.M;
+        cm[r] = in ? p.c_m[m0 + r] : 0;
+        sa[r] = in ? p.sA[(i64)l*p.M + m0 + r] : 0;
+        fast = fast && sa[r] > -500 && sa[r] < 500;
+        rsc[r] = in ? pow2i(-sa[r]) : 0.0;
+    }
+    const unsigned char* base = p.R + ((((i64)l*p.tiles_m + tm)*p.tiles_n + tn)*NM)*(i64)CRT_OUT_TILE + lane*RW;
+    const int c0 = blockIdx.z*(CRT_BN/4), c1 = c0 + CRT_BN/4;
+    // the first chunk's residues of the next column are loaded while this
+    // one is combined
+    uint32_t wn[NM];
+    auto load = [&](int col) {
+        #pragma unroll
+        for (int q = 0; q < NM; q++)
+            wn[q] = *reinterpret_cast<const uint32_t*>(base + q*(i64)CRT_OUT_TILE + col*OZ_BM);
+    };
+    if (tn*CRT_BN + c0 + warp < p.N) load(c0 + warp);
+    for (int col = c0 + warp; col < c1; col += 8)
+    {
+        const i64 n = tn*CRT_BN + col;
+        if (n >= p.N) break;
+        uint32_t wc[NM];
+        #pragma unroll
+        for (int q = 0; q < NM; q++) wc[q] = wn[q];
+        if (col + 8 < c1 && n + 8 < p.N) load(col + 8);
+        float v[RW][NM];
+        #pragma unroll
+        for (int q = 0; q < NM; q++)
+        {
+            uint32_t rs[RW];
+            #pragma unroll
+            for (int r = 0; r < RW; r++) rs[r] = (wc[q] >> (8*r)) & 0xFFu;
+            for (int ch = 1; ch < p.chunks; ch++)
+            {
+                const uint32_t w = *reinterpret_cast<const uint32_t*>(base + ch*p.chunk_bytes +
+                                                                      q*(i64)CRT_OUT_TILE + col*OZ_BM);
+                #pragma unroll
+                for (int r = 0; r < RW; r++) rs[r] += (w >> (8*r)) & 0xFFu;
+            }
+            const float mq = p.cc.m[q], inv = p.cc.inv[q], gi = p.cc.ginv[q];
+            #pragma unroll
+            for (int r = 0; r < RW; r++)
+            {
+                // r_q minus the digits found so far at their weights, times the
+                // inverse weight, modulo m_q, balanced: |.| < 2^18 and 2^14, exact
+                float t = __fsub_rn(__int_as_float(0x4B000000 | (int)rs[r]), F_BIAS);
+                #pragma unroll
+                for (int i = 0; i < q; i++) t = __fmaf_rn(-v[r][i], p.cc.g[q][i], t);
+                t = crt_reduce(t, mq, inv);
+                v[r][q] = crt_reduce(__fmul_rn(t, gi), mq, inv);
+            }
+        }
+        const int sb = p.sB[(i64)l*p.N + n];
+        const double csc = pow2i(-sb);
+        const i64 cn = p.c_n[n];
+        #pragma unroll
+        for (int r = 0; r < RW; r++)
+        {
+            if (m0 + r >= p.M) break;
+            double x = (double)v[r][NM - 1];
+            #pragma unroll
+            for (int q = NM - 2; q >= 0; q--) x = fma(x, p.cc.md[q], (double)v[r][q]);
+            // 2^-(sA+sB) as two normal powers of two where the shifts allow
+            const double val = p.alpha*((fast && sb > -500 && sb < 500) ? x*rsc[r]*csc : ldexp(x, -(sa[r] + sb)));
+            double* dst = C + cm[r] + cn;
+            *dst = p.beta == 0.0 ? val : val + p.beta*(*dst);
+        }
+    }
 }
 
 void stats(const OzOperand& o, int* e_out, double* ss_out, cudaStream_t st)
@@ -1004,6 +1505,275 @@ double diagonal_weight(int kind, int d)
     return kind == OZ_I8 ? 1.0/(127.0*127.0*std::pow(254.0, d - 2)) : std::ldexp(1.0, 2 - 7*d);
 }
 
+// ---- scheme II host side ------------------------------------------------------
+
+// (2 m + 1)/2 rounded: x mod m in [-(m-1)/2, (m-1)/2] ([-128, 127] for 256)
+i64 centred(i64 x, i64 m)
+{
+    x %= m;
+    if (x < 0) x += m;
+    if (2*x >= m) x -= m;
+    return x;
+}
+
+i64 powmod(i64 b, i64 e, i64 m)
+{
+    i64 r = 1 % m;
+    b %= m;
+    for (; e > 0; e >>= 1, b = b*b % m)
+        if (e & 1) r = r*b % m;
+    return r;
+}
+
+i64 invmod(i64 a, i64 m)
+{
+    // extended Euclid; a and m coprime
+    i64 g = m, x = 0, x1 = 1, a1 = ((a % m) + m) % m;
+    while (a1)
+    {
+        const i64 q = g/a1;
+        i64 t = g - q*a1; g = a1; a1 = t;
+        t = x - q*x1; x = x1; x1 = t;
+    }
+    return ((x % m) + m) % m;
+}
+
+// a residue plane buffer (blocks [l][row tile][k step] of nm 4 KB tiles) as
+// a 4-D map: 256-byte rows, 16 rows per tile, nm tiles per block, blocks;
+// a box of one modulus's tiles in four consecutive blocks (one stage's k
+// steps) lands as four contiguous tiles; no swizzle
+CUtensorMap plane_map(const void* base, size_t bytes, int nm)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    TB_CHECK(encode, TB_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const size_t block = (size_t)nm*CRT2_TILE;
+    TB_CHECK(bytes % block == 0 && bytes/block < ((size_t)1 << 31), TB_ERR_SIZE, "Ozaki moduli planes too large");
+    CUtensorMap m;
+    const cuuint64_t dims[4] = {256, CRT2_TILE/256, (cuuint64_t)nm, (cuuint64_t)(bytes/block)};
+    const cuuint64_t strides[3] = {256, CRT2_TILE, block};
+    const cuuint32_t box[4] = {256, CRT2_TILE/256, 1, CRT_KSUB};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TB_CHECK(r == CUDA_SUCCESS, TB_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Ozaki moduli planes");
+    return m;
+}
+
+CrtConsts crt_consts(int nm)
+{
+    CrtConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.nm = nm;
+    for (int q = 0; q < nm; q++)
+    {
+        const i64 m = crt_modulus(q);
+        c.m[q] = (float)m;
+        c.inv[q] = 1.0f/(float)m;
+        c.md[q] = (double)m;
+        c.invd[q] = 1.0/(double)m;
+        c.c16[q] = (float)powmod(2, 16, m);
+        i64 P = 1 % m;                               // m_0 ... m_(j-1) mod m_q
+        for (int j = 0; j < q; j++)
+        {
+            c.g[q][j] = (float)centred(P, m);
+            P = P*crt_modulus(j) % m;
+        }
+        c.ginv[q] = q == 0 ? 1.0f : (float)centred(invmod(P, m), m);
+    }
+    return c;
+}
+
+double crt_log2_modulus(int nm)
+{
+    double s = 0;
+    for (int q = 0; q < nm; q++) s += std::log2((double)crt_modulus(q));
+    return s;
+}
+
+// norm bound exponent P of the scaled rows and columns: |sum_k a b| <=
+// ||a|| ||b|| <= (2^P + sqrt(K)/2)^2 stays below M/2; at most 50, so that
+// |a| < 2^51 fits the digit extraction
+int crt_norm_bits(int nm)
+{
+    return std::min(50, (int)std::floor((crt_log2_modulus(nm) - 1.05)/2.0));
+}
+
+// a-priori normwise error of scheme II with nm moduli: rounding x*2^s to an
+// integer leaves an error below 1/2 (uniform, variance 1/12) per element, so
+// ||dA||^2 ~ K/12 sum_i 4^(-s_i) with 2^-s_i ~ 2^(e_i - P)
+struct CrtErrorModel
+{
+    double ra = 0, rb = 0;   // sqrt(K/12 sum 4^(e_i - emax)/sum ss) ...
+    int ea = 0, eb = 0;      // ... and emax
+    static void build(const std::vector<double>& ss, i64 K, double& r, int& emax)
+    {
+        std::vector<int> e(ss.size());
+        emax = -100000;
+        double den = 0.0;
+        for (size_t i = 0; i < ss.size(); i++)
+        {
+            const double v = std::sqrt(ss[i]);
+            int x = -100000;
+            if (v > 0.0 && v <= 1.7e308) std::frexp(v*(1.0 + 0x1p-20), &x);
+            e[i] = x;
+            emax = std::max(emax, x);
+            den += ss[i];
+        }
+        double num = 0.0;
+        for (int x : e)
+            if (x > -100000) num += std::ldexp(1.0, 2*(x - emax));
+        r = den > 0.0 && num > 0.0 ? std::sqrt((double)K/12.0*num/den) : 0.0;
+    }
+    CrtErrorModel(const std::vector<double>& ssA, const std::vector<double>& ssB, i64 K)
+    {
+        build(ssA, K, ra, ea);
+        build(ssB, K, rb, eb);
+    }
+    double operator()(int nm) const
+    {
+        const int P = crt_norm_bits(nm);
+        return (ra > 0 ? std::ldexp(ra, ea - P) : 0.0) + (rb > 0 ? std::ldexp(rb, eb - P) : 0.0);
+    }
+};
+
+// work of one scheme II modulus GEMM relative to one scheme I slice pair
+// (the plain 128 x 256 GEMM against the fused diagonal kernel, plus the
+// residue planes' extra slicing), measured on the ladder contraction
+constexpr double kCrtGemmCost = 1.15;
+
+template <int NM>
+void launch_crt_slice(const OzOperand& o, const int* s, void* out, const PlaneGeom& pg, const CrtConsts& cc,
+                      cudaStream_t st)
+{
+    launch_slice<NM, OZ_I8, false, true>(o, s, out, pg, st, &cc);
+}
+
+void crt_slice_dispatch(int nm, const OzOperand& o, const int* s, void* out, const PlaneGeom& pg,
+                        const CrtConsts& cc, cudaStream_t st)
+{
+    switch (nm)
+    {
+        case 2: launch_crt_slice<2>(o, s, out, pg, cc, st); break;
+        case 3: launch_crt_slice<3>(o, s, out, pg, cc, st); break;
+        case 4: launch_crt_slice<4>(o, s, out, pg, cc, st); break;
+        case 5: launch_crt_slice<5>(o, s, out, pg, cc, st); break;
+        case 6: launch_crt_slice<6>(o, s, out, pg, cc, st); break;
+        case 7: launch_crt_slice<7>(o, s, out, pg, cc, st); break;
+        case 8: launch_crt_slice<8>(o, s, out, pg, cc, st); break;
+        case 9: launch_crt_slice<9>(o, s, out, pg, cc, st); break;
+        case 10: launch_crt_slice<10>(o, s, out, pg, cc, st); break;
+        case 11: launch_crt_slice<11>(o, s, out, pg, cc, st); break;
+        case 12: launch_crt_slice<12>(o, s, out, pg, cc, st); break;
+        case 13: launch_crt_slice<13>(o, s, out, pg, cc, st); break;
+        case 14: launch_crt_slice<14>(o, s, out, pg, cc, st); break;
+        case 15: launch_crt_slice<15>(o, s, out, pg, cc, st); break;
+        default: launch_crt_slice<16>(o, s, out, pg, cc, st); break;
+    }
+}
+
+void crt_combine_dispatch(const CrtCombineArgs& a, i64 tiles, i64 L, cudaStream_t st)
+{
+    dim3 grid((unsigned)tiles, (unsigned)L, 4);
+    switch (a.cc.nm)
+    {
+#define TB_CRT_CASE(n) case n: oz_crt_combine<n><<<grid, 256, 0, st>>>(a); break;
+        TB_CRT_CASE(2) TB_CRT_CASE(3) TB_CRT_CASE(4) TB_CRT_CASE(5) TB_CRT_CASE(6) TB_CRT_CASE(7)
+        TB_CRT_CASE(8) TB_CRT_CASE(9) TB_CRT_CASE(10) TB_CRT_CASE(11) TB_CRT_CASE(12) TB_CRT_CASE(13)
+        TB_CRT_CASE(14) TB_CRT_CASE(15)
+        default: oz_crt_combine<16><<<grid, 256, 0, st>>>(a); break;
+#undef TB_CRT_CASE
+    }
+    check_launch("oz_crt_combine");
+}
+
+// scheme II on the statistics already computed: shifts, residue planes,
+// one INT8 GEMM per modulus (per exact run of k), CRT combination into C
+void crt_run(OzakiJob& j, int nm, cudaStream_t st)
+{
+    const GemmView& v = j.v;
+    TB_CHECK(nm >= 2 && nm <= CRT_MAX, TB_ERR_ARG, "Ozaki moduli count must be 2..16");
+    const CrtConsts cc = crt_consts(nm);
+    const int P = crt_norm_bits(nm);
+    dbuf shA((size_t)v.l*v.m*sizeof(int), st), shB((size_t)v.l*v.n*sizeof(int), st);
+    if (v.l*v.m > 0)
+    {
+        oz_crt_shifts<<<(unsigned)((v.l*v.m + 255)/256), 256, 0, st>>>(j.sA.as<double>(), v.l*v.m, P, shA.as<int>());
+        check_launch("oz_crt_shifts");
+    }
+    if (v.l*v.n > 0)
+    {
+        oz_crt_shifts<<<(unsigned)((v.l*v.n + 255)/256), 256, 0, st>>>(j.sB.as<double>(), v.l*v.n, P, shB.as<int>());
+        check_launch("oz_crt_shifts");
+    }
+    OzOperand oa = {j.A, j.tab->a_m, j.tab->a_k, j.tab->a_l, v.m, v.k, v.l, v.amode,
+                    j.tab->a_m_step, j.tab->a_k_step};
+    OzOperand ob = {j.B, j.tab->b_n, j.tab->b_k, j.tab->b_l, v.n, v.k, v.l, v.bmode,
+                    j.tab->b_n_step, j.tab->b_k_step};
+    // 128-row tiles of A and B, an even number of each: a CTA pair takes
+    // 256 rows of A and 256 columns (two B tiles) of the output
+    const i64 k_steps = ((v.k + OZ_BK*CRT_KSUB - 1)/(OZ_BK*CRT_KSUB))*CRT_KSUB;   // a multiple of four
+    const PlaneGeom ga = {OZ_BM, 2*((v.m + 255)/256), k_steps, nm};
+    const PlaneGeom gb = {OZ_BM, 2*((v.n + CRT_BN - 1)/CRT_BN), k_steps, nm};
+    TB_CHECK(ga.k_steps < (1ll << 31), TB_ERR_SIZE, "Ozaki contraction length above 2^31");
+    dbuf pa((size_t)(v.l*ga.tiles*ga.k_steps*nm*A_TILE), st);
+    dbuf pb((size_t)(v.l*gb.tiles*gb.k_steps*nm*CRT2_TILE), st);
+    crt_slice_dispatch(nm, oa, shA.as<int>(), pa.ptr, ga, cc, st);
+    crt_slice_dispatch(nm, ob, shB.as<int>(), pb.ptr, gb, cc, st);
+
+    // one launch per exact run of k steps; each writes its own residues of
+    // the 128 x 256 tiles
+    const i64 tiles_n = gb.tiles/2;
+    const i64 tiles = ga.tiles*tiles_n;
+    const int chunks = (int)((ga.k_steps + CRT_KT_RUN - 1)/CRT_KT_RUN);
+    const i64 chunk_bytes = v.l*tiles*nm*(i64)CRT_OUT_TILE;
+    TB_CHECK(tiles < (1ll << 31) && v.l*nm < 65536, TB_ERR_SIZE, "Ozaki moduli path: grid too large");
+    dbuf res((size_t)(chunks*chunk_bytes), st);
+    CrtGemmArgs g;
+    g.pA = pa.as<unsigned char>(); g.pB = pb.as<unsigned char>();
+    g.tmA = plane_map(pa.ptr, (size_t)(v.l*ga.tiles*ga.k_steps*nm*A_TILE), nm);
+    g.tmB = plane_map(pb.ptr, (size_t)(v.l*gb.tiles*gb.k_steps*nm*CRT2_TILE), nm);
+    g.tiles_m = ga.tiles; g.tiles_n = tiles_n;
+    g.k_steps = (int)ga.k_steps;
+    g.nm = nm;
+    g.L = (int)v.l;
+    for (int q = 0; q < CRT_MAX; q++) { g.m[q] = cc.m[q]; g.inv[q] = cc.inv[q]; g.c16[q] = cc.c16[q]; }
+    const size_t smem = crt_gemm2_smem();
+    TB_CUDA(cudaFuncSetAttribute(oz_crt_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int c = 0; c < chunks; c++)
+    {
+        g.R = res.as<unsigned char>() + c*chunk_bytes;
+        g.kt0 = c*CRT_KT_RUN;
+        g.kt1 = (int)std::min<i64>(ga.k_steps, (i64)(c + 1)*CRT_KT_RUN);
+        TimedLaunch t("oz_crt_gemm", st);
+        const i64 items = nm*v.l*tiles/2;
+        const i64 pairs = std::max<i64>(1, std::min<i64>(items, device_sm_count()/2));
+        oz_crt_gemm2<<<(unsigned)(2*pairs), OZ_THREADS, smem, st>>>(g);
+        check_launch("oz_crt_gemm");
+    }
+
+    CrtCombineArgs a;
+    a.R = res.as<unsigned char>();
+    a.chunks = chunks;
+    a.chunk_bytes = chunk_bytes;
+    a.C = j.C;
+    a.c_m = j.tab->c_m; a.c_n = j.tab->c_n; a.c_l = j.tab->c_l;
+    a.sA = shA.as<int>(); a.sB = shB.as<int>();
+    a.M = v.m; a.N = v.n; a.tiles_m = ga.tiles; a.tiles_n = tiles_n;
+    a.alpha = j.alpha; a.beta = j.beta;
+    a.cc = cc;
+    TimedLaunch t("oz_crt_combine", st);
+    crt_combine_dispatch(a, tiles, v.l, st);
+}
+
 } // namespace
 
 int ozaki_error_flag()
@@ -1068,14 +1838,41 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
             TB_CUDA(cudaStreamSynchronize(st));
         }
         const ErrorModel est(heA, hsA, heB, hsB, v.k);
+        // scheme II (moduli) is an INT8 option: its count from the
+        // tolerance, or the caller's when it forces the scheme
+        int nm = 0;
+        double nm_err = 0;
+        if (kind == OZ_I8 && j.scheme != 1)
+        {
+            const CrtErrorModel est2(hsA, hsB, v.k);
+            if (j.scheme == 2 && S > 0) nm = S;
+            else
+                for (int q = 2; q <= CRT_MAX; q++)
+                    if (est2(q)*4.0 <= j.tol) { nm = q; break; }
+            if (j.scheme == 2 && nm == 0) nm = CRT_MAX;
+            if (nm > 0) nm_err = est2(nm);
+        }
+        bool feasible1 = S > 0;
         if (S <= 0)
         {
             S = OZ_SMAX;
             for (int s = 1; s <= OZ_SMAX; s++)
             {
                 // safety factor 4 between the estimate and the target
-                if (est(s, kind)*4.0 <= j.tol) { S = s; break; }
+                if (est(s, kind)*4.0 <= j.tol) { S = s; feasible1 = true; break; }
             }
+        }
+        // moduli when forced, or when they meet the tolerance with less
+        // work than the slice pairs (S(S+1)/2 GEMMs)
+        const bool use2 = nm > 0 && (j.scheme == 2 ||
+                                     (j.scheme == 0 && (!feasible1 || nm*kCrtGemmCost < 0.5*S*(S + 1))));
+        if (use2)
+        {
+            j.res.scheme = 2;
+            j.res.slices = nm;
+            j.res.est_error = nm_err;
+            crt_run(j, nm, st);
+            return;
         }
         if (S >= 1 && S <= OZ_SMAX) j.res.est_error = est(S, kind);
     }
@@ -1123,12 +1920,12 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
 
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
                        double alpha, double beta, double tol, int slices, cudaStream_t st,
-                       int kind, bool single)
+                       int kind, bool single, int scheme)
 {
     OzakiJob j;
     j.v = v; j.A = A; j.B = B; j.C = C;
     j.alpha = alpha; j.beta = beta; j.tol = tol; j.slices = slices;
-    j.kind = kind; j.single = single;
+    j.kind = kind; j.single = single; j.scheme = scheme;
     ozaki_begin(j, st);
     ozaki_end(j, st, false);
     return j.res;

@@ -12,15 +12,19 @@ enum OzKind { OZ_I8 = 0, OZ_BF16 = 1, OZ_TF32 = 2 };
 
 struct OzakiResult
 {
-    int slices = 0;
+    int scheme = 1;          // 1: slices (scheme I), 2: moduli (scheme II)
+    int slices = 0;          // slice count, or the number of moduli for scheme II
     double est_error = 0;
 };
 
 // kind OZ_I8 / OZ_BF16 with single = false: Ozaki slices (slices = 0
-// chooses the count from tol); single = true: one BF16 or TF32 pass
+// chooses the count from tol); single = true: one BF16 or TF32 pass.
+// scheme (OZ_I8 only): 0 picks slices or moduli, whichever needs fewer INT8
+// GEMMs for tol; 1 forces slices; 2 forces moduli (slices then counts the
+// moduli, 0 = from tol)
 OzakiResult ozaki_mult(const GemmView& v, const double* A, const double* B, double* C,
                        double alpha, double beta, double tol, int slices, cudaStream_t st,
-                       int kind = OZ_I8, bool single = false);
+                       int kind = OZ_I8, bool single = false, int scheme = 0);
 
 // the same contraction in two phases, so a caller can queue the statistics
 // of several contractions, do other work, and wait only for the statistics
@@ -34,6 +38,7 @@ struct OzakiJob
     int slices = 0;
     int kind = OZ_I8;
     bool single = false;
+    int scheme = 0;
     std::shared_ptr<GemmTables> tab;
     dbuf eA, eB, sA, sB;             // row exponents and sums of squares
     OzakiResult res;
