@@ -394,6 +394,7 @@ def main():
     # 1e-12, kept when it meets 1e-12 against the FP64 path on this input, else
     # the plain FP64 DMMA path (its error is the FP64 rounding itself)
     method, method_name, cfg_name = 1, "fp64_dmma", "b200_fp64"
+    used_method = 1
     Cfp = torch.zeros_like(C)
     tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cfp, "abij", method=1)
     try:
@@ -401,7 +402,10 @@ def main():
         torch.cuda.synchronize()
         err = (torch.linalg.vector_norm(C - Cfp) / torch.linalg.vector_norm(Cfp)).item()
         if err <= 1e-12:
-            method, method_name, cfg_name = 2, "ozaki_int8_%d_slices" % rep["slices"], "b200_ozaki_i8"
+            # the INT8 config picks slices (scheme I) or moduli (scheme II, reported as method 6)
+            method, cfg_name = 2, "b200_ozaki_i8"
+            method_name = ("ozaki_int8_%d_moduli" if rep["method"] == 6 else "ozaki_int8_%d_slices") % rep["slices"]
+            used_method = rep["method"]
     except tb.TblisError:
         pass
 
@@ -422,11 +426,11 @@ def main():
     tb.kernel_timer(True)
     total_ms, per = time_steps(torch, step, args.steps, stream)
     launches = tb.kernel_count() - k0
-    kname = "ozaki_gemm_kernel" if method == 2 else "gemm_f64_kernel"
+    kname = {1: "gemm_f64_kernel", 2: "ozaki_gemm_kernel", 6: "oz_crt_gemm"}[used_method]
     k_total_ms, k_launches = tb.kernel_time(kname)
     # device time per step of each stage of the contraction
-    stage_ms = {n: tb.kernel_time(n)[0] / args.steps
-                for n in (("oz_stats", "oz_slice", kname) if method == 2 else (kname,))}
+    stages = {1: (kname,), 2: ("oz_stats", "oz_slice", kname), 6: ("oz_stats", "oz_slice", kname, "oz_crt_combine")}
+    stage_ms = {n: tb.kernel_time(n)[0] / args.steps for n in stages[used_method]}
     tb.kernel_timer(False)
     clocks = sampler.stop()
     total_ms = max_over_ranks(dist, torch, total_ms, dev)
@@ -485,10 +489,12 @@ def main():
                                   "kernel": "gemm_f64_kernel", "launch_ms": launch_ms,
                                   "share_of_step": k_total_ms / total_ms}
         else:
-            # the dominant kernel is the fused INT8 slice-pair GEMM: its work is
-            # S(S+1)/2 INT8 GEMMs of m x n x k (2 ops per MAC)
+            # the dominant kernel is the INT8 GEMM: S(S+1)/2 GEMMs of m x n x k
+            # for S slices (the fused slice-pair kernel), or one per modulus
+            # (2 ops per MAC)
             S = int(method_name.split("_")[2])
-            int8_ops = S * (S + 1) / 2 * FLOPS_LADDER * units_per_launch
+            gemms = S if used_method == 6 else S * (S + 1) / 2
+            int8_ops = gemms * FLOPS_LADDER * units_per_launch
             achieved = int8_ops / (launch_ms * 1e-3) / 1e12
             i8peak = measure_int8_peak(torch, dev)
             src = "cuBLAS int8 GEMM 8192^3 (torch._int_mm) measured in this run"
@@ -497,7 +503,7 @@ def main():
                 src = "2 x measured bf16 dense GEMM (MEASURED_PEAKS.json)"
             result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": i8peak, "unit": "TOP/s (int8)",
                                   "frac": achieved / i8peak, "traffic": None, "peak_source": src,
-                                  "kernel": "ozaki_gemm_kernel", "launch_ms": launch_ms,
+                                  "kernel": kname, "launch_ms": launch_ms, "int8_gemms_per_launch": gemms,
                                   "share_of_step": k_total_ms / total_ms,
                                   "fp64_equivalent_tflops_kernel": FLOPS_LADDER * units_per_launch /
                                                                    (launch_ms * 1e-3) / 1e12}
@@ -549,13 +555,15 @@ def main():
 
 def precision_variants(torch, tb, A, B, C, stream, Cref):
     """The ladder under every arithmetic the library offers: plain FP64 DMMA,
-    Ozaki INT8 and BF16 slices with 3..8 slices, one TF32 and one BF16 pass.
+    Ozaki INT8 slices (3..8), Ozaki INT8 moduli (8..16), Ozaki BF16 slices
+    (3..8), one TF32 and one BF16 pass.
     Error = normwise relative difference to Cref (the reference's own FP64
     result on the same inputs at N=1); rate = FP64-equivalent GFLOP/s of the
     whole call (statistics, slicing and GEMM), mean of 2."""
     nref = torch.linalg.vector_norm(Cref).item()
     runs = [("fp64_dmma", 1, 0)]
     runs += [("ozaki_int8", 2, s) for s in range(3, 9)]
+    runs += [("ozaki_int8_moduli", 6, n) for n in (8, 10, 11, 12, 13, 14, 16)]
     runs += [("ozaki_bf16", 3, s) for s in range(3, 9)]
     runs += [("tf32_single_pass", 4, 1), ("bf16_single_pass", 5, 1)]
     out = []

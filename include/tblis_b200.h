@@ -229,8 +229,9 @@ int64_t tblis_b200_kernel_count(void);
 
 /* Per-kernel device timing (no reference counterpart). While enabled, the
  * library brackets each launch of its contraction and transpose kernels
- * (gemm_f64_kernel, gemm_f64_grouped_kernel, ozaki_gemm_kernel, k_transpose,
- * k_add_rows) with a CUDA event pair on the launching stream. Enabling or
+ * (gemm_f64_kernel, gemm_f64_grouped_kernel, ozaki_gemm_kernel, oz_stats,
+ * oz_slice, oz_crt_gemm, oz_crt_combine, k_transpose, k_add_rows) with a
+ * CUDA event pair on the launching stream. Enabling or
  * disabling clears the records; reading waits for the recorded launches and
  * returns their summed device time and count for one kernel name. */
 int tblis_b200_kernel_timer(int enable);

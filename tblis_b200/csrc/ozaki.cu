@@ -1645,10 +1645,20 @@ struct CrtErrorModel
     }
 };
 
-// work of one scheme II modulus GEMM relative to one scheme I slice pair
-// (the plain 128 x 256 GEMM against the fused diagonal kernel, plus the
-// residue planes' extra slicing), measured on the ladder contraction
-constexpr double kCrtGemmCost = 1.15;
+// modelled device time of the two INT8 schemes, from rates measured on the
+// ladder contraction (m = 25600, n = 2304, k = 25600) on one B200: the fused
+// slice-pair kernel runs 2.7e15 INT8 ops/s per pair, the moduli GEMM 2.8e15
+// per modulus; writing a plane costs 5.3e-13 s (digits) or 4.1e-13 s
+// (residues) per operand element, and the CRT combination 1.1e-12 s per
+// output element and modulus
+double scheme1_seconds(int S, double m, double n, double k)
+{
+    return 0.5*S*(S + 1)*2.0*m*n*k/2.7e15 + S*(m + n)*k*5.3e-13;
+}
+double scheme2_seconds(int N, double m, double n, double k)
+{
+    return N*2.0*m*n*k/2.8e15 + N*(m + n)*k*4.1e-13 + N*m*n*1.1e-12;
+}
 
 template <int NM>
 void launch_crt_slice(const OzOperand& o, const int* s, void* out, const PlaneGeom& pg, const CrtConsts& cc,
@@ -1862,10 +1872,12 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready)
                 if (est(s, kind)*4.0 <= j.tol) { S = s; feasible1 = true; break; }
             }
         }
-        // moduli when forced, or when they meet the tolerance with less
-        // work than the slice pairs (S(S+1)/2 GEMMs)
+        // moduli when forced, or when they meet the tolerance in less
+        // modelled time than the slices
+        const double mm = (double)v.m*v.l, nn = (double)v.n, kk = (double)v.k;
         const bool use2 = nm > 0 && (j.scheme == 2 ||
-                                     (j.scheme == 0 && (!feasible1 || nm*kCrtGemmCost < 0.5*S*(S + 1))));
+                                     (j.scheme == 0 && (!feasible1 || scheme2_seconds(nm, mm, nn, kk) <
+                                                                      scheme1_seconds(S, mm, nn, kk))));
         if (use2)
         {
             j.res.scheme = 2;

@@ -122,20 +122,27 @@ def test_zero_rows_columns_and_integers(cuda):
 
 
 def test_auto_choice_follows_work(cuda):
-    """Method 2 picks moduli where they need fewer INT8 GEMMs than slice
-    pairs (1e-12 on spread inputs: 13 moduli against 21 pairs) and slices
-    where those are cheaper (1e-3: 2 slices, 3 pairs, against 5 moduli)."""
+    """Method 2 picks whichever scheme its time model (INT8 GEMMs plus plane
+    writing plus, for moduli, the combination) puts first: on a large
+    GEMM-dominated contraction at 1e-12 that is 13 moduli against 21 slice
+    pairs; at 1e-3 two slices (3 pairs) against five moduli."""
     import torch
-    rng = np.random.default_rng(11)
-    A = _spread(rng, (256, 2048))
-    B = _spread(rng, (2048, 256))
-    C = np.zeros((256, 256))
-    ref = C.copy()
-    oracle.orc_mult(1.0, A, "ik", B, "kj", 0.0, ref, "ij")
-    got, rep = _run(torch, cuda, 2, 1.0, A, "ik", B, "kj", 0.0, C, "ij", tol=1e-12)
-    assert rep["method"] == 6 and normwise_rel(got, ref) <= 1e-12
-    got, rep = _run(torch, cuda, 2, 1.0, A, "ik", B, "kj", 0.0, C, "ij", tol=1e-3)
-    assert rep["method"] == 2 and rep["slices"] <= 3 and normwise_rel(got, ref) <= 1e-3
+    import tblis_b200 as tb
+    g = torch.Generator(device=cuda)
+    g.manual_seed(11)
+    A = torch.empty((8192, 4096), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    A = torch.ldexp(A, torch.randint(-20, 21, A.shape, device=cuda, generator=g, dtype=torch.int32))
+    B = torch.empty((4096, 8192), dtype=torch.float64, device=cuda).uniform_(-1, 1, generator=g).t()
+    ref = torch.zeros((4096, 4096), dtype=torch.float64, device=cuda)
+    tb.mult_ex(1.0, A, "ik", B, "kj", 0.0, ref, "ij", method=1)
+    nref = torch.linalg.vector_norm(ref).item()
+    for tol, method in ((1e-12, 6), (1e-3, 2)):
+        C = torch.zeros_like(ref)
+        rep = tb.mult_ex(1.0, A, "ik", B, "kj", 0.0, C, "ij", method=2, tolerance=tol)
+        tb.synchronize()
+        err = torch.linalg.vector_norm(C - ref).item() / nref
+        assert rep["method"] == method and err <= tol, (tol, rep, err)
+    assert rep["slices"] <= 3
 
 
 def test_medium_size_matches_fp64_path(cuda):
