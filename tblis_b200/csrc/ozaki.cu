@@ -977,26 +977,30 @@ struct CrtGemmArgs
     float m[CRT_MAX], inv[CRT_MAX], c16[CRT_MAX];
 };
 
-// ---- the modulus GEMMs on CTA pairs (tcgen05 cta_group::2), persistent -------
+// ---- the modulus GEMMs on CTA pairs (tcgen05 cta_group::2) ----------------------
 //
-// A cluster of two CTAs on one SM pair computes 256 x 256 output tiles: CTA
-// r holds rows 128r..128r+127 of A and columns 128r..128r+127 of B in its
-// shared memory, and each MMA of 256 x 256 x 32 issued by CTA 0 reads both
-// halves of B, so each SM reads half of B per MAC. A stage holds four k
-// steps (four MMAs per barrier round). Both CTAs copy their tiles with
-// cta_group::2 tensor copies (no multicast) that complete on CTA 0's
-// barrier, which expects the bytes of both; CTA 0's commits arrive on both
-// CTAs' barriers (tcgen05.commit multicast). The pair walks its share of
-// the (modulus, 256 x 256 tile) work items with two accumulators in tensor
-// memory, so the epilogue of one item (each CTA reading its accumulator
-// rows) overlaps the MMAs of the next; the epilogue warps of both CTAs
-// release an accumulator on CTA 0's barrier.
+// A cluster of two CTAs on one SM pair computes one 256 x 256 output tile of
+// one modulus: CTA r holds rows 128r..128r+127 of A and columns
+// 128r..128r+127 of B in its shared memory, and each MMA of 256 x 256 x 32
+// issued by CTA 0 reads both halves of B, so each SM reads half of B per
+// MAC. A stage holds two k steps (two MMAs per barrier round). Both CTAs
+// copy their tiles with cta_group::2 tensor copies (no multicast) that
+// complete on CTA 0's barrier, which expects the bytes of both; CTA 0's
+// commits arrive on both CTAs' barriers (tcgen05.commit multicast). Each
+// CTA's epilogue reduces the accumulator rows in its own SM's tensor memory.
+// One work item per cluster, launched in order (modulus, batch index, row
+// tile, column tile): the clusters on the GPU at any time work on
+// consecutive tiles, so the nine column tiles of a row tile read its A
+// rows within a short time of each other and share them through L2 (a
+// persistent loop over a static share of the items drifted apart and read
+// A from DRAM up to eight times); two clusters per SM pair overlap one's
+// epilogue with the other's MMAs.
 
-constexpr int CRT_KSUB = 4;                    // k steps per stage
-constexpr int CRT2_STAGES = 6;                 // 32 KB per stage: 192 KB, one CTA per SM
+constexpr int CRT_KSUB = 2;                    // k steps per stage
+constexpr int CRT2_STAGES = 6;                 // 16 KB per stage: 97 KB, two CTAs per SM
 constexpr int CRT2_TILE = OZ_BM*OZ_BK;         // one 128-row x 32-byte tile (A, or a CTA's half of B)
 constexpr int CRT2_STAGE_BYTES = 2*CRT_KSUB*CRT2_TILE;
-constexpr uint32_t CRT2_TMEM_COLS = 512;       // two 128 x 256 INT32 accumulators
+constexpr uint32_t CRT2_TMEM_COLS = 256;       // one 128 x 256 INT32 accumulator
 
 __device__ __forceinline__ uint32_t cluster_ctarank()
 {
@@ -1018,13 +1022,7 @@ __device__ __forceinline__ void cluster_sync_all()
                  "barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-// arrives on a barrier of another CTA of the cluster (a shared::cluster address)
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
-{
-    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" :: "r"(cluster_addr) : "memory");
-}
-
-// modulus q's tiles of four consecutive plane blocks from block w (one
+// modulus q's tiles of CRT_KSUB consecutive plane blocks from block w (one
 // stage) into this CTA's shared memory, completing on CTA 0's barrier (a
 // shared::cluster address)
 __device__ __forceinline__ void tma_load_pair(void* dst, const CUtensorMap* map, int q, int w, uint32_t bar_cluster)
@@ -1064,12 +1062,12 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uin
 
 constexpr size_t crt_gemm2_smem()
 {
-    return (size_t)CRT2_STAGES*CRT2_STAGE_BYTES + 1024 + (2*CRT2_STAGES + 4)*8 + 16;
+    return (size_t)CRT2_STAGES*CRT2_STAGE_BYTES + 1024 + (2*CRT2_STAGES + 1)*8 + 16;
 }
 
-// work item w of n_items: modulus-major, then the batch index, then 256-row
-// tiles, then 256-column tiles (consecutive pairs share A rows, and one
-// modulus's B planes stay in L2 while its items run)
+// work item w: modulus-major, then the batch index, then 256-row tiles, then
+// 256-column tiles (consecutive items share A rows, and one modulus's B
+// planes stay in L2 while its items run)
 struct CrtItem { int q, l; i64 tm2, tn; };
 __device__ __forceinline__ CrtItem crt_item(i64 w, int L, i64 tiles_m2, i64 tiles_n)
 {
@@ -1084,10 +1082,10 @@ __device__ __forceinline__ CrtItem crt_item(i64 w, int L, i64 tiles_m2, i64 tile
     return it;
 }
 
-// grid.x = 2 x (number of pairs), one CTA per SM; the planes have 128-row
-// tiles of A and B in blocks [l][row tile][k step] of nm tiles (k steps a
-// multiple of four); residues go out as column-major 128 x 256 tiles
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
+// grid.x = 2 x (work items); the planes have 128-row tiles of A and B in
+// blocks [l][row tile][k step] of nm tiles (k steps a multiple of
+// CRT_KSUB); residues go out as column-major 128 x 256 tiles
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 2)
 oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
 {
     constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(CRT_BN >> 3) << 17) |
@@ -1096,16 +1094,16 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
     unsigned char* smem = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + CRT2_STAGES*CRT2_STAGE_BYTES);
     uint64_t* empty = full + CRT2_STAGES;
-    uint64_t* tfull = empty + CRT2_STAGES;       // [2] accumulator ready
-    uint64_t* tempty = tfull + 2;                // [2] accumulator drained (CTA 0's count 8)
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* tfull = empty + CRT2_STAGES;       // accumulator ready
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tfull + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_ctarank();
-    const i64 pair0 = blockIdx.x >> 1, npairs = gridDim.x >> 1;
     const i64 tiles_m2 = p.tiles_m >> 1;
-    const i64 n_items = (i64)p.nm*p.L*tiles_m2*p.tiles_n;
+    const CrtItem it = crt_item(blockIdx.x >> 1, p.L, tiles_m2, p.tiles_n);
+    const i64 tm = 2*it.tm2 + rank;              // this CTA's 128-row tile of A and C
+    const i64 tb = 2*it.tn + rank;               // this CTA's 128-row tile of the B plane
     const int kt0 = p.kt0, kt_count = p.kt1 - p.kt0;    // a multiple of CRT_KSUB
     const int nstage = kt_count/CRT_KSUB;
 
@@ -1116,18 +1114,14 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
             mbar_init(&full[s], 1);       // CTA 0's: its producer's arrival plus both CTAs' bytes
             mbar_init(&empty[s], 1);      // CTA 0's MMA commit, multicast to both
         }
-        for (int b = 0; b < 2; b++)
-        {
-            mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 8);     // the four epilogue warps of each CTA
-        }
+        mbar_init(tfull, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (warp == 1) tmem_alloc_pair(tmem_slot, CRT2_TMEM_COLS);
     tc_fence_before();
-    // both CTAs' barriers and tensor memory exist before any remote arrive or MMA
+    // both CTAs' barriers and tensor memory exist before any remote arrival or MMA
     cluster_sync_all();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
@@ -1137,24 +1131,18 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
         if (lane == 0)
         {
             const uint32_t full0 = mapa_shared(smem_u32(full), 0);
-            int g = 0;                    // stage counter over all items
-            for (i64 w = pair0; w < n_items && !*abort_flag; w += npairs)
+            // plane blocks of this CTA's A and B tiles at k step kt0
+            const i64 a_blk = ((i64)it.l*p.tiles_m + tm)*p.k_steps + kt0;
+            const i64 b_blk = ((i64)it.l*2*p.tiles_n + tb)*p.k_steps + kt0;
+            for (int i = 0; i < nstage && !*abort_flag; i++)
             {
-                const CrtItem it = crt_item(w, p.L, tiles_m2, p.tiles_n);
-                const i64 tm = 2*it.tm2 + rank, tb = 2*it.tn + rank;
-                // plane blocks of this CTA's A and B tiles at k step kt0
-                const i64 a_blk = ((i64)it.l*p.tiles_m + tm)*p.k_steps + kt0;
-                const i64 b_blk = ((i64)it.l*2*p.tiles_n + tb)*p.k_steps + kt0;
-                for (int i = 0; i < nstage; i++, g++)
-                {
-                    const int s = g % CRT2_STAGES;
-                    if (g >= CRT2_STAGES && !mbar_wait(&empty[s], ((g/CRT2_STAGES) & 1) ^ 1, abort_flag)) break;
-                    unsigned char* st = smem + s*CRT2_STAGE_BYTES;
-                    if (rank == 0) mbar_expect_tx(&full[s], 2*CRT2_STAGE_BYTES);
-                    tma_load_pair(st, &p.tmA, it.q, (int)(a_blk + i*CRT_KSUB), full0 + 8u*(uint32_t)s);
-                    tma_load_pair(st + CRT_KSUB*CRT2_TILE, &p.tmB, it.q, (int)(b_blk + i*CRT_KSUB),
-                                  full0 + 8u*(uint32_t)s);
-                }
+                const int s = i % CRT2_STAGES;
+                if (i >= CRT2_STAGES && !mbar_wait(&empty[s], ((i/CRT2_STAGES) & 1) ^ 1, abort_flag)) break;
+                unsigned char* st = smem + s*CRT2_STAGE_BYTES;
+                if (rank == 0) mbar_expect_tx(&full[s], 2*CRT2_STAGE_BYTES);
+                tma_load_pair(st, &p.tmA, it.q, (int)(a_blk + i*CRT_KSUB), full0 + 8u*(uint32_t)s);
+                tma_load_pair(st + CRT_KSUB*CRT2_TILE, &p.tmB, it.q, (int)(b_blk + i*CRT_KSUB),
+                              full0 + 8u*(uint32_t)s);
             }
         }
     }
@@ -1162,30 +1150,20 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
     {
         if (lane == 0 && rank == 0)
         {
-            int g = 0, j = 0;
-            for (i64 w = pair0; w < n_items && !*abort_flag; w += npairs, j++)
+            bool ok = true;
+            for (int i = 0; i < nstage; i++)
             {
-                const int b = j & 1;
-                // the epilogues of both CTAs have drained this accumulator
-                if (j >= 2 && !mbar_wait(&tempty[b], ((j >> 1) & 1) ^ 1, abort_flag)) break;
+                const int s = i % CRT2_STAGES;
+                if (!mbar_wait(&full[s], (i/CRT2_STAGES) & 1, abort_flag)) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t acc_addr = tmem_base + (uint32_t)(b*CRT_BN);
-                bool ok = true;
-                for (int i = 0; i < nstage; i++, g++)
-                {
-                    const int s = g % CRT2_STAGES;
-                    if (!mbar_wait(&full[s], (g/CRT2_STAGES) & 1, abort_flag)) { ok = false; break; }
-                    tc_fence_after();
-                    const unsigned char* st = smem + s*CRT2_STAGE_BYTES;
-                    #pragma unroll
-                    for (int u = 0; u < CRT_KSUB; u++)
-                        mma_i8_pair(acc_addr, sdesc_kmajor(st + u*CRT2_TILE),
-                                    sdesc_kmajor(st + (CRT_KSUB + u)*CRT2_TILE), IDESC, (i > 0 || u > 0) ? 1u : 0u);
-                    mma_commit_pair(&empty[s]);
-                }
-                if (!ok) break;
-                mma_commit_pair(&tfull[b]);
+                const unsigned char* st = smem + s*CRT2_STAGE_BYTES;
+                #pragma unroll
+                for (int u = 0; u < CRT_KSUB; u++)
+                    mma_i8_pair(tmem_base, sdesc_kmajor(st + u*CRT2_TILE),
+                                sdesc_kmajor(st + (CRT_KSUB + u)*CRT2_TILE), IDESC, (i > 0 || u > 0) ? 1u : 0u);
+                mma_commit_pair(&empty[s]);
             }
+            if (ok) mma_commit_pair(tfull);
         }
     }
     else
@@ -1193,46 +1171,34 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
         // warps 2..5: TMEM lane quarter warp % 4, one output row per thread
         const int quarter = warp & 3;
         const int row = quarter*32 + lane;
-        const uint32_t tempty0 = mapa_shared(smem_u32(tempty), 0);
-        int j = 0;
-        for (i64 w = pair0; w < n_items; w += npairs, j++)
+        const bool ok = mbar_wait(tfull, 0, abort_flag);
+        tc_fence_after();
+        const int q = it.q;
+        const int mq = (int)p.m[q];
+        const float mf = p.m[q], inv = p.inv[q], c16 = p.c16[q];
+        // residue tiles are column-major (byte (col, row) at col*128 + row)
+        unsigned char* out = p.R + ((((i64)it.l*p.tiles_m + tm)*p.tiles_n + it.tn)*p.nm + q)*(i64)CRT_OUT_TILE + row;
+        #pragma unroll 1
+        for (int c = 0; c < CRT_BN/16 && ok; c++)
         {
-            const int b = j & 1;
-            if (!mbar_wait(&tfull[b], (j >> 1) & 1, abort_flag)) break;
-            tc_fence_after();
-            const CrtItem it = crt_item(w, p.L, tiles_m2, p.tiles_n);
-            const i64 tm = 2*it.tm2 + rank;
-            const int q = it.q;
-            const int mq = (int)p.m[q];
-            const float mf = p.m[q], inv = p.inv[q], c16 = p.c16[q];
-            // residue tiles are column-major (byte (col, row) at col*128 + row)
-            unsigned char* out = p.R + ((((i64)it.l*p.tiles_m + tm)*p.tiles_n + it.tn)*p.nm + q)*(i64)CRT_OUT_TILE + row;
-            #pragma unroll 1
-            for (int c = 0; c < CRT_BN/16; c++)
+            int r[16];
+            tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)(c*16), r);
+            #pragma unroll
+            for (int jj = 0; jj < 16; jj++)
             {
-                int r[16];
-                tmem_ld16(tmem_base + ((uint32_t)(quarter*32) << 16) + (uint32_t)(b*CRT_BN + c*16), r);
-                #pragma unroll
-                for (int jj = 0; jj < 16; jj++)
+                uint32_t v;
+                if (mq == 256) v = (uint32_t)r[jj] & 0xFFu;
+                else
                 {
-                    uint32_t v;
-                    if (mq == 256) v = (uint32_t)r[jj] & 0xFFu;
-                    else
-                    {
-                        // r = hi*2^16 + lo: hi*(2^16 mod m) + lo is below 2^23 in magnitude, exact in FP32
-                        const float fh = __fsub_rn(__int_as_float(0x4B400000 + (r[jj] >> 16)), F_SHIFT);
-                        const float fl = __fsub_rn(__int_as_float(0x4B000000 | (r[jj] & 0xFFFF)), F_BIAS);
-                        float x = crt_reduce(__fmaf_rn(fh, c16, fl), mf, inv);
-                        if (x < 0.0f) x += mf;
-                        v = (uint32_t)__float_as_int(__fadd_rn(x, F_SHIFT));
-                    }
-                    out[(c*16 + jj)*OZ_BM] = (unsigned char)v;
+                    // r = hi*2^16 + lo: hi*(2^16 mod m) + lo is below 2^23 in magnitude, exact in FP32
+                    const float fh = __fsub_rn(__int_as_float(0x4B400000 + (r[jj] >> 16)), F_SHIFT);
+                    const float fl = __fsub_rn(__int_as_float(0x4B000000 | (r[jj] & 0xFFFF)), F_BIAS);
+                    float x = crt_reduce(__fmaf_rn(fh, c16, fl), mf, inv);
+                    if (x < 0.0f) x += mf;
+                    v = (uint32_t)__float_as_int(__fadd_rn(x, F_SHIFT));
                 }
+                out[(c*16 + jj)*OZ_BM] = (unsigned char)v;
             }
-            // this warp's reads of the accumulator are done: release it on CTA 0
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_cluster(tempty0 + 8u*(uint32_t)b);
         }
     }
 
@@ -1765,8 +1731,8 @@ void crt_run(OzakiJob& j, int nm, cudaStream_t st)
         g.kt1 = (int)std::min<i64>(ga.k_steps, (i64)(c + 1)*CRT_KT_RUN);
         TimedLaunch t("oz_crt_gemm", st);
         const i64 items = nm*v.l*tiles/2;
-        const i64 pairs = std::max<i64>(1, std::min<i64>(items, device_sm_count()/2));
-        oz_crt_gemm2<<<(unsigned)(2*pairs), OZ_THREADS, smem, st>>>(g);
+        TB_CHECK(2*items < ((i64)1 << 31), TB_ERR_SIZE, "Ozaki moduli path: grid too large");
+        oz_crt_gemm2<<<(unsigned)(2*items), OZ_THREADS, smem, st>>>(g);
         check_launch("oz_crt_gemm");
     }
 
