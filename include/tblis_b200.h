@@ -168,8 +168,19 @@ void tblis_b200_clear_error(void);
  * on; NULL = the legacy default stream. */
 void tblis_b200_set_stream(void* stream);
 void* tblis_b200_get_stream(void);
-/* Waits for all work this library enqueued on the current stream. */
+/* Waits for all work this library enqueued on the current stream. Records
+ * TB_ERR_TIMEOUT (6) as the last error when an Ozaki kernel gave up one of its
+ * bounded waits since the previous check (the flag is then cleared). */
 void tblis_b200_synchronize(void);
+
+/* Test support for the failure detection of the Ozaki kernels (no reference
+ * counterpart): the INT8/BF16 slice GEMM and the moduli GEMM skip the operand
+ * copies of k step (moduli kernel: pipeline stage) `step`, so the wait for it
+ * runs out after wait_seconds instead of the default 2 s; the kernel then
+ * records the timeout, drains its copies in flight, frees its tensor memory
+ * and returns, and tblis_b200_synchronize reports it. step = -1 and
+ * wait_seconds <= 0 restore normal operation. Returns 0 or an error code. */
+int tblis_b200_ozaki_inject_wait_timeout(int step, double wait_seconds);
 
 /* Normwise relative tolerance carried by a configuration (used by the Ozaki
  * configurations to pick the slice count; 0 restores the default 1e-12). */

@@ -71,9 +71,14 @@ constexpr int OZ_BK = 32;            // k bytes per stage (one MMA K step of any
 constexpr int OZ_SMAX = 8;           // 8 diagonals x 64 columns = all 512 TMEM columns
 constexpr int OZ_THREADS = 192;      // warp 0 bulk copies, warp 1 MMA, warps 2-5 epilogue
 constexpr int A_TILE = OZ_BM*OZ_BK;  // bytes of one A slice tile
-constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded waits: 2 s
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // bounded waits: 2 s by default
 
 __device__ int g_oz_error = 0;       // set by a kernel whose bounded wait gave up
+// test support: the limit of every bounded wait, and a k step (stage for the
+// moduli kernel) whose operand copies the slice and moduli GEMM kernels skip
+// (-1: none), so that a test can make a wait run out without any fault
+__device__ unsigned long long g_oz_wait_ns = WAIT_NS;
+__device__ int g_oz_skip_step = -1;
 
 // ---------------------------------------------------------------------------------
 // PTX helpers
@@ -113,8 +118,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// waits for the phase with the given parity to complete, at most WAIT_NS;
-// returns false (and records the error) when the wait gave up
+// waits for the phase with the given parity to complete, at most
+// g_oz_wait_ns; returns false (and records the error) when the wait gave up
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
 {
     if (mbar_try_wait(bar, parity)) return true;
@@ -125,7 +130,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
         if ((it & 255) == 0)
         {
             if (*abort_flag) return false;
-            if (globaltimer() - t0 > WAIT_NS)
+            if (globaltimer() - t0 > g_oz_wait_ns)
             {
                 *abort_flag = 1;
                 atomicExch(&g_oz_error, 1);
@@ -317,10 +322,14 @@ ozaki_gemm_kernel(const OzGemmArgs p)
         // ---- bulk-copy producer -------------------------------------------------
         if (lane == 0)
         {
+            const int skip = g_oz_skip_step;
+            int kt_end = 0;                              // k steps whose copies were issued
             for (int kt = 0; kt < kt_count && !*abort_flag; kt++)
             {
                 const int s = kt % STAGES;
                 if (kt >= STAGES && !mbar_wait(&empty[s], ((kt/STAGES) & 1) ^ 1, abort_flag)) break;
+                kt_end = kt + 1;
+                if (kt == skip) continue;                // test support: this stage never fills
                 unsigned char* st = smem + s*STAGE_BYTES;
                 mbar_expect_tx(&full[s], STAGE_BYTES);
                 // the S slice tiles of A, then those of B, each one contiguous block
@@ -328,13 +337,10 @@ ozaki_gemm_kernel(const OzGemmArgs p)
                 bulk_load(st + S*A_TILE, p.pB + (((i64)l*p.tiles_n + tn)*p.k_steps + kt)*(S*B_TILE),
                           S*B_TILE, &full[s]);
             }
-            // drain: the copies of the last stages must have landed before exit
-            const int last = min(kt_count, STAGES);
-            for (int i = 0; i < last; i++)
-            {
-                const int kt = kt_count - 1 - i;
-                mbar_wait(&full[kt % STAGES], (kt/STAGES) & 1, abort_flag);
-            }
+            // drain: the copies of the last stages issued must have landed
+            // before exit (bounded waits, also after a wait that gave up)
+            for (int kt = max(0, kt_end - STAGES); kt < kt_end; kt++)
+                if (kt != skip) mbar_wait(&full[kt % STAGES], (kt/STAGES) & 1, abort_flag);
         }
     }
     else if (warp == 1)
@@ -381,7 +387,11 @@ ozaki_gemm_kernel(const OzGemmArgs p)
             }
             mma_commit(accum);
             mma_commit(done);
-            mbar_wait(done, 0, abort_flag);
+            // the MMAs issued so far finish before the tensor memory is freed,
+            // also after a wait that gave up (a separate flag: only a timeout
+            // of this wait itself ends it early)
+            volatile int own_timeout = 0;
+            mbar_wait(done, 0, &own_timeout);
         }
     }
     else
@@ -1134,15 +1144,33 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
             // plane blocks of this CTA's A and B tiles at k step kt0
             const i64 a_blk = ((i64)it.l*p.tiles_m + tm)*p.k_steps + kt0;
             const i64 b_blk = ((i64)it.l*2*p.tiles_n + tb)*p.k_steps + kt0;
-            for (int i = 0; i < nstage && !*abort_flag; i++)
+            // both CTAs issue the same stages: each stage after the first
+            // CRT2_STAGES waits for the same multicast commit, and a producer
+            // stops only when that wait fails (not on the other warps' abort)
+            const int skip = g_oz_skip_step;
+            int i_end = 0;                               // stages whose copies were issued
+            volatile int own_timeout = 0;                // this producer's waits only
+            for (int i = 0; i < nstage; i++)
             {
                 const int s = i % CRT2_STAGES;
-                if (i >= CRT2_STAGES && !mbar_wait(&empty[s], ((i/CRT2_STAGES) & 1) ^ 1, abort_flag)) break;
+                if (i >= CRT2_STAGES && !mbar_wait(&empty[s], ((i/CRT2_STAGES) & 1) ^ 1, &own_timeout)) break;
+                i_end = i + 1;
+                // test support: neither CTA copies this stage (nor does CTA 0
+                // expect it), so it never completes
+                if (i == skip) continue;
                 unsigned char* st = smem + s*CRT2_STAGE_BYTES;
                 if (rank == 0) mbar_expect_tx(&full[s], 2*CRT2_STAGE_BYTES);
                 tma_load_pair(st, &p.tmA, it.q, (int)(a_blk + i*CRT_KSUB), full0 + 8u*(uint32_t)s);
                 tma_load_pair(st + CRT_KSUB*CRT2_TILE, &p.tmB, it.q, (int)(b_blk + i*CRT_KSUB),
                               full0 + 8u*(uint32_t)s);
+            }
+            if (rank == 0)
+            {
+                // the copies of both CTAs for the last stages issued have landed
+                // (their bytes complete CTA 0's barriers) before either CTA
+                // leaves; after a wait that gave up, each of these is bounded too
+                for (int i = max(0, i_end - CRT2_STAGES); i < i_end; i++)
+                    if (i != skip) mbar_wait(&full[i % CRT2_STAGES], (i/CRT2_STAGES) & 1, abort_flag);
             }
         }
     }
@@ -1150,11 +1178,10 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
     {
         if (lane == 0 && rank == 0)
         {
-            bool ok = true;
             for (int i = 0; i < nstage; i++)
             {
                 const int s = i % CRT2_STAGES;
-                if (!mbar_wait(&full[s], (i/CRT2_STAGES) & 1, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(&full[s], (i/CRT2_STAGES) & 1, abort_flag)) break;
                 tc_fence_after();
                 const unsigned char* st = smem + s*CRT2_STAGE_BYTES;
                 #pragma unroll
@@ -1163,7 +1190,9 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
                                 sdesc_kmajor(st + (CRT_KSUB + u)*CRT2_TILE), IDESC, (i > 0 || u > 0) ? 1u : 0u);
                 mma_commit_pair(&empty[s]);
             }
-            if (ok) mma_commit_pair(tfull);
+            // also after a wait that gave up: the epilogues learn from this
+            // commit that the MMAs issued so far are complete
+            mma_commit_pair(tfull);
         }
     }
     else
@@ -1171,7 +1200,11 @@ oz_crt_gemm2(const __grid_constant__ CrtGemmArgs p)
         // warps 2..5: TMEM lane quarter warp % 4, one output row per thread
         const int quarter = warp & 3;
         const int row = quarter*32 + lane;
-        const bool ok = mbar_wait(tfull, 0, abort_flag);
+        // waits for the MMAs to finish (a separate flag: another warp's
+        // timeout does not end this wait early), then writes only if no wait
+        // of this CTA gave up
+        volatile int own_timeout = 0;
+        const bool ok = mbar_wait(tfull, 0, &own_timeout) && !*abort_flag;
         tc_fence_after();
         const int q = it.q;
         const int mq = (int)p.m[q];
@@ -1756,7 +1789,20 @@ int ozaki_error_flag()
 {
     int v = 0;
     cudaMemcpyFromSymbol(&v, g_oz_error, sizeof(int));
+    if (v)
+    {
+        // reported once: the next check starts clean
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_oz_error, &zero, sizeof(int));
+    }
     return v;
+}
+
+void ozaki_inject_wait_timeout(int step, double wait_seconds)
+{
+    const unsigned long long ns = wait_seconds > 0.0 ? (unsigned long long)(wait_seconds*1e9) : WAIT_NS;
+    TB_CUDA(cudaMemcpyToSymbol(g_oz_skip_step, &step, sizeof(int)));
+    TB_CUDA(cudaMemcpyToSymbol(g_oz_wait_ns, &ns, sizeof(ns)));
 }
 
 void ozaki_begin(OzakiJob& j, cudaStream_t st)

@@ -53,6 +53,11 @@ void ozaki_end(OzakiJob& j, cudaStream_t st, bool stats_ready);
 
 namespace tb
 {
-// nonzero when an Ozaki kernel gave up a bounded wait (reads a device flag)
+// nonzero when an Ozaki kernel gave up a bounded wait since the last check
+// (reads and clears a device flag)
 int ozaki_error_flag();
+// test support: the Ozaki GEMM kernels skip the copies of k step (moduli
+// kernel: stage) `step` (-1: none) and bound every wait by wait_seconds (<= 0:
+// the default 2 s)
+void ozaki_inject_wait_timeout(int step, double wait_seconds);
 }
