@@ -1,40 +1,25 @@
-// dpd_driver.cxx -- test driver for libtblis_b200_cxx.so: builds MArray DPD
-// views over caller-provided storage and calls tblis::mult exactly as a C++
-// program written against TBLIS does (src/iface/3t/mult.h:56-60), so the
-// tests reach the library's mangled C++ entry point.
-//
-// A one-thread communicator stands in for TCI's: the entry point only reads
-// its thread count and thread index (tci/communicator.h:8-15).
-#include "dpd_varray_view.hpp"
+// dpd_driver.cxx -- test driver for libtblis_b200_cxx.so: a C++ caller
+// written against TBLIS's own headers (src/tblis.h, which declares the
+// tblis::mult overloads over MArray DPD and indexed-DPD views,
+// src/iface/3t/mult.h:56-60 and 92-96) with TCI's own communicator. It links
+// against libtblis_b200_cxx.so, libtblis_b200.so and TCI's library (the one a
+// TBLIS caller links beside libtblis), so the tests reach the library's
+// mangled C++ entry points exactly as such a program does.
+#include "tblis.h"
 #include "indexed_dpd_varray.hpp"
-
-#include "../../include/tblis_b200.h"
 
 #include <vector>
 
-namespace tci
-{
-class communicator
-{
-    public:
-        void* context = nullptr;
-        unsigned ngang = 1, gid = 0, nthread = 1, tid = 0;
-};
+// the library's extension entry points this driver uses (no counterpart in
+// TBLIS's headers; the rest of include/tblis_b200.h restates TBLIS's types,
+// which tblis.h already declares)
+extern "C" {
+int tblis_b200_last_error(void);
+void tblis_b200_clear_error(void);
+void tblis_b200_synchronize(void);
 }
 
-namespace tblis
-{
-template <typename T>
-void mult(const tci::communicator& comm,
-          T alpha, MArray::dpd_varray_view<const T> A, const label_type* idx_A,
-                   MArray::dpd_varray_view<const T> B, const label_type* idx_B,
-          T  beta, MArray::dpd_varray_view<      T> C, const label_type* idx_C);
-template <typename T>
-void mult(const tci::communicator& comm,
-          T alpha, MArray::indexed_dpd_varray_view<const T> A, const label_type* idx_A,
-                   MArray::indexed_dpd_varray_view<const T> B, const label_type* idx_B,
-          T  beta, MArray::indexed_dpd_varray_view<      T> C, const label_type* idx_C);
-}
+using tblis::len_type;
 
 namespace
 {
