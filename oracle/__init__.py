@@ -426,6 +426,13 @@ def ref_dense_impl(impl):
     return shim().refshim_set_dense_impl(int(impl))
 
 
+def ref_dpd_impl(impl):
+    """Selects the reference's DPD contraction implementation for the plain
+    DPD entry points: 0 = its default block path (BLIS), 1 = BLOCKED, 2 =
+    FULL (dense round trip). Returns the previous value."""
+    return shim().refshim_set_dpd_impl(int(impl))
+
+
 def _dpd_flat(nirrep, lens):
     return (_sz * (len(lens) * nirrep))(*[x for row in lens for x in row])
 

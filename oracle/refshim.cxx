@@ -107,6 +107,20 @@ int refshim_set_dense_impl(int impl)
     return old;
 }
 
+/*
+ * Selects the reference's DPD contraction implementation
+ * (src/internal/3t/dpd/mult.cxx:26): 0 = BLIS (its default block path),
+ * 1 = BLOCKED, 2 = FULL (dense round trip). Returns the previous value.
+ */
+int refshim_set_dpd_impl(int impl)
+{
+    const int old = tblis::internal::dpd_impl == tblis::internal::FULL ? 2 :
+                    tblis::internal::dpd_impl == tblis::internal::BLOCKED ? 1 : 0;
+    tblis::internal::dpd_impl = impl == 2 ? tblis::internal::FULL : impl == 1 ? tblis::internal::BLOCKED
+                                                                            : tblis::internal::BLIS;
+    return old;
+}
+
 void refshim_fill_block_scatter(unsigned ndim, const len_type* len, const stride_type* stride,
                                 len_type BS, stride_type off, stride_type size,
                                 stride_type* scat, stride_type* bs, int pack_3d)

@@ -452,7 +452,7 @@ DpdLabels dpd_labels(const DpdTensor& A, const char* idx_A, const DpdTensor& B, 
     return r;
 }
 
-// the cached grouped plan of a DPD contraction without batch labels
+// the cached grouped plan of a DPD contraction
 std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
                                       const DpdTensor& C, const char* idx_C, const DpdLabels& lab, cudaStream_t st)
 {
@@ -508,6 +508,109 @@ std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, con
 
     const std::string key = dpd_key(A, idx_A, B, idx_B, C, idx_C);
     auto plan = grouped_plan_cache().find(key);
+    if (!plan && !lab.ABC.empty())
+    {
+        // batch labels (in A, B and C): C = alpha*A*B + beta*C element-wise
+        // along them, as the reference's FULL and BLOCKED paths compute it
+        // (src/internal/3t/dpd/mult.cxx:28-74, 670-847). For every stored C
+        // block, split its irreps into AC (r), BC (c) and batch (t) parts.
+        // Only blocks with XOR(t) = irrep(A)^irrep(B)^irrep(C) receive
+        // products (A and B blocks exist for both only then); each batch
+        // element z of such a block is one group of the grouped launch
+        // (rows AC, columns BC, one K segment per AB irrep combination, every
+        // offset shifted by z through that block's own batch strides). Other
+        // blocks, and groups without contracted blocks, are beta-only patches.
+        auto p = std::make_shared<GroupedPlan>();
+        double flops = 0;
+        const std::string ABC = lab.ABC;
+        const unsigned x_need = A.lay.irrep ^ B.lay.irrep ^ C.lay.irrep;
+        const auto dAC = dims(AC, iA), dAB = dims(AB, iA), dBAB = dims(AB, iB), dBBC = dims(BC, iB);
+        const auto dCAC = dims(AC, iC), dCBC = dims(BC, iC);
+        const auto zA = dims(ABC, iA), zB = dims(ABC, iB), zC = dims(ABC, iC);
+        std::vector<unsigned> dCACZ = dCAC;
+        dCACZ.insert(dCACZ.end(), zC.begin(), zC.end());
+        C.lay.for_each_block([&](const std::vector<unsigned>& irrC, const std::vector<i64>& cl,
+                                 const std::vector<i64>& cs, i64 baseC)
+        {
+            unsigned xr = 0, xt = 0;
+            std::vector<unsigned> r(AC.size()), c(BC.size()), t(ABC.size());
+            for (size_t i = 0; i < AC.size(); i++) { r[i] = irrC[dCAC[i]]; xr ^= r[i]; }
+            for (size_t i = 0; i < BC.size(); i++) c[i] = irrC[dCBC[i]];
+            for (size_t i = 0; i < ABC.size(); i++) { t[i] = irrC[zC[i]]; xt ^= t[i]; }
+            i64 dummy;
+            if (xt != x_need)
+            {
+                // no A and B blocks meet here: beta only, over the whole block
+                ivec pm = block_part(C.lay, irrC, dCACZ, dummy), pn = block_part(C.lay, irrC, dCBC, dummy);
+                for (i64& x : pm) x += baseC;
+                if (!pm.empty() && !pn.empty()) p->empty_patches.push_back({std::move(pm), std::move(pn)});
+                return;
+            }
+            // the A and B blocks of each AB irrep combination k
+            const auto kc = combos((unsigned)AB.size(), A.lay.irrep ^ xr ^ xt, nirrep);
+            struct Pair { std::vector<unsigned> ia, ib; };
+            std::vector<Pair> pairs;
+            for (auto& k : kc)
+            {
+                Pair q;
+                q.ia.assign(A.lay.ndim, 0);
+                q.ib.assign(B.lay.ndim, 0);
+                for (size_t i = 0; i < AC.size(); i++) q.ia[dAC[i]] = r[i];
+                for (size_t i = 0; i < AB.size(); i++) { q.ia[dAB[i]] = k[i]; q.ib[dBAB[i]] = k[i]; }
+                for (size_t i = 0; i < BC.size(); i++) q.ib[dBBC[i]] = c[i];
+                for (size_t i = 0; i < ABC.size(); i++) { q.ia[zA[i]] = t[i]; q.ib[zB[i]] = t[i]; }
+                pairs.push_back(std::move(q));
+            }
+            ivec cm0 = block_part(C.lay, irrC, dCAC, dummy), cn = block_part(C.lay, irrC, dCBC, dummy);
+            if (cm0.empty() || cn.empty()) return;
+            // batch elements of this block (odometer over the batch dims, first fastest)
+            std::vector<i64> zl(ABC.size());
+            i64 nz = 1;
+            for (size_t i = 0; i < ABC.size(); i++) { zl[i] = cl[zC[i]]; nz *= zl[i]; }
+            std::vector<i64> z(ABC.size(), 0);
+            for (i64 e = 0; e < nz; e++)
+            {
+                i64 offC = baseC;
+                for (size_t i = 0; i < ABC.size(); i++) offC += z[i]*cs[zC[i]];
+                GroupTables gb;
+                gb.c_m = cm0;
+                for (i64& x : gb.c_m) x += offC;
+                gb.c_n = cn;
+                gb.M = (i64)gb.c_m.size(); gb.N = (i64)gb.c_n.size(); gb.K = 0;
+                for (const Pair& q : pairs)
+                {
+                    std::vector<i64> al(A.lay.ndim), as(A.lay.ndim), bl(B.lay.ndim), bs(B.lay.ndim);
+                    i64 baseA, baseB;
+                    A.lay.block(q.ia.data(), al.data(), as.data(), baseA);
+                    B.lay.block(q.ib.data(), bl.data(), bs.data(), baseB);
+                    SegTables sg;
+                    sg.a_k = block_part(A.lay, q.ia, dAB, dummy);
+                    if (sg.a_k.empty()) continue;
+                    for (size_t i = 0; i < ABC.size(); i++) { baseA += z[i]*as[zA[i]]; baseB += z[i]*bs[zB[i]]; }
+                    sg.a_m = block_part(A.lay, q.ia, dAC, dummy);
+                    sg.b_k = block_part(B.lay, q.ib, dBAB, dummy);
+                    sg.b_n = block_part(B.lay, q.ib, dBBC, dummy);
+                    for (i64& x : sg.a_m) x += baseA;
+                    for (i64& x : sg.b_k) x += baseB;
+                    gb.K += (i64)sg.a_k.size();
+                    gb.segs.push_back(std::move(sg));
+                }
+                if (gb.segs.empty()) p->empty_patches.push_back({gb.c_m, gb.c_n});
+                else
+                {
+                    gb.amode = gather_mode(gb.segs[0].a_m, gb.segs[0].a_k);
+                    gb.bmode = gather_mode(gb.segs[0].b_n, gb.segs[0].b_k);
+                    gb.a_slot = 0; gb.b_slot = 1; gb.c_slot = 2;
+                    flops += 2.0*gb.M*gb.N*gb.K;
+                    p->groups.push_back(std::move(gb));
+                }
+                for (size_t i = 0; i < ABC.size() && ++z[i] == zl[i]; i++) z[i] = 0;
+            }
+        });
+        p->flops = flops;
+        p->finalize(st);
+        plan = grouped_plan_cache().insert(key, p);
+    }
     if (!plan)
     {
         auto p = std::make_shared<GroupedPlan>();
@@ -627,7 +730,6 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
         else l1_scale<double>(C.data, s, beta, st);
         return;
     }
-    TB_CHECK(lab.ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
     const std::shared_ptr<GroupedPlan> plan = dpd_plan(A, idx_A, B, idx_B, C, idx_C, lab, st);
 
     const double* ptrs[3] = {A.data, B.data, C.data};
@@ -656,7 +758,6 @@ int dpd_mult_terms(const std::vector<DpdTerm>& terms, cudaStream_t st, DpdMultRe
         const DpdTerm& x = terms[t];
         const DpdLabels lab = dpd_labels(*x.a, x.ia, *x.b, x.ib, *x.c, x.ic, reference_irrep_check);
         if (x.alpha == 0.0 || (lab.ABC.empty() && lab.mismatch)) continue;
-        TB_CHECK(lab.ABC.empty(), TB_ERR_ARG, "DPD: batch labels (in A, B and C) are not supported on the GPU path");
         plans[t] = dpd_plan(*x.a, x.ia, *x.b, x.ib, *x.c, x.ic, lab, st);
         // beta = 1: C patches without contracted blocks stay as they are
         if (plans[t]->groups.empty()) continue;

@@ -297,8 +297,8 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
         }
     }
 
-    // labels shared by all three tensors must not be dense in all of them
-    // (batch labels are not supported, as in the DPD contraction)
+    // labels shared by all three tensors and dense in all of them are batch
+    // labels of each entry triple's DPD contraction
     auto indexed_in = [&](int t, char c, unsigned& slot)
     {
         const size_t p = I[t]->find(c);
@@ -327,12 +327,6 @@ void indexed_dpd_mult(const tblis_b200_indexed_dpd_tensor* A_, const label_type*
     double flops = 0;
     if (!skip)
     {
-        for (char c : iA)
-        {
-            if (iB.find(c) == std::string::npos || iC.find(c) == std::string::npos) continue;
-            TB_CHECK(fixed_irrep.count(c), TB_ERR_ARG,
-                     "indexed DPD: labels dense in all three tensors are not supported on the GPU path");
-        }
         // per tensor: dense dims kept (label dense everywhere) or cut (label indexed elsewhere)
         Slicing S[3];
         for (int t = 0; t < 3; t++)
