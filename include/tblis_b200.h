@@ -399,6 +399,29 @@ int tblis_b200_indexed_dpd_shift(const tblis_scalar* alpha, tblis_b200_indexed_d
 /* Offset (from data), lengths and strides of one block (one irrep per
  * dimension), as dpd_varray_view::operator()(irreps) gives them
  * (dpd_marray_base.hpp:171-228). Returns 0 or an error code. */
+/* A DPD contraction split across ranks (one process per GPU), with no
+ * collective on the data path (no counterpart in the reference, which runs
+ * on CPU threads). The unit of work is a row band of one irrep GEMM of
+ * src/internal/3t/dpd/mult.cxx:308: the C blocks that share their AC (and
+ * batch) irreps. Units go to ranks largest first onto the least loaded rank,
+ * by FLOPs computed from the lengths alone, so every rank derives the same
+ * split without a device.
+ * tblis_b200_dpd_shard_plan (host-only): owner[t] = the rank that computes
+ * the C block with irrep tuple t (t = sum_d irrep_d * nirrep^d, dimension 0
+ * fastest; -1 where no block is stored; nirrep^ndim(C) entries), and, if
+ * flops is not NULL, each rank's FLOPs (nranks entries).
+ * tblis_b200_dpd_mult_shard: this rank's blocks of C = alpha*A*B + beta*C
+ * (double tensors); the other blocks of C are left as they are. Both return
+ * 0 or an error code. */
+int tblis_b200_dpd_shard_plan(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                              const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                              const tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                              int nranks, int* owner, double* flops);
+int tblis_b200_dpd_mult_shard(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                              const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                                    tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                              int nranks, int rank, tblis_b200_report* report);
+
 int tblis_b200_dpd_block(const tblis_b200_dpd_tensor* A, const unsigned* irreps, len_type* len,
                          stride_type* stride, stride_type* offset);
 

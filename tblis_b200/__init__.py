@@ -446,6 +446,75 @@ def dpd_mult(alpha, A, idx_A, B, idx_B, beta, C, idx_C):
     return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
 
 
+lib.tblis_b200_dpd_shard_plan.restype = ctypes.c_int
+lib.tblis_b200_dpd_mult_shard.restype = ctypes.c_int
+
+
+def dpd_shard_plan(A, idx_A, B, idx_B, C, idx_C, nranks):
+    """(owner, flops): the rank that computes each C block of a DPD
+    contraction split over nranks processes, keyed by the block's irrep
+    tuple, and each rank's FLOPs (tblis_b200_dpd_shard_plan; host-only: needs
+    no GPU). Units of work are the irrep GEMMs (irrep of the contracted
+    labels), placed longest first onto the least loaded rank."""
+    import itertools
+    a, b, c = A.struct(), B.struct(), C.struct()
+    n, nd = C.nirrep, len(C.lens)
+    owner = (ctypes.c_int * (n ** nd))()
+    flops = (ctypes.c_double * int(nranks))()
+    lib.tblis_b200_dpd_shard_plan(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B), ctypes.byref(c),
+                                  _labels(idx_C), int(nranks), owner, flops)
+    _check()
+    out = {}
+    for t in itertools.product(range(n), repeat=nd):
+        k = sum(t[d] * n ** d for d in range(nd))
+        if owner[k] >= 0:
+            out[t] = owner[k]
+    return out, list(flops)
+
+
+def dpd_mult_shard(alpha, A, idx_A, B, idx_B, beta, C, idx_C, rank=None, nranks=None, gather=False, group=None):
+    """This rank's blocks of C = alpha*A*B + beta*C over DPD tensors
+    (tblis_b200_dpd_mult_shard); the others stay as they are. rank / nranks
+    default to the torch.distributed group's; gather=True then hands every
+    rank's blocks to every rank (dpd_gather_shards)."""
+    rank, nranks = _rank_world(rank, nranks, group)
+    a, b, c = A.struct(alpha), B.struct(), C.struct(beta)
+    r = tblis_b200_report()
+    lib.tblis_b200_dpd_mult_shard(ctypes.byref(a), _labels(idx_A), ctypes.byref(b), _labels(idx_B), ctypes.byref(c),
+                                  _labels(idx_C), int(nranks), int(rank), ctypes.byref(r))
+    _check()
+    if gather:
+        dpd_gather_shards(A, idx_A, B, idx_B, C, idx_C, rank, nranks, group)
+    return {f: getattr(r, f) for f, _ in tblis_b200_report._fields_}
+
+
+def dpd_gather_shards(A, idx_A, B, idx_B, C, idx_C, rank=None, nranks=None, group=None):
+    """Every rank broadcasts the elements of its blocks of C (C.data: a flat
+    torch tensor of the same layout on every rank) in rank order; afterwards
+    all ranks hold the whole C. Over NCCL on GPUs, gloo on CPU tensors."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    rank, nranks = _rank_world(rank, nranks, group)
+    owner, _ = dpd_shard_plan(A, idx_A, B, idx_B, C, idx_C, nranks)
+    per_rank = [[] for _ in range(nranks)]
+    for t, r in owner.items():
+        off, L, S = C.block(t)
+        if np.prod(L) == 0:
+            continue
+        grid = np.indices(L).reshape(len(L), -1)
+        per_rank[r].append(off + (np.asarray(S)[:, None] * grid).sum(0))
+    flat = C.data.view(-1)
+    for r in range(nranks):
+        if not per_rank[r]:
+            continue
+        idx = torch.from_numpy(np.concatenate(per_rank[r]).astype(np.int64)).to(flat.device)
+        buf = flat.index_select(0, idx) if r == rank else flat.new_empty(idx.numel())
+        dist.broadcast(buf, src=dist.get_global_rank(group, r) if group is not None else r, group=group)
+        if r != rank:
+            flat.index_copy_(0, idx, buf)
+
+
 class tblis_b200_dpd_block_table(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("conj", ctypes.c_int), ("scalar", tblis_scalar),
                 ("data", ctypes.c_void_p), ("ndim", ctypes.c_uint), ("nirrep", ctypes.c_uint),

@@ -305,6 +305,69 @@ int tblis_b200_dpd_mult_blocks(const tblis_b200_dpd_block_table* A, const label_
     return guarded([&] { run_dpd_mult(A, idx_A, B, idx_B, C, idx_C, report); });
 }
 
+int tblis_b200_dpd_shard_plan(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                              const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                              const tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                              int nranks, int* owner, double* flops)
+{
+    return guarded([&]
+    {
+        TB_CHECK(owner, TB_ERR_ARG, "null owner array");
+        DpdTensor a, b, c;
+        to_layout(A, a.lay);
+        to_layout(B, b.lay);
+        to_layout(C, c.lay);
+        std::vector<double> load;
+        const std::vector<int> own = dpd_shard_owner(a, idx_A, b, idx_B, c, idx_C, nranks, &load);
+        std::copy(own.begin(), own.end(), owner);
+        if (flops) std::copy(load.begin(), load.end(), flops);
+    });
+}
+
+int tblis_b200_dpd_mult_shard(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
+                              const tblis_b200_dpd_tensor* B, const label_type* idx_B,
+                                    tblis_b200_dpd_tensor* C, const label_type* idx_C,
+                              int nranks, int rank, tblis_b200_report* report)
+{
+    return guarded([&]
+    {
+        ensure_device();
+        cudaStream_t st = current_stream();
+        const int k0 = (int)g_kernel_count.load();
+        TB_CHECK(A && B && C, TB_ERR_ARG, "null DPD tensor");
+        TB_CHECK(A->type == TYPE_DOUBLE && B->type == TYPE_DOUBLE && C->type == TYPE_DOUBLE, TB_ERR_TYPE,
+                 "DPD shard: double tensors only");
+        DpdTensor a, b, c;
+        to_layout(A, a.lay);
+        to_layout(B, b.lay);
+        to_layout(C, c.lay);
+        const double alpha = A->scalar.data.d*B->scalar.data.d, beta = C->scalar.data.d;
+        DpdStage sa, sb, sc;
+        sa.init(A->data, a.lay.total(), sizeof(double), true, st);
+        sb.init(B->data, b.lay.total(), sizeof(double), true, st);
+        // blocks of other ranks come back unchanged: C is copied in
+        sc.init(C->data, c.lay.total(), sizeof(double), true, st);
+        a.data = reinterpret_cast<double*>(sa.dev);
+        b.data = reinterpret_cast<double*>(sb.dev);
+        c.data = reinterpret_cast<double*>(sc.dev);
+        DpdMultReport r;
+        dpd_mult_shard(a, idx_A, b, idx_B, c, idx_C, alpha, beta, nranks, rank, st, &r);
+        sc.out(st);
+        if (sa.host || sb.host || sc.host) TB_CUDA(cudaStreamSynchronize(st));
+        C->scalar.data.d = 1.0;
+        C->scalar.type = TYPE_DOUBLE;
+        C->conj = 0;
+        if (report)
+        {
+            memset(report, 0, sizeof(*report));
+            report->method = 1;
+            report->flops = r.flops;
+            report->m = r.groups;
+            report->kernels = (int)g_kernel_count.load() - k0;
+        }
+    });
+}
+
 int tblis_b200_dpd_block(const tblis_b200_dpd_tensor* A, const unsigned* irreps, len_type* len,
                          stride_type* stride, stride_type* offset)
 {

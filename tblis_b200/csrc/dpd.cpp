@@ -453,8 +453,37 @@ DpdLabels dpd_labels(const DpdTensor& A, const char* idx_A, const DpdTensor& B, 
 }
 
 // the cached grouped plan of a DPD contraction
+// the unit of work a stored C block belongs to: its AC and batch irreps, a
+// row band of one irrep GEMM (src/internal/3t/dpd/mult.cxx:308; the irrep of
+// the contracted labels follows from them), numbered over those dims of C in
+// C's dimension order
+size_t dpd_block_unit(const DpdLabels& lab, const std::string& iC, unsigned nirrep,
+                      const std::vector<unsigned>& irrC)
+{
+    size_t u = 0;
+    for (size_t d = iC.size(); d-- > 0;)
+        if (lab.AC.find(iC[d]) != std::string::npos || lab.ABC.find(iC[d]) != std::string::npos)
+            u = u*nirrep + irrC[d];
+    return u;
+}
+
+// the C blocks a plan covers: every block (owned == nullptr) or those whose
+// unit is marked in *owned
+struct DpdShare
+{
+    const std::vector<char>* owned = nullptr;
+    const DpdLabels* lab = nullptr;
+    std::string iC;
+    unsigned nirrep = 1;
+    bool covers(const std::vector<unsigned>& irrC) const
+    {
+        return !owned || (*owned)[dpd_block_unit(*lab, iC, nirrep, irrC)];
+    }
+};
+
 std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
-                                      const DpdTensor& C, const char* idx_C, const DpdLabels& lab, cudaStream_t st)
+                                      const DpdTensor& C, const char* idx_C, const DpdLabels& lab, cudaStream_t st,
+                                      const DpdShare& share = DpdShare())
 {
     const unsigned nirrep = A.lay.nirrep;
     const std::string iA(idx_A, A.lay.ndim), iB(idx_B, B.lay.ndim), iC(idx_C, C.lay.ndim);
@@ -506,7 +535,12 @@ std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, con
         return d;
     };
 
-    const std::string key = dpd_key(A, idx_A, B, idx_B, C, idx_C);
+    std::string key = dpd_key(A, idx_A, B, idx_B, C, idx_C);
+    if (share.owned)
+    {
+        key += "|units:";
+        for (char o : *share.owned) key.push_back(o ? '1' : '0');
+    }
     auto plan = grouped_plan_cache().find(key);
     if (!plan && !lab.ABC.empty())
     {
@@ -537,6 +571,7 @@ std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, con
             for (size_t i = 0; i < AC.size(); i++) { r[i] = irrC[dCAC[i]]; xr ^= r[i]; }
             for (size_t i = 0; i < BC.size(); i++) c[i] = irrC[dCBC[i]];
             for (size_t i = 0; i < ABC.size(); i++) { t[i] = irrC[zC[i]]; xt ^= t[i]; }
+            if (!share.covers(irrC)) return;                              // another rank's unit
             i64 dummy;
             if (xt != x_need)
             {
@@ -620,6 +655,21 @@ std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, con
             const unsigned irr_AC = irrA ^ h, irr_BC = irrB ^ h;
             auto rc = combos((unsigned)AC.size(), irr_AC, nirrep);
             auto cc = combos((unsigned)BC.size(), irr_BC, nirrep);
+            if (share.owned && !cc.empty())
+            {
+                // this rank's row bands only (every block of a band shares its unit)
+                std::vector<std::vector<unsigned>> mine;
+                const auto dCAC0 = dims(AC, iC), dCBC0 = dims(BC, iC);
+                for (auto& r : rc)
+                {
+                    std::vector<unsigned> irrC(C.lay.ndim, 0);
+                    for (size_t i = 0; i < AC.size(); i++) irrC[dCAC0[i]] = r[i];
+                    for (size_t i = 0; i < BC.size(); i++) irrC[dCBC0[i]] = cc[0][i];
+                    if (share.covers(irrC)) mine.push_back(r);
+                }
+                rc.swap(mine);
+            }
+            if (rc.empty()) continue;
             auto kc = combos((unsigned)AB.size(), h, nirrep);
             GroupTables g;
             bool ok = patch_view(A.lay, dims(AC, iA), rc, dims(AB, iA), kc, g.a_m, g.a_k) &&
@@ -703,19 +753,26 @@ std::shared_ptr<GroupedPlan> dpd_plan(const DpdTensor& A, const char* idx_A, con
 
 void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
-              DpdMultReport* rep, bool reference_irrep_check)
+              DpdMultReport* rep, bool reference_irrep_check, const std::vector<char>* owned)
 {
     const DpdLabels lab = dpd_labels(A, idx_A, B, idx_B, C, idx_C, reference_irrep_check);
     const i64 ctotal = C.lay.total();
+    DpdShare share;
+    share.owned = owned;
+    share.lab = &lab;
+    share.iC.assign(idx_C, C.lay.ndim);
+    share.nirrep = C.lay.nirrep;
     if (alpha == 0.0 || (lab.ABC.empty() && lab.mismatch))
     {
         if (beta == 1.0 || ctotal == 0) return;
-        if (C.lay.is_explicit())
+        if (C.lay.is_explicit() || owned)
         {
-            // a view's blocks need not fill [0, extent): scale block by block
-            C.lay.for_each_block([&](const std::vector<unsigned>&, const std::vector<i64>& bl,
+            // a view's blocks need not fill [0, extent), and a rank's share is
+            // a set of blocks: scale block by block
+            C.lay.for_each_block([&](const std::vector<unsigned>& irrC, const std::vector<i64>& bl,
                                      const std::vector<i64>& bs, i64 off)
             {
+                if (!share.covers(irrC)) return;
                 TB_CHECK(C.lay.ndim <= (unsigned)L1_MAX_DIM, TB_ERR_SIZE, "DPD: too many dimensions");
                 Strided s;
                 s.ndim = (int)C.lay.ndim;
@@ -730,7 +787,7 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
         else l1_scale<double>(C.data, s, beta, st);
         return;
     }
-    const std::shared_ptr<GroupedPlan> plan = dpd_plan(A, idx_A, B, idx_B, C, idx_C, lab, st);
+    const std::shared_ptr<GroupedPlan> plan = dpd_plan(A, idx_A, B, idx_B, C, idx_C, lab, st, share);
 
     const double* ptrs[3] = {A.data, B.data, C.data};
     // C patches without contracted blocks: beta scaling (rare; irreps with K_h == 0)
@@ -743,6 +800,83 @@ void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const c
         rep->flops = plan->flops;
         rep->variant = plan->variant;
     }
+}
+
+std::vector<int> dpd_shard_owner(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                                 const DpdTensor& C, const char* idx_C, int nranks, std::vector<double>* load,
+                                 std::vector<int>* unit_rank_out)
+{
+    TB_CHECK(nranks >= 1, TB_ERR_ARG, "DPD shard: nranks must be at least 1");
+    const DpdLabels lab = dpd_labels(A, idx_A, B, idx_B, C, idx_C, true);
+    const unsigned nirrep = C.lay.nirrep;
+    const std::string iA(idx_A, A.lay.ndim), iC(idx_C, C.lay.ndim);
+    size_t nunits = 1;
+    for (char c : iC)
+        if (lab.AC.find(c) != std::string::npos || lab.ABC.find(c) != std::string::npos) nunits *= nirrep;
+    // flops of each unit from the lengths alone: every C block of the band
+    // times the K extent of the AB irrep combinations that reach it
+    std::vector<double> flops(nunits, 0.0);
+    std::vector<unsigned> ab;
+    for (char c : lab.AB) ab.push_back((unsigned)iA.find(c));
+    C.lay.for_each_block([&](const std::vector<unsigned>& irrC, const std::vector<i64>& bl,
+                             const std::vector<i64>&, i64)
+    {
+        unsigned h = A.lay.irrep;
+        for (char c : lab.AC) h ^= irrC[iC.find(c)];
+        for (char c : lab.ABC) h ^= irrC[iC.find(c)];
+        double mnz = 1.0;
+        for (i64 x : bl) mnz *= (double)x;
+        double k = 0.0;
+        for (auto& kc : combos((unsigned)ab.size(), h, nirrep))
+        {
+            double e = 1.0;
+            for (size_t i = 0; i < ab.size(); i++) e *= (double)A.lay.len[ab[i]][kc[i]];
+            k += e;
+        }
+        flops[dpd_block_unit(lab, iC, nirrep, irrC)] += 2.0*mnz*std::max(k, 1.0);
+    });
+    // largest unit first onto the least loaded rank (ties: lower unit, lower rank)
+    std::vector<size_t> order(nunits);
+    for (size_t u = 0; u < nunits; u++) order[u] = u;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return flops[x] > flops[y]; });
+    std::vector<int> unit_rank(nunits, 0);
+    std::vector<double> rl(nranks, 0.0);
+    for (size_t u : order)
+    {
+        if (flops[u] == 0.0) continue;
+        int best = 0;
+        for (int r = 1; r < nranks; r++) if (rl[r] < rl[best]) best = r;
+        unit_rank[u] = best;
+        rl[best] += flops[u];
+    }
+    if (load) *load = rl;
+    if (unit_rank_out) *unit_rank_out = unit_rank;
+    // the owner of every irrep tuple of C (dimension 0 fastest); -1 where no
+    // block is stored
+    size_t nt = 1;
+    for (unsigned d = 0; d < C.lay.ndim; d++) nt *= nirrep;
+    std::vector<int> owner(nt, -1);
+    C.lay.for_each_block([&](const std::vector<unsigned>& irrC, const std::vector<i64>&, const std::vector<i64>&, i64)
+    {
+        size_t t = 0;
+        for (unsigned d = C.lay.ndim; d-- > 0;) t = t*nirrep + irrC[d];
+        owner[t] = unit_rank[dpd_block_unit(lab, iC, nirrep, irrC)];
+    });
+    return owner;
+}
+
+void dpd_mult_shard(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                    DpdTensor& C, const char* idx_C, double alpha, double beta, int nranks, int rank,
+                    cudaStream_t st, DpdMultReport* rep)
+{
+    TB_CHECK(rank >= 0 && rank < nranks, TB_ERR_ARG, "DPD shard: rank out of range");
+    std::vector<int> unit_rank;
+    dpd_shard_owner(A, idx_A, B, idx_B, C, idx_C, nranks, nullptr, &unit_rank);
+    std::vector<char> owned(unit_rank.size());
+    bool any = false;
+    for (size_t u = 0; u < unit_rank.size(); u++) { owned[u] = unit_rank[u] == rank; any = any || owned[u]; }
+    if (!any) { if (rep) *rep = DpdMultReport(); return; }
+    dpd_mult(A, idx_A, B, idx_B, C, idx_C, alpha, beta, st, rep, true, &owned);
 }
 
 int dpd_mult_terms(const std::vector<DpdTerm>& terms, cudaStream_t st, DpdMultReport* rep,

@@ -80,9 +80,28 @@ struct DpdMultReport
 // does (its operator precedence included); false: skip only when
 // irrep(A) ^ irrep(B) != irrep(C), as the internal block loops of the
 // indexed-DPD contraction see it
+// owned (optional) marks the units of work whose C blocks are computed, for a
+// rank's share of a sharded contraction (dpd_shard_owner's units); the other
+// blocks of C are left untouched
 void dpd_mult(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
               DpdTensor& C, const char* idx_C, double alpha, double beta, cudaStream_t st,
-              DpdMultReport* rep, bool reference_irrep_check = true);
+              DpdMultReport* rep, bool reference_irrep_check = true, const std::vector<char>* owned = nullptr);
+
+// A DPD contraction split across ranks with no collective on the data path.
+// The unit of work is a row band of one irrep GEMM
+// (src/internal/3t/dpd/mult.cxx:308): the C blocks that share their AC (and
+// batch) irreps. Units go to ranks largest first onto the least loaded one,
+// by FLOPs computed from the lengths alone, so every rank derives the same
+// split without a device. Returns the owner of every irrep tuple of C
+// (dimension 0 fastest, -1 where no block is stored) and, when asked, each
+// rank's FLOPs and each unit's rank.
+std::vector<int> dpd_shard_owner(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                                 const DpdTensor& C, const char* idx_C, int nranks, std::vector<double>* load,
+                                 std::vector<int>* unit_rank = nullptr);
+// rank's blocks of C = alpha*A*B + beta*C; the others stay as they are
+void dpd_mult_shard(const DpdTensor& A, const char* idx_A, const DpdTensor& B, const char* idx_B,
+                    DpdTensor& C, const char* idx_C, double alpha, double beta, int nranks, int rank,
+                    cudaStream_t st, DpdMultReport* rep);
 
 // One real term C += alpha*A*B (beta = 1) of a sequence of DPD contractions.
 // Terms whose C storage may overlap carry the same c_key.
