@@ -50,7 +50,7 @@ def parse(argv=None):
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) leg")
     p.add_argument("--o", type=int, default=48, help="occupied extent (profiling runs use a smaller case)")
     p.add_argument("--v", type=int, default=160, help="virtual extent")
-    p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce", "dpd"],
+    p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce", "dpd", "serve", "batch"],
                    help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
     a = p.parse_args(argv)
     global O, V, FLOPS_LADDER, WORKLOAD
@@ -379,6 +379,12 @@ def main():
     stream = torch.cuda.current_stream()
     tb.set_stream(stream.cuda_stream)
 
+    if args.case == "serve":
+        print(json.dumps(serve_workloads(torch, tb, dev)))
+        return
+    if args.case == "batch":
+        print(json.dumps(batch_workload(torch, tb, dev, stream)))
+        return
     if args.case:
         print(json.dumps(single_case(torch, tb, dev, stream, args)))
         return
@@ -747,24 +753,26 @@ def batch_workload(torch, tb, dev, stream, count=10000, serial_sample=500, check
     return out
 
 
-def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
-    """Stream of pairwise 4-index contraction requests: 6 labels split 2/2/2
-    into contracted, A-only and B-only groups at random, every operand's index
-    order permuted, extents log-uniform in 8..128, each operand at most 256 MB
-    (resampled otherwise), FP64, requested tolerance 1e-10 or 1e-13 (50/50),
-    Poisson arrivals at `rate` per second. Operands are device-resident: the
-    requests draw from a pool of `pool_size` resident problems (a solver's
-    amplitudes), each with two output buffers used alternately. Returns the
-    server's p50/p99 latency and throughput, and the throughput of the same
-    requests issued as serial plain calls."""
+SERVE_REQUESTS = 20000
+SERVE_POOL_BYTES = 48 << 30
+SERVE_RATES = (50, 200, 500, 1000, 2000)
+SERVE_WINDOW_S = 4.0
+
+
+def serve_pool(torch, dev, budget_bytes, seed=0):
+    """Resident problems of the serving stream: 6 labels split 2/2/2 at random
+    into contracted, A-only and B-only groups, every operand's index order
+    permuted, extents log-uniform in 8..128, each operand at most 256 MB
+    (resampled otherwise), FP64 uniform(-1,1); drawn until A, B and C of all
+    problems fill budget_bytes of HBM (a solver's resident amplitudes)."""
     import math
     import random
     rnd = random.Random(seed)
     g = torch.Generator(device=dev)
     g.manual_seed(seed + 1)
     cap = (256 << 20) // 8
-    pool = []
-    while len(pool) < pool_size:
+    pool, used = [], 0
+    while True:
         labs = list("abcdef")
         rnd.shuffle(labs)
         AB, AC, BC = labs[0:2], labs[2:4], labs[4:6]
@@ -773,45 +781,32 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
         sizes = [math.prod(l[c] for c in x) for x in (ia, ib, ic)]
         if max(sizes) > cap:
             continue
+        if used + 8 * sum(sizes) > budget_bytes:
+            break
+        used += 8 * sum(sizes)
         rnd.shuffle(ia); rnd.shuffle(ib); rnd.shuffle(ic)
         ia, ib, ic = "".join(ia), "".join(ib), "".join(ic)
         mk = lambda ix: torch.empty([l[c] for c in ix], dtype=torch.float64, device=dev).uniform_(-1, 1, generator=g)
-        fl = 2.0 * math.prod(l.values())
-        pool.append(dict(A=mk(ia), B=mk(ib), C=[mk(ic), mk(ic)], ia=ia, ib=ib, ic=ic, flops=fl))
-    picks = [rnd.randrange(pool_size) for _ in range(nreq)]
-    tols = [1e-10 if rnd.random() < 0.5 else 1e-13 for _ in range(nreq)]
-    gaps = [rnd.expovariate(rate) for _ in range(nreq)]
-    total_flops = sum(pool[i]["flops"] for i in picks)
+        pool.append(dict(A=mk(ia), B=mk(ib), C=mk(ic), ia=ia, ib=ib, ic=ic, flops=2.0 * math.prod(l.values()),
+                         c_bytes=8 * sizes[2]))
+    return pool, used
 
-    # serial plain calls, back to back
-    for i in picks[:10]:
-        p = pool[i]
-        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][0], p["ic"])
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for j, i in enumerate(picks):
-        p = pool[i]
-        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"])
-    torch.cuda.synchronize()
-    serial_s = time.perf_counter() - t0
 
-    # serial plain calls under the same arrivals: each request waits for its
-    # predecessor and for its own result (a plain caller's latency)
-    lat_serial = []
-    t0 = time.perf_counter()
-    due = t0
-    for j, i in enumerate(picks):
-        due += gaps[j]
-        now = time.perf_counter()
-        if due > now:
-            time.sleep(due - now)
-        p = pool[i]
-        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"])
-        torch.cuda.synchronize()
-        lat_serial.append((time.perf_counter() - due) * 1e3)
-    serial_arr_s = time.perf_counter() - t0
-    lat_serial.sort()
+def serve_stream(n, npool, rate, seed):
+    """n requests: a uniformly drawn resident problem each, tolerance 1e-10 or
+    1e-13 (50/50), Poisson gaps at `rate` per second."""
+    import random
+    rnd = random.Random(seed)
+    picks = [rnd.randrange(npool) for _ in range(n)]
+    tols = [1e-10 if rnd.random() < 0.5 else 1e-13 for _ in range(n)]
+    gaps = [rnd.expovariate(rate) for _ in range(n)] if rate else [0.0] * n
+    return picks, tols, gaps
 
+
+def serve_run(torch, tb, pool, picks, tols, gaps, outs=None):
+    """Submits the requests at their arrival times to a server with the
+    150 GB admission budget and waits for all; returns (seconds from the
+    first arrival to the last completion, arrival window, server stats)."""
     srv = tb.Server(hbm_budget_bytes=150 << 30, slots=4)
     ids = []
     t0 = time.perf_counter()
@@ -822,26 +817,116 @@ def serve_workload(torch, tb, dev, rate, nreq, pool_size=96, seed=0):
         if due > now:
             time.sleep(due - now)
         p = pool[i]
-        ids.append(srv.submit(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"][j & 1], p["ic"], tols[j]))
+        C = outs[j] if outs is not None else p["C"]
+        ids.append(srv.submit(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, C, p["ic"], tols[j]))
     for rid in ids:
         srv.wait(rid)
-    served_s = time.perf_counter() - t0
-    arrivals_s = due - t0
+    served = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
+    return served, due - t0, st
+
+
+def serial_run(torch, tb, pool, picks, gaps):
+    """The same requests as plain tblis_tensor_mult calls (FP64 path), each
+    waiting for its arrival and its predecessor; returns (seconds, latencies
+    in ms, sorted)."""
+    lat = []
+    t0 = time.perf_counter()
+    due = t0
+    for j, i in enumerate(picks):
+        due += gaps[j]
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        p = pool[i]
+        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, p["C"], p["ic"])
+        if gaps[j]:
+            torch.cuda.synchronize()
+            lat.append((time.perf_counter() - due) * 1e3)
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, sorted(lat)
+
+
+def serve_check(torch, tb, pool, picks, tols, chunk_bytes=8 << 30):
+    """Every request of the stream again through the server (bursts of
+    requests whose outputs fit chunk_bytes, each into its own output buffer),
+    each result against the same problem computed alone on the plain FP64
+    path; returns (requests checked, requests over their tolerance, largest
+    error / tolerance)."""
+    refs = {}
+    for i in sorted(set(picks)):
+        p = pool[i]
+        r = torch.empty_like(p["C"])
+        tb.mult(1.0, p["A"], p["ia"], p["B"], p["ib"], 0.0, r, p["ic"])
+        refs[i] = (r, torch.linalg.vector_norm(r).item())
+    checked, bad, worst = 0, 0, 0.0
+    j = 0
+    while j < len(picks):
+        k, size = j, 0
+        while k < len(picks) and (k == j or size + pool[picks[k]]["c_bytes"] <= chunk_bytes):
+            size += pool[picks[k]]["c_bytes"]
+            k += 1
+        outs = [torch.empty_like(pool[picks[x]]["C"]) for x in range(j, k)]
+        serve_run(torch, tb, pool, picks[j:k], tols[j:k], [0.0] * (k - j), outs)
+        for x, o in zip(range(j, k), outs):
+            r, nr = refs[picks[x]]
+            err = torch.linalg.vector_norm(o - r).item() / (nr if nr else 1.0)
+            worst = max(worst, err / tols[x])
+            bad += err > tols[x]
+            checked += 1
+        del outs
+        j = k
+    del refs
+    torch.cuda.empty_cache()
+    return checked, bad, worst
+
+
+def serve_workloads(torch, tb, dev):
+    """Config 5: a stream of 20,000 pairwise 4-index contraction requests over
+    a resident pool filling 48 GB of HBM, as a burst and under Poisson
+    arrivals at 50-2,000 req/s (4 s of arrivals per rate), against serial
+    plain calls under the same arrivals; every request of the burst checked
+    against the same request run alone on the plain FP64 path."""
+    out = {}
+    pool, used = serve_pool(torch, dev, SERVE_POOL_BYTES)
+    out["serve_pool"] = {"problems": len(pool), "operand_gb": used / 1e9}
+    picks, tols, gaps = serve_stream(SERVE_REQUESTS, len(pool), 0, seed=3)
+    flops = sum(pool[i]["flops"] for i in picks)
+    # warm-up: the shapes' first plans
+    serve_run(torch, tb, pool, picks[:64], tols[:64], [0.0] * 64)
+    serial_s, _ = serial_run(torch, tb, pool, picks, gaps)
+    served, _, st = serve_run(torch, tb, pool, picks, tols, gaps)
+    out["serve_burst"] = {
+        "requests": SERVE_REQUESTS, "tflop": flops / 1e12, "distinct_problems": len(set(picks)),
+        "served_req_s": SERVE_REQUESTS / served, "served_gflops": flops / served / 1e9,
+        "serial_req_s": SERVE_REQUESTS / serial_s, "serial_gflops": flops / serial_s / 1e9,
+        "throughput_vs_serial": serial_s / served,
+        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+        "batches": st["batches"], "mean_batch": st["mean_batch"],
+        "max_concurrent_batches": st["max_concurrent_batches"], "ozaki_requests": st["ozaki"],
+        "shape_cache_hit_rate": st["shape_hits"] / max(1, st["shape_hits"] + st["shape_misses"])}
+    checked, bad, worst = serve_check(torch, tb, pool, picks, tols)
+    out["serve_burst"].update({"checked_requests": checked, "requests_over_tolerance": bad,
+                               "max_err_over_tolerance": worst})
+    for rate in SERVE_RATES:
+        n = int(rate * SERVE_WINDOW_S)
+        picks, tols, gaps = serve_stream(n, len(pool), rate, seed=rate)
+        flops = sum(pool[i]["flops"] for i in picks)
+        served, window, st = serve_run(torch, tb, pool, picks, tols, gaps)
+        serial_s, lat = serial_run(torch, tb, pool, picks, gaps)
+        out["serve_%d" % rate] = {
+            "rate_req_s": rate, "requests": n, "arrival_window_s": window,
+            "served_req_s": n / served, "served_gflops": flops / served / 1e9,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+            "batches": st["batches"], "mean_batch": st["mean_batch"],
+            "shape_cache_hit_rate": st["shape_hits"] / max(1, st["shape_hits"] + st["shape_misses"]),
+            "serial_same_arrivals": {"req_s": n / serial_s, "p50_ms": lat[len(lat) // 2],
+                                     "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "throughput_vs_serial_same_arrivals": serial_s / served}
     del pool
     torch.cuda.empty_cache()
-    return {"rate_req_s": rate, "requests": nreq, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "max_ms": st["max_ms"], "batches": st["batches"], "mean_batch": st["mean_batch"],
-            "max_concurrent_batches": st["max_concurrent_batches"],
-            "served_req_s": nreq / served_s, "served_gflops": total_flops / served_s / 1e9,
-            "arrival_window_s": arrivals_s,
-            "serial_req_s": nreq / serial_s, "serial_gflops": total_flops / serial_s / 1e9,
-            "throughput_vs_serial": serial_s / served_s,
-            "serial_same_arrivals": {"req_s": nreq / serial_arr_s,
-                                     "p50_ms": lat_serial[len(lat_serial) // 2],
-                                     "p99_ms": lat_serial[min(len(lat_serial) - 1, int(0.99 * len(lat_serial)))]},
-            "throughput_vs_serial_same_arrivals": serial_arr_s / served_s}
+    return out
 
 
 def single_case(torch, tb, dev, stream, args):
@@ -905,11 +990,10 @@ def single_case(torch, tb, dev, stream, args):
 
 def extra_workloads(torch, tb, dev, stream, peaks, check=True):
     out = {}
-    for rate, n in ((2000, 2000), (50, 150), (1e9, 2000)):
-        try:
-            out["serve_%s" % ("burst" if rate > 1e6 else int(rate))] = serve_workload(torch, tb, dev, rate, n)
-        except Exception as e:
-            out["serve_%d_error" % rate] = str(e)[:200]
+    try:
+        out.update(serve_workloads(torch, tb, dev))
+    except Exception as e:     # keep the headline line even if a secondary workload fails
+        out["serve_error"] = str(e)[:200]
     try:
         out.update(dpd_workload(torch, tb, dev, stream, check))
     except Exception as e:     # keep the headline line even if a secondary workload fails

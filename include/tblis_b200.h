@@ -466,6 +466,8 @@ typedef struct tblis_b200_server_stats
     int max_concurrent_batches;      /* most launches seen in flight at once */
     double p50_ms, p99_ms, max_ms;   /* submit-to-completion latency */
     int64_t ozaki;                   /* requests run on the INT8 Ozaki path */
+    int64_t shape_hits, shape_misses; /* requests whose shape (GEMM view and device
+                                        scatter vectors) was cached / built */
 } tblis_b200_server_stats;
 
 tblis_b200_server* tblis_b200_server_create(size_t hbm_budget_bytes, int slots);

@@ -843,7 +843,8 @@ class tblis_b200_server_stats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
                 ("queued", ctypes.c_int64), ("mean_batch", ctypes.c_double),
                 ("max_concurrent_batches", ctypes.c_int), ("p50_ms", ctypes.c_double),
-                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("ozaki", ctypes.c_int64)]
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("ozaki", ctypes.c_int64),
+                ("shape_hits", ctypes.c_int64), ("shape_misses", ctypes.c_int64)]
 
 
 lib.tblis_b200_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int]

@@ -128,9 +128,10 @@ struct Server
     int max_batch = 256;
     // request shapes seen so far (scheduler thread only)
     std::unordered_map<std::string, std::shared_ptr<ShapeEntry>> shape_cache;
-    static constexpr size_t kShapeCap = 1024;
+    static constexpr size_t kShapeCap = 4096;
     // statistics
     int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_requests = 0, n_ozaki = 0;
+    int64_t shape_hits = 0, shape_misses = 0;
     int max_running = 0;
     std::vector<double> latencies;
     std::string fatal;
@@ -255,7 +256,12 @@ struct Server
             key.push_back('|');
         }
         auto it = shape_cache.find(key);
-        if (it != shape_cache.end()) return it->second;
+        if (it != shape_cache.end())
+        {
+            shape_hits++;
+            return it->second;
+        }
+        shape_misses++;
         auto e = std::make_shared<ShapeEntry>();
         e->v = gemm_view(mult_groups(&r.A, r.idx[0].c_str(), &r.B, r.idx[1].c_str(), &r.C, r.idx[2].c_str()));
         // entries still used by running batches stay alive through the slots
@@ -637,6 +643,8 @@ int tblis_b200_server_get_stats(tblis_b200_server* srv, tblis_b200_server_stats*
         out->max_concurrent_batches = s.max_running;
         out->queued = (int64_t)s.queue.size();
         out->ozaki = s.n_ozaki;
+        out->shape_hits = s.shape_hits;
+        out->shape_misses = s.shape_misses;
         std::vector<double> l = s.latencies;
         if (!l.empty())
         {
