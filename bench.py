@@ -52,6 +52,8 @@ def parse(argv=None):
     p.add_argument("--v", type=int, default=160, help="virtual extent")
     p.add_argument("--case", default=None, choices=["ring", "transpose", "dot", "reduce", "dpd", "serve", "batch"],
                    help="run only one secondary kernel at extents --o/--v (profiling); prints its own line")
+    p.add_argument("--batch-count", type=int, default=10000,
+                   help="members of the --case batch workload (profiling runs use fewer)")
     a = p.parse_args(argv)
     global O, V, FLOPS_LADDER, WORKLOAD
     if (a.o, a.v) != (O, V):
@@ -383,7 +385,9 @@ def main():
         print(json.dumps(serve_workloads(torch, tb, dev)))
         return
     if args.case == "batch":
-        print(json.dumps(batch_workload(torch, tb, dev, stream)))
+        print(json.dumps(batch_workload(torch, tb, dev, stream, count=args.batch_count,
+                                        serial_sample=min(500, args.batch_count),
+                                        check_sample=min(400, args.batch_count))))
         return
     if args.case:
         print(json.dumps(single_case(torch, tb, dev, stream, args)))

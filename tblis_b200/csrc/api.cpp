@@ -567,6 +567,7 @@ void tblis_b200_synchronize(void)
     {
         TB_CUDA(cudaStreamSynchronize(t_stream));
         TB_CHECK(ozaki_error_flag() == 0, TB_ERR_TIMEOUT, "an Ozaki kernel gave up a bounded wait");
+        TB_CHECK(gemm_f64_error_flag() == 0, TB_ERR_TIMEOUT, "a grouped FP64 kernel gave up a bounded wait");
     });
 }
 

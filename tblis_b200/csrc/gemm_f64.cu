@@ -12,7 +12,7 @@
 // scatter vectors in the epilogue; beta == 0 never reads C.
 //
 // A family of tile shapes shares one kernel template: CTA tile BM x BN x 16,
-// warps of WM x WN built from mma.sync.m8n8k4 f64 (sm_100a has no tcgen05
+// warps of WM x WN built from mma.sync.m16n8k8 f64 (sm_100a has no tcgen05
 // FP64 kind; DMMA is the FP64 tensor-core path), a STAGES-deep cp.async
 // pipeline. Each operand is gathered along the GEMM dimension with its
 // smallest stride (m or k for A, n or k for B) and laid out in shared memory
@@ -23,6 +23,7 @@
 // Split-K partial tiles go to a workspace and are summed in a fixed order by
 // gemm_f64_reduce (no atomics: results do not depend on scheduling).
 #include "gemm_f64.hpp"
+#include "gemm_f64_dev.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -34,84 +35,7 @@ namespace tb
 namespace
 {
 
-constexpr int BK = 16;
-constexpr int PAD = 4;                         // doubles of padding per smem row
-
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid)
-{
-    unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
-    int src_size = valid ? 8 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
-                 :: "r"(saddr), "l"(gmem), "r"(src_size));
-}
-
-__device__ __forceinline__ void cp_async16(double* smem, const double* gmem)
-{
-    unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" :: "r"(saddr), "l"(gmem));
-}
-
-// two adjacent tile elements (smem 16-byte aligned): one 16-byte copy when both
-// are valid and adjacent, 16-byte aligned, in global memory; else two 8-byte
-// copies (zero-filled where not valid)
-__device__ __forceinline__ void cp_pair(double* smem, const double* X, i64 off0, bool ok0, i64 off1, bool ok1,
-                                        const double* dummy)
-{
-    if (ok0 && ok1 && off1 == off0 + 1 && (((uintptr_t)(X + off0)) & 15) == 0)
-    {
-        cp_async16(smem, X + off0);
-        return;
-    }
-    cp_async8(smem, ok0 ? X + off0 : dummy, ok0);
-    cp_async8(smem + 1, ok1 ? X + off1 : dummy, ok1);
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
-
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
-}
-
-// shared-memory geometry of one operand tile (ROWS = BM or BN)
-template <int ROWS, int MODE>
-struct Tile
-{
-    // MODE 0: [BK][ROWS+PAD] (rows contiguous); MODE 1: [ROWS][BK+PAD] (k contiguous)
-    static constexpr int SIZE = MODE == 0 ? BK*(ROWS + PAD) : ROWS*(BK + PAD);
-    __device__ static __forceinline__ int idx(int r, int k)
-    {
-        return MODE == 0 ? k*(ROWS + PAD) + r : r*(BK + PAD) + k;
-    }
-};
-
-// k-offset information of one BK block of one operand
-struct KInfo
-{
-    i64 first;     // offset of the block's first k
-    i64 stride;    // common stride inside the block, 0 if irregular
-};
-
-__device__ __forceinline__ KInfo fetch_kinfo(const i64* __restrict__ scat, const i64* __restrict__ bstr,
-                                             i64 k0, bool valid)
-{
-    KInfo r = {0, 1};
-    if (valid)
-    {
-        r.first = __ldg(scat + k0);
-        r.stride = __ldg(bstr + k0/BK);
-    }
-    return r;
-}
-
-__device__ __forceinline__ i64 koff(const i64* __restrict__ scat, const KInfo& ki, i64 k0, int kl)
-{
-    return ki.stride != 0 ? ki.first + (i64)kl*ki.stride : __ldg(scat + k0 + kl);
-}
+using namespace f64dev;
 
 // arguments of one output tile
 struct TileArgs
@@ -145,7 +69,8 @@ template <int BM, int BN, int WM, int WN, int STAGES, int AMODE, int BMODE, bool
 __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* sAm, i64* sBn, i64* sCm, i64* sCn)
 {
     constexpr int NT = (BM/WM)*(BN/WN)*32;
-    constexpr int MS = WM/8, NS = WN/8;
+    // m16n8k8: MS 16-row by NS 8-column fragments per warp, 4 values each
+    constexpr int MS = WM/16, NS = WN/8;
     using TA = Tile<BM, AMODE>;
     using TB = Tile<BN, BMODE>;
     constexpr int STAGE = TA::SIZE + TB::SIZE;
@@ -167,11 +92,13 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
         sCn[i] = n < p.N ? p.c_n[n] : -1;
     }
 
-    double acc[MS][NS][2];
+    double acc[MS][NS][4];
     #pragma unroll
     for (int i = 0; i < MS; i++)
         #pragma unroll
-        for (int j = 0; j < NS; j++) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
+        for (int j = 0; j < NS; j++)
+            #pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
 
     const int wm0 = (warp / (BN/WN))*WM;
     const int wn0 = (warp % (BN/WN))*WN;
@@ -329,18 +256,24 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
             const double* As = smem + (kt % STAGES)*STAGE;
             const double* Bs = As + TA::SIZE;
             #pragma unroll
-            for (int kk = 0; kk < BK; kk += 4)
+            for (int kk = 0; kk < BK; kk += 8)
             {
-                double af[MS], bf[NS];
+                double af[MS][4], bf[NS][2];
                 #pragma unroll
-                for (int i = 0; i < MS; i++) af[i] = As[TA::idx(wm0 + i*8 + fr, kk + fc)];
+                for (int i = 0; i < MS; i++)
+                    #pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        af[i][q] = As[TA::idx(wm0 + i*16 + fr + 8*(q & 1), kk + fc + 4*(q >> 1))];
                 #pragma unroll
-                for (int j = 0; j < NS; j++) bf[j] = Bs[TB::idx(wn0 + j*8 + fr, kk + fc)];
+                for (int j = 0; j < NS; j++)
+                    #pragma unroll
+                    for (int q = 0; q < 2; q++)
+                        bf[j][q] = Bs[TB::idx(wn0 + j*8 + fr, kk + fc + 4*q)];
                 #pragma unroll
                 for (int i = 0; i < MS; i++)
                     #pragma unroll
                     for (int j = 0; j < NS; j++)
-                        dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                        dmma16(acc[i][j], af[i], bf[j]);
             }
         }
         cp_async_wait<0>();
@@ -348,23 +281,26 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
         __syncthreads();
     }
 
+    // each accumulator fragment holds rows fr and fr + 8 of a 16-row block
     if (p.W)
     {
         // raw partial sums, dense [m][n]
         #pragma unroll
         for (int i = 0; i < MS; i++)
-        {
-            const i64 m = m0 + wm0 + i*8 + fr;
-            if (m >= p.M) continue;
             #pragma unroll
-            for (int j = 0; j < NS; j++)
+            for (int hh = 0; hh < 2; hh++)
+            {
+                const i64 m = m0 + wm0 + i*16 + 8*hh + fr;
+                if (m >= p.M) continue;
                 #pragma unroll
-                for (int h = 0; h < 2; h++)
-                {
-                    const i64 n = n0 + wn0 + j*8 + fc*2 + h;
-                    if (n < p.N) p.W[m*p.N + n] = acc[i][j][h];
-                }
-        }
+                for (int j = 0; j < NS; j++)
+                    #pragma unroll
+                    for (int h = 0; h < 2; h++)
+                    {
+                        const i64 n = n0 + wn0 + j*8 + fc*2 + h;
+                        if (n < p.N) p.W[m*p.N + n] = acc[i][j][2*hh + h];
+                    }
+            }
     }
     else
     {
@@ -372,21 +308,23 @@ __device__ __forceinline__ void tile_body(const TileArgs& p, double* smem, i64* 
         const double alpha = p.alpha, beta = p.beta;
         #pragma unroll
         for (int i = 0; i < MS; i++)
-        {
-            const i64 rc = sCm[wm0 + i*8 + fr];
-            if (rc < 0) continue;
             #pragma unroll
-            for (int j = 0; j < NS; j++)
+            for (int hh = 0; hh < 2; hh++)
+            {
+                const i64 rc = sCm[wm0 + i*16 + 8*hh + fr];
+                if (rc < 0) continue;
                 #pragma unroll
-                for (int h = 0; h < 2; h++)
-                {
-                    const i64 cc = sCn[wn0 + j*8 + fc*2 + h];
-                    if (cc < 0) continue;
-                    double* dst = C + rc + cc;
-                    const double v = alpha*acc[i][j][h];
-                    *dst = beta == 0.0 ? v : v + beta*(*dst);
-                }
-        }
+                for (int j = 0; j < NS; j++)
+                    #pragma unroll
+                    for (int h = 0; h < 2; h++)
+                    {
+                        const i64 cc = sCn[wn0 + j*8 + fc*2 + h];
+                        if (cc < 0) continue;
+                        double* dst = C + rc + cc;
+                        const double v = alpha*acc[i][j][2*hh + h];
+                        *dst = beta == 0.0 ? v : v + beta*(*dst);
+                    }
+            }
     }
     // shared memory is reused by the next tile of a persistent CTA
     __syncthreads();
@@ -623,10 +561,14 @@ void gemm_f64_variant_tile(int variant, int& bm, int& bn)
     bm = v.bm; bn = v.bn;
 }
 
+int gemm_f64_grouped_num_variants() { return kNumVariants + 1; }
+bool gemm_f64_is_ws_variant(int variant) { return variant == kNumVariants + 1; }
+
 void gemm_f64_grouped_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups,
                              i64 total_tiles, int variant, cudaStream_t stream, unsigned long long* d_counter)
 {
     if (ngroups <= 0 || total_tiles <= 0) return;
+    TB_CHECK(!gemm_f64_is_ws_variant(variant), TB_ERR_ARG, "the packed variant runs through its grouped plan");
     const Variant& v = kVariants[std::max(1, std::min(variant, kNumVariants)) - 1];
     if (d_counter) TB_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), stream));
     v.grouped(d_groups, d_tile_begin, ngroups, total_tiles, d_counter, stream);

@@ -47,10 +47,49 @@ struct GroupDesc
     int amode, bmode;
     int nseg;
     const SegDesc* segs;
+    // packed path (gemm_f64_ws.cu): tile shape (gemm_f64_ws_shape), k steps
+    // over all segments, and the offsets (in doubles) of the group's packed A
+    // panels and B panels
+    int shape;
+    int nst;
+    i64 pa, pb;
+};
+
+// one piece of a panel to pack: k steps [s0, s0 + ns) of rows
+// [panel*BM, ...) of group g's A (side 0), or of columns [panel*BN, ...) of
+// its B (side 1); steps are counted over all segments of the group
+struct PackItem
+{
+    int g, side, panel, s0, ns, pad;
 };
 
 int gemm_f64_num_variants();
 void gemm_f64_variant_tile(int variant, int& bm, int& bn);
+// variants of a grouped launch: the tile family above, then the packed path
+// (variant gemm_f64_num_variants() + 1, tiles of each group's own shape; run
+// by the grouped plan, not by gemm_f64_grouped_launch)
+int gemm_f64_grouped_num_variants();
+bool gemm_f64_is_ws_variant(int variant);
+
+// The packed grouped path (gemm_f64_ws.cu): gemm_f64_ws_pack gathers the A
+// row panels and B column panels of every group into contiguous, swizzled
+// 16-wide k steps (panel p of group g at pa / pb + p*nst*P*16, P the panel
+// width of the group's shape); gemm_f64_ws_launch then runs the groups' tiles
+// on them, one producer lane streaming the blocks with bulk copies and four
+// consumer warps running the MMAs, consecutive tiles overlapping.
+// shape: bit 1 = 32 rows (else 64), bit 0 = 32 columns (else 64)
+int gemm_f64_ws_shape(i64 M, i64 N, i64 K);
+void gemm_f64_ws_tile(int shape, int& bm, int& bn);
+void gemm_f64_ws_pack(const GroupDesc* d_groups, const PackItem* d_items, int nitems, double* packA,
+                      double* packB, cudaStream_t stream);
+// tile_begin[g] = first tile of group g in tiles of its own shape; d_counter
+// as for gemm_f64_grouped_launch
+void gemm_f64_ws_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int ngroups, i64 total_tiles,
+                        const double* packA, const double* packB, cudaStream_t stream,
+                        unsigned long long* d_counter);
+// 1 when a kernel of gemm_f64_ws.cu gave up a bounded wait since the last
+// call (the flag is cleared by reading it)
+int gemm_f64_error_flag();
 // tile_begin[g] = first global tile of group g (tiles of BM x BN of the variant).
 // d_counter (optional, one 64-bit word of device memory, zeroed by the launch)
 // turns the static tile striding into a dynamic queue.

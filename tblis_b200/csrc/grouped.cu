@@ -74,9 +74,26 @@ bool grouped_use_graphs()
 void GroupedPlan::finalize(cudaStream_t st)
 {
     const i64 BK = gemm_f64_tile_k();
-    // longest K first: with the dynamic tile queue the longest tiles start first
-    std::stable_sort(groups.begin(), groups.end(),
-                     [](const GroupTables& a, const GroupTables& b) { return a.K > b.K; });
+    for (auto& g : groups)
+    {
+        i64 K = g.K;
+        if (!g.segs.empty())
+        {
+            K = 0;
+            for (auto& sg : g.segs) K += (i64)sg.a_k.size();
+        }
+        g.ws_shape = gemm_f64_ws_shape(g.M, g.N, K);
+    }
+    // groups that run the same code (tile shape and gather layouts) together,
+    // so a CTA's consecutive tiles stay in the instruction cache; within each
+    // such class longest K first: with the dynamic tile queue the longest
+    // tiles start first
+    auto code_class = [](const GroupTables& g) { return g.ws_shape*4 + g.amode*2 + g.bmode; };
+    std::stable_sort(groups.begin(), groups.end(), [&](const GroupTables& a, const GroupTables& b)
+    {
+        const int ca = code_class(a), cb = code_class(b);
+        return ca != cb ? ca < cb : a.K > b.K;
+    });
     // device tables: for each group a_m, a_k, b_k, b_n, c_m, c_n, a_kbs, b_kbs,
     // then for each segment a_m, a_k, b_k, b_n, a_kbs, b_kbs
     std::vector<i64> host;
@@ -146,17 +163,19 @@ void GroupedPlan::finalize(cudaStream_t st)
         TB_CUDA(cudaMemcpy(d_segs, hs.data(), hs.size()*sizeof(SegDesc), cudaMemcpyHostToDevice));
     }
 
-    const int nv = gemm_f64_num_variants();
+    const int nv = gemm_f64_grouped_num_variants();
     tile_begin.assign(nv, {});
     total_tiles.assign(nv, 0);
     std::vector<i64> all;
     for (int v = 1; v <= nv; v++)
     {
-        int bm, bn;
-        gemm_f64_variant_tile(v, bm, bn);
+        const bool ws = gemm_f64_is_ws_variant(v);
+        int bm = 0, bn = 0;
+        if (!ws) gemm_f64_variant_tile(v, bm, bn);
         i64 t = 0;
         for (auto& g : groups)
         {
+            if (ws) gemm_f64_ws_tile(g.ws_shape, bm, bn);
             tile_begin[v - 1].push_back(t);
             t += ((g.M + bm - 1)/bm)*((g.N + bn - 1)/bn);
         }
@@ -167,6 +186,42 @@ void GroupedPlan::finalize(cudaStream_t st)
     {
         TB_CUDA(cudaMalloc(&d_tile_begin, all.size()*sizeof(i64)));
         TB_CUDA(cudaMemcpy(d_tile_begin, all.data(), all.size()*sizeof(i64), cudaMemcpyHostToDevice));
+    }
+    // packed path: each group's k steps, its packed panel offsets, and the
+    // panels to pack in pieces of at most kPackSteps k steps (so that the few
+    // long panels of a large GEMM spread over the whole GPU)
+    {
+        constexpr i64 kPackSteps = 64;
+        pack_a = pack_b = 0;
+        pack_items.clear();
+        for (size_t gi = 0; gi < groups.size(); gi++)
+        {
+            GroupTables& g = groups[gi];
+            i64 nst = 0;
+            if (g.segs.empty()) nst = (g.K + BK - 1)/BK;
+            else for (auto& sg : g.segs) nst += ((i64)sg.a_k.size() + BK - 1)/BK;
+            TB_CHECK(nst < (1ll << 31), TB_ERR_SIZE, "contracted extent too large");
+            g.nst = (int)nst;
+            int bm, bn;
+            gemm_f64_ws_tile(g.ws_shape, bm, bn);
+            const i64 pan_a = (g.M + bm - 1)/bm, pan_b = (g.N + bn - 1)/bn;
+            g.pa = pack_a;
+            g.pb = pack_b;
+            pack_a += pan_a*bm*nst*BK;
+            pack_b += pan_b*bn*nst*BK;
+            if (nst == 0) continue;
+            for (int side = 0; side < 2; side++)
+                for (i64 p = 0, np = side ? pan_b : pan_a; p < np; p++)
+                    for (i64 s0 = 0; s0 < nst; s0 += kPackSteps)
+                        pack_items.push_back({(int)gi, side, (int)p, (int)s0, (int)std::min(kPackSteps, nst - s0), 0});
+        }
+        TB_CHECK(pack_items.size() < (1ull << 31), TB_ERR_SIZE, "too many panels");
+        if (!pack_items.empty())
+        {
+            TB_CUDA(cudaMalloc(&d_pack_items, pack_items.size()*sizeof(PackItem)));
+            TB_CUDA(cudaMemcpy(d_pack_items, pack_items.data(), pack_items.size()*sizeof(PackItem),
+                               cudaMemcpyHostToDevice));
+        }
     }
     TB_CUDA(cudaMalloc(&d_counter, sizeof(unsigned long long)));
     if (!groups.empty())
@@ -189,6 +244,8 @@ GroupedPlan::~GroupedPlan()
     if (d_descs) cudaFree(d_descs);
     if (d_counter) cudaFree(d_counter);
     if (h_descs) cudaFreeHost(h_descs);
+    if (d_pack_items) cudaFree(d_pack_items);
+    if (d_pack) cudaFree(d_pack);
 }
 
 GroupedPlanCache& grouped_plan_cache()
@@ -235,12 +292,50 @@ static void fill_descs(GroupedPlan& plan, GroupDesc* out, const double* const* p
         d.amode = g.amode; d.bmode = g.bmode;
         d.nseg = (int)g.segs.size();
         d.segs = g.segs.empty() ? nullptr : plan.d_segs + plan.seg_begin[i];
+        d.shape = g.ws_shape;
+        d.nst = g.nst;
+        d.pa = g.pa;
+        d.pb = g.pb;
     }
 }
 
 static const i64* variant_tile_begin(GroupedPlan& plan, int v)
 {
     return plan.d_tile_begin + (size_t)(v - 1)*plan.groups.size();
+}
+
+// the packed panels' buffer, allocated on the packed path's first use; false
+// (and the path is not used for this plan) when the device has no room
+static bool ensure_pack(GroupedPlan& plan)
+{
+    if (plan.d_pack) return true;
+    if (plan.pack_failed) return false;
+    const size_t bytes = (size_t)std::max<i64>(plan.pack_a + plan.pack_b, 1)*sizeof(double);
+    if (cudaMalloc(&plan.d_pack, bytes) != cudaSuccess)
+    {
+        cudaGetLastError();
+        plan.d_pack = nullptr;
+        plan.pack_failed = true;
+        return false;
+    }
+    return true;
+}
+
+// one run of variant v of the plan on the descriptors descs
+static void launch_variant(GroupedPlan& plan, const GroupDesc* descs, int v, cudaStream_t st)
+{
+    const int ng = (int)plan.groups.size();
+    if (gemm_f64_is_ws_variant(v))
+    {
+        TB_CHECK(plan.d_pack, TB_ERR_ARG, "packed path without its buffer");
+        gemm_f64_ws_pack(descs, plan.d_pack_items, (int)plan.pack_items.size(), plan.d_pack,
+                         plan.d_pack + plan.pack_a, st);
+        gemm_f64_ws_launch(descs, variant_tile_begin(plan, v), ng, plan.total_tiles[v - 1], plan.d_pack,
+                           plan.d_pack + plan.pack_a, st, plan.d_counter);
+    }
+    else
+        gemm_f64_grouped_launch(descs, variant_tile_begin(plan, v), ng, plan.total_tiles[v - 1], v, st,
+                                plan.d_counter);
 }
 
 static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* alphas, const double* betas,
@@ -252,7 +347,9 @@ static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* 
         if (it != g_tuned.end()) return it->second;
     }
     const char* env = getenv("TBLIS_B200_GEMM_VARIANT");
-    if (env && atoi(env) >= 1 && atoi(env) <= gemm_f64_num_variants()) return atoi(env);
+    if (env && atoi(env) >= 1 && atoi(env) <= gemm_f64_grouped_num_variants() &&
+        (!gemm_f64_is_ws_variant(atoi(env)) || ensure_pack(plan)))
+        return atoi(env);
 
     // scratch C covering the offsets of every group: candidates write there
     const i64 span = plan.c_hi - plan.c_lo + 1;
@@ -268,13 +365,12 @@ static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* 
     TB_CUDA(cudaEventCreate(&e1));
     int best = 1;
     float best_ms = 1e30f;
-    for (int v = 1; v <= gemm_f64_num_variants(); v++)
+    for (int v = 1; v <= gemm_f64_grouped_num_variants(); v++)
     {
-        gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st, plan.d_counter);     // warm-up
+        if (gemm_f64_is_ws_variant(v) && !ensure_pack(plan)) continue;
+        launch_variant(plan, dd.as<GroupDesc>(), v, st);     // warm-up
         TB_CUDA(cudaEventRecord(e0, st));
-        gemm_f64_grouped_launch(dd.as<GroupDesc>(), variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st, plan.d_counter);
+        launch_variant(plan, dd.as<GroupDesc>(), v, st);
         TB_CUDA(cudaEventRecord(e1, st));
         TB_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
@@ -283,6 +379,12 @@ static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* 
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (!gemm_f64_is_ws_variant(best) && plan.d_pack)
+    {
+        // the timed launches are complete (event synchronised): give the room back
+        cudaFree(plan.d_pack);
+        plan.d_pack = nullptr;
+    }
     std::lock_guard<std::mutex> lk(g_tune_mtx);
     g_tuned[plan.histogram] = best;
     return best;
@@ -292,7 +394,13 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
                  cudaStream_t st)
 {
     if (plan.groups.empty()) return;
-    if (plan.variant == 0) plan.variant = autotune(plan, ptrs, alphas, betas, st);
+    if (plan.variant == 0)
+    {
+        plan.variant = autotune(plan, ptrs, alphas, betas, st);
+        // a variant tuned on another plan of the same shape histogram: the
+        // packed path needs this plan's buffer too
+        if (gemm_f64_is_ws_variant(plan.variant) && !ensure_pack(plan)) plan.variant = 4;
+    }
     const int v = plan.variant;
 
     // the pinned descriptor buffer is read by the previous launch: wait for it
@@ -314,8 +422,7 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
             {
                 try
                 {
-                    gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                            plan.total_tiles[v - 1], v, cs, plan.d_counter);
+                    launch_variant(plan, plan.d_descs, v, cs);
                 }
                 catch (const error&) { ok = false; }
             }
@@ -335,16 +442,17 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
     }
     if (plan.graph)
     {
-        TimedLaunch t("gemm_f64_grouped_kernel", st);
+        const bool ws = gemm_f64_is_ws_variant(v);
+        TimedLaunch t(ws ? "gemm_f64_pack_kernel+gemm_f64_ws_kernel" : "gemm_f64_grouped_kernel", st);
         TB_CUDA(cudaGraphLaunch(plan.graph, st));
         count_launch();
+        if (ws) count_launch();             // the pack kernel and the GEMM kernel
     }
     else
     {
         TB_CUDA(cudaMemcpyAsync(plan.d_descs, plan.h_descs, plan.groups.size()*sizeof(GroupDesc),
                                 cudaMemcpyHostToDevice, st));
-        gemm_f64_grouped_launch(plan.d_descs, variant_tile_begin(plan, v), (int)plan.groups.size(),
-                                plan.total_tiles[v - 1], v, st, plan.d_counter);
+        launch_variant(plan, plan.d_descs, v, st);
     }
     TB_CUDA(cudaEventRecord(plan.last_use, st));
 }

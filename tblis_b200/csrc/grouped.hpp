@@ -30,6 +30,9 @@ struct GroupTables
     int a_slot = 0, b_slot = 1, c_slot = 2;   // indices into the run's pointer array
     i64 a_off = 0, b_off = 0, c_off = 0;      // element offsets added to those pointers
     int sidx = 0;                             // index into the run's alpha/beta arrays
+    int ws_shape = 0;                         // tile shape of the packed path (finalize)
+    int nst = 0;                              // k steps over all segments (finalize)
+    i64 pa = 0, pb = 0;                       // offsets of the packed A / B panels (finalize)
 };
 
 struct GroupedPlan
@@ -55,6 +58,13 @@ struct GroupedPlan
     bool graph_failed = false;
     cudaEvent_t last_use = nullptr;
     i64 c_lo = 0, c_hi = -1;                  // extent of C offsets (for the tuner's scratch)
+    // packed path: the panels to pack, the packed sizes (doubles) and the
+    // buffer (allocated on first use; A panels, then B panels)
+    std::vector<PackItem> pack_items;
+    PackItem* d_pack_items = nullptr;
+    i64 pack_a = 0, pack_b = 0;
+    double* d_pack = nullptr;
+    bool pack_failed = false;
     std::string histogram;
     std::vector<std::shared_ptr<GroupedPlan>> parts;   // plans whose groups this one merges (kept alive)
 

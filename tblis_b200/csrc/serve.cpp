@@ -442,7 +442,7 @@ struct Server
                 d.M = v.m; d.N = v.n; d.K = v.k;
                 d.alpha = p.alpha; d.beta = p.beta;
                 d.amode = v.amode; d.bmode = v.bmode;
-                d.nseg = 0; d.segs = nullptr;
+                d.nseg = 0; d.segs = nullptr; d.shape = 0; d.nst = 0; d.pa = 0; d.pb = 0;
                 htb[g] = tiles;
                 tiles += ((v.m + bm - 1)/bm)*((v.n + bn - 1)/bn);
                 g++;
