@@ -19,7 +19,7 @@
 //    tile's C row and column offsets in a ring of tile slots and streams the
 //    tile's packed A and B blocks into a ring of shared-memory stages with
 //    bulk copies (cp.async.bulk, completing on an mbarrier by transaction
-//    bytes); four consumer warps run the m16n8k8 FP64 MMAs on each stage and,
+//    bytes); four consumer warps run the m16n8k16 FP64 MMAs on each stage and,
 //    after a tile's last k step, scatter alpha*AB + beta*C through the tile's
 //    C offsets. The next tile's copies overlap the current tile's MMAs and C
 //    update.
@@ -196,19 +196,15 @@ __device__ __forceinline__ void pack_panel(const GroupDesc& g, bool sideB, int p
         const i64 lo = max(s0, step), hi = min(s0 + ns, step + nk);
         if (lo < hi)
         {
-            __syncthreads();                          // the previous pass is done with sRow
-            for (int r = t; r < P; r += PK_THREADS) sRow[r] = r0 + r < extent ? __ldg(rvec + r0 + r) : -1;
-            for (i64 kb = lo - step; kb < hi - step; kb += PK_STEPS)
+            // valid k of the pass starting at step kb (a multiple of PK_STEPS past lo)
+            auto valid_k = [&](i64 kb) -> int
             {
-                const int steps = (int)min((i64)PK_STEPS, hi - step - kb);
-                const i64 k0 = kb*BK;
-                const int kc = (int)min((i64)steps*BK, K - k0);     // valid k of this pass
-                __syncthreads();                      // T and sK of the previous pass are read
-                for (int k = t; k < PK_K; k += PK_THREADS) sK[k] = k < kc ? __ldg(kvec + k0 + k) : 0;
-                __syncthreads();
-                // gather P x PK_K, coalesced along the dimension contiguous in memory
-                constexpr int N = P*PK_K/PK_THREADS;
-                double v[N];
+                return kb < hi - step ? (int)min(min((i64)PK_STEPS, hi - step - kb)*BK, K - kb*BK) : 0;
+            };
+            // this thread's share of the gather of one pass (k offsets in kofs)
+            constexpr int N = P*PK_K/PK_THREADS;
+            auto gather = [&](const i64* kofs, int kc, double (&v)[N])
+            {
                 #pragma unroll
                 for (int j = 0; j < N; j++)
                 {
@@ -216,8 +212,26 @@ __device__ __forceinline__ void pack_panel(const GroupDesc& g, bool sideB, int p
                     const int r = rows_contig ? e % P : e / PK_K;
                     const int k = rows_contig ? e / P : e % PK_K;
                     const i64 ro = sRow[r];
-                    v[j] = (k < kc && ro >= 0) ? __ldg(X + ro + sK[k]) : 0.0;
+                    v[j] = (k < kc && ro >= 0) ? __ldg(X + ro + kofs[k]) : 0.0;
                 }
+            };
+            static_assert(PK_K <= PK_THREADS, "one k offset per thread");
+            const i64 kb0 = lo - step;
+            __syncthreads();                          // the previous pass is done with sRow and sK
+            for (int r = t; r < P; r += PK_THREADS) sRow[r] = r0 + r < extent ? __ldg(rvec + r0 + r) : -1;
+            if (t < PK_K) sK[t] = t < valid_k(kb0) ? __ldg(kvec + kb0*BK + t) : 0;
+            // the k offsets of the second pass, stored when the first one is gathered
+            i64 knext = t < valid_k(kb0 + PK_STEPS) ? __ldg(kvec + (kb0 + PK_STEPS)*BK + t) : 0;
+            __syncthreads();
+            double v[N];
+            gather(sK, valid_k(kb0), v);
+            // Each iteration stores the gathered pass into T, issues the gather
+            // of the next pass, and writes this pass's blocks while those loads
+            // are in flight. sK holds two passes' k offsets (pass parity).
+            int par = 0;
+            for (i64 kb = kb0; kb < hi - step; kb += PK_STEPS, par ^= 1)
+            {
+                const int steps = (int)min((i64)PK_STEPS, hi - step - kb);
                 #pragma unroll
                 for (int j = 0; j < N; j++)
                 {
@@ -226,8 +240,13 @@ __device__ __forceinline__ void pack_panel(const GroupDesc& g, bool sideB, int p
                     const int k = rows_contig ? e / P : e % PK_K;
                     T[k][r] = v[j];
                 }
-                __syncthreads();
-                // the steps' blocks, rows of 16 k, k swizzled by row
+                i64* snext = sK + (par ^ 1)*PK_K;
+                if (t < PK_K) snext[t] = knext;
+                __syncthreads();                      // T of this pass and the next k offsets are visible
+                const i64 kn = kb + PK_STEPS;
+                if (t < valid_k(kn + PK_STEPS)) knext = __ldg(kvec + (kn + PK_STEPS)*BK + t);
+                if (kn < hi - step) gather(snext, valid_k(kn), v);
+                // this pass's blocks, rows of 16 k, k swizzled by row
                 double* __restrict__ o = out + (step + kb)*P*BK;
                 const int m = steps*P*BK;
                 for (int e = t; e < m; e += PK_THREADS)
@@ -235,6 +254,7 @@ __device__ __forceinline__ void pack_panel(const GroupDesc& g, bool sideB, int p
                     const int c = e/(P*BK), w = e % (P*BK), r = w/BK, kq = w % BK;
                     o[e] = T[c*BK + (kq ^ ((r & 3) << 2))][r];
                 }
+                __syncthreads();                      // T is read before the next pass stores into it
             }
         }
         step += nk;
@@ -247,7 +267,7 @@ gemm_f64_pack_kernel(const GroupDesc* __restrict__ groups, const PackItem* __res
 {
     __shared__ double T[PK_K][WS_EDGE + 1];
     __shared__ i64 sRow[WS_EDGE];
-    __shared__ i64 sK[PK_K];
+    __shared__ i64 sK[2*PK_K];
     for (int item = blockIdx.x; item < nitems; item += gridDim.x)
     {
         const PackItem pi = items[item];
@@ -262,6 +282,18 @@ gemm_f64_pack_kernel(const GroupDesc* __restrict__ groups, const PackItem* __res
 }
 
 // ---- GEMM consumers ------------------------------------------------------------
+
+// D(16x8) += A(16x16) * B(16x8), FP64. Fragments (g = lane/4, t = lane%4):
+// a[q] = A(g + 8*(q%2), t + 4*(q/2)), b[q] = B(t + 4*q, g),
+// c[q] = C(g + 8*(q/2), 2*t + q%2)
+__device__ __forceinline__ void dmma_k16(double* c, const double* a, const double* b)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+                 "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+                   "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
 
 // nst k steps of one BM x BN tile (warp tile BM/2 x BN/2) into acc; the stage
 // holds the packed A block (BM rows of 16) and the packed B block (BN rows of 16)
@@ -279,26 +311,23 @@ __device__ __forceinline__ bool ws_consume(double (&acc)[2][4][4], int nst, cons
         if (!mb_wait_warp(&sh.full[s], (uint32_t)((it/WS_STAGES) & 1), abort_flag)) return false;
         const double* As = stages + (size_t)s*WS_STAGE;
         const double* Bs = As + WS_OPER;
+        // the whole 16-wide step in one m16n8k16 MMA per fragment pair
+        double af[MS][8], bf[NS][4];
         #pragma unroll
-        for (int kk = 0; kk < BK; kk += 8)
-        {
-            double af[MS][4], bf[NS][2];
+        for (int i = 0; i < MS; i++)
             #pragma unroll
-            for (int i = 0; i < MS; i++)
-                #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    af[i][q] = As[(wm0 + i*16 + fr + 8*(q & 1))*BK + (((kk + 4*(q >> 1)) ^ sw) + fc)];
+            for (int q = 0; q < 8; q++)
+                af[i][q] = As[(wm0 + i*16 + fr + 8*(q & 1))*BK + (((4*(q >> 1)) ^ sw) + fc)];
+        #pragma unroll
+        for (int j = 0; j < NS; j++)
+            #pragma unroll
+            for (int q = 0; q < 4; q++)
+                bf[j][q] = Bs[(wn0 + j*8 + fr)*BK + (((4*q) ^ sw) + fc)];
+        #pragma unroll
+        for (int i = 0; i < MS; i++)
             #pragma unroll
             for (int j = 0; j < NS; j++)
-                #pragma unroll
-                for (int q = 0; q < 2; q++)
-                    bf[j][q] = Bs[(wn0 + j*8 + fr)*BK + (((kk + 4*q) ^ sw) + fc)];
-            #pragma unroll
-            for (int i = 0; i < MS; i++)
-                #pragma unroll
-                for (int j = 0; j < NS; j++)
-                    dmma16(acc[i][j], af[i], bf[j]);
-        }
+                dmma_k16(acc[i][j], af[i], bf[j]);
         // the fragments are in registers: the stage may be refilled
         __syncwarp();
         if (lane == 0) mb_arrive(&sh.empty[s]);
