@@ -511,8 +511,21 @@ def main():
             if not i8peak:
                 i8peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
                 src = "2 x measured bf16 dense GEMM (MEASURED_PEAKS.json)"
+            # DRAM bytes (read + write) of one full-size oz_crt_gemm2 launch of this
+            # workload with 13 moduli, from a one-pass ncu capture
+            # (profiles/oz_crt_gemm_ladder.md): 15.79 GB read + 0.78 GB written
+            traffic = None
+            if used_method == 6 and gemms == 13 and (O, V) == (48, 160):
+                traffic = 15.79e9 + 0.78e9
+            m_, n_, k_ = V * V, O * O, V * V
             result["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": i8peak, "unit": "TOP/s (int8)",
-                                  "frac": achieved / i8peak, "traffic": None, "peak_source": src,
+                                  "frac": achieved / i8peak, "traffic": traffic,
+                                  "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                                    "full-size launch (profiles/oz_crt_gemm_ladder.md)"
+                                                    if traffic else None,
+                                  "algorithmic_bytes": gemms * (m_ * k_ + n_ * k_ + m_ * n_) if used_method == 6
+                                                       else None,
+                                  "peak_source": src,
                                   "kernel": kname, "launch_ms": launch_ms, "int8_gemms_per_launch": gemms,
                                   "share_of_step": k_total_ms / total_ms,
                                   "fp64_equivalent_tflops_kernel": FLOPS_LADDER * units_per_launch /
