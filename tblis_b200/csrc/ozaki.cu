@@ -711,7 +711,7 @@ struct PlaneGeom
 };
 
 constexpr int SL_LD = SL_T + 1;            // padded smem row (doubles)
-constexpr int SL_BLOCKS_PER_SM = 3;
+constexpr int SL_BLOCKS_PER_SM = 2;       // 128 registers a thread: more of the 16 elements' FP64 chains in flight
 constexpr size_t SL_SMEM = 2*SL_T*SL_LD*sizeof(double);
 
 // writes the S tiled planes (PlaneGeom) of 64x64 tiles of the operand:
