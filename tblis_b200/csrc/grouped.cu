@@ -9,6 +9,7 @@
 #include "grouped.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <list>
@@ -234,6 +235,8 @@ void GroupedPlan::finalize(cudaStream_t st)
     (void)st;
 }
 
+static void release_pack(GroupedPlan& plan);
+
 GroupedPlan::~GroupedPlan()
 {
     if (graph) cudaGraphExecDestroy(graph);
@@ -245,7 +248,7 @@ GroupedPlan::~GroupedPlan()
     if (d_counter) cudaFree(d_counter);
     if (h_descs) cudaFreeHost(h_descs);
     if (d_pack_items) cudaFree(d_pack_items);
-    if (d_pack) cudaFree(d_pack);
+    release_pack(*this);
 }
 
 GroupedPlanCache& grouped_plan_cache()
@@ -304,20 +307,48 @@ static const i64* variant_tile_begin(GroupedPlan& plan, int v)
     return plan.d_tile_begin + (size_t)(v - 1)*plan.groups.size();
 }
 
+// device memory held by the packed-panel buffers of all live plans, and its
+// cap: 40% of the device's memory, so that cached plans never crowd out the
+// caller's own allocations
+static std::atomic<size_t> g_pack_held{0};
+
+static size_t pack_cap()
+{
+    static size_t cap = 0;
+    if (!cap)
+    {
+        size_t freeb = 0, total = 0;
+        cap = cudaMemGetInfo(&freeb, &total) == cudaSuccess ? total/10*4 : ((size_t)8 << 30);
+    }
+    return cap;
+}
+
+static void release_pack(GroupedPlan& plan)
+{
+    if (!plan.d_pack) return;
+    cudaFree(plan.d_pack);
+    plan.d_pack = nullptr;
+    g_pack_held -= plan.pack_held;
+    plan.pack_held = 0;
+}
+
 // the packed panels' buffer, allocated on the packed path's first use; false
-// (and the path is not used for this plan) when the device has no room
+// (and the path is not used for this plan) when it would pass the cap or the
+// device has no room
 static bool ensure_pack(GroupedPlan& plan)
 {
     if (plan.d_pack) return true;
     if (plan.pack_failed) return false;
     const size_t bytes = (size_t)std::max<i64>(plan.pack_a + plan.pack_b, 1)*sizeof(double);
-    if (cudaMalloc(&plan.d_pack, bytes) != cudaSuccess)
+    if (g_pack_held.load() + bytes > pack_cap() || cudaMalloc(&plan.d_pack, bytes) != cudaSuccess)
     {
         cudaGetLastError();
         plan.d_pack = nullptr;
         plan.pack_failed = true;
         return false;
     }
+    plan.pack_held = bytes;
+    g_pack_held += bytes;
     return true;
 }
 
@@ -379,12 +410,8 @@ static int autotune(GroupedPlan& plan, const double* const* ptrs, const double* 
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (!gemm_f64_is_ws_variant(best) && plan.d_pack)
-    {
-        // the timed launches are complete (event synchronised): give the room back
-        cudaFree(plan.d_pack);
-        plan.d_pack = nullptr;
-    }
+    // the timed launches are complete (event synchronised): give the room back
+    if (!gemm_f64_is_ws_variant(best)) release_pack(plan);
     std::lock_guard<std::mutex> lk(g_tune_mtx);
     g_tuned[plan.histogram] = best;
     return best;

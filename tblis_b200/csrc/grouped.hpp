@@ -64,6 +64,7 @@ struct GroupedPlan
     PackItem* d_pack_items = nullptr;
     i64 pack_a = 0, pack_b = 0;
     double* d_pack = nullptr;
+    size_t pack_held = 0;                     // bytes of d_pack counted against the cap
     bool pack_failed = false;
     std::string histogram;
     std::vector<std::shared_ptr<GroupedPlan>> parts;   // plans whose groups this one merges (kept alive)
