@@ -169,8 +169,9 @@ void tblis_b200_clear_error(void);
 void tblis_b200_set_stream(void* stream);
 void* tblis_b200_get_stream(void);
 /* Waits for all work this library enqueued on the current stream. Records
- * TB_ERR_TIMEOUT (6) as the last error when an Ozaki kernel gave up one of its
- * bounded waits since the previous check (the flag is then cleared). */
+ * TB_ERR_TIMEOUT (6) as the last error when an Ozaki kernel or the packed
+ * grouped FP64 kernel gave up one of its bounded waits since the previous
+ * check (the flag is then cleared). */
 void tblis_b200_synchronize(void);
 
 /* Test support for the failure detection of the Ozaki kernels (no reference
@@ -181,6 +182,14 @@ void tblis_b200_synchronize(void);
  * and returns, and tblis_b200_synchronize reports it. step = -1 and
  * wait_seconds <= 0 restore normal operation. Returns 0 or an error code. */
 int tblis_b200_ozaki_inject_wait_timeout(int step, double wait_seconds);
+
+/* The same for the packed grouped FP64 GEMM (DPD, indexed DPD and batches on
+ * the packed path; no reference counterpart): its producer issues no copy for
+ * the CTA's pipeline stage `step`, and every bounded wait gives up after
+ * wait_seconds; the kernel records the timeout, waits for the copies it
+ * issued and returns. step = -1 and wait_seconds <= 0 restore normal
+ * operation. Returns 0 or an error code. */
+int tblis_b200_grouped_inject_wait_timeout(int step, double wait_seconds);
 
 /* Normwise relative tolerance carried by a configuration (used by the Ozaki
  * configurations to pick the slice count; 0 restores the default 1e-12). */

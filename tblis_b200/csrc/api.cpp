@@ -576,6 +576,11 @@ int tblis_b200_ozaki_inject_wait_timeout(int step, double wait_seconds)
     return guarded([&] { ensure_device(); ozaki_inject_wait_timeout(step, wait_seconds); });
 }
 
+int tblis_b200_grouped_inject_wait_timeout(int step, double wait_seconds)
+{
+    return guarded([&] { ensure_device(); gemm_f64_inject_wait_timeout(step, wait_seconds); });
+}
+
 void tblis_b200_fill_block_scatter(unsigned ndim, const len_type* len, const stride_type* stride,
                                    len_type BS, stride_type off, stride_type size,
                                    stride_type* scat, stride_type* bs, int pack_3d)

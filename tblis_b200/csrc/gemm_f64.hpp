@@ -90,6 +90,10 @@ void gemm_f64_ws_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int 
 // 1 when a kernel of gemm_f64_ws.cu gave up a bounded wait since the last
 // call (the flag is cleared by reading it)
 int gemm_f64_error_flag();
+// test support: the packed GEMM's producer issues no copy for the CTA's
+// stage number `step` (-1: none) and every bounded wait gives up after
+// wait_seconds (<= 0: the default 2 s)
+void gemm_f64_inject_wait_timeout(int step, double wait_seconds);
 // tile_begin[g] = first global tile of group g (tiles of BM x BN of the variant).
 // d_counter (optional, one 64-bit word of device memory, zeroed by the launch)
 // turns the static tile striding into a dynamic queue.

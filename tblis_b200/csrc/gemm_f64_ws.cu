@@ -82,6 +82,7 @@ constexpr size_t ws_smem_bytes() { return (size_t)WS_STAGES*WS_STAGE*sizeof(doub
 
 __device__ int g_f64_error = 0;
 __device__ unsigned long long g_f64_wait_ns = WS_WAIT_NS;
+__device__ int g_f64_skip_step = -1;       // test support: a stage whose copies are never issued
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -481,6 +482,7 @@ gemm_f64_ws_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__
             const double* srcA = packA + g.pa + tmi*nst*BMs*BK;
             const double* srcB = packB + g.pb + tni*nst*BNs*BK;
             const uint32_t bytesA = (uint32_t)(BMs*BK*sizeof(double)), bytesB = (uint32_t)(BNs*BK*sizeof(double));
+            const int skip = g_f64_skip_step;
             bool ok = true;
             for (int st = 0; st < nst; st++)
             {
@@ -491,7 +493,7 @@ gemm_f64_ws_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__
                     ok = false;
                     break;
                 }
-                if (lane == 0)
+                if (lane == 0 && it != skip)
                 {
                     double* As = stages + (size_t)s*WS_STAGE;
                     mb_arrive_expect(&sh.full[s], bytesA + bytesB);
@@ -505,9 +507,12 @@ gemm_f64_ws_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__
         // the copies of the last stages issued land before the CTA is gone
         // (bounded waits; on the normal path these phases are complete)
         if (lane == 0)
+        {
+            const int skip = g_f64_skip_step;
             for (i64 k = it > WS_STAGES ? it - WS_STAGES : 0; k < it; k++)
-                if (!mb_try(&sh.full[k % WS_STAGES], (uint32_t)((k/WS_STAGES) & 1)))
+                if (k != skip && !mb_try(&sh.full[k % WS_STAGES], (uint32_t)((k/WS_STAGES) & 1)))
                     mb_wait_slow(&sh.full[k % WS_STAGES], (uint32_t)((k/WS_STAGES) & 1), abort_flag, true);
+        }
         __syncwarp();
     }
     else
@@ -591,6 +596,13 @@ void gemm_f64_ws_launch(const GroupDesc* d_groups, const i64* d_tile_begin, int 
     gemm_f64_ws_kernel<<<(unsigned)grid, WS_THREADS, bytes, s>>>(d_groups, d_tile_begin, ngroups, total_tiles,
                                                                   packA, packB, d_counter);
     check_launch("gemm_f64_ws_kernel");
+}
+
+void gemm_f64_inject_wait_timeout(int step, double wait_seconds)
+{
+    const unsigned long long ns = wait_seconds > 0.0 ? (unsigned long long)(wait_seconds*1e9) : WS_WAIT_NS;
+    TB_CUDA(cudaMemcpyToSymbol(g_f64_skip_step, &step, sizeof(int)));
+    TB_CUDA(cudaMemcpyToSymbol(g_f64_wait_ns, &ns, sizeof(ns)));
 }
 
 int gemm_f64_error_flag()
