@@ -430,9 +430,27 @@ void grouped_run(GroupedPlan& plan, const double* const* ptrs, const double* alp
     }
     const int v = plan.variant;
 
-    // the pinned descriptor buffer is read by the previous launch: wait for it
-    TB_CUDA(cudaEventSynchronize(plan.last_use));
-    fill_descs(plan, plan.h_descs, ptrs, alphas, betas, nullptr);
+    // The descriptors depend only on the run's pointers and scalars. A run
+    // with the same ones as the last (an iterative solver's repeated step)
+    // reuses them as they are, without waiting for the previous launch.
+    // Otherwise the pinned descriptor buffer is read by the previous launch:
+    // wait for it, then rebuild.
+    int nsc = 0;
+    for (auto& g : plan.groups) nsc = std::max(nsc, g.sidx + 1);
+    const bool same = plan.descs_valid && (int)plan.last_ptrs.size() == plan.nslots &&
+                      (int)plan.last_scalars.size() == 2*nsc &&
+                      std::equal(ptrs, ptrs + plan.nslots, plan.last_ptrs.begin()) &&
+                      std::equal(alphas, alphas + nsc, plan.last_scalars.begin()) &&
+                      std::equal(betas, betas + nsc, plan.last_scalars.begin() + nsc);
+    if (!same)
+    {
+        TB_CUDA(cudaEventSynchronize(plan.last_use));
+        fill_descs(plan, plan.h_descs, ptrs, alphas, betas, nullptr);
+        plan.last_ptrs.assign(ptrs, ptrs + plan.nslots);
+        plan.last_scalars.assign(alphas, alphas + nsc);
+        plan.last_scalars.insert(plan.last_scalars.end(), betas, betas + nsc);
+        plan.descs_valid = true;
+    }
 
     if (grouped_use_graphs() && !plan.graph_failed)
     {

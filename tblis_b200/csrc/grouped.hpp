@@ -57,6 +57,10 @@ struct GroupedPlan
     cudaGraphExec_t graph = nullptr;
     bool graph_failed = false;
     cudaEvent_t last_use = nullptr;
+    // the pointers and scalars the pinned descriptors were last built from
+    std::vector<const double*> last_ptrs;
+    std::vector<double> last_scalars;         // alphas, then betas
+    bool descs_valid = false;
     i64 c_lo = 0, c_hi = -1;                  // extent of C offsets (for the tuner's scratch)
     // packed path: the panels to pack, the packed sizes (doubles) and the
     // buffer (allocated on first use; A panels, then B panels)
