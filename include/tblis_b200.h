@@ -284,9 +284,10 @@ typedef struct tblis_b200_dpd_tensor
  * C.scalar), the C entry of tblis::mult over dpd_varray_view
  * (src/iface/3t/mult.cxx:170-289, src/internal/3t/dpd/mult.cxx:223-356): one
  * GEMM per irrep of the contracted labels, all in one grouped launch. Labels
- * must be unique per tensor; labels shared by all three tensors are not
- * supported. Returns 0 or an error code. report->m = irrep GEMMs launched,
- * report->n = tile configuration picked by the autotuner. */
+ * must be unique per tensor; labels shared by all three tensors (batch
+ * labels) are supported as in src/internal/3t/dpd/mult.cxx:1082-1115.
+ * Returns 0 or an error code. report->m = irrep GEMMs launched, report->n =
+ * tile configuration picked by the autotuner. */
 int tblis_b200_dpd_mult(const tblis_b200_dpd_tensor* A, const label_type* idx_A,
                         const tblis_b200_dpd_tensor* B, const label_type* idx_B,
                               tblis_b200_dpd_tensor* C, const label_type* idx_C,
@@ -339,6 +340,20 @@ int tblis_b200_dpd_reduce(reduce_t op, const tblis_b200_dpd_block_table* A, cons
 int tblis_b200_dpd_scale(tblis_b200_dpd_block_table* A, const label_type* idx_A);
 int tblis_b200_dpd_set(const tblis_scalar* alpha, tblis_b200_dpd_block_table* A, const label_type* idx_A);
 int tblis_b200_dpd_shift(const tblis_scalar* alpha, tblis_b200_dpd_block_table* A, const label_type* idx_A);
+
+/* The dense form of a DPD tensor (block_to_full,
+ * src/internal/1t/dpd/util.hpp:70-102): dimension d of the dense tensor F
+ * has the sum over irreps of A's lengths of dimension d, irrep x occupying
+ * the range after the lengths of the irreps below x. F (any strides, A's
+ * element type) is set to zero, then every stored block of A is copied into
+ * its region. Scalars and conjugation flags do not apply. Returns 0 or an
+ * error code. */
+int tblis_b200_dpd_block_to_full(const tblis_b200_dpd_block_table* A, tblis_tensor* F);
+
+/* The reverse (full_to_block, src/internal/1t/dpd/util.hpp:104-133): every
+ * stored block of A gets a copy of its region of the dense tensor F; storage
+ * of A outside its blocks is left as it is. Returns 0 or an error code. */
+int tblis_b200_dpd_full_to_block(const tblis_tensor* F, tblis_b200_dpd_block_table* A);
 
 /* An indexed DPD tensor as MArray's indexed_dpd_varray holds it
  * (indexed_dpd_varray_base.hpp, indexed_dpd_varray.hpp:309-370): the first

@@ -315,6 +315,59 @@ def ref_dpd_layout(irrep, nirrep, lens, layout=5):
     return total, offs, strides.reshape(nb, ndim)
 
 
+def _dpd_blocks_ref(irrep, nirrep, lens):
+    """(irreps, offset, strides) of every stored block of a default-layout DPD
+    tensor, from the reference's MArray layout (ref_dpd_layout); the block
+    order is the one refshim_dpd_layout walks: irreps of dimensions 1.. (the
+    first fastest), dimension 0 closing the XOR."""
+    ndim = len(lens)
+    total, offs, strides = ref_dpd_layout(irrep, nirrep, lens, 5)
+    out = []
+    for b in range(len(offs)):
+        irr = [0] * ndim
+        t, x = b, irrep
+        for i in range(1, ndim):
+            irr[i] = t % nirrep
+            t //= nirrep
+            x ^= irr[i]
+        irr[0] = x
+        out.append((irr, int(offs[b]), [int(v) for v in strides[b]]))
+    return total, out
+
+
+def orc_dpd_block_to_full(irrep, nirrep, lens, data):
+    """The dense form of a default-layout DPD tensor, restating
+    src/internal/1t/dpd/util.hpp:70-102 (block_to_full): dimension d has the
+    sum of the lengths over the irreps, irrep x starting after the lengths of
+    the irreps below it; zero everywhere, then every stored block copied into
+    its region. Block geometry from the reference's MArray layout."""
+    dims = [sum(r) for r in lens]
+    full = np.zeros(dims, dtype=data.dtype)
+    _, blocks = _dpd_blocks_ref(irrep, nirrep, lens)
+    for irr, off, strides in blocks:
+        bl = [lens[d][irr[d]] for d in range(len(lens))]
+        if 0 in bl:
+            continue
+        blk = np.lib.stride_tricks.as_strided(data[off:], shape=bl, strides=[data.itemsize * s for s in strides])
+        sl = tuple(slice(sum(lens[d][:irr[d]]), sum(lens[d][:irr[d]]) + bl[d]) for d in range(len(lens)))
+        full[sl] = blk
+    return full
+
+
+def orc_dpd_full_to_block(irrep, nirrep, lens, full, data):
+    """The reverse, restating src/internal/1t/dpd/util.hpp:104-133
+    (full_to_block): every stored block of `data` (updated in place) gets a
+    copy of its region of `full`."""
+    _, blocks = _dpd_blocks_ref(irrep, nirrep, lens)
+    for irr, off, strides in blocks:
+        bl = [lens[d][irr[d]] for d in range(len(lens))]
+        if 0 in bl:
+            continue
+        blk = np.lib.stride_tricks.as_strided(data[off:], shape=bl, strides=[data.itemsize * s for s in strides])
+        sl = tuple(slice(sum(lens[d][:irr[d]]), sum(lens[d][:irr[d]]) + bl[d]) for d in range(len(lens)))
+        blk[...] = full[sl]
+
+
 # ---- DPD ----------------------------------------------------------------------------------
 
 def orc_dpd_block(irrep, nirrep, lens, layout, irreps):

@@ -530,6 +530,8 @@ lib.tblis_b200_dpd_reduce.argtypes = [ctypes.c_int, _DT, ctypes.c_char_p, _P(tbl
 lib.tblis_b200_dpd_scale.argtypes = [_DT, ctypes.c_char_p]
 lib.tblis_b200_dpd_set.argtypes = [_P(tblis_scalar), _DT, ctypes.c_char_p]
 lib.tblis_b200_dpd_shift.argtypes = [_P(tblis_scalar), _DT, ctypes.c_char_p]
+lib.tblis_b200_dpd_block_to_full.argtypes = [_DT, _P(tblis_tensor)]
+lib.tblis_b200_dpd_full_to_block.argtypes = [_P(tblis_tensor), _DT]
 
 
 def _dpd_table(T, scalar=1.0):
@@ -563,6 +565,26 @@ def _dpd_table(T, scalar=1.0):
     b.offset = ctypes.cast(keep[1], _P(ctypes.c_ssize_t))
     b.stride = ctypes.cast(keep[2], _P(ctypes.c_ssize_t))
     return b, keep
+
+
+def dpd_block_to_full(A, F):
+    """F = the dense form of the DPD tensor A (block_to_full,
+    src/internal/1t/dpd/util.hpp:70-102): F's length in dimension d is the
+    sum of A's lengths over the irreps; F is zeroed, then each stored block of
+    A is copied into its region (irrep x after the irreps below it)."""
+    a, ka = _dpd_table(A)
+    f = _View(F)
+    lib.tblis_b200_dpd_block_to_full(ctypes.byref(a), f.ref)
+    _check()
+
+
+def dpd_full_to_block(F, A):
+    """Every stored block of the DPD tensor A gets its region of the dense
+    tensor F (full_to_block, src/internal/1t/dpd/util.hpp:104-133)."""
+    a, ka = _dpd_table(A)
+    f = _View(F)
+    lib.tblis_b200_dpd_full_to_block(f.ref, ctypes.byref(a))
+    _check()
 
 
 def dpd_add(alpha, A, idx_A, beta, B, idx_B):

@@ -444,11 +444,80 @@ void dpd_unary(int kind, const tblis_scalar* alpha, tblis_b200_dpd_block_table* 
     A_->conj = 0;
 }
 
+// The dense form of a DPD tensor and back (block_to_full / full_to_block,
+// src/internal/1t/dpd/util.hpp:70-133): dimension d of the dense tensor F has
+// the sum of A's lengths over the irreps, irrep x occupying
+// [sum of the lengths of irreps < x, + length of x); block_to_full sets all
+// of F to zero and copies every stored block of A into its region, and
+// full_to_block copies every region back into A's block. Scalars and
+// conjugation flags do not apply (plain copies, as in the reference).
+void dpd_full_copy(tblis_b200_dpd_block_table* A_, tblis_tensor* F, bool to_full)
+{
+    ensure_device();
+    cudaStream_t st = current_stream();
+    TB_CHECK(A_ && F, TB_ERR_ARG, "null tensor");
+    DpdLayout A;
+    to_layout(A_, A);
+    const int type = A_->type;
+    TB_CHECK(F->type == type, TB_ERR_TYPE, "DPD dense form: element types differ");
+    TB_CHECK(F->ndim == A.ndim, TB_ERR_ARG, "DPD dense form: dimensions differ");
+    TB_CHECK(A.ndim <= 26, TB_ERR_SIZE, "DPD dense form: too many dimensions");
+    std::vector<std::vector<i64>> off(A.ndim, std::vector<i64>(A.nirrep, 0));
+    for (unsigned d = 0; d < A.ndim; d++)
+    {
+        i64 o = 0;
+        for (unsigned x = 0; x < A.nirrep; x++) { off[d][x] = o; o += A.len[d][x]; }
+        TB_CHECK(F->len[d] == o, TB_ERR_ARG, "DPD dense form: a dense length is not the sum of the irrep lengths");
+    }
+    std::string idx;
+    for (unsigned d = 0; d < A.ndim; d++) idx.push_back((char)('a' + d));
+    const size_t esz = elem_size(type);
+    Storage sa;
+    sa.init(A_->data, A.total(), esz, true, st);       // read, or kept where no block is stored
+    // F is staged by the dense entry points themselves when it is on the host
+    tblis_tensor f = *F;
+    if (to_full)
+    {
+        tblis_scalar z;
+        scalar_put(z, type, 0.0);
+        checked([&] { tblis_tensor_set(nullptr, nullptr, &z, &f, idx.c_str()); });
+    }
+    std::vector<len_type> flen(A.ndim);
+    A.for_each_block([&](const std::vector<unsigned>& irr, const std::vector<i64>&, const std::vector<i64>&, i64)
+    {
+        BlockView blk(type, A, sa.dev, irr, to_full ? zd(1.0) : zd(0.0));
+        if (blk.empty) return;
+        tblis_tensor sub = *F;
+        char* base = static_cast<char*>(F->data);
+        for (unsigned d = 0; d < A.ndim; d++) base += off[d][irr[d]]*F->stride[d]*(i64)esz;
+        for (unsigned d = 0; d < A.ndim; d++) flen[d] = blk.len[d];
+        sub.data = base;
+        sub.len = flen.data();
+        sub.conj = 0;
+        scalar_put(sub.scalar, type, to_full ? 0.0 : 1.0);
+        if (to_full) checked([&] { tblis_tensor_add(nullptr, nullptr, &blk.t, idx.c_str(), &sub, idx.c_str()); });
+        else checked([&] { tblis_tensor_add(nullptr, nullptr, &sub, idx.c_str(), &blk.t, idx.c_str()); });
+    });
+    if (!to_full) sa.out(st);
+    sa.finish(st);
+}
+
 } // namespace
 
 } // namespace tb
 
 extern "C" {
+
+int tblis_b200_dpd_block_to_full(const tblis_b200_dpd_block_table* A, tblis_tensor* F)
+{
+    return tb::guarded([&] { tb::dpd_full_copy(const_cast<tblis_b200_dpd_block_table*>(A), F, true); });
+}
+
+int tblis_b200_dpd_full_to_block(const tblis_tensor* F, tblis_b200_dpd_block_table* A)
+{
+    return tb::guarded([&] { tb::dpd_full_copy(A, const_cast<tblis_tensor*>(F), false); });
+}
+
 
 int tblis_b200_dpd_add(const tblis_b200_dpd_block_table* A, const label_type* idx_A,
                        tblis_b200_dpd_block_table* B, const label_type* idx_B)
