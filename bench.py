@@ -236,7 +236,7 @@ def headline_config():
 # ---------------------------------------------------------------------------------------
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -257,12 +257,15 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, window=None):
+        """Median SM clock, max clock and throttle reasons of the samples
+        taken inside `window` (host times (t0, t1) of the timed region), or of
+        all samples when none fall inside it (then "window" says so)."""
         if not self.proc:
             return None
         self.proc.terminate()
@@ -271,23 +274,26 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, mx, reasons = [], None, set()
+        import datetime
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                t = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((t, float(parts[2]), float(parts[3]),
+                             [nm for nm, v in zip(names, parts[6:10]) if v.lower().startswith("active")]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+        inside = [r for r in rows if window and window[0] <= r[0] <= window[1]]
+        use = inside if inside else rows
+        if not use:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = sorted({nm for r in use for nm in r[3]})
+        return {"sm_mhz": statistics.median(r[1] for r in use), "sm_max_mhz": use[-1][2], "reasons": reasons,
+                "samples": len(use), "window": "timed region" if inside else "warm-up and timed region"}
 
 
 def time_steps(torch, fn, steps, stream):
@@ -425,16 +431,20 @@ def main():
     def step_fp64():
         tb.mult_ex(1.0, A, "abef", B, "efij", 0.0, Cfp, "abij", method=1)
 
+    # clocks sampled every 50 ms from before the warm-up on; the samples
+    # inside the timed region are the ones reported
+    sampler = ClockSampler(local)
+    sampler.start()
     for _ in range(args.warmup):
         step()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
     k0 = tb.kernel_count()
     tb.kernel_timer(True)
+    t_timed0 = time.time()
     total_ms, per = time_steps(torch, step, args.steps, stream)
+    t_timed1 = time.time()
     launches = tb.kernel_count() - k0
     kname = {1: "gemm_f64_kernel", 2: "ozaki_gemm_kernel", 6: "oz_crt_gemm"}[used_method]
     k_total_ms, k_launches = tb.kernel_time(kname)
@@ -442,7 +452,7 @@ def main():
     stages = {1: (kname,), 2: ("oz_stats", "oz_slice", kname), 6: ("oz_stats", "oz_slice", kname, "oz_crt_combine")}
     stage_ms = {n: tb.kernel_time(n)[0] / args.steps for n in stages[used_method]}
     tb.kernel_timer(False)
-    clocks = sampler.stop()
+    clocks = sampler.stop((t_timed0, t_timed1))
     total_ms = max_over_ranks(dist, torch, total_ms, dev)
     ms_per_step = total_ms / args.steps
     value = job_value(world, args.steps, total_ms)

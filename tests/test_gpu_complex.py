@@ -93,3 +93,28 @@ def test_complex_beta_zero_never_reads_c(cuda):
     got = _gpu_mult(torch, cuda, 1.0 - 1j, A, "ik", B, "kj", 0.0, C, "ij")
     assert np.all(np.isfinite(got))
     assert _rel(got, (1.0 - 1j) * (A @ B)) <= 1e-13
+
+
+@pytest.mark.parametrize("method", [2, 6])
+def test_complex_contraction_on_the_ozaki_paths(cuda, method):
+    """A dcomplex contraction on an Ozaki method (2: INT8 slices or moduli,
+    whichever the models pick; 6: moduli): each real product of the 4M split
+    runs on that INT8 path, with slices or moduli chosen for the tolerance,
+    and the complex result stays within it against the reference's own
+    complex contraction."""
+    import torch
+    import tblis_b200 as tb
+    rng = np.random.default_rng(77)
+    lens = {"a": 40, "b": 36, "e": 48, "f": 30, "i": 20, "j": 24}
+    A = _cplx(rng, [lens[c] for c in "abef"], [2, 0, 3, 1])
+    B = _cplx(rng, [lens[c] for c in "efij"], [1, 3, 0, 2])
+    C = _cplx(rng, [lens[c] for c in "abij"], [0, 1, 2, 3])
+    alpha, beta = 0.5 - 0.25j, 0.3 + 0.7j
+    want = C.copy()
+    oracle.ref_mult(alpha, A, "abef", B, "efij", beta, want, "abij")
+    dA, dB, dC = _dev_view(torch, A, cuda), _dev_view(torch, B, cuda), _dev_view(torch, C, cuda)
+    rep = tb.mult_ex(alpha, dA, "abef", dB, "efij", beta, dC, "abij", method=method, tolerance=1e-12)
+    torch.cuda.synchronize()
+    assert rep["slices"] > 0                      # the real products ran on the INT8 path
+    err = _rel(dC.cpu().numpy(), want)
+    assert err <= 1e-12, err
