@@ -114,7 +114,7 @@ __device__ __forceinline__ void mb_arrive_expect(uint64_t* b, uint32_t bytes)
 // aligned addresses, a multiple of 16 bytes), completing on the mbarrier
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  :: "r"(su32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(su32(bar)) : "memory");
 }
 
@@ -329,7 +329,13 @@ __device__ __forceinline__ bool ws_consume(double (&acc)[2][4][4], int nst, cons
             #pragma unroll
             for (int j = 0; j < NS; j++)
                 dmma_k16(acc[i][j], af[i], bf[j]);
-        // the fragments are in registers: the stage may be refilled
+        // the fragments are in registers: the stage may be refilled. The
+        // refill is a bulk copy (async proxy) over what these generic loads
+        // read, so each thread orders its reads before it with a proxy
+        // fence; without it, refills overtook reads still in flight when
+        // other kernels' blocks shared the SM, and whole warp tiles came out
+        // wrong
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
         if (lane == 0) mb_arrive(&sh.empty[s]);
         it++;
@@ -424,6 +430,9 @@ gemm_f64_ws_kernel(const GroupDesc* __restrict__ groups, const i64* __restrict__
             mb_init(&sh.tempty[t], WS_CONSUMERS);      // the consumer warps, once C is written
         }
         sh.abort = 0;
+        // the initialised barriers, visible to the bulk copies' completions
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
     // from here on the roles never wait on a CTA-wide barrier

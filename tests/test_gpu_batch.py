@@ -78,3 +78,42 @@ def test_batch_of_ladder_like_4index(cuda):
     torch.cuda.synchronize()
     for ref, dC in zip(refs, outs):
         assert normwise_rel(dC.cpu().numpy(), ref) <= TOL
+
+
+def test_batch_of_1500_4index_members(cuda):
+    """1,500 4-index members (extents 8..20, every operand in a random index
+    order), tens of thousands of tiles in one grouped launch. Every member
+    against numpy's FP64 einsum, a seeded sample against the oracle; run
+    twice (the second run replays the plan's graph), beta 1 so that the
+    second result holds both runs."""
+    import torch
+    import tblis_b200 as tb
+    rng = np.random.default_rng(2024)
+    items, hosts = [], []
+    for _ in range(1500):
+        l = {c: int(rng.integers(8, 21)) for c in "abefij"}
+        ia = "".join(rng.permutation(list("abef")))
+        ib = "".join(rng.permutation(list("efij")))
+        ic = "".join(rng.permutation(list("abij")))
+        A = rng.uniform(-1, 1, [l[c] for c in ia])
+        B = rng.uniform(-1, 1, [l[c] for c in ib])
+        C = rng.uniform(-1, 1, [l[c] for c in ic])
+        items.append((0.5, torch.from_numpy(A).to(cuda), ia, torch.from_numpy(B).to(cuda), ib, 1.0,
+                      torch.from_numpy(C).to(cuda), ic))
+        hosts.append((A, B, C))
+    prepared = tb.PreparedBatch(items)
+    prepared.run()
+    prepared.run()
+    torch.cuda.synchronize()
+    sample = set(np.random.default_rng(5).choice(len(items), 25, replace=False).tolist())
+    worst = 0.0
+    for j, ((_, _, ia, _, ib, _, dC, ic), (A, B, C)) in enumerate(zip(items, hosts)):
+        ref = C + 2*0.5*np.einsum("%s,%s->%s" % (ia, ib, ic), A, B, optimize=True)
+        got = dC.cpu().numpy()
+        worst = max(worst, normwise_rel(got, ref))
+        if j in sample:
+            want = C.copy()
+            oracle.orc_mult(0.5, A, ia, B, ib, 1.0, want, ic)
+            oracle.orc_mult(0.5, A, ia, B, ib, 1.0, want, ic)
+            assert normwise_rel(got, want) <= TOL
+    assert worst <= TOL
